@@ -1,0 +1,349 @@
+"""TEST INFRASTRUCTURE — Python access to the CPU oracle.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this module, and
+only as the checker.  Two backends with one API:
+
+* ``"port"``: ``oracle/liboracle.so``, the plain-C FP64 restatement (hgx_oracle.c);
+* ``"ref"``:  ``oracle/_ref/libhigref.so``, the reference's own CPU sources compiled by
+  ``make -C oracle ref`` (present only where the reference tree was available to build it).
+
+Complex arrays are numpy complex128.  Grids follow the reference's layout: N = nrow*ncol
+pixels flattened row-major, extended (DWBA) arrays hold 4 blocks of N.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libhigref.so")
+
+# enums of include/common/enums.hpp (reference)
+SHAPE = {"box": 2, "cube": 3, "cylinder": 4, "sphere": 5, "prism3": 8, "prism6": 9,
+         "pyramid": 14}
+PARAM = {"radius": 2, "xsize": 3, "ysize": 4, "height": 5, "edge": 6, "baseangle": 7}
+STAT = {"null": 0, "none": 2, "gaussian": 4, "uniform": 8}
+LATTICE = {"bcc": 2, "cubic": 3, "fcc": 4, "fco": 5, "hcp": 6, "hex": 7}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_up = C.POINTER(C.c_uint)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _cbuf(a):
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    return a, a.view(np.float64)
+
+
+_libs: dict = {}
+
+
+def available(backend: str) -> bool:
+    return os.path.exists(PORT_SO if backend == "port" else REF_SO)
+
+
+def lib(backend: str = "port"):
+    if backend in _libs:
+        return _libs[backend]
+    path = PORT_SO if backend == "port" else REF_SO
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`"
+                                f"{' ref' if backend == 'ref' else ''})")
+    L = C.CDLL(path)
+    for name in dir(L):
+        pass
+    _libs[backend] = L
+    return L
+
+
+def set_threads(n: int, backend: str = "port") -> int:
+    L = lib(backend)
+    f = L.orc_set_threads if backend == "port" else L.ref_set_threads
+    f.restype = C.c_int
+    return f(C.c_int(n))
+
+
+def k0_from_kev(energy_kev: float) -> float:
+    """HipGISAXS::init, src/sim/hipgisaxs_main.cpp:144-158: lambda = 1.23984/E, k0 = 2pi/lambda."""
+    lam = 1.23984 / energy_kev
+    return 2 * 3.141592653589793 / lam
+
+
+class Grid:
+    """A detector q-grid (QGrid::create) plus the DWBA extended qz for a particle layer."""
+
+    _current_ref = None  # the reference keeps one QGrid singleton
+
+    def __init__(self, ncol, nrow, qmin_y, qmin_z, qmax_y, qmax_z, alpha_i_deg, energy_kev,
+                 dn2=(0.0, 0.0), backend="port"):
+        self.ncol, self.nrow = int(ncol), int(nrow)
+        self.n = self.ncol * self.nrow
+        self.region = (qmin_y, qmin_z, qmax_y, qmax_z)
+        self.alpha_i = alpha_i_deg * 3.141592653589793 / 180  # PI_ as the reference uses
+        self.k0 = k0_from_kev(energy_kev)
+        self.dn2 = dn2
+        self.backend = backend
+        self.qx = np.zeros(self.n)
+        self.qy = np.zeros(self.n)
+        self.qz = np.zeros(self.n)
+        self.alpha = np.zeros(self.nrow)
+        self.qz_ext = np.zeros(4 * self.n, dtype=np.complex128)
+        self._build()
+
+    def _build(self):
+        L = lib(self.backend)
+        a = (C.c_double(self.region[0]), C.c_double(self.region[1]), C.c_double(self.region[2]),
+             C.c_double(self.region[3]), C.c_double(self.alpha_i), C.c_double(self.k0))
+        if self.backend == "port":
+            rc = L.orc_qgrid_create(C.c_int(self.ncol), C.c_int(self.nrow), *a, _p(self.qx),
+                                    _p(self.qy), _p(self.qz), _p(self.alpha))
+            assert rc == 0, rc
+            ext = self.qz_ext.view(np.float64)
+            rc = L.orc_qz_extended(C.c_int(self.n), _p(self.qz), C.c_double(self.k0),
+                                   C.c_double(self.alpha_i), C.c_double(self.dn2[0]),
+                                   C.c_double(self.dn2[1]), _p(ext))
+            assert rc == 0, rc
+        else:
+            self.activate()
+
+    def activate(self):
+        """Make this grid the reference's QGrid singleton (ref backend only)."""
+        if self.backend != "ref":
+            return
+        if Grid._current_ref is self:
+            return
+        L = lib("ref")
+        a = (C.c_double(self.region[0]), C.c_double(self.region[1]), C.c_double(self.region[2]),
+             C.c_double(self.region[3]), C.c_double(self.alpha_i), C.c_double(self.k0))
+        rc = L.ref_qgrid_create(C.c_int(self.ncol), C.c_int(self.nrow), *a, _p(self.qx),
+                                _p(self.qy), _p(self.qz), _p(self.alpha))
+        assert rc == 0, rc
+        ext = self.qz_ext.view(np.float64)
+        rc = L.ref_qz_extended(C.c_double(self.k0), C.c_double(self.alpha_i),
+                               C.c_double(self.dn2[0]), C.c_double(self.dn2[1]), _p(ext))
+        assert rc == 0, rc
+        Grid._current_ref = self
+
+
+def ff_approx_triangle(shape_def, qx, qy, qz, rot=None, backend="port"):
+    """NumericFormFactorC::compute_approx_triangle on explicit arrays (qz complex, any length
+    that is a multiple of len(qx))."""
+    L = lib(backend)
+    sd = np.ascontiguousarray(shape_def, dtype=np.float64).reshape(-1, 8)
+    qx = np.ascontiguousarray(qx, dtype=np.float64)
+    qy = np.ascontiguousarray(qy, dtype=np.float64)
+    qz, qzf = _cbuf(qz)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    out = np.zeros(len(qz), dtype=np.complex128)
+    f = L.orc_ff_approx_triangle if backend == "port" else L.ref_ff_approx_triangle
+    rc = f(_p(sd), C.c_int(len(sd)), C.c_int(len(qx)), _p(qx), _p(qy), C.c_int(len(qz)),
+           _p(qzf), _p(r), _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"ff_approx_triangle failed rc={rc}")
+    return out
+
+
+def mesh_to_shape_def(verts, faces):
+    L = lib("port")
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
+    out = np.zeros((len(f), 8))
+    t = L.orc_mesh_to_shape_def(C.c_int(len(v)), _p(v), C.c_int(len(f)),
+                                f.ctypes.data_as(_ip), _p(out))
+    if t < 0:
+        raise ValueError("bad face index")
+    return out[:t]
+
+
+def param_rows(params):
+    """params: list of dicts {type, stat, min, max, mean, deviation, nvalues} -> (n, 7)."""
+    rows = []
+    for p in params:
+        rows.append([PARAM[p["type"]], STAT[p.get("stat", "none")], p.get("min", 0.0),
+                     p.get("max", 0.0), p.get("mean", float("nan")), p.get("deviation", 0.0),
+                     p.get("nvalues", 1)])
+    return np.ascontiguousarray(np.array(rows, dtype=np.float64).reshape(-1, 7))
+
+
+def param_distribution(stat, pmin, pmax, mean, dev, nvalues):
+    L = lib("port")
+    cap = max(16, 4 * int(nvalues) + 8)
+    dim = np.zeros(cap)
+    w = np.zeros(cap)
+    n = L.orc_param_distribution(C.c_int(STAT[stat]), C.c_double(pmin), C.c_double(pmax),
+                                 C.c_double(mean), C.c_double(dev), C.c_int(int(nvalues)),
+                                 _p(dim), _p(w), C.c_int(cap))
+    if n < 0:
+        raise ValueError("param_distribution failed")
+    return dim[:n].copy(), w[:n].copy()
+
+
+def ff_analytic(grid: Grid, shape, params, tau=0.0, eta=0.0, transvec=(0, 0, 0), rot=None,
+                backend=None):
+    backend = backend or grid.backend
+    L = lib(backend)
+    P = param_rows(params)
+    tv = np.ascontiguousarray(transvec, dtype=np.float64)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    out = np.zeros(4 * grid.n, dtype=np.complex128)
+    if backend == "port":
+        qz, qzf = _cbuf(grid.qz_ext)
+        rc = L.orc_ff_analytic(C.c_int(SHAPE[shape]), C.c_int(len(P)), _p(P), C.c_double(tau),
+                               C.c_double(eta), _p(tv), _p(r), C.c_int(grid.n), _p(grid.qx),
+                               _p(grid.qy), C.c_int(4 * grid.n), _p(qzf),
+                               _p(out.view(np.float64)))
+    else:
+        grid.activate()
+        rc = L.ref_ff_analytic(C.c_int(SHAPE[shape]), C.c_int(len(P)), _p(P), C.c_double(tau),
+                               C.c_double(eta), _p(tv), _p(r), _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"ff_analytic({shape}) failed rc={rc}")
+    return out
+
+
+def lattice_vectors(kind, hkl="100"):
+    L = lib("port")
+    a, b, c, t = (np.zeros(3) for _ in range(4))
+    rc = L.orc_lattice_vectors(C.c_int(LATTICE[kind]), C.c_char_p(hkl.encode()), _p(a), _p(b),
+                               _p(c), _p(t))
+    if rc != 0:
+        raise ValueError(f"lattice {kind}/{hkl}")
+    return a, b, c, t
+
+
+def sf_lattice(grid: Grid, abc, repet, scaling, center=(0, 0, 0), rot=None, backend=None):
+    backend = backend or grid.backend
+    L = lib(backend)
+    abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
+    rp = np.ascontiguousarray(repet, dtype=np.float64)
+    sc = np.ascontiguousarray(scaling, dtype=np.float64)
+    ce = np.ascontiguousarray(center, dtype=np.float64)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    out = np.zeros(4 * grid.n, dtype=np.complex128)
+    if backend == "port":
+        qz, qzf = _cbuf(grid.qz_ext)
+        rc = L.orc_sf_lattice(_p(abc9), _p(rp), _p(sc), _p(ce), _p(r), C.c_int(grid.n),
+                              _p(grid.qx), _p(grid.qy), C.c_int(4 * grid.n), _p(qzf),
+                              _p(out.view(np.float64)))
+    else:
+        grid.activate()
+        rc = L.ref_sf_lattice(_p(abc9), _p(rp), _p(sc), _p(ce), _p(r), C.c_int(1),
+                              _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"sf_lattice failed rc={rc}")
+    return out
+
+
+def propagation_coeffs(grid: Grid, layers, particle_order=0, backend=None):
+    """layers: list of (delta, beta, thickness, order); order -1 = substrate."""
+    backend = backend or grid.backend
+    L = lib(backend)
+    d = np.ascontiguousarray([l[0] for l in layers], dtype=np.float64)
+    b = np.ascontiguousarray([l[1] for l in layers], dtype=np.float64)
+    t = np.ascontiguousarray([l[2] for l in layers], dtype=np.float64)
+    o = np.ascontiguousarray([l[3] for l in layers], dtype=np.int32)
+    out = np.zeros(4 * grid.n, dtype=np.complex128)
+    if backend == "port":
+        rc = L.orc_propagation_coeffs(C.c_int(len(layers)), _p(d), _p(b), _p(t),
+                                      o.ctypes.data_as(_ip), C.c_double(grid.k0),
+                                      C.c_double(grid.alpha_i), C.c_int(particle_order),
+                                      C.c_int(grid.nrow), C.c_int(grid.ncol), _p(grid.alpha),
+                                      _p(out.view(np.float64)))
+        if rc != 0:
+            raise RuntimeError(f"propagation_coeffs failed rc={rc}")
+    else:
+        grid.activate()
+        rc = L.ref_propagation_coeffs(C.c_int(len(layers)), _p(d), _p(b), _p(t),
+                                      o.ctypes.data_as(_ip), C.c_double(grid.k0),
+                                      C.c_double(grid.alpha_i), C.c_int(particle_order),
+                                      _p(out.view(np.float64)))
+        if rc <= 0:
+            raise RuntimeError(f"propagation_coeffs failed rc={rc}")
+    return out
+
+
+def parratt(layers_stack, alpha, k0, order, backend="port"):
+    """layers_stack for the port: list of (one_minus_n2 complex, z) in reference order."""
+    L = lib("port")
+    om = np.ascontiguousarray([[complex(l[0]).real, complex(l[0]).imag] for l in layers_stack],
+                              dtype=np.float64)
+    z = np.ascontiguousarray([l[1] for l in layers_stack], dtype=np.float64)
+    tr = np.zeros(4)
+    L.orc_parratt(C.c_int(len(z)), _p(om), _p(z), C.c_double(alpha), C.c_double(k0),
+                  C.c_int(order), _p(tr))
+    return complex(tr[0], tr[1]), complex(tr[2], tr[3])
+
+
+def rot_axis(axis, angle):
+    L = lib("port")
+    r = np.zeros(9)
+    L.orc_rot_axis(C.c_int(axis), C.c_double(angle), _p(r))
+    return r.reshape(3, 3)
+
+
+def rot_mul(a, b):
+    L = lib("port")
+    a = np.ascontiguousarray(a, dtype=np.float64).reshape(9)
+    b = np.ascontiguousarray(b, dtype=np.float64).reshape(9)
+    r = np.zeros(9)
+    L.orc_rot_mul(_p(a), _p(b), _p(r))
+    return r.reshape(3, 3)
+
+
+def dwba_combine(fc, sf, ff, weight=1.0, intensity=None):
+    L = lib("port")
+    n = len(fc) // 4
+    out = np.zeros(n) if intensity is None else np.ascontiguousarray(intensity, dtype=np.float64)
+    fc, fcf = _cbuf(fc)
+    sf, sff = _cbuf(sf)
+    ff, fff = _cbuf(ff)
+    L.orc_dwba_combine(C.c_int(n), _p(fcf), _p(sff), _p(fff), C.c_double(weight), _p(out))
+    return out
+
+
+def chi2(model, counts, mask=None, scale=1.0):
+    L = lib("port")
+    L.orc_chi2.restype = C.c_double
+    m = np.ascontiguousarray(model, dtype=np.float64)
+    c = np.ascontiguousarray(counts, dtype=np.float64)
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint32)
+    return L.orc_chi2(C.c_int(len(m)), _p(m), _p(c),
+                      None if mk is None else mk.ctypes.data_as(_up), C.c_double(scale))
+
+
+def abs_diff_square(ref, data, mask):
+    L = lib("port")
+    L.orc_abs_diff_square.restype = C.c_double
+    r = np.ascontiguousarray(ref, dtype=np.float64)
+    d = np.ascontiguousarray(data, dtype=np.float64)
+    mk = np.ascontiguousarray(mask, dtype=np.uint32)
+    return L.orc_abs_diff_square(C.c_int(len(r)), _p(r), _p(d), mk.ctypes.data_as(_up))
+
+
+def cylinder_params(radius, height, spread=0.0, nvalues=1):
+    """Cylinder parameters; with spread > 0 a Gaussian over +-3 sigma sampled at nvalues points
+    (param_distribution semantics; the reference sums these radii/heights unweighted)."""
+    if spread > 0:
+        sr, sh = spread * radius, spread * height
+        return [dict(type="radius", stat="gaussian", min=radius - 3 * sr, max=radius + 3 * sr,
+                     mean=radius, deviation=sr, nvalues=nvalues),
+                dict(type="height", stat="gaussian", min=height - 3 * sh, max=height + 3 * sh,
+                     mean=height, deviation=sh, nvalues=nvalues)]
+    return [dict(type="radius", min=radius, max=radius, nvalues=1),
+            dict(type="height", min=height, max=height, nvalues=1)]
+
+
+def rel_err(a, b):
+    """Norm-wise relative error ||a-b||_2 / ||b||_2 (the project's single error definition)."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    den = float(np.linalg.norm(b.ravel()))
+    return float(np.linalg.norm((a - b).ravel())) / (den if den > 0 else 1.0)

@@ -1,0 +1,98 @@
+"""Generates the golden fixtures in this folder from the reference's OWN CPU code.
+
+The reference (tacaswell/hipgisaxs) is C++; ``make -C oracle ref`` compiles its CPU hot-path
+sources where they lie into ``oracle/_ref/libhigref.so``.  This script drives that library
+through ``oracle/pyoracle.py`` (backend "ref") on small seeded cases and writes one .npz per
+case: the inputs and the reference's outputs.  The tests check the plain-C oracle and the
+CUDA path against these files, so parity stays pinned where the reference tree is absent.
+
+Run from the repository root:  python tests/golden/gen_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import pyoracle as po  # noqa: E402
+
+
+def tri_case(rng, T, scale):
+    sd = np.zeros((T, 8))
+    sd[:, 0] = rng.uniform(0.2, 3.0, T)
+    n = rng.normal(size=(T, 3))
+    sd[:, 1:4] = n / np.linalg.norm(n, axis=1)[:, None]
+    sd[:, 4:7] = rng.normal(scale=scale, size=(T, 3))
+    return sd
+
+
+def main():
+    if not po.available("ref"):
+        sys.exit("oracle/_ref/libhigref.so missing: run `make -C oracle ref` first")
+    po.set_threads(4, "ref")
+    rng = np.random.default_rng(20240601)
+    out = {}
+    # grids: a Born-like vacuum layer and a buried (absorbing) particle layer
+    grids = {
+        "g16": dict(ncol=16, nrow=12, region=(-1.0, 0.0, 1.0, 2.0), ai=0.16, e=10.0, dn2=(0, 0)),
+        "g16abs": dict(ncol=16, nrow=12, region=(-2.0, 0.0, 2.0, 3.0), ai=0.20, e=10.0,
+                       dn2=(2 * 3e-6, 2 * 2e-8)),
+    }
+    rots = {"id": np.eye(3),
+            "r3": po.rot_mul(po.rot_mul(po.rot_axis(2, 0.35), po.rot_axis(0, 0.12)),
+                             po.rot_axis(1, -0.2))}
+    for gname, g in grids.items():
+        G = po.Grid(g["ncol"], g["nrow"], *g["region"], g["ai"], g["e"], g["dn2"], backend="ref")
+        base = dict(ncol=G.ncol, nrow=G.nrow, region=np.array(g["region"]), alpha_i_deg=g["ai"],
+                    energy_kev=g["e"], dn2=np.array(g["dn2"], dtype=float), qx=G.qx, qy=G.qy,
+                    qz=G.qz, alpha=G.alpha, qz_ext=G.qz_ext)
+        np.savez_compressed(os.path.join(HERE, f"qgrid_{gname}.npz"), **base)
+        # numeric form factor (approx triangle)
+        for rname, R in rots.items():
+            sd = tri_case(rng, 53, 6.0)
+            ff = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext, R, "ref")
+            np.savez_compressed(os.path.join(HERE, f"fftri_{gname}_{rname}.npz"), shape_def=sd,
+                                rot=R, ff=ff, grid=gname)
+        # analytic shapes
+        shapes = {
+            "cylinder": po.cylinder_params(5.0, 10.0, 0.05, 7),
+            "sphere": [dict(type="radius", stat="gaussian", min=4, max=6, mean=5, deviation=0.3,
+                            nvalues=5)],
+            "box": [dict(type="xsize", stat="uniform", min=3, max=5, nvalues=3),
+                    dict(type="ysize", min=4, max=4), dict(type="height", min=2, max=2)],
+            "cube": [dict(type="height", stat="uniform", min=3, max=4, nvalues=2)],
+            "prism3": [dict(type="edge", min=5, max=5), dict(type="height", min=3, max=3)],
+            "prism6": [dict(type="edge", min=5, max=5), dict(type="height", min=3, max=3)],
+            "pyramid": [dict(type="xsize", min=10, max=10), dict(type="ysize", min=10, max=10),
+                        dict(type="height", min=3, max=3), dict(type="baseangle", min=60, max=60)],
+        }
+        for sname, params in shapes.items():
+            ff = po.ff_analytic(G, sname, params, 0.1, 0.2, (1.0, 2.0, 3.0), rots["r3"])
+            np.savez_compressed(os.path.join(HERE, f"ffana_{sname}_{gname}.npz"),
+                                params=po.param_rows(params), tau=0.1, eta=0.2,
+                                transvec=np.array([1.0, 2.0, 3.0]), rot=rots["r3"], ff=ff,
+                                grid=gname)
+        # lattice structure factor
+        for lname, hkl, rep in (("hex", "100", [20, 20, 1]), ("cubic", "100", [5, 7, 3]),
+                                ("fcc", "100", [4, 4, 4])):
+            abc = np.array(po.lattice_vectors(lname, hkl)[:3])
+            sf = po.sf_lattice(G, abc, rep, [20.0, 20.0, 20.0], (1.0, 2.0, 3.0), rots["r3"])
+            np.savez_compressed(os.path.join(HERE, f"sf_{lname}_{gname}.npz"), abc=abc,
+                                repet=np.array(rep, dtype=float), scaling=np.array([20.0] * 3),
+                                center=np.array([1.0, 2.0, 3.0]), rot=rots["r3"], sf=sf,
+                                grid=gname)
+        # Fresnel / DWBA coefficients: substrate only, and a 3-layer stack
+        for lname, layers, order in (
+                ("sub", [(4.88e-6, 7.37e-8, 0.0, -1)], 0),
+                ("stack", [(4.88e-6, 7.37e-8, 0.0, -1), (3e-6, 2e-8, 7.0, 1),
+                           (1e-6, 1e-9, 3.0, 2)], 1)):
+            fc = po.propagation_coeffs(G, layers, order)
+            np.savez_compressed(os.path.join(HERE, f"fc_{lname}_{gname}.npz"),
+                                layers=np.array(layers, dtype=float), order=order, fc=fc,
+                                grid=gname)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
