@@ -1,0 +1,348 @@
+"""Benchmark: q.triangle evals/s of the numeric (mesh) form factor on one B200.
+
+Workload (large numeric form factor, DWBA): a seeded closed star-shaped mesh of 50,000
+triangles (UV sphere 250 x 101 bands, radius 15 nm perturbed by real spherical harmonics
+l <= 8) on a 2048 x 2048 detector (qy in [-2, 2], qz in [0, 3] 1/nm, 10 keV, alpha_i =
+0.20 deg, vacuum particle layer), four DWBA qz blocks: 4 * 2048^2 * 50,000 = 8.39e11
+q.triangle evaluations per step.  A step is one FP32-compensated triangle sum over the
+whole grid, inputs resident in HBM (the q-grid is 332 MB, larger than L2).
+
+Reported beside it: the plain FP64 kernel on the same inputs, the end-to-end number through
+the reference-shaped C-ABI call with host buffers (H2D + D2H inside the timed region), the
+roofline of the dominant kernel against FP32 and SFU throughput measured on the same GPU,
+and the reference's own CPU implementation timed on the host cores on a bounded sample.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl hgx|reference]
+Under torchrun (N > 1) every rank runs an independent replica (the form factor needs no
+exchange): weak scaling, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NCOL = NROW = 2048
+QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z = -2.0, 0.0, 2.0, 3.0
+ENERGY_KEV, ALPHA_I_DEG = 10.0, 0.20
+PI_REF = 3.141592653589793
+# FP32 FLOP of the row-factorised kernel per (pixel, triangle) for the 4 paired real
+# DWBA blocks (FMA = 2): in-plane phase 3, reduction 2, angle scale 1, in-plane q.n 3,
+# U = q.n E 2, 16 FFMA accumulations 32  -> 43 FLOP and 2 SFU ops per 4 evaluations.
+FLOP_PER_PIXEL_TRI = 43.0
+SFU_PER_PIXEL_TRI = 2.0
+
+
+def k0_from_kev(e):
+    return 2 * PI_REF / (1.23984 / e)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hgx", choices=["hgx", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-f64", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        load = [s for s in sm]
+        return {"sm_mhz": float(np.median(load)) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def workload_mesh():
+    from hipgisaxs_b200 import meshes
+    V, F = meshes.star_mesh(15.0, 250, 101, 8, 0.05, meshes.DEFAULT_SEED)
+    return meshes.shape_def_from_mesh(V, F)
+
+
+def cpu_sample_rate(sd, qx, qy, qz_ext, budget_s=12.0, backend=None):
+    """Times the reference's compute_approx_triangle (oracle/_ref, else the port) on whole
+    detector rows of the workload; returns (evals/s, threads, kind, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    kind = "reference" if po.available("ref") else "port"
+    be = "ref" if kind == "reference" else "port"
+    threads = po.set_threads(os.cpu_count() or 1, be)
+    n = NCOL * NROW
+    ext = qz_ext.reshape(4, n)
+
+    def run(rows):
+        idx = np.concatenate([np.arange(r * NCOL, (r + 1) * NCOL) for r in rows])
+        qz = ext[:, idx].ravel()
+        t = time.perf_counter()
+        po.ff_approx_triangle(sd, qx[idx], qy[idx], qz, None, be)
+        dt = time.perf_counter() - t
+        return 4 * len(idx) * len(sd), dt
+
+    ev, dt = run([NROW // 2])
+    nrows = int(max(1, min(64, budget_s / max(dt, 1e-3))))
+    rows = list(np.linspace(0, NROW - 1, nrows).astype(int))
+    ev, dt = run(rows)
+    desc = (f"{nrows} full detector rows x 4 DWBA blocks x {len(sd)} triangles "
+            f"({ev:.3e} evals, {dt:.1f} s); cost is linear in q-points")
+    return ev / dt, threads, kind, desc
+
+
+def run_reference(args, rank):
+    """The reference's own CPU implementation of the path on this host's cores."""
+    if rank != 0:
+        return
+    sd = workload_mesh()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    G = po.Grid(NCOL, NROW, QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z, ALPHA_I_DEG, ENERGY_KEV)
+    kind = "reference" if po.available("ref") else "port"
+    be = "ref" if kind == "reference" else "port"
+    threads = po.set_threads(os.cpu_count() or 1, be)
+    n = NCOL * NROW
+    ext = G.qz_ext.reshape(4, n)
+    # each step: 2 full detector rows (spread over the detector) x 4 blocks x all triangles
+    def step(i):
+        r = [(i * 997 + 13) % NROW, (i * 389 + 1024) % NROW]
+        idx = np.concatenate([np.arange(x * NCOL, (x + 1) * NCOL) for x in r])
+        po.ff_approx_triangle(sd, G.qx[idx], G.qy[idx], ext[:, idx].ravel(), None, be)
+        return 4 * len(idx) * len(sd)
+
+    for i in range(args.warmup):
+        step(i)
+    t = time.perf_counter()
+    ev = 0
+    for i in range(args.steps):
+        ev += step(args.warmup + i)
+    dt = time.perf_counter() - t
+    v = ev / dt
+    sample = "2 full detector rows x 4 DWBA blocks x 50,000 triangles per step"
+    line = {"metric": "q.triangle evals/s", "value": v, "unit": "evals/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "mesh50k-dwba-2048sq (bounded sample per step)",
+                       "triangles": len(sd), "grid": [NCOL, NROW], "blocks": 4},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import hipgisaxs_b200 as hg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    ctx = hg.Context(local, stream=stream)
+
+    sd = workload_mesh()
+    ntri = len(sd)
+    alpha_i = ALPHA_I_DEG * PI_REF / 180
+    k0 = k0_from_kev(ENERGY_KEV)
+    grid = hg.QGrid.create(ctx, NCOL, NROW, QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z, alpha_i, k0)
+    assert grid.mode == 1, grid.mode
+    n = NCOL * NROW
+    evals = 4.0 * n * ntri
+    sd_dev = torch.tensor(sd, device=dev)
+    out = torch.empty(4 * n, dtype=torch.complex64, device=dev)
+
+    def step():
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f32c", out=out, out_type="c64")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+
+    peak_fp32, peak_sfu = hg.measure_peaks(ctx, sustained_ms=2000)
+
+    clk = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clk.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ctx.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * evals * args.steps / (ms * 1e-3)
+
+    # FP64 plain kernel on the same inputs (the denominator of the FP32 speed-up)
+    f64 = None
+    if not args.no_f64:
+        out64 = torch.empty(4 * n, dtype=torch.complex128, device=dev)
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = a0.elapsed_time(a1)
+        # accuracy of the timed FP32 output against the FP64 kernel (norm-wise)
+        d = (out.to(torch.complex128) - out64)
+        relerr = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(out64))
+        v64 = evals / (ms64 * 1e-3)
+        f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64,
+               "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr}
+        del out64
+
+    # end to end through the reference-shaped C-ABI call with host (pinned) buffers
+    e2e = None
+    if not args.no_e2e:
+        g = grid.read(qz_det=False, alpha=False)
+        h_sd = torch.tensor(sd).pin_memory()
+        h_qx = torch.tensor(g["qx"]).pin_memory()
+        h_qy = torch.tensor(g["qy"]).pin_memory()
+        h_qz = torch.tensor(g["qz_ext"]).pin_memory()
+        h_out = torch.empty(4 * n, dtype=torch.complex128).pin_memory()
+        hg.ff_triangles_arrays(ctx, h_sd, h_qx, h_qy, h_qz, None, "f32c", out=h_out)
+        torch.cuda.synchronize()
+        k = max(1, min(args.steps, 3))
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(k):
+            hg.ff_triangles_arrays(ctx, h_sd, h_qx, h_qy, h_qz, None, "f32c", out=h_out)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        mse = b0.elapsed_time(b1) / k
+        if dist is not None:
+            t = torch.tensor([mse], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            mse = float(t.item())
+        e2e = {"value": world * evals / (mse * 1e-3), "unit": "evals/s",
+               "h2d_bytes_per_step": int(sd.nbytes + 2 * 8 * n + 16 * 4 * n),
+               "d2h_bytes_per_step": int(16 * 4 * n), "ms_per_step": mse,
+               "path": "hgx_ff_triangles (reference-shaped, host buffers, complex128 out)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        g = grid.read(qz_det=False, alpha=False)
+        rate, threads, kind, desc = cpu_sample_rate(sd, g["qx"], g["qy"], g["qz_ext"])
+        cpu = {"value": rate, "unit": "evals/s", "cores": threads, "kind": kind, "sample": desc}
+
+    if rank == 0:
+        flop = FLOP_PER_PIXEL_TRI * n * ntri
+        achieved = flop / (ms_step * 1e-3) / 1e12
+        sfu_rate = SFU_PER_PIXEL_TRI * n * ntri / (ms_step * 1e-3) / 1e9
+        line = {
+            "metric": "q.triangle evals/s", "value": value, "unit": "evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (compensated; FP64 q-grid/epilogue)",
+            "data": "synthetic (seeded star mesh, 50,000 triangles)",
+            "config": {"workload": "mesh50k-dwba-2048sq: numeric FF, 50,000-triangle star "
+                                   "mesh, 2048x2048 detector, 4 DWBA blocks",
+                       "triangles": ntri, "grid": [NCOL, NROW], "blocks": 4,
+                       "evals_per_step": evals, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (q-grid 332 MB)"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32,
+                         "unit": "TFLOP/s", "frac": achieved / peak_fp32,
+                         "traffic": None,
+                         "peak_source": "hgx_measure_peaks FFMA probe, sustained 2 s, same GPU",
+                         "flop_per_pixel_triangle": FLOP_PER_PIXEL_TRI,
+                         "sfu": {"achieved_gops": sfu_rate, "peak_gops": peak_sfu,
+                                 "frac": sfu_rate / peak_sfu}},
+            "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64,
+            "gpu_launches": 2 * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    grid.close()
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,12 @@
+"""hipgisaxs_b200 — a B200-native (sm_100a) GISAXS forward model.
+
+The hot path of the reference simulator (tacaswell/hipgisaxs) — the triangulated-mesh
+form factor, the analytic form factors, the lattice structure factor and the four-term
+DWBA combination — as hand-written CUDA kernels behind a C ABI (include/hgx.h,
+libhgx.so).  This Python package is a thin host-side mirror of that ABI; the C++ drop-in
+classes with the reference's signatures live in csrc/hig/.
+"""
+from ._capi import HgxError, lib  # noqa: F401
+from .core import Context, QGrid, ff_triangles, ff_triangles_arrays, measure_peaks  # noqa: F401
+
+__all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "HgxError", "lib"]

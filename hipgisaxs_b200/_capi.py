@@ -1,0 +1,78 @@
+"""ctypes bindings to libhgx.so (the C ABI declared in include/hgx.h).
+
+The library is built in-tree (python -m hipgisaxs_b200.build).  Loading fails loudly when
+it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhgx.so")
+
+HGX_OK = 0
+F64, F32C = 0, 1
+C128, C64 = 0, 1
+
+_vp = C.c_void_p
+_i = C.c_int
+_d = C.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "hgx_last_error": (C.c_char_p, []),
+    "hgx_status_string": (C.c_char_p, [_i]),
+    "hgx_version": (_i, []),
+    "hgx_create": (_i, [_i, C.POINTER(_vp)]),
+    "hgx_destroy": (_i, [_vp]),
+    "hgx_set_stream": (_i, [_vp, _vp]),
+    "hgx_get_stream": (_vp, [_vp]),
+    "hgx_synchronize": (_i, [_vp]),
+    "hgx_qgrid_from_arrays": (_i, [_vp, _i, _vp, _vp, _i, _vp, _i, C.POINTER(_vp)]),
+    "hgx_qgrid_create": (_i, [_vp, _i, _i, _d, _d, _d, _d, _d, _d, _d, _d, C.POINTER(_vp)]),
+    "hgx_qgrid_read": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hgx_qgrid_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i),
+                            C.POINTER(_i)]),
+    "hgx_qgrid_destroy": (_i, [_vp]),
+    "hgx_ff_triangles_q": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i]),
+    "hgx_ff_triangles_q_ex": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i]),
+    "hgx_ff_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
+}
+
+_lib = None
+
+
+class HgxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"hgx status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m hipgisaxs_b200.build`"
+                              " (the CUDA library is required; there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in include/hgx.h that the loaded library exports."""
+    L = lib()
+    return [n for n in SIGNATURES if hasattr(L, n)]
+
+
+def check(status: int):
+    if status != HGX_OK:
+        msg = lib().hgx_last_error()
+        raise HgxError(status, msg.decode() if msg else "")
+    return status

@@ -1,0 +1,621 @@
+// Numeric (triangulated-mesh) form factor:  F(q) = sum_t (-i)(q'.n_t) s_t e^{i q'.c_t} / |q'|^2,
+// q' = R q — the reference's "approx triangle" formula (src/ff/cpu/ff_tri_cpu.cpp:233-240,
+// src/ff/gpu/ff_tri_gpu.cu:371-384).
+//
+// Three kernels:
+//  * ff_tri_f64_kernel     — the plain FP64 form: one thread per q-point, triangles staged
+//                            through shared memory, reference arithmetic.  Parity reference
+//                            on the device and the denominator of the FP32 speed-up.
+//  * ff_tri_rows_kernel    — FP32, for q-grids laid out by detector rows (QGrid layout: qz
+//                            depends on the row only).  The rotation is folded into the
+//                            triangles (q'.c = q.(R^T c)), the phase splits into an in-plane
+//                            part e^{i(qx c'x + qy c'y)} evaluated per (pixel, triangle) and a
+//                            row part e^{i qz_k c'z} evaluated once per (row, triangle) and
+//                            block k.  With the four real DWBA blocks (qz_3 = -qz_0,
+//                            qz_1 = -qz_2) one in-plane sincos serves all four blocks.
+//                            Triangle tiles arrive in shared memory by TMA bulk copies,
+//                            double-buffered on mbarriers.  Phases are carried in turns and
+//                            reduced exactly (r = t - rint t) before the SFU sincos.  Sums are
+//                            blocked per tile and folded with TwoSum (compensated).
+//  * ff_tri_points_kernel  — FP32 for arbitrary q-point sets (one thread per q-point), the
+//                            same phase/accumulation scheme without the row factorisation.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "hgx_internal.cuh"
+#include "ptx.cuh"
+
+namespace hgx {
+
+constexpr int TILE = 64;                    // triangles per shared-memory tile
+constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (cx,cy,nx,ny) + float2 B[TILE] (cz,nz)
+constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
+constexpr double TWO_PI = 6.283185307179586476925286766559;
+constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
+
+struct Rot9 {
+  double r[9];
+};
+
+// ------------------------------------------------------------- triangle prep ----
+// shape_def (T x 8 FP64) -> FP32 tiles.  n' = R^T n and c' = R^T c in FP64; the area is
+// folded into the normal (n~ = s n') and the centroid is carried in turns (c~ = c'/2pi).
+// Padding triangles are zero (they contribute nothing).
+__global__ void tri_prep_kernel(const double* __restrict__ sd, int ntri, int ntiles, Rot9 R,
+                                float* __restrict__ tiles) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntiles * TILE) return;
+  int tile = t / TILE, j = t - tile * TILE;
+  float4* A = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_FLOATS);
+  float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_FLOATS + 4 * TILE);
+  if (t < ntri) {
+    const double* p = sd + 8L * t;
+    double s = p[0];
+    double n[3] = {p[1], p[2], p[3]}, c[3] = {p[4], p[5], p[6]};
+    double np[3], cp[3];
+    for (int l = 0; l < 3; ++l) {
+      np[l] = R.r[0 * 3 + l] * n[0] + R.r[1 * 3 + l] * n[1] + R.r[2 * 3 + l] * n[2];
+      cp[l] = R.r[0 * 3 + l] * c[0] + R.r[1 * 3 + l] * c[1] + R.r[2 * 3 + l] * c[2];
+    }
+    A[j] = make_float4((float)(cp[0] * INV_TWO_PI), (float)(cp[1] * INV_TWO_PI),
+                       (float)(s * np[0]), (float)(s * np[1]));
+    B[j] = make_float2((float)(cp[2] * INV_TWO_PI), (float)(s * np[2]));
+  } else {
+    A[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    B[j] = make_float2(0.f, 0.f);
+  }
+}
+
+// ------------------------------------------------------------------ helpers ----
+__device__ __forceinline__ void two_sum_fold(float& sum, float& part, float& comp) {
+  float s = sum + part;
+  float bp = s - sum;
+  float err = (sum - (s - bp)) + (part - bp);
+  sum = s;
+  comp += err;
+  part = 0.f;
+}
+
+// |R (qx, qy, qz)|^2 with complex qz, as RotMatrix_t::rotate + cuCnorm3 evaluate it.
+__device__ __forceinline__ double rotated_q2(const Rot9& R, double qx, double qy, double2 qz) {
+  double q2 = 0.0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double re = R.r[3 * j] * qx + R.r[3 * j + 1] * qy + R.r[3 * j + 2] * qz.x;
+    double im = R.r[3 * j + 2] * qz.y;
+    q2 += re * re + im * im;
+  }
+  return q2;
+}
+
+template <typename OUT>
+__device__ __forceinline__ void store_ff(OUT* out, long idx, double re, double im);
+template <>
+__device__ __forceinline__ void store_ff<float2>(float2* out, long idx, double re, double im) {
+  out[idx] = make_float2((float)re, (float)im);
+}
+template <>
+__device__ __forceinline__ void store_ff<double2>(double2* out, long idx, double re, double im) {
+  out[idx] = make_double2(re, im);
+}
+
+// ------------------------------------------------------------- row kernel ----
+struct RowArgs {
+  const float* tiles;
+  int ntiles;
+  const double* qx;
+  const double* qy;
+  const double2* rowqz;  // nrow x NK
+  int nqy, nrow, ncol, rows_per_cta;
+  Rot9 R;
+  void* out;
+  unsigned* err;
+};
+
+// Row factor of one (row, triangle) for a real block pair (qz, -qz):
+// Z = e^{i 2pi qz cz~} = (x, y), D = qz n~z; returns (x, y, D*y, D*x).
+__device__ __forceinline__ float4 paired_factor(double q, float cz, float nz) {
+  double u = q * (double)cz;
+  u -= rint(u);
+  float s, c;
+  sincospif((float)(2.0 * u), &s, &c);
+  float D = (float)(q * (double)nz);
+  return make_float4(c, s, D * s, D * c);
+}
+
+// Row factor for a general complex block: Z = e^{i 2pi qz cz~}, D = qz n~z; returns (Z, D Z).
+__device__ __forceinline__ float4 complex_factor(double2 q, float cz, float nz) {
+  double u = q.x * (double)cz;
+  u -= rint(u);
+  double amp = exp(-TWO_PI * q.y * (double)cz);
+  double s, c;
+  sincospi(2.0 * u, &s, &c);
+  double zr = amp * c, zi = amp * s;
+  double dr = q.x * (double)nz, di = q.y * (double)nz;
+  return make_float4((float)zr, (float)zi, (float)(dr * zr - di * zi), (float)(dr * zi + di * zr));
+}
+
+template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
+__global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
+  constexpr int NF = PAIRED ? 2 : NK;        // float4 row factors per (row, triangle)
+  constexpr int NACC = PAIRED ? 8 : 2 * NK;  // float accumulators per pixel
+  __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  extern __shared__ __align__(16) float4 s_rf[];  // rows_per_cta x TILE x NF
+
+  const int R = a.rows_per_cta;
+  const int tpr = BLOCK / R;
+  const int lr = threadIdx.x / tpr;
+  const int lane = threadIdx.x - lr * tpr;
+  const int row = blockIdx.y * R + lr;
+  const int colbase = blockIdx.x * (tpr * P) + lane;
+
+  float qxf[P], qyf[P];
+  float acc[P][NACC], sum[P][NACC], cmp[P][NACC];
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    int col = colbase + i * tpr;
+    bool v = row < a.nrow && col < a.ncol;
+    long p = (long)row * a.ncol + col;
+    qxf[i] = v ? (float)a.qx[p] : 0.f;
+    qyf[i] = v ? (float)a.qy[p] : 0.f;
+#pragma unroll
+    for (int n = 0; n < NACC; ++n) acc[i][n] = sum[i][n] = cmp[i][n] = 0.f;
+  }
+
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2 && s < a.ntiles; ++s) {
+      mbar_arrive_expect_tx(&s_bar[s], TILE_BYTES);
+      bulk_g2s(s_tile[s], a.tiles + (size_t)s * TILE_FLOATS, TILE_BYTES, &s_bar[s]);
+    }
+  }
+
+  for (int s = 0; s < a.ntiles; ++s) {
+    const int b = s & 1;
+    const bool ok = mbar_wait(&s_bar[b], (s >> 1) & 1);
+    const float4* A = reinterpret_cast<const float4*>(s_tile[b]);
+    const float2* B = reinterpret_cast<const float2*>(s_tile[b] + 4 * TILE);
+    if (ok) {
+      for (int it = threadIdx.x; it < R * TILE; it += BLOCK) {
+        int r = it / TILE, j = it - r * TILE;
+        int grow = blockIdx.y * R + r;
+        float2 bz = B[j];
+        float4* dst = s_rf + (size_t)(r * TILE + j) * NF;
+        if (PAIRED) {
+          float4 f0 = make_float4(1.f, 0.f, 0.f, 0.f), f2 = f0;
+          if (grow < a.nrow) {
+            f0 = paired_factor(a.rowqz[(long)grow * 4 + 0].x, bz.x, bz.y);
+            f2 = paired_factor(a.rowqz[(long)grow * 4 + 2].x, bz.x, bz.y);
+          }
+          dst[0] = f0;
+          dst[1] = f2;
+        } else {
+#pragma unroll
+          for (int k = 0; k < NK; ++k)
+            dst[k] = grow < a.nrow ? complex_factor(a.rowqz[(long)grow * NK + k], bz.x, bz.y)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      // A bulk copy did not arrive in time: record it, wait (bounded) for the copies this
+      // CTA still has in flight so none lands after exit, then leave.
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, (unsigned)DEV_ERR_WAIT_TIMEOUT);
+        mbar_wait(&s_bar[b], (s >> 1) & 1);
+        if (s + 1 < a.ntiles) mbar_wait(&s_bar[b ^ 1], ((s + 1) >> 1) & 1);
+      }
+      __syncthreads();
+      return;
+    }
+
+    const float4* RF = s_rf + (size_t)lr * TILE * NF;
+#pragma unroll 2
+    for (int j = 0; j < TILE; ++j) {
+      const float4 t = A[j];
+      float4 f[NF];
+#pragma unroll
+      for (int n = 0; n < NF; ++n) f[n] = RF[j * NF + n];
+#pragma unroll
+      for (int i = 0; i < P; ++i) {
+        float tp = fmaf(qxf[i], t.x, qyf[i] * t.y);  // in-plane phase, turns
+        float rr = tp - rintf(tp);                   // exact reduction to [-1/2, 1/2]
+        float sn, cs;
+        __sincosf(rr * 6.28318530717958648f, &sn, &cs);
+        float aq = fmaf(qxf[i], t.z, qyf[i] * t.w);  // in-plane part of q.n~
+        float ur = aq * cs, ui = aq * sn;            // U = aq * E
+        if (PAIRED) {
+#pragma unroll
+          for (int pr = 0; pr < 2; ++pr) {
+            const float4 g = f[pr];  // (x, y, beta, gamma)
+            float* q = acc[i] + 4 * pr;
+            q[0] = fmaf(g.x, ur, q[0]);
+            q[0] = fmaf(-g.z, sn, q[0]);  // P.re += x Ur - beta s
+            q[1] = fmaf(g.x, ui, q[1]);
+            q[1] = fmaf(g.z, cs, q[1]);   // P.im += x Ui + beta c
+            q[2] = fmaf(-g.y, ui, q[2]);
+            q[2] = fmaf(g.w, cs, q[2]);   // M.re += -y Ui + gamma c
+            q[3] = fmaf(g.y, ur, q[3]);
+            q[3] = fmaf(g.w, sn, q[3]);   // M.im += y Ur + gamma s
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NK; ++k) {
+            const float4 g = f[k];  // (Zr, Zi, DZr, DZi)
+            float* q = acc[i] + 2 * k;
+            q[0] = fmaf(ur, g.x, q[0]);
+            q[0] = fmaf(-ui, g.y, q[0]);
+            q[0] = fmaf(g.z, cs, q[0]);
+            q[0] = fmaf(-g.w, sn, q[0]);
+            q[1] = fmaf(ur, g.y, q[1]);
+            q[1] = fmaf(ui, g.x, q[1]);
+            q[1] = fmaf(g.z, sn, q[1]);
+            q[1] = fmaf(g.w, cs, q[1]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+#pragma unroll
+      for (int n = 0; n < NACC; ++n) two_sum_fold(sum[i][n], acc[i][n], cmp[i][n]);
+    __syncthreads();  // every thread is done with tile buffer b and the row factors
+    if (threadIdx.x == 0 && s + 2 < a.ntiles) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&s_bar[b], TILE_BYTES);
+      bulk_g2s(s_tile[b], a.tiles + (size_t)(s + 2) * TILE_FLOATS, TILE_BYTES, &s_bar[b]);
+    }
+  }
+
+  // epilogue: F_k = (-i) S_k / |R q_k|^2
+  OUT* out = reinterpret_cast<OUT*>(a.out);
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    int col = colbase + i * tpr;
+    if (row >= a.nrow || col >= a.ncol) continue;
+    long p = (long)row * a.ncol + col;
+    double qx = a.qx[p], qy = a.qy[p];
+    double T[NACC];
+#pragma unroll
+    for (int n = 0; n < NACC; ++n) T[n] = (double)sum[i][n] + (double)cmp[i][n];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) {
+      double sr, si;
+      if (PAIRED) {
+        // blocks 0,3 from pair 0 (P0 +- M0); blocks 2,1 from pair 2 (P2 +- M2)
+        const int pr = (k == 0 || k == 3) ? 0 : 1;
+        const double sg = (k == 0 || k == 2) ? 1.0 : -1.0;
+        sr = T[4 * pr + 0] + sg * T[4 * pr + 2];
+        si = T[4 * pr + 1] + sg * T[4 * pr + 3];
+      } else {
+        sr = T[2 * k];
+        si = T[2 * k + 1];
+      }
+      double2 qz = a.rowqz[(long)row * NK + k];
+      double q2 = rotated_q2(a.R, qx, qy, qz);
+      store_ff<OUT>(out, (long)k * a.nqy + p, si / q2, -sr / q2);
+    }
+  }
+}
+
+// ----------------------------------------------------------- points kernel ----
+struct PointArgs {
+  const float* tiles;
+  int ntiles;
+  const double* qx;
+  const double* qy;
+  const double2* qz;
+  int nqy, nqz;
+  Rot9 R;
+  void* out;
+  unsigned* err;
+};
+
+template <int BLOCK, typename OUT>
+__global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
+  __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  const long iz = (long)blockIdx.x * BLOCK + threadIdx.x;
+  const bool valid = iz < a.nqz;
+  float qxf = 0.f, qyf = 0.f, qzr = 0.f, qzi = 0.f;
+  if (valid) {
+    long iy = iz % a.nqy;
+    qxf = (float)a.qx[iy];
+    qyf = (float)a.qy[iy];
+    double2 q = a.qz[iz];
+    qzr = (float)q.x;
+    qzi = (float)q.y;
+  }
+  const float kexp = (float)(-TWO_PI) * qzi;
+  float acc[2] = {0.f, 0.f}, sum[2] = {0.f, 0.f}, cmp[2] = {0.f, 0.f};
+
+  if (threadIdx.x == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 2 && s < a.ntiles; ++s) {
+      mbar_arrive_expect_tx(&s_bar[s], TILE_BYTES);
+      bulk_g2s(s_tile[s], a.tiles + (size_t)s * TILE_FLOATS, TILE_BYTES, &s_bar[s]);
+    }
+  }
+  for (int s = 0; s < a.ntiles; ++s) {
+    const int b = s & 1;
+    const bool ok = mbar_wait(&s_bar[b], (s >> 1) & 1);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, (unsigned)DEV_ERR_WAIT_TIMEOUT);
+        mbar_wait(&s_bar[b], (s >> 1) & 1);
+        if (s + 1 < a.ntiles) mbar_wait(&s_bar[b ^ 1], ((s + 1) >> 1) & 1);
+      }
+      __syncthreads();
+      return;
+    }
+    const float4* A = reinterpret_cast<const float4*>(s_tile[b]);
+    const float2* B = reinterpret_cast<const float2*>(s_tile[b] + 4 * TILE);
+#pragma unroll 4
+    for (int j = 0; j < TILE; ++j) {
+      const float4 t = A[j];
+      const float2 z = B[j];
+      float tp = fmaf(qzr, z.x, fmaf(qxf, t.x, qyf * t.y));
+      float rr = tp - rintf(tp);
+      float sn, cs;
+      __sincosf(rr * 6.28318530717958648f, &sn, &cs);
+      if (qzi != 0.f) {
+        float amp = __expf(kexp * z.x);
+        sn *= amp;
+        cs *= amp;
+      }
+      float ar = fmaf(qzr, z.y, fmaf(qxf, t.z, qyf * t.w));
+      float ai = qzi * z.y;
+      acc[0] = fmaf(ar, cs, acc[0]);
+      acc[0] = fmaf(-ai, sn, acc[0]);
+      acc[1] = fmaf(ar, sn, acc[1]);
+      acc[1] = fmaf(ai, cs, acc[1]);
+    }
+    two_sum_fold(sum[0], acc[0], cmp[0]);
+    two_sum_fold(sum[1], acc[1], cmp[1]);
+    __syncthreads();
+    if (threadIdx.x == 0 && s + 2 < a.ntiles) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&s_bar[b], TILE_BYTES);
+      bulk_g2s(s_tile[b], a.tiles + (size_t)(s + 2) * TILE_FLOATS, TILE_BYTES, &s_bar[b]);
+    }
+  }
+  if (!valid) return;
+  long iy = iz % a.nqy;
+  double q2 = rotated_q2(a.R, a.qx[iy], a.qy[iy], a.qz[iz]);
+  double sr = (double)sum[0] + (double)cmp[0], si = (double)sum[1] + (double)cmp[1];
+  store_ff<OUT>(reinterpret_cast<OUT*>(a.out), iz, si / q2, -sr / q2);
+}
+
+// -------------------------------------------------------------- FP64 kernel ----
+constexpr int TILE64 = 64;
+
+struct F64Args {
+  const double* sd;  // T x 8
+  int ntri;
+  const double* qx;
+  const double* qy;
+  const double2* qz;
+  int nqy, nqz;
+  Rot9 R;
+  void* out;
+};
+
+// The plain FP64 form: one thread per q-point, reference arithmetic
+// (src/ff/gpu/ff_tri_gpu.cu:319-390) without its shared-memory race; 1/|q'|^2 is applied
+// once per q-point instead of once per term.
+template <int BLOCK, typename OUT>
+__global__ void __launch_bounds__(BLOCK) ff_tri_f64_kernel(F64Args a) {
+  __shared__ double s_sd[TILE64 * 8];
+  const long iz = (long)blockIdx.x * BLOCK + threadIdx.x;
+  const bool valid = iz < a.nqz;
+  double2 m[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+  double q2 = 1.0;
+  if (valid) {
+    long iy = iz % a.nqy;
+    double qx = a.qx[iy], qy = a.qy[iy];
+    double2 qz = a.qz[iz];
+    q2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      m[j].x = a.R.r[3 * j] * qx + a.R.r[3 * j + 1] * qy + a.R.r[3 * j + 2] * qz.x;
+      m[j].y = a.R.r[3 * j + 2] * qz.y;
+      q2 += m[j].x * m[j].x + m[j].y * m[j].y;
+    }
+  }
+  const bool real_q = m[0].y == 0.0 && m[1].y == 0.0 && m[2].y == 0.0;
+  double accr = 0.0, acci = 0.0;
+  for (int t0 = 0; t0 < a.ntri; t0 += TILE64) {
+    __syncthreads();
+    const int nt = min(TILE64, a.ntri - t0);
+    for (int k = threadIdx.x; k < nt * 8; k += BLOCK) s_sd[k] = a.sd[8L * t0 + k];
+    __syncthreads();
+    for (int j = 0; j < nt; ++j) {
+      const double* p = s_sd + 8 * j;
+      double s = p[0];
+      double qnr = m[0].x * p[1] + m[1].x * p[2] + m[2].x * p[3];
+      double qni = m[0].y * p[1] + m[1].y * p[2] + m[2].y * p[3];
+      double qtr = m[0].x * p[4] + m[1].x * p[5] + m[2].x * p[6];
+      double sn, cs;
+      sincos(qtr, &sn, &cs);
+      if (!real_q) {
+        double qti = m[0].y * p[4] + m[1].y * p[5] + m[2].y * p[6];
+        double e = exp(-qti);
+        sn *= e;
+        cs *= e;
+      }
+      // (-i) qn s = (qni s, -qnr s); times e^{i qt}
+      double ar = qni * s, ai = -qnr * s;
+      accr += ar * cs - ai * sn;
+      acci += ar * sn + ai * cs;
+    }
+  }
+  if (valid) store_ff<OUT>(reinterpret_cast<OUT*>(a.out), iz, accr / q2, acci / q2);
+}
+
+// ------------------------------------------------------------------ launch ----
+static Rot9 make_rot(const double* r9) {
+  Rot9 R;
+  static const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int i = 0; i < 9; ++i) R.r[i] = r9 ? r9[i] : eye[i];
+  return R;
+}
+
+template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
+static int launch_rows(const RowArgs& a, dim3 grid, cudaStream_t st) {
+  constexpr int NF = PAIRED ? 2 : NK;
+  size_t smem = (size_t)a.rows_per_cta * TILE * NF * sizeof(float4);
+  ff_tri_rows_kernel<BLOCK, P, NK, PAIRED, OUT><<<grid, BLOCK, smem, st>>>(a);
+  HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+template <int P, typename OUT>
+static int dispatch_rows(const RowArgs& a, dim3 grid, int nk, bool paired, cudaStream_t st) {
+  if (paired) return launch_rows<256, P, 4, true, OUT>(a, grid, st);
+  if (nk == 4) return launch_rows<256, P, 4, false, OUT>(a, grid, st);
+  return launch_rows<256, P, 1, false, OUT>(a, grid, st);
+}
+
+// Launch shape for the row kernel: P pixels per thread, threads per row a power of two
+// (>= 32) covering the row when it is short, several rows per CTA in that case.
+struct RowShape {
+  int P, tpr, R;
+  dim3 grid;
+};
+
+static RowShape row_shape(int nrow, int ncol, int sm_count, int want_p) {
+  const int BLOCK = 256;
+  RowShape best{};
+  for (int P = want_p; P >= 1; P >>= 1) {
+    int tpr = 32;
+    while (tpr < BLOCK && tpr * P < ncol) tpr <<= 1;
+    int R = BLOCK / tpr;
+    dim3 g((ncol + tpr * P - 1) / (tpr * P), (nrow + R - 1) / R);
+    best = RowShape{P, tpr, R, g};
+    if ((long)g.x * g.y >= 2L * sm_count) break;  // enough CTAs to fill the GPU
+  }
+  return best;
+}
+
+int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, const double* rot9,
+                        int precision, void* out, int ff_type, int want_p) {
+  cudaStream_t st = c->stream;
+  Rot9 R = make_rot(rot9);
+  const bool c64 = ff_type == HGX_C64;
+  if (precision == HGX_F64) {
+    F64Args a{sd, ntri, g->qx, g->qy, g->qz, g->nqy, g->nqz, R, out};
+    dim3 grid((g->nqz + 127) / 128);
+    if (c64) ff_tri_f64_kernel<128, float2><<<grid, 128, 0, st>>>(a);
+    else ff_tri_f64_kernel<128, double2><<<grid, 128, 0, st>>>(a);
+    HGX_CUDA(cudaGetLastError());
+    return HGX_OK;
+  }
+  // FP32: triangle tiles in scratch
+  const int ntiles = (ntri + TILE - 1) / TILE;
+  HGX_TRY(c->scratch.reserve((size_t)ntiles * TILE_BYTES));
+  float* tiles = reinterpret_cast<float*>(c->scratch.p);
+  {
+    int n = ntiles * TILE;
+    tri_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(sd, ntri, ntiles, R, tiles);
+    HGX_CUDA(cudaGetLastError());
+  }
+  if (g->mode == 0) {
+    PointArgs a{tiles, ntiles, g->qx, g->qy, g->qz, g->nqy, g->nqz, R, out, c->d_err};
+    dim3 grid((g->nqz + 127) / 128);
+    if (c64) ff_tri_points_kernel<128, float2><<<grid, 128, 0, st>>>(a);
+    else ff_tri_points_kernel<128, double2><<<grid, 128, 0, st>>>(a);
+    HGX_CUDA(cudaGetLastError());
+    return HGX_OK;
+  }
+  RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, want_p > 0 ? want_p : 2);
+  if (sh.grid.y > 65535u)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: too many detector rows for one launch");
+  RowArgs a{tiles, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R, out,
+            c->d_err};
+  const bool paired = g->mode == 1;
+  switch (sh.P) {
+    case 4:
+      return c64 ? dispatch_rows<4, float2>(a, sh.grid, g->nk, paired, st)
+                 : dispatch_rows<4, double2>(a, sh.grid, g->nk, paired, st);
+    case 2:
+      return c64 ? dispatch_rows<2, float2>(a, sh.grid, g->nk, paired, st)
+                 : dispatch_rows<2, double2>(a, sh.grid, g->nk, paired, st);
+    default:
+      return c64 ? dispatch_rows<1, float2>(a, sh.grid, g->nk, paired, st)
+                 : dispatch_rows<1, double2>(a, sh.grid, g->nk, paired, st);
+  }
+}
+
+}  // namespace hgx
+
+using namespace hgx;
+
+extern "C" {
+
+int hgx_ff_triangles_q_ex(hgx_ctx c, hgx_qgrid g, const double* shape_def, int ntri,
+                         const double* rot9, int precision, void* ff, int ff_type, int pixels) {
+  if (!c || !g || !shape_def || !ff)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: null argument");
+  if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: no triangles");
+  if (precision != HGX_F64 && precision != HGX_F32C)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: unknown precision");
+  if (ff_type != HGX_C128 && ff_type != HGX_C64)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: unknown output type");
+  if (g->ctx != c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: grid of another context");
+  HGX_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  const double* sd = shape_def;
+  if (!is_device_ptr(shape_def)) {
+    HGX_TRY(c->staging.reserve(sizeof(double) * 8 * (size_t)ntri));
+    HGX_CUDA(cudaMemcpyAsync(c->staging.p, shape_def, sizeof(double) * 8 * (size_t)ntri,
+                             cudaMemcpyHostToDevice, st));
+    sd = reinterpret_cast<const double*>(c->staging.p);
+  }
+  const size_t esz = ff_type == HGX_C64 ? sizeof(float2) : sizeof(double2);
+  const bool host_out = !is_device_ptr(ff);
+  void* dout = ff;
+  DevBuf tmp;
+  if (host_out) {
+    HGX_TRY(tmp.reserve(esz * (size_t)g->nqz));
+    dout = tmp.p;
+  }
+  HGX_TRY(ff_triangles_device(c, g, sd, ntri, rot9, precision, dout, ff_type, pixels));
+  if (host_out) {
+    HGX_CUDA(cudaMemcpyAsync(ff, dout, esz * (size_t)g->nqz, cudaMemcpyDeviceToHost, st));
+    return hgx_synchronize(c);
+  }
+  return HGX_OK;
+}
+
+int hgx_ff_triangles_q(hgx_ctx c, hgx_qgrid g, const double* shape_def, int ntri,
+                       const double* rot9, int precision, void* ff, int ff_type) {
+  return hgx_ff_triangles_q_ex(c, g, shape_def, ntri, rot9, precision, ff, ff_type, 0);
+}
+
+int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, const double* qx,
+                     const double* qy, int nqz, const double* qz, const double* rot9,
+                     int precision, double* ff) {
+  if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: no triangles");
+  hgx_qgrid g = nullptr;
+  HGX_TRY(hgx_qgrid_from_arrays(c, nqy, qx, qy, nqz, qz, 0, &g));
+  int s = hgx_ff_triangles_q(c, g, shape_def, ntri, rot9, precision, ff, HGX_C128);
+  if (s == HGX_OK && is_device_ptr(ff)) s = hgx_synchronize(c);
+  hgx_qgrid_destroy(g);
+  return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,291 @@
+// Context, errors, device buffers and q-grid objects of the hgx C ABI.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "hgx_internal.cuh"
+
+namespace hgx {
+
+static thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a non-sticky error so the context stays usable
+  return fail(e == cudaErrorMemoryAllocation ? HGX_ERR_NO_MEMORY : HGX_ERR_CUDA, m);
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int DevBuf::reserve(size_t n) {
+  if (n <= bytes) return HGX_OK;
+  release();
+  size_t want = n < 4096 ? 4096 : n;
+  cudaError_t e = cudaMalloc(&p, want);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    bytes = 0;
+    return cuda_fail(e, "cudaMalloc(scratch)");
+  }
+  bytes = want;
+  return HGX_OK;
+}
+
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+// ------------------------------------------------------------- row table ----
+// For q-grids laid out by detector rows: records each row's qz per block and checks that
+// qz is constant along every row and, for 4 blocks, that the blocks pair as the DWBA
+// construction makes them (block 3 = -block 0, block 1 = -block 2, all real).
+__global__ void row_table_kernel(const double2* __restrict__ qz, int nqy, int nk, int ncol,
+                                 double2* __restrict__ rowqz, unsigned* __restrict__ flags) {
+  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nqy) return;
+  int row = (int)(p / ncol);
+  long first = (long)row * ncol;
+  bool row_ok = true, paired = (nk == 4);
+  for (int k = 0; k < nk; ++k) {
+    double2 v = qz[(long)k * nqy + p];
+    double2 f = qz[(long)k * nqy + first];
+    if (v.x != f.x || v.y != f.y) row_ok = false;
+    if (p == first) rowqz[(long)row * nk + k] = v;
+    if (v.y != 0.0) paired = false;
+  }
+  if (nk == 4) {
+    double2 a = qz[p], b = qz[(long)nqy + p], c = qz[2L * nqy + p], d = qz[3L * nqy + p];
+    if (d.x != -a.x || b.x != -c.x) paired = false;
+  }
+  if (!row_ok) atomicOr(flags, 1u);
+  if (!paired) atomicOr(flags, 2u);
+}
+
+int qgrid_finalize(hgx_qgrid g) {
+  g->mode = 0;
+  if (g->nk != 1 && g->nk != 4) return HGX_OK;
+  if (g->ncol <= 0 || g->nqy % g->ncol != 0) return HGX_OK;
+  g->nrow = g->nqy / g->ncol;
+  HGX_CUDA(cudaMalloc(&g->rowqz, sizeof(double2) * (size_t)g->nrow * g->nk));
+  unsigned* d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
+  HGX_TRY(g->ctx->scratch.reserve(256));
+  d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
+  cudaStream_t st = g->ctx->stream;
+  HGX_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(unsigned), st));
+  int threads = 256;
+  int blocks = (g->nqy + threads - 1) / threads;
+  row_table_kernel<<<blocks, threads, 0, st>>>(g->qz, g->nqy, g->nk, g->ncol, g->rowqz, d_flags);
+  HGX_CUDA(cudaGetLastError());
+  unsigned flags = 0;
+  HGX_CUDA(cudaMemcpyAsync(&flags, d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  if (flags & 1u) {  // not row-constant: the per-q-point kernels handle it
+    cudaFree(g->rowqz);
+    g->rowqz = nullptr;
+    g->nrow = 0;
+    g->mode = 0;
+    return HGX_OK;
+  }
+  g->mode = (g->nk == 4 && !(flags & 2u)) ? 1 : 2;
+  return HGX_OK;
+}
+
+}  // namespace hgx
+
+using namespace hgx;
+
+extern "C" {
+
+const char* hgx_last_error(void) { return g_last_error.c_str(); }
+
+const char* hgx_status_string(int s) {
+  switch (s) {
+    case HGX_OK: return "ok";
+    case HGX_ERR_INVALID_ARG: return "invalid argument";
+    case HGX_ERR_CUDA: return "CUDA error";
+    case HGX_ERR_NO_MEMORY: return "out of memory";
+    case HGX_ERR_DEVICE: return "device-side error";
+    case HGX_ERR_NOT_FINITE: return "non-finite result";
+    default: return "unknown status";
+  }
+}
+
+int hgx_version(void) { return 10000; }
+
+int hgx_create(int device, hgx_ctx* out) {
+  if (!out) return fail(HGX_ERR_INVALID_ARG, "hgx_create: out is NULL");
+  *out = nullptr;
+  int dev = device;
+  if (dev < 0) HGX_CUDA(cudaGetDevice(&dev));
+  int ndev = 0;
+  HGX_CUDA(cudaGetDeviceCount(&ndev));
+  if (dev >= ndev) return fail(HGX_ERR_INVALID_ARG, "hgx_create: no such device");
+  HGX_CUDA(cudaSetDevice(dev));
+  hgx_ctx c = new (std::nothrow) hgx_ctx_s();
+  if (!c) return fail(HGX_ERR_NO_MEMORY, "hgx_create: host allocation");
+  c->device = dev;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+    c->sm_count = prop.multiProcessorCount;
+    c->max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+  }
+  cudaError_t e = cudaMalloc(&c->d_err, sizeof(unsigned));
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaMalloc(error word)");
+  }
+  cudaMemset(c->d_err, 0, sizeof(unsigned));
+  *out = c;
+  return HGX_OK;
+}
+
+int hgx_destroy(hgx_ctx c) {
+  if (!c) return HGX_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (c->d_err) cudaFree(c->d_err);
+  c->scratch.release();
+  c->staging.release();
+  delete c;
+  return HGX_OK;
+}
+
+int hgx_set_stream(hgx_ctx c, void* stream) {
+  if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_set_stream: ctx is NULL");
+  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  return HGX_OK;
+}
+
+void* hgx_get_stream(hgx_ctx c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }
+
+int hgx_synchronize(hgx_ctx c) {
+  if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_synchronize: ctx is NULL");
+  HGX_CUDA(cudaSetDevice(c->device));
+  HGX_CUDA(cudaStreamSynchronize(c->stream));
+  unsigned err = 0;
+  HGX_CUDA(cudaMemcpy(&err, c->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (err) {
+    cudaMemset(c->d_err, 0, sizeof(unsigned));
+    char buf[160];
+    snprintf(buf, sizeof buf, "device error bits 0x%x (1=wait timeout, 2=row mismatch, "
+             "4=bad index, 8=queue timeout)", err);
+    return fail(HGX_ERR_DEVICE, buf);
+  }
+  return HGX_OK;
+}
+
+int hgx_qgrid_from_arrays(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz,
+                          const double* qz, int ncol, hgx_qgrid* out) {
+  if (!c || !out || !qx || !qy || !qz) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_from_arrays: null argument");
+  *out = nullptr;
+  if (nqy < 1 || nqz < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_from_arrays: empty grid");
+  if (ncol < 0) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_from_arrays: ncol < 0");
+  HGX_CUDA(cudaSetDevice(c->device));
+  hgx_qgrid g = new (std::nothrow) hgx_qgrid_s();
+  if (!g) return fail(HGX_ERR_NO_MEMORY, "hgx_qgrid_from_arrays: host allocation");
+  g->ctx = c;
+  g->nqy = nqy;
+  g->nqz = nqz;
+  g->nk = (nqz % nqy == 0) ? nqz / nqy : 0;
+  cudaStream_t st = c->stream;
+  auto cleanup = [&](int s) {
+    hgx_qgrid_destroy(g);
+    return s;
+  };
+  if (cudaMalloc(&g->qx, sizeof(double) * nqy) != cudaSuccess ||
+      cudaMalloc(&g->qy, sizeof(double) * nqy) != cudaSuccess ||
+      cudaMalloc(&g->qz, sizeof(double2) * nqz) != cudaSuccess)
+    return cleanup(cuda_fail(cudaErrorMemoryAllocation, "hgx_qgrid_from_arrays: cudaMalloc"));
+  auto kind = [](const void* p) { return is_device_ptr(p) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; };
+  cudaError_t e = cudaMemcpyAsync(g->qx, qx, sizeof(double) * nqy, kind(qx), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->qy, qy, sizeof(double) * nqy, kind(qy), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->qz, qz, sizeof(double2) * nqz, kind(qz), st);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "hgx_qgrid_from_arrays: copy"));
+  // detector row length: given, or found where qz of block 0 first changes
+  if (ncol == 0 && g->nk >= 1) {
+    std::vector<double> h;
+    const double* src = qz;
+    if (is_device_ptr(qz)) {
+      h.resize(2 * (size_t)nqy);
+      e = cudaMemcpyAsync(h.data(), qz, sizeof(double2) * nqy, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return cleanup(cuda_fail(e, "hgx_qgrid_from_arrays: read qz"));
+      src = h.data();
+    }
+    int n = 1;
+    while (n < nqy && src[2 * n] == src[0] && src[2 * n + 1] == src[1]) ++n;
+    ncol = n;
+  }
+  g->ncol = ncol;
+  int s = qgrid_finalize(g);
+  if (s != HGX_OK) return cleanup(s);
+  *out = g;
+  return HGX_OK;
+}
+
+int hgx_qgrid_info(hgx_qgrid g, int* nqy, int* nqz, int* nrow, int* ncol, int* mode) {
+  if (!g) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_info: grid is NULL");
+  if (nqy) *nqy = g->nqy;
+  if (nqz) *nqz = g->nqz;
+  if (nrow) *nrow = g->nrow;
+  if (ncol) *ncol = g->ncol;
+  if (mode) *mode = g->mode;
+  return HGX_OK;
+}
+
+int hgx_qgrid_read(hgx_ctx c, hgx_qgrid g, double* qx, double* qy, double* qz, double* alpha,
+                   double* qz_ext) {
+  if (!c || !g) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_read: null argument");
+  HGX_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  auto kind = [](const void* p) { return is_device_ptr(p) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost; };
+  if (qx) HGX_CUDA(cudaMemcpyAsync(qx, g->qx, sizeof(double) * g->nqy, kind(qx), st));
+  if (qy) HGX_CUDA(cudaMemcpyAsync(qy, g->qy, sizeof(double) * g->nqy, kind(qy), st));
+  if (qz) {
+    if (!g->qz_det) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_read: grid has no detector qz");
+    HGX_CUDA(cudaMemcpyAsync(qz, g->qz_det, sizeof(double) * g->nqy, kind(qz), st));
+  }
+  if (alpha) {
+    if (!g->alpha) return fail(HGX_ERR_INVALID_ARG, "hgx_qgrid_read: grid has no exit angles");
+    HGX_CUDA(cudaMemcpyAsync(alpha, g->alpha, sizeof(double) * g->nrow, kind(alpha), st));
+  }
+  if (qz_ext) HGX_CUDA(cudaMemcpyAsync(qz_ext, g->qz, sizeof(double2) * g->nqz, kind(qz_ext), st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  return HGX_OK;
+}
+
+int hgx_qgrid_destroy(hgx_qgrid g) {
+  if (!g) return HGX_OK;
+  if (g->ctx) cudaSetDevice(g->ctx->device);
+  if (g->ctx) cudaStreamSynchronize(g->ctx->stream);
+  cudaFree(g->qx);
+  cudaFree(g->qy);
+  cudaFree(g->qz);
+  cudaFree(g->rowqz);
+  cudaFree(g->qz_det);
+  cudaFree(g->alpha);
+  delete g;
+  return HGX_OK;
+}
+
+}  // extern "C"

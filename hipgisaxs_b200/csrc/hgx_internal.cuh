@@ -1,0 +1,79 @@
+// Internal declarations shared by the hgx CUDA sources (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "hgx.h"
+
+namespace hgx {
+
+// ------------------------------------------------------------------ errors ----
+// Records a message for hgx_last_error() and returns the status.
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+#define HGX_CUDA(call)                                        \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::hgx::cuda_fail(e_, #call); \
+  } while (0)
+#define HGX_TRY(call)          \
+  do {                         \
+    int s_ = (call);           \
+    if (s_ != HGX_OK) return s_; \
+  } while (0)
+
+// Error bits a kernel may set in the context's device error word.
+enum DeviceError : unsigned {
+  DEV_ERR_WAIT_TIMEOUT = 1u << 0,   // a bounded mbarrier wait gave up
+  DEV_ERR_ROW_MISMATCH = 1u << 1,   // qz not constant along a row the caller declared
+  DEV_ERR_BAD_INDEX = 1u << 2,      // an index outside its array (mesh faces, ROIs)
+  DEV_ERR_QUEUE_TIMEOUT = 1u << 3,  // the persistent work queue gave up
+};
+
+// ------------------------------------------------------------- memory kind ----
+// True when p is device (or managed) memory usable by the current device.
+bool is_device_ptr(const void* p);
+
+// A device buffer owned by an object.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int reserve(size_t n);  // grows (never shrinks); contents are not preserved
+  void release();
+  ~DevBuf() { release(); }
+};
+
+}  // namespace hgx
+
+// -------------------------------------------------------------- the context ----
+struct hgx_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  unsigned* d_err = nullptr;  // device error word (DeviceError bits)
+  hgx::DevBuf scratch;        // per-call scratch, grown on demand
+  hgx::DevBuf staging;        // device copies of host inputs
+  int sm_count = 148;
+  int max_smem_optin = 227 * 1024;
+};
+
+// -------------------------------------------------------------- the q-grid ----
+struct hgx_qgrid_s {
+  hgx_ctx ctx = nullptr;
+  int nqy = 0, nqz = 0, nrow = 0, ncol = 0, nk = 0;  // nk = nqz / nqy when integral
+  int mode = 0;                  // 0 per-q-point, 1 rows paired-real, 2 rows complex
+  double* qx = nullptr;          // nqy
+  double* qy = nullptr;          // nqy
+  double2* qz = nullptr;         // nqz
+  double2* rowqz = nullptr;      // nrow x nk: the row-constant qz of each block (modes 1, 2)
+  double* qz_det = nullptr;      // nqy: detector qz (grids made by hgx_qgrid_create)
+  double* alpha = nullptr;       // nrow exit angles (grids made by hgx_qgrid_create)
+};
+
+namespace hgx {
+// Prepares triangle tiles for the FP32 kernels (see ff_tri.cu).
+int qgrid_finalize(hgx_qgrid g);  // builds the row table and picks the mode
+}  // namespace hgx

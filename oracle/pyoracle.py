@@ -58,8 +58,6 @@ def lib(backend: str = "port"):
         raise FileNotFoundError(f"oracle library missing: {path} (run `make -C oracle`"
                                 f"{' ref' if backend == 'ref' else ''})")
     L = C.CDLL(path)
-    for name in dir(L):
-        pass
     _libs[backend] = L
     return L
 
@@ -239,6 +237,42 @@ def sf_lattice(grid: Grid, abc, repet, scaling, center=(0, 0, 0), rot=None, back
                               _p(out.view(np.float64)))
     if rc <= 0:
         raise RuntimeError(f"sf_lattice failed rc={rc}")
+    return out
+
+
+def sf_lattice_arrays(abc, repet, scaling, center, rot, qx, qy, qz):
+    """Port backend on explicit arrays (qz complex; q-point i uses qx/qy[i % len(qx)])."""
+    L = lib("port")
+    abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
+    rp = np.ascontiguousarray(repet, dtype=np.float64)
+    sc = np.ascontiguousarray(scaling, dtype=np.float64)
+    ce = np.ascontiguousarray(center, dtype=np.float64)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    qx = np.ascontiguousarray(qx, dtype=np.float64)
+    qy = np.ascontiguousarray(qy, dtype=np.float64)
+    qz, qzf = _cbuf(qz)
+    out = np.zeros(len(qz), dtype=np.complex128)
+    L.orc_sf_lattice(_p(abc9), _p(rp), _p(sc), _p(ce), _p(r), C.c_int(len(qx)), _p(qx), _p(qy),
+                     C.c_int(len(qz)), _p(qzf), _p(out.view(np.float64)))
+    return out
+
+
+def ff_analytic_arrays(shape, params, qx, qy, qz, tau=0.0, eta=0.0, transvec=(0, 0, 0),
+                       rot=None):
+    """Port backend on explicit arrays."""
+    L = lib("port")
+    P = param_rows(params)
+    tv = np.ascontiguousarray(transvec, dtype=np.float64)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    qx = np.ascontiguousarray(qx, dtype=np.float64)
+    qy = np.ascontiguousarray(qy, dtype=np.float64)
+    qz, qzf = _cbuf(qz)
+    out = np.zeros(len(qz), dtype=np.complex128)
+    rc = L.orc_ff_analytic(C.c_int(SHAPE[shape]), C.c_int(len(P)), _p(P), C.c_double(tau),
+                           C.c_double(eta), _p(tv), _p(r), C.c_int(len(qx)), _p(qx), _p(qy),
+                           C.c_int(len(qz)), _p(qzf), _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"ff_analytic({shape}) failed rc={rc}")
     return out
 
 

@@ -1,0 +1,163 @@
+"""Numeric (mesh) form factor on the GPU against the CPU oracle.
+
+Tolerances (norm-wise relative error ||x - ref||_2 / ||ref||_2 over all q-points):
+  FP64 kernel : 1e-12
+  FP32C kernel: 1e-5  (the bound the project promises; typical values are ~1e-7)
+"""
+import numpy as np
+import pytest
+
+import hipgisaxs_b200 as hg
+from hipgisaxs_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def tri_cloud(rng, T, scale=6.0):
+    sd = np.zeros((T, 8))
+    sd[:, 0] = rng.uniform(0.2, 3.0, T)
+    n = rng.normal(size=(T, 3))
+    sd[:, 1:4] = n / np.linalg.norm(n, axis=1)[:, None]
+    sd[:, 4:7] = rng.normal(scale=scale, size=(T, 3))
+    return sd
+
+
+@pytest.mark.parametrize("grid", ["g16", "g16abs"])
+@pytest.mark.parametrize("rot", ["id", "r3"])
+def test_golden_fixtures(ctx, po, golden, golden_grid, grid, rot):
+    d = golden(f"fftri_{grid}_{rot}")
+    G, _ = golden_grid(grid)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    assert g.mode == (1 if grid == "g16" else 2)
+    assert g.ncol == G.ncol and g.nrow == G.nrow
+    f64 = hg.ff_triangles(ctx, g, d["shape_def"], d["rot"], precision="f64")
+    assert po.rel_err(f64, d["ff"]) < TOL64
+    f32 = hg.ff_triangles(ctx, g, d["shape_def"], d["rot"], precision="f32c")
+    assert po.rel_err(f32, d["ff"]) < TOL32
+
+
+@pytest.mark.parametrize("ntri", [1, 63, 64, 65, 200])
+@pytest.mark.parametrize("ppt", [1, 2, 4])
+def test_ragged_triangle_counts_and_launch_shapes(ctx, po, golden_grid, ntri, ppt):
+    rng = np.random.default_rng(ntri)
+    G, _ = golden_grid("g16")
+    sd = tri_cloud(rng, ntri)
+    R = po.rot_mul(po.rot_axis(2, 0.2), po.rot_axis(1, 0.1))
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext, R)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    f32 = hg.ff_triangles(ctx, g, sd, R, "f32c", pixels_per_thread=ppt)
+    assert po.rel_err(f32, ref) < TOL32
+    f64 = hg.ff_triangles(ctx, g, sd, R, "f64")
+    assert po.rel_err(f64, ref) < TOL64
+
+
+def test_points_mode_for_irregular_q(ctx, po):
+    rng = np.random.default_rng(7)
+    n = 777
+    qx, qy = rng.uniform(-2, 2, n), rng.uniform(-2, 2, n)
+    qz = rng.uniform(0, 3, 3 * n) + 1j * rng.uniform(0, 0.01, 3 * n)
+    sd = tri_cloud(rng, 130)
+    g = hg.QGrid.from_arrays(ctx, qx, qy, qz)
+    assert g.mode == 0
+    ref = po.ff_approx_triangle(sd, qx, qy, qz)
+    assert po.rel_err(hg.ff_triangles(ctx, g, sd, None, "f32c"), ref) < TOL32
+    assert po.rel_err(hg.ff_triangles(ctx, g, sd, None, "f64"), ref) < TOL64
+
+
+def test_born_single_block_rows(ctx, po, golden_grid):
+    G, _ = golden_grid("g16")
+    rng = np.random.default_rng(11)
+    sd = tri_cloud(rng, 99)
+    qz = G.qz + 0j
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, qz)
+    assert g.mode == 2 and g.nrow == G.nrow
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, qz)
+    assert po.rel_err(hg.ff_triangles(ctx, g, sd, None, "f32c"), ref) < TOL32
+
+
+def test_reference_shaped_call(ctx, po, golden_grid):
+    G, _ = golden_grid("g16abs")
+    sd = tri_cloud(np.random.default_rng(2), 70)
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext)
+    out = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f64")
+    assert po.rel_err(out, ref) < TOL64
+    out = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
+    assert po.rel_err(out, ref) < TOL32
+
+
+def test_device_qgrid_matches_oracle(ctx, po):
+    for dn2 in ((0.0, 0.0), (6e-6, 4e-8)):
+        G = po.Grid(40, 30, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0, dn2)
+        g = hg.QGrid.create(ctx, 40, 30, -2.0, 0.0, 2.0, 3.0, G.alpha_i, G.k0, dn2)
+        r = g.read()
+        for k in ("qx", "qy", "qz", "alpha"):
+            np.testing.assert_allclose(r[k], getattr(G, k), rtol=1e-13, atol=1e-13)
+        np.testing.assert_allclose(r["qz_ext"], G.qz_ext, rtol=1e-12, atol=1e-12)
+        assert g.mode == (1 if dn2 == (0.0, 0.0) else 2)
+
+
+def test_device_inputs_async(ctx, po, golden_grid):
+    torch = pytest.importorskip("torch")
+    G, _ = golden_grid("g16")
+    sd = tri_cloud(np.random.default_rng(4), 150)
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext)
+    dev = torch.device("cuda:0")
+    qx = torch.tensor(G.qx, device=dev)
+    qy = torch.tensor(G.qy, device=dev)
+    qz = torch.tensor(G.qz_ext, device=dev)
+    g = hg.QGrid.from_arrays(ctx, qx, qy, qz, ncol=G.ncol)
+    assert g.mode == 1
+    out = torch.zeros(4 * G.n, dtype=torch.complex64, device=dev)
+    hg.ff_triangles(ctx, g, torch.tensor(sd, device=dev), None, "f32c", out=out, out_type="c64")
+    ctx.synchronize()
+    assert po.rel_err(out.cpu().numpy(), ref) < TOL32
+
+
+def test_config0_icosphere_born(ctx, po):
+    """256 x 256 Born numeric FF of the 1280-triangle icosphere (R = 10 nm)."""
+    V, F = meshes.icosphere(10.0, 3)
+    sd = meshes.shape_def_from_mesh(V, F)
+    G = po.Grid(256, 256, -1.0, 0.0, 1.0, 2.0, 0.16, 10.0)
+    qz = G.qz + 0j
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, qz)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, qz)
+    f32 = hg.ff_triangles(ctx, g, sd, None, "f32c")
+    f64 = hg.ff_triangles(ctx, g, sd, None, "f64")
+    assert po.rel_err(f64, ref) < TOL64
+    assert po.rel_err(f32, ref) < TOL32
+    assert po.rel_err(np.abs(f32) ** 2, np.abs(ref) ** 2) < TOL32
+
+
+def test_config2_mesh_fp32_vs_fp64_and_oracle_sample(ctx, po):
+    """50,000-triangle star mesh, DWBA, full triangle count on a 256 x 256 detector of the
+    config-2 q-range; FP32C against the FP64 kernel everywhere and the oracle on a sample."""
+    V, F = meshes.star_mesh()
+    sd = meshes.shape_def_from_mesh(V, F)
+    assert len(sd) == 50000
+    G = po.Grid(256, 256, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    f32 = hg.ff_triangles(ctx, g, sd, None, "f32c")
+    f64 = hg.ff_triangles(ctx, g, sd, None, "f64")
+    assert po.rel_err(f32, f64) < TOL32
+    idx = np.random.default_rng(0).choice(G.n, 48, replace=False)
+    qz = G.qz_ext.reshape(4, -1)[:, idx].ravel()
+    ref = po.ff_approx_triangle(sd, G.qx[idx], G.qy[idx], qz)
+    got64 = f64.reshape(4, -1)[:, idx].ravel()
+    assert po.rel_err(got64, ref) < TOL64
+
+
+def test_linearity_in_triangles(ctx, po, golden_grid):
+    G, _ = golden_grid("g16")
+    sd = tri_cloud(np.random.default_rng(9), 300)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    full = hg.ff_triangles(ctx, g, sd, None, "f64")
+    parts = hg.ff_triangles(ctx, g, sd[:137], None, "f64") + hg.ff_triangles(ctx, g, sd[137:], None, "f64")
+    assert po.rel_err(parts, full) < 1e-13
+
+
+def test_errors_are_reported(ctx):
+    g = hg.QGrid.from_arrays(ctx, np.zeros(4), np.zeros(4), np.ones(4, complex))
+    with pytest.raises(hg.HgxError):
+        hg.ff_triangles(ctx, g, np.zeros((0, 8)), None, "f32c")
