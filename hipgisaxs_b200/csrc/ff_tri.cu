@@ -30,7 +30,7 @@
 
 namespace hgx {
 
-constexpr int TILE = 64;                    // triangles per shared-memory tile
+constexpr int TILE = 128;                   // triangles per shared-memory tile
 constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (cx,cy,nx,ny) + float2 B[TILE] (cz,nz)
 constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
 constexpr double TWO_PI = 6.283185307179586476925286766559;
@@ -138,13 +138,24 @@ __device__ __forceinline__ float4 complex_factor(double2 q, float cz, float nz) 
   return make_float4((float)zr, (float)zi, (float)(dr * zr - di * zi), (float)(dr * zi + di * zr));
 }
 
+// Rounds x to the nearest integer (ties to even) with two FP32 adds — valid for
+// |x| < 2^22 — so the reduction stays on the FMA pipe instead of the conversion unit.
+__device__ __forceinline__ float round_nearest(float x) {
+  const float magic = 12582912.0f;  // 1.5 * 2^23
+  return (x + magic) - magic;
+}
+
 template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
 __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
   constexpr int NF = PAIRED ? 2 : NK;        // float4 row factors per (row, triangle)
   constexpr int NACC = PAIRED ? 8 : 2 * NK;  // float accumulators per pixel
   __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
   __shared__ __align__(8) uint64_t s_bar[2];
-  extern __shared__ __align__(16) float4 s_rf[];  // rows_per_cta x TILE x NF
+  // dynamic: row factors (rows_per_cta x TILE x NF float4), then the compensation terms of
+  // the running sums (P x NACC x BLOCK floats, thread-minor so accesses are conflict-free)
+  extern __shared__ __align__(16) float4 s_dyn[];
+  float4* s_rf = s_dyn;
+  float* s_cmp = reinterpret_cast<float*>(s_dyn + (size_t)a.rows_per_cta * TILE * NF);
 
   const int R = a.rows_per_cta;
   const int tpr = BLOCK / R;
@@ -154,7 +165,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
   const int colbase = blockIdx.x * (tpr * P) + lane;
 
   float qxf[P], qyf[P];
-  float acc[P][NACC], sum[P][NACC], cmp[P][NACC];
+  float acc[P][NACC], sum[P][NACC];
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     int col = colbase + i * tpr;
@@ -163,7 +174,10 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
     qxf[i] = v ? (float)a.qx[p] : 0.f;
     qyf[i] = v ? (float)a.qy[p] : 0.f;
 #pragma unroll
-    for (int n = 0; n < NACC; ++n) acc[i][n] = sum[i][n] = cmp[i][n] = 0.f;
+    for (int n = 0; n < NACC; ++n) {
+      acc[i][n] = sum[i][n] = 0.f;
+      s_cmp[(i * NACC + n) * BLOCK + threadIdx.x] = 0.f;
+    }
   }
 
   if (threadIdx.x == 0) {
@@ -185,25 +199,22 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
     const float4* A = reinterpret_cast<const float4*>(s_tile[b]);
     const float2* B = reinterpret_cast<const float2*>(s_tile[b] + 4 * TILE);
     if (ok) {
-      for (int it = threadIdx.x; it < R * TILE; it += BLOCK) {
-        int r = it / TILE, j = it - r * TILE;
-        int grow = blockIdx.y * R + r;
-        float2 bz = B[j];
-        float4* dst = s_rf + (size_t)(r * TILE + j) * NF;
+      // one float4 row factor per item: (row, triangle, pair or block)
+      for (int it = threadIdx.x; it < R * TILE * NF; it += BLOCK) {
+        const int f = it % NF;
+        const int rj = it / NF;
+        const int r = rj / TILE, j = rj - r * TILE;
+        const int grow = blockIdx.y * R + r;
+        const float2 bz = B[j];
+        float4 v;
         if (PAIRED) {
-          float4 f0 = make_float4(1.f, 0.f, 0.f, 0.f), f2 = f0;
-          if (grow < a.nrow) {
-            f0 = paired_factor(a.rowqz[(long)grow * 4 + 0].x, bz.x, bz.y);
-            f2 = paired_factor(a.rowqz[(long)grow * 4 + 2].x, bz.x, bz.y);
-          }
-          dst[0] = f0;
-          dst[1] = f2;
+          v = grow < a.nrow ? paired_factor(a.rowqz[(long)grow * 4 + 2 * f].x, bz.x, bz.y)
+                            : make_float4(1.f, 0.f, 0.f, 0.f);
         } else {
-#pragma unroll
-          for (int k = 0; k < NK; ++k)
-            dst[k] = grow < a.nrow ? complex_factor(a.rowqz[(long)grow * NK + k], bz.x, bz.y)
-                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+          v = grow < a.nrow ? complex_factor(a.rowqz[(long)grow * NK + f], bz.x, bz.y)
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        s_rf[it] = v;  // == ((r * TILE + j) * NF + f)
       }
     }
     if (__syncthreads_or(!ok)) {
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
 #pragma unroll
       for (int i = 0; i < P; ++i) {
         float tp = fmaf(qxf[i], t.x, qyf[i] * t.y);  // in-plane phase, turns
-        float rr = tp - rintf(tp);                   // exact reduction to [-1/2, 1/2]
+        float rr = tp - round_nearest(tp);           // exact reduction to [-1/2, 1/2]
         float sn, cs;
         __sincosf(rr * 6.28318530717958648f, &sn, &cs);
         float aq = fmaf(qxf[i], t.z, qyf[i] * t.w);  // in-plane part of q.n~
@@ -264,10 +275,16 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
         }
       }
     }
+    // fold the tile's partial sums into the running sums (TwoSum; error terms in smem)
 #pragma unroll
     for (int i = 0; i < P; ++i)
 #pragma unroll
-      for (int n = 0; n < NACC; ++n) two_sum_fold(sum[i][n], acc[i][n], cmp[i][n]);
+      for (int n = 0; n < NACC; ++n) {
+        float* cp = s_cmp + (i * NACC + n) * BLOCK + threadIdx.x;
+        float c = *cp;
+        two_sum_fold(sum[i][n], acc[i][n], c);
+        *cp = c;
+      }
     __syncthreads();  // every thread is done with tile buffer b and the row factors
     if (threadIdx.x == 0 && s + 2 < a.ntiles) {
       fence_proxy_async_smem();
@@ -286,7 +303,8 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
     double qx = a.qx[p], qy = a.qy[p];
     double T[NACC];
 #pragma unroll
-    for (int n = 0; n < NACC; ++n) T[n] = (double)sum[i][n] + (double)cmp[i][n];
+    for (int n = 0; n < NACC; ++n)
+      T[n] = (double)sum[i][n] + (double)s_cmp[(i * NACC + n) * BLOCK + threadIdx.x];
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
       double sr, si;
@@ -477,7 +495,12 @@ static Rot9 make_rot(const double* r9) {
 template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
 static int launch_rows(const RowArgs& a, dim3 grid, cudaStream_t st) {
   constexpr int NF = PAIRED ? 2 : NK;
-  size_t smem = (size_t)a.rows_per_cta * TILE * NF * sizeof(float4);
+  constexpr int NACC = PAIRED ? 8 : 2 * NK;
+  size_t smem = (size_t)a.rows_per_cta * TILE * NF * sizeof(float4) +
+                (size_t)P * NACC * BLOCK * sizeof(float);
+  if (smem > 48 * 1024)  // opt in to more than 48 KB of dynamic shared memory
+    HGX_CUDA(cudaFuncSetAttribute(ff_tri_rows_kernel<BLOCK, P, NK, PAIRED, OUT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   ff_tri_rows_kernel<BLOCK, P, NK, PAIRED, OUT><<<grid, BLOCK, smem, st>>>(a);
   HGX_CUDA(cudaGetLastError());
   return HGX_OK;
@@ -541,7 +564,7 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
     HGX_CUDA(cudaGetLastError());
     return HGX_OK;
   }
-  RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, want_p > 0 ? want_p : 2);
+  RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, want_p > 0 ? want_p : 4);
   if (sh.grid.y > 65535u)
     return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: too many detector rows for one launch");
   RowArgs a{tiles, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R, out,
