@@ -38,6 +38,7 @@ SIGNATURES = {
     "hgx_ff_triangles_q": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i]),
     "hgx_ff_triangles_q_ex": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i]),
     "hgx_ff_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }
 

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "hgx_internal.cuh"
 #include "ptx.cuh"
@@ -642,3 +643,88 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------ allocation-free entry ----
+// hgx_ff_triangles_noalloc: the FP32C per-q-point form factor for callers that must not
+// allocate device memory — code running while a CUDA graph is being captured, code that
+// runs inside another framework's memory pool or under a fixed memory budget, and
+// real-time loops where cudaMalloc/cudaFree would synchronise the device.  Its scratch (the
+// FP32 triangle tiles and an error word) is a file-scope static device array of fixed size,
+// reserved when the library's device code is loaded on a GPU and held until exit.
+//
+// In host code the array name below is only a host-side stand-in, not a device address:
+// the device address is obtained once per device with cudaGetSymbolAddress (set-up done by
+// the first call on each device, with that device current) and passed to the kernels.
+// Every call shares the array: the triangle tiles are fully rewritten by each call and the
+// error word is cleared at its start; calls that overlap on the GPU (different streams,
+// no ordering) race on the array and must be ordered by the caller.
+constexpr int NOALLOC_MAX_TRIANGLES = 65536;
+constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 512 tiles, 1.5 MiB
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) float g_noalloc_tiles[NOALLOC_MAX_TILES * TILE_FLOATS];
+static __device__ __align__(256) unsigned g_noalloc_err;
+
+namespace {
+struct NoallocSlot {
+  float* tiles = nullptr;
+  unsigned* err = nullptr;
+};
+NoallocSlot g_noalloc_slots[NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mutex;
+
+int noalloc_setup(int dev, NoallocSlot* out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoallocSlot& s = g_noalloc_slots[dev];
+  if (!s.tiles) {
+    void* t = nullptr;
+    void* e = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&t, g_noalloc_tiles);
+    if (rc != cudaSuccess) return cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_tiles)");
+    rc = cudaGetSymbolAddress(&e, g_noalloc_err);
+    if (rc != cudaSuccess) return cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_err)");
+    s.tiles = static_cast<float*>(t);
+    s.err = static_cast<unsigned*>(e);
+  }
+  *out = s;
+  return HGX_OK;
+}
+}  // namespace
+
+extern "C" int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int nqy,
+                                        const double* qx, const double* qy, int nqz,
+                                        const double* qz, const double* rot9, void* ff,
+                                        int ff_type, void* stream) {
+  if (!shape_def || !qx || !qy || !qz || !ff)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc: null argument");
+  if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc: no triangles");
+  if (ntri > NOALLOC_MAX_TRIANGLES)
+    return fail(HGX_ERR_INVALID_ARG,
+                "hgx_ff_triangles_noalloc: more than 65536 triangles (the fixed scratch limit); "
+                "use hgx_ff_triangles_q");
+  if (nqy < 1 || nqz < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc: empty q-grid");
+  if (ff_type != HGX_C128 && ff_type != HGX_C64)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc: unknown output type");
+  int dev = 0;
+  HGX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc: device index too large");
+  NoallocSlot slot;
+  HGX_TRY(noalloc_setup(dev, &slot));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  Rot9 R = make_rot(rot9);
+  const int ntiles = (ntri + TILE - 1) / TILE;
+  HGX_CUDA(cudaMemsetAsync(slot.err, 0, sizeof(unsigned), st));
+  {
+    int n = ntiles * TILE;
+    tri_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(shape_def, ntri, ntiles, R, slot.tiles);
+    HGX_CUDA(cudaGetLastError());
+  }
+  PointArgs a{slot.tiles, ntiles, qx, qy, reinterpret_cast<const double2*>(qz), nqy, nqz, R, ff,
+              slot.err};
+  dim3 grid((nqz + 127) / 128);
+  if (ff_type == HGX_C64) ff_tri_points_kernel<128, float2><<<grid, 128, 0, st>>>(a);
+  else ff_tri_points_kernel<128, double2><<<grid, 128, 0, st>>>(a);
+  HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}

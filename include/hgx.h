@@ -102,6 +102,22 @@ int hgx_ff_triangles(hgx_ctx ctx, const double* shape_def, int ntri, int nqy, co
                      const double* qy, int nqz, const double* qz, const double* rot9,
                      int precision, double* ff);
 
+/* The FP32C numeric form factor for callers that cannot allocate device memory: code
+ * running inside CUDA graph capture, inside another framework's memory pool or under a
+ * fixed memory budget, where a cudaMalloc would fail, break the capture or synchronise the
+ * device.  No counterpart in the reference.  Allocates nothing: its scratch is a fixed
+ * static device array (1.5 MiB per GPU, held until exit), so ntri <= 65536 (larger
+ * requests return HGX_ERR_INVALID_ARG).  All array arguments are device memory (same
+ * layouts as hgx_ff_triangles; q-point i uses qx/qy[i % nqy]); rot9 is 9 host doubles or
+ * NULL for the identity; ff is nqz complex of type ff_type.  Asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  The first call on each device looks up
+ * the scratch address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Calls share the scratch: calls that can overlap on the
+ * GPU (unordered streams) race and must be ordered by the caller. */
+int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int nqy, const double* qx,
+                             const double* qy, int nqz, const double* qz, const double* rot9,
+                             void* ff, int ff_type, void* stream);
+
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA
  * throughput (TFLOP/s, an FMA counted as 2 FLOP) and SFU __sinf throughput (Gop/s),
