@@ -38,6 +38,17 @@ SIGNATURES = {
     "hgx_ff_triangles_q": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i]),
     "hgx_ff_triangles_q_ex": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i]),
     "hgx_ff_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "hgx_param_distribution": (_i, [_i, _d, _d, _d, _d, _i, _vp, _vp, _i, C.POINTER(_i)]),
+    "hgx_ff_analytic": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp,
+                             _vp, _d, _d, _vp, _vp, _vp, _i]),
+    "hgx_ff_analytic_params": (_i, [_vp, _vp, _i, _i, _vp, _d, _d, _vp, _vp, _vp, _i]),
+    "hgx_lattice_vectors": (_i, [_i, C.c_char_p, _vp, _vp]),
+    "hgx_sf_lattice": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "hgx_propagation_coeffs": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _i]),
+    "hgx_dwba_combine": (_i, [_vp, C.c_long, _vp, _vp, _vp, _i, _d, _vp]),
+    "hgx_abs_diff_square": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
+    "hgx_residual_vector": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
+    "hgx_chi2": (_i, [_vp, C.c_long, _vp, _vp, _vp, _d, _vp]),
     "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }

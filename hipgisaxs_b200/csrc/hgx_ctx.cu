@@ -81,15 +81,46 @@ __global__ void row_table_kernel(const double2* __restrict__ qz, int nqy, int nk
   if (!paired) atomicOr(flags, 2u);
 }
 
+int stage_in(hgx_ctx c, const void* p, size_t bytes, DevBuf& buf, const void** dev) {
+  if (!p) {
+    *dev = nullptr;
+    return HGX_OK;
+  }
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return HGX_OK;
+  }
+  HGX_TRY(buf.reserve(bytes));
+  HGX_CUDA(cudaMemcpyAsync(buf.p, p, bytes, cudaMemcpyHostToDevice, c->stream));
+  *dev = buf.p;
+  return HGX_OK;
+}
+
+int stage_out(hgx_ctx c, void* p, size_t bytes, DevBuf& buf, void** dev) {
+  (void)c;
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return HGX_OK;
+  }
+  HGX_TRY(buf.reserve(bytes));
+  *dev = buf.p;
+  return HGX_OK;
+}
+
+int finish_out(hgx_ctx c, void* p, size_t bytes, const void* dev) {
+  if (p == dev) return HGX_OK;
+  HGX_CUDA(cudaMemcpyAsync(p, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+  return hgx_synchronize(c);
+}
+
 int qgrid_finalize(hgx_qgrid g) {
   g->mode = 0;
   if (g->nk != 1 && g->nk != 4) return HGX_OK;
   if (g->ncol <= 0 || g->nqy % g->ncol != 0) return HGX_OK;
   g->nrow = g->nqy / g->ncol;
   HGX_CUDA(cudaMalloc(&g->rowqz, sizeof(double2) * (size_t)g->nrow * g->nk));
-  unsigned* d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
   HGX_TRY(g->ctx->scratch.reserve(256));
-  d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
+  unsigned* d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
   cudaStream_t st = g->ctx->stream;
   HGX_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(unsigned), st));
   int threads = 256;

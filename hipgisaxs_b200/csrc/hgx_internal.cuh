@@ -77,3 +77,13 @@ namespace hgx {
 // Prepares triangle tiles for the FP32 kernels (see ff_tri.cu).
 int qgrid_finalize(hgx_qgrid g);  // builds the row table and picks the mode
 }  // namespace hgx
+
+namespace hgx {
+// Device view of a caller array: the array itself when it is device memory, else a copy in
+// `buf` (host -> device on the context's stream).
+int stage_in(hgx_ctx c, const void* p, size_t bytes, DevBuf& buf, const void** dev);
+// Device buffer for an output: the array itself when device memory, else `buf`; after the
+// kernels, finish_out copies back and synchronises when the output is host memory.
+int stage_out(hgx_ctx c, void* p, size_t bytes, DevBuf& buf, void** dev);
+int finish_out(hgx_ctx c, void* p, size_t bytes, const void* dev);
+}  // namespace hgx

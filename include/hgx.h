@@ -102,6 +102,75 @@ int hgx_ff_triangles(hgx_ctx ctx, const double* shape_def, int ntri, int nqy, co
                      const double* qy, int nqz, const double* qz, const double* rot9,
                      int precision, double* ff);
 
+/* ------------------------------------------------------- analytic form factors ---- */
+/* AnalyticFormFactor::param_distribution (src/ff/ff_ana.cpp:235-284): the sample values
+ * and weights of one shape parameter.  stat: StatisticType (0 null, 2 none, 4 gaussian,
+ * 8 uniform; include/common/enums.hpp:74-84).  Host-only, no GPU needed. */
+int hgx_param_distribution(int stat, double pmin, double pmax, double mean, double dev,
+                           int nvalues, double* values, double* weights, int cap, int* count);
+/* The analytic form factor of one shape on the grid, FP64 — replaces the
+ * AnalyticFormFactorG::compute_* family (include/ff/gpu/ff_ana_gpu.cuh:28-96) and the CPU
+ * AnalyticFormFactor::compute_* functions (src/ff/ff_ana_*.cpp).  shape: ShapeName
+ * (include/common/enums.hpp:24-43) among box 2, cube 3, cylinder 4, sphere 5, prism3 8,
+ * prism6 9, pyramid 14.  Up to four sampled dimensions (n_i values v_i with weights w_i,
+ * at most 64 each; w_i NULL = 1):
+ *   box: x, y, height; cube: edge; cylinder: radius, -, height (unweighted, as the
+ *   reference sums them); sphere: radius; prism3/prism6: edge, -, height (unweighted);
+ *   pyramid: x, y, height, base angle (degrees).
+ * tau, eta: the prism tilt angles; transvec: translation (3); rot9: rotation or NULL. */
+int hgx_ff_analytic(hgx_ctx ctx, hgx_qgrid g, int shape, int n1, const double* v1,
+                    const double* w1, int n2, const double* v2, const double* w2, int n3,
+                    const double* v3, const double* w3, int n4, const double* v4,
+                    const double* w4, double tau, double eta, const double* transvec,
+                    const double* rot9, void* ff, int ff_type);
+/* AnalyticFormFactor::compute (src/ff/ff_ana.cpp:61-161) from HiG-style shape parameters:
+ * 7 doubles per parameter (ShapeParamType, StatisticType, min, max, mean, deviation,
+ * nvalues), routed to dimensions and sampled as the reference's compute_* functions do. */
+int hgx_ff_analytic_params(hgx_ctx ctx, hgx_qgrid g, int shape, int nparam,
+                           const double* params, double tau, double eta,
+                           const double* transvec, const double* rot9, void* ff, int ff_type);
+
+/* ---------------------------------------------------------- structure factor ---- */
+/* Lattice::construct_vectors (src/model/structure.cpp:86-182): unscaled a, b, c (9) and
+ * basis offset t (3, may be NULL).  type: LatticeType (bcc 2, cubic 3, fcc 4, fco 5, hcp 6,
+ * hex 7); hkl "100", "110" or "111" where the reference defines it. */
+int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3);
+/* StructureFactor::compute_structure_factor, lattice branch (src/sf/sf.cpp:85-285):
+ * abc9 lattice vectors, repet (3) repetitions, scaling (3), center (3), rot9.  FP64. */
+int hgx_sf_lattice(hgx_ctx ctx, hgx_qgrid g, const double* abc9, const double* repet,
+                   const double* scaling, const double* center, const double* rot9, void* sf,
+                   int sf_type);
+
+/* ---------------------------------------------------------------- DWBA terms ---- */
+/* MultiLayer::init + propagation_coeffs (src/model/multilayer.cpp:29-58,110-155), FP64:
+ * user layers (delta, beta, thickness, order; order -1 = substrate; host arrays), the
+ * particle layer's order, the grid's exit angles (alpha: nrow values, or NULL for a grid
+ * made by hgx_qgrid_create).  fc: 4N complex128 in the reference's layout, or with
+ * per_row != 0 the nrow x 4 per-row coefficients. */
+int hgx_propagation_coeffs(hgx_ctx ctx, hgx_qgrid g, int nlayers, const double* delta,
+                           const double* beta, const double* thickness, const int* order,
+                           double k0, double alpha_i, int particle_order, const double* alpha,
+                           double* fc, int per_row);
+/* The DWBA combination (src/sim/hipgisaxs_main.cpp:1086-1100):
+ * intensity[i] += |weight * sum_k fc[k n + i] sf[k n + i] ff[k n + i]|^2 over 4 blocks of n;
+ * sf may be NULL (1).  With fc NULL the SAXS branch (:1102-1105): intensity[i] =
+ * |weight sf[i] ff[i]|^2.  fc, sf complex128; ff of type ff_type. */
+int hgx_dwba_combine(hgx_ctx ctx, long n, const double* fc, const double* sf, const void* ff,
+                     int ff_type, double weight, double* intensity);
+
+/* ------------------------------------------------------------------ distances ---- */
+/* AbsoluteDifferenceSquare (include/analyzer/distance_functions.hpp:125-143):
+ * sum (mask |ref - data|)^2, deterministic FP64 reduction. */
+int hgx_abs_diff_square(hgx_ctx ctx, long n, const double* ref, const double* data,
+                        const unsigned* mask, double* out);
+/* ResidualVector (include/analyzer/distance_functions.hpp:89-103): mask (ref - data). */
+int hgx_residual_vector(hgx_ctx ctx, long n, const double* ref, const double* data,
+                        const unsigned* mask, double* out);
+/* Poisson-weighted chi^2 of the fitting front end: sum mask (scale model - counts)^2 /
+ * max(counts, 1) (mask may be NULL); deterministic FP64 reduction. */
+int hgx_chi2(hgx_ctx ctx, long n, const double* model, const double* counts,
+             const unsigned* mask, double scale, double* out);
+
 /* The FP32C numeric form factor for callers that cannot allocate device memory: code
  * running inside CUDA graph capture, inside another framework's memory pool or under a
  * fixed memory budget, where a cudaMalloc would fail, break the capture or synchronise the
