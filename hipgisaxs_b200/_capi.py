@@ -49,6 +49,12 @@ SIGNATURES = {
     "hgx_abs_diff_square": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_residual_vector": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_chi2": (_i, [_vp, C.c_long, _vp, _vp, _vp, _d, _vp]),
+    "hgx_cyl_batch_create": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _d, _i, C.POINTER(_vp)]),
+    "hgx_cyl_batch_eval": (_i, [_vp, _vp, _vp]),
+    "hgx_cyl_batch_forward": (_i, [_vp, _vp, _vp]),
+    "hgx_cyl_plain_forward": (_i, [_vp, _i, _vp, _vp]),
+    "hgx_cyl_batch_info": (_i, [_vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]),
+    "hgx_cyl_batch_destroy": (_i, [_vp]),
     "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }

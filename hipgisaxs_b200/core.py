@@ -7,6 +7,7 @@ whose inputs and outputs are all CUDA tensors run asynchronously on the context'
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -45,8 +46,12 @@ class Context:
         check(lib().hgx_create(int(device), C.byref(h)))
         self._h = h
         self.device = device
+        self._children = []  # weak references to grids and batches made on this context
         if stream is not None:
             self.set_stream(stream)
+
+    def _register(self, obj):
+        self._children.append(weakref.ref(obj))
 
     @property
     def handle(self):
@@ -61,7 +66,13 @@ class Context:
         check(lib().hgx_synchronize(self._h))
 
     def close(self):
+        """Closes the objects made on this context (newest first), then the context."""
         if getattr(self, "_h", None):
+            for ref in reversed(self._children):
+                obj = ref()
+                if obj is not None:
+                    obj.close()
+            self._children = []
             lib().hgx_destroy(self._h)
             self._h = None
 
@@ -78,6 +89,7 @@ class QGrid:
     def __init__(self, ctx: Context, handle):
         self.ctx = ctx
         self._h = handle
+        ctx._register(self)
         a = [C.c_int() for _ in range(5)]
         check(lib().hgx_qgrid_info(self._h, *[C.byref(x) for x in a]))
         self.nqy, self.nqz, self.nrow, self.ncol, self.mode = (x.value for x in a)

@@ -1,0 +1,93 @@
+"""Python mirror of the fitting entry points: the fused cylinder-lattice model with its
+chi^2 and adjoint gradient, batched over candidates (hgx_cyl_batch_*), plus the
+finite-difference gradient of the plain FP64 form (the reference fitter's method)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._capi import F32C, F64, check, lib
+from .core import Context, QGrid
+
+MODEL_LEN = 16
+THETA = ("radius", "height", "lattice_a", "phi")
+
+
+def model_block(radius, height, lattice_a, phi=0.0, spread=0.0, nsamples=1, repet=(20, 20, 1),
+                dn2=(0.0, 0.0), center=(0.0, 0.0, 0.0), weight=1.0, smooth_sampling=False):
+    """The 16-double model block of hgx_cyl_batch_* (see include/hgx.h)."""
+    m = np.zeros(MODEL_LEN)
+    m[15] = 1.0 if smooth_sampling else 0.0
+    m[0], m[1], m[2], m[3] = radius, height, lattice_a, phi
+    m[4], m[5] = spread, nsamples
+    m[6:9] = repet
+    m[9:11] = dn2
+    m[11:14] = center
+    m[14] = weight
+    return m
+
+
+class CylinderBatch:
+    """hgx_cyl_batch: candidates with ROIs on one device grid."""
+
+    def __init__(self, ctx: Context, grid: QGrid, rowfc, abc, rois, counts=None, mask=None,
+                 scale=1.0, precision="f32c"):
+        self.ctx, self.grid = ctx, grid
+        rf = np.ascontiguousarray(rowfc, dtype=np.complex128)
+        abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
+        r = np.ascontiguousarray(np.asarray(rois, dtype=np.int32).reshape(-1, 4))
+        self.rois = r
+        self.ncand = len(r)
+        cnt = None if counts is None else np.ascontiguousarray(counts, dtype=np.float64)
+        mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib().hgx_cyl_batch_create(ctx.handle, grid.handle, rf.ctypes.data, abc9.ctypes.data,
+                                         self.ncand, r.ctypes.data,
+                                         None if cnt is None else cnt.ctypes.data,
+                                         None if mk is None else mk.ctypes.data, float(scale),
+                                         F64 if precision == "f64" else F32C, C.byref(h)))
+        self._h = h
+        ctx._register(self)
+        n1, n2 = C.c_long(), C.c_long()
+        check(lib().hgx_cyl_batch_info(h, C.byref(n1), C.byref(n2)))
+        self.npx, self.nitems = n1.value, n2.value
+        self.offsets = np.concatenate([[0], np.cumsum(r[:, 2].astype(np.int64) * r[:, 3])])
+
+    def _models(self, models):
+        m = np.ascontiguousarray(np.asarray(models, dtype=np.float64).reshape(-1, MODEL_LEN))
+        if len(m) != self.ncand:
+            raise ValueError("one model block per candidate")
+        return m
+
+    def eval(self, models):
+        """(chi2[ncand], grad[ncand, 4]) for theta = (R, H, a, phi)."""
+        m = self._models(models)
+        out = np.zeros((self.ncand, 5))
+        check(lib().hgx_cyl_batch_eval(self._h, m.ctypes.data, out.ctypes.data))
+        return out[:, 0].copy(), out[:, 1:].copy()
+
+    def forward(self, models):
+        m = self._models(models)
+        out = np.zeros(self.npx)
+        check(lib().hgx_cyl_batch_forward(self._h, m.ctypes.data, out.ctypes.data))
+        return [out[self.offsets[i]:self.offsets[i + 1]].reshape(self.rois[i, 2], self.rois[i, 3])
+                for i in range(self.ncand)]
+
+    def plain_forward(self, cand, model):
+        m = np.ascontiguousarray(model, dtype=np.float64)
+        n = int(self.rois[cand, 2]) * int(self.rois[cand, 3])
+        out = np.zeros(n)
+        check(lib().hgx_cyl_plain_forward(self._h, int(cand), m.ctypes.data, out.ctypes.data))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hgx_cyl_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

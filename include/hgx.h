@@ -46,7 +46,9 @@ const char* hgx_last_error(void);
 const char* hgx_status_string(int status);
 int hgx_version(void);
 
-/* One context per (thread, device).  `device` < 0 uses the current device. */
+/* One context per (thread, device).  `device` < 0 uses the current device.  Objects made on
+ * a context (q-grids, batches) must be destroyed before the context; a batch must be
+ * destroyed before its q-grid. */
 int hgx_create(int device, hgx_ctx* out);
 int hgx_destroy(hgx_ctx ctx);
 /* Stream for asynchronous work (a cudaStream_t; NULL = the legacy default stream). */
@@ -170,6 +172,48 @@ int hgx_residual_vector(hgx_ctx ctx, long n, const double* ref, const double* da
  * max(counts, 1) (mask may be NULL); deterministic FP64 reduction. */
 int hgx_chi2(hgx_ctx ctx, long n, const double* model, const double* counts,
              const unsigned* mask, double scale, double* out);
+
+/* -------------------------------------------- fitting: chi^2 and its gradient ---- */
+/* A fused model for the fitting front end: cylinders on a 2-D lattice in DWBA (one grain,
+ * as HipGISAXS::run_gisaxs computes it, src/sim/hipgisaxs_main.cpp:694-1100), its Poisson
+ * chi^2 (hgx_chi2) and the gradient of chi^2 with respect to theta = (R, H, a, phi) by a
+ * hand-written adjoint — in place of the central finite differences of the reference's
+ * LMVM fitter (src/analyzer/hipgisaxs_fit_lmvm.cpp:190-223) and of PSO's one-particle-at-a-
+ * time loop (src/analyzer/hipgisaxs_fit_pso.cpp:521-545): many candidates, each with its own
+ * detector region of interest, evaluated in one CUDA-graph launch.
+ *
+ * Model block: 16 doubles per candidate
+ *   [0] cylinder radius R   [1] height H   [2] lattice constant a (scales a, b, c)
+ *   [3] in-plane rotation phi (radians)    [4] relative Gaussian size spread (0 = one size)
+ *   [5] samples over +-3 spread (param_distribution stepping, summed unweighted)
+ *   [6..8] lattice repetitions   [9..10] particle contrast dn2 (complex)
+ *   [11..13] grain centre   [14] weight
+ *   [15] sampling: 0 = the reference's param_distribution stepping (which can gain or lose
+ *        the last sample as R or H moves — a jump in chi^2), 1 = exactly [5] evenly spaced
+ *        samples (smooth in R and H, for gradient-based fitting).
+ * The grid must be a DWBA grid with real qz constant along rows (a vacuum particle layer);
+ * rowfc: the per-row Fresnel coefficients (hgx_propagation_coeffs with per_row = 1);
+ * abc9: unscaled lattice vectors with a, b in the plane and c along z (hex, cubic).
+ * rois: 4 ints per candidate (row0, col0, nrows, ncols); counts: the candidates' ROI images
+ * concatenated (row-major), or NULL for forward-only batches; mask: same layout or NULL;
+ * scale: the model-to-counts factor of the chi^2.  precision: HGX_F32C (FP32 Bessel sums,
+ * FP64 lattice phases and reductions) or HGX_F64. */
+typedef struct hgx_cyl_batch_s* hgx_cyl_batch;
+int hgx_cyl_batch_create(hgx_ctx ctx, hgx_qgrid g, const double* rowfc, const double* abc9,
+                         int ncand, const int* rois, const double* counts,
+                         const unsigned* mask, double scale, int precision,
+                         hgx_cyl_batch* out);
+/* chi^2 and gradient of every candidate: out = 5 doubles per candidate (chi2, dR, dH, da,
+ * dphi).  The first call records the work into a CUDA graph; later calls replay it. */
+int hgx_cyl_batch_eval(hgx_cyl_batch b, const double* models, double* out);
+/* Model intensities of every candidate (the ROI images concatenated). */
+int hgx_cyl_batch_forward(hgx_cyl_batch b, const double* models, double* intensity);
+/* The plain FP64 form of candidate `cand`'s intensity: one thread per pixel with the
+ * reference's loop structure (per DWBA block, the (radius, height) double loop and the
+ * complex-power lattice factor).  Baseline for the finite-difference gradient. */
+int hgx_cyl_plain_forward(hgx_cyl_batch b, int cand, const double* model, double* intensity);
+int hgx_cyl_batch_info(hgx_cyl_batch b, long* npx, long* nitems);
+int hgx_cyl_batch_destroy(hgx_cyl_batch b);
 
 /* The FP32C numeric form factor for callers that cannot allocate device memory: code
  * running inside CUDA graph capture, inside another framework's memory pool or under a
