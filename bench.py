@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
+    ap.add_argument("--no-fitting", action="store_true")
     return ap.parse_args()
 
 
@@ -141,6 +142,145 @@ def cpu_sample_rate(sd, qx, qy, qz_ext, budget_s=12.0, backend=None):
     desc = (f"{nrows} full detector rows x 4 DWBA blocks x {len(sd)} triangles "
             f"({ev:.3e} evals, {dt:.1f} s); cost is linear in q-points")
     return ev / dt, threads, kind, desc
+
+
+def fitting_bench(ctx, torch, dev, stream, steps=5):
+    """Configs 3 and 4: chi^2 + gradient of the cylinder-lattice model (R 5, H 10 nm, 5% size
+    spread over 11 samples, hex lattice a = 20 nm, 20 x 20 repetitions, Si-like substrate,
+    10 keV, alpha_i 0.20 deg, 1024 x 1024 detector) against a Poisson target (peak 1e4 counts)
+    simulated at R*1.03, H*0.96, a*1.02, phi + 5 deg.  The fused FP32C forward + adjoint is
+    timed against the plain FP64 form with the reference fitter's central differences
+    (1 + 2*4 forward runs + chi^2 each)."""
+    import hipgisaxs_b200 as hg
+    from hipgisaxs_b200 import fitting, model
+    n = 1024
+    alpha_i = ALPHA_I_DEG * PI_REF / 180
+    k0 = k0_from_kev(ENERGY_KEV)
+    g = hg.QGrid.create(ctx, n, n, QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z, alpha_i, k0)
+    rowfc = model.propagation_coeffs(ctx, g, [(4.88e-6, 7.37e-8, 0.0, -1)], k0, alpha_i, 0,
+                                     per_row=True)
+    abc, _ = model.lattice_vectors("hex")
+    dn2 = (-2 * 4.88e-6, -2 * 7.37e-8)
+
+    def mb(R, H, a, phi):
+        # 11 evenly spaced size samples (smooth in R and H; see include/hgx.h model slot 15)
+        return fitting.model_block(R, H, a, phi, 0.05, 11, (20, 20, 1), dn2, (0, 0, 0), 1.0,
+                                   smooth_sampling=True)
+
+    p0 = mb(5.0, 10.0, 20.0, 0.0)
+    truth = mb(5.0 * 1.03, 10.0 * 0.96, 20.0 * 1.02, np.deg2rad(5.0))
+    full = [0, 0, n, n]
+    fwd = fitting.CylinderBatch(ctx, g, rowfc, abc, [full], precision="f64")
+    target = fwd.forward([truth])[0].ravel()
+    rng = np.random.default_rng(20240601)
+    scale = 1e4 / target.max()
+    counts = rng.poisson(scale * target).astype(np.float64)
+    fwd.close()
+
+    out = {}
+    # ---- config 3: one candidate, full detector
+    b32 = fitting.CylinderBatch(ctx, g, rowfc, abc, [full], counts, None, scale, "f32c")
+    b64 = fitting.CylinderBatch(ctx, g, rowfc, abc, [full], counts, None, scale, "f64")
+    c32, g32 = b32.eval([p0])
+    c64, g64 = b64.eval([p0])
+    for _ in range(3):
+        b32.eval([p0])
+    t = time.perf_counter()
+    for _ in range(steps):
+        b32.eval([p0])
+    dt32 = (time.perf_counter() - t) / steps
+    # plain FP64 form, central differences: 9 forwards + chi^2 on the device
+    d_counts = torch.tensor(counts, device=dev)
+    d_I = torch.empty(n * n, dtype=torch.float64, device=dev)
+
+    def chi2_plain(m):
+        hg._capi.check(hg.lib().hgx_cyl_plain_forward(b64._h, 0, np.ascontiguousarray(m).ctypes.data,
+                                                      d_I.data_ptr()))
+        return model.chi2(ctx, d_I, d_counts, None, scale)
+
+    def fd_grad(m):
+        c = chi2_plain(m)
+        gr = np.zeros(4)
+        for j in range(4):
+            h = 1e-4 * (abs(m[j]) if j < 3 else 1.0)
+            mp, mm = m.copy(), m.copy()
+            mp[j] += h
+            mm[j] -= h
+            gr[j] = (chi2_plain(mp) - chi2_plain(mm)) / (2 * h)
+        return c, gr
+
+    fd_grad(p0)
+    t = time.perf_counter()
+    cfd, gfd = fd_grad(p0)
+    dtfd = time.perf_counter() - t
+    out["chi2_grad_1024sq"] = {
+        "metric": "chi2+grad evals/s", "value": 1.0 / dt32, "ms_per_eval": 1e3 * dt32,
+        "plain_fp64_fd": {"value": 1.0 / dtfd, "ms_per_eval": 1e3 * dtfd,
+                          "method": "plain FP64 forward x 9 (central differences, h 1e-4 rel)"},
+        "speedup_vs_plain_fp64": dtfd / dt32,
+        "rel_err_chi2_vs_fp64": abs(c32[0] - c64[0]) / abs(c64[0]),
+        "rel_err_grad_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+        "fd_vs_adjoint_rel": float(np.linalg.norm(gfd - g64[0]) / np.linalg.norm(g64[0])),
+        "pixels": n * n, "params": 4}
+    b32.close()
+    b64.close()
+
+    # ---- config 4: 256 candidates with uneven ROIs in one graph-captured launch
+    rng = np.random.default_rng(20240602)
+    nc = 256
+    ny = rng.integers(128, 1025, nc)
+    nz = rng.integers(128, 1025, nc)
+    rois = np.array([[rng.integers(0, n - z + 1), rng.integers(0, n - y + 1), z, y]
+                     for y, z in zip(ny, nz)], dtype=np.int32)
+    cimg = counts.reshape(n, n)
+    cat = np.concatenate([cimg[r0:r0 + z, c0:c0 + y].ravel() for r0, c0, z, y in rois])
+    f = 1 + rng.uniform(-0.1, 0.1, (nc, 3))
+    models = np.array([mb(5.0 * f[i, 0], 10.0 * f[i, 1], 20.0 * f[i, 2],
+                          np.deg2rad(rng.uniform(-10, 10))) for i in range(nc)])
+    bb32 = fitting.CylinderBatch(ctx, g, rowfc, abc, rois, cat, None, scale, "f32c")
+    bb64 = fitting.CylinderBatch(ctx, g, rowfc, abc, rois, cat, None, scale, "f64")
+    cc32, gg32 = bb32.eval(models)
+    cc64, gg64 = bb64.eval(models)
+    for _ in range(3):
+        bb32.eval(models)
+    t = time.perf_counter()
+    for _ in range(steps):
+        bb32.eval(models)
+    dtb = (time.perf_counter() - t) / steps
+    # 256 sequential plain launches: the plain FP64 central-difference evaluation of a
+    # subsample of candidates, scaled by pixel count
+    sub = 8
+    pix = rois[:, 2].astype(np.int64) * rois[:, 3]
+    t = time.perf_counter()
+    for i in range(sub):
+        r0, c0, z, y = rois[i]
+        cb = fitting.CylinderBatch(ctx, g, rowfc, abc, [rois[i]],
+                                   cat[bb32.offsets[i]:bb32.offsets[i + 1]], None, scale, "f64")
+        dI = torch.empty(int(z) * int(y), dtype=torch.float64, device=dev)
+        dC = torch.tensor(cat[bb32.offsets[i]:bb32.offsets[i + 1]], device=dev)
+        for j in range(9):
+            m = models[i].copy()
+            if j:
+                k = (j - 1) // 2
+                m[k] += (1 if j % 2 else -1) * 1e-4 * (abs(m[k]) if k < 3 else 1.0)
+            hg._capi.check(hg.lib().hgx_cyl_plain_forward(cb._h, 0, np.ascontiguousarray(m).ctypes.data,
+                                                          dI.data_ptr()))
+            model.chi2(ctx, dI, dC, None, scale)
+        cb.close()
+    dts = (time.perf_counter() - t) * pix.sum() / pix[:sub].sum()
+    rel_c = float(np.max(np.abs(cc32 - cc64) / np.abs(cc64)))
+    rel_g = float(np.max(np.linalg.norm(gg32 - gg64, axis=1) / np.linalg.norm(gg64, axis=1)))
+    out["batch_256_rois"] = {
+        "metric": "chi2+grad evals/s", "value": nc / dtb, "ms_per_batch": 1e3 * dtb,
+        "candidates": nc, "pixels": int(pix.sum()), "work_items": bb32.nitems,
+        "sequential_plain_fp64_fd": {"value": nc / dts, "s_per_batch": dts,
+                                     "sample": f"{sub} candidates timed, scaled by pixels"},
+        "speedup_vs_sequential_plain": dts / dtb,
+        "max_rel_err_chi2_vs_fp64": rel_c, "max_rel_err_grad_vs_fp64": rel_g}
+    bb32.close()
+    bb64.close()
+    g.close()
+    return out
 
 
 def run_reference(args, rank):
@@ -305,6 +445,10 @@ def main():
                "d2h_bytes_per_step": int(16 * 4 * n), "ms_per_step": mse,
                "path": "hgx_ff_triangles (reference-shaped, host buffers, complex128 out)"}
 
+    fit = None
+    if not args.no_fitting:
+        fit = fitting_bench(ctx, torch, dev, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         g = grid.read(qz_det=False, alpha=False)
@@ -333,7 +477,7 @@ def main():
                          "flop_per_pixel_triangle": FLOP_PER_PIXEL_TRI,
                          "sfu": {"achieved_gops": sfu_rate, "peak_gops": peak_sfu,
                                  "frac": sfu_rate / peak_sfu}},
-            "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64,
+            "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
