@@ -55,6 +55,9 @@ SIGNATURES = {
     "hgx_cyl_plain_forward": (_i, [_vp, _i, _vp, _vp]),
     "hgx_cyl_batch_info": (_i, [_vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]),
     "hgx_cyl_batch_destroy": (_i, [_vp]),
+    "hgx_mesh_to_shape_def": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
+    "hgx_mesh_chi2_grad": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
+                                _vp, _vp, _vp]),
     "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }

@@ -28,6 +28,38 @@ def model_block(radius, height, lattice_a, phi=0.0, spread=0.0, nsamples=1, repe
     return m
 
 
+def mesh_to_shape_def(ctx: Context, verts, faces):
+    """Triangle tuples (s, n, c) of a mesh on the device, one row per face (degenerate faces
+    get s = 0)."""
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
+    out = np.zeros((len(f), 8))
+    check(lib().hgx_mesh_to_shape_def(ctx.handle, len(v), v.ctypes.data, len(f), f.ctypes.data,
+                                      out.ctypes.data))
+    return out
+
+
+def mesh_chi2_grad(ctx: Context, grid: QGrid, verts, faces, rowfc, dn2, counts=None, mask=None,
+                   scale=1.0, weight=1.0, rot=None, want_grad=True, want_intensity=False):
+    """(chi2, grad[nv, 3] or None, intensity[N] or None) for a mesh in DWBA."""
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
+    rf = np.ascontiguousarray(rowfc, dtype=np.complex128)
+    r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64).reshape(9)
+    cnt = None if counts is None else np.ascontiguousarray(counts, dtype=np.float64)
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint32)
+    chi = C.c_double()
+    gv = np.zeros((len(v), 3)) if want_grad else None
+    inten = np.zeros(grid.nrow * grid.ncol) if want_intensity else None
+    check(lib().hgx_mesh_chi2_grad(
+        ctx.handle, grid.handle, len(v), v.ctypes.data, len(f), f.ctypes.data,
+        None if r is None else r.ctypes.data, rf.ctypes.data, float(dn2[0]), float(dn2[1]),
+        float(weight), None if cnt is None else cnt.ctypes.data,
+        None if mk is None else mk.ctypes.data, float(scale), C.byref(chi),
+        None if gv is None else gv.ctypes.data, None if inten is None else inten.ctypes.data))
+    return chi.value, gv, inten
+
+
 class CylinderBatch:
     """hgx_cyl_batch: candidates with ROIs on one device grid."""
 

@@ -215,6 +215,26 @@ int hgx_cyl_plain_forward(hgx_cyl_batch b, int cand, const double* model, double
 int hgx_cyl_batch_info(hgx_cyl_batch b, long* npx, long* nitems);
 int hgx_cyl_batch_destroy(hgx_cyl_batch b);
 
+/* ------------------------------------------------------------ triangle meshes ---- */
+/* ObjectShapeReader::get_triangle_params / convert_to_shape
+ * (src/file/objectshape_reader.cpp:248-300) on the device: vertices nv x 3, faces nf x 3
+ * (0-based) -> shape_def nf x 8 (s, n, c, pad) in face order; a degenerate face (which the
+ * reference drops) gets s = 0, n = 0 and contributes nothing.  Bad indices: HGX_ERR_DEVICE. */
+int hgx_mesh_to_shape_def(hgx_ctx ctx, int nv, const double* verts, int nf, const int* faces,
+                          double* shape_def);
+/* chi^2 of a triangle mesh in DWBA and its gradient with respect to every vertex
+ * coordinate (hand-written adjoint; no counterpart in the reference, whose fitter can only
+ * difference the forward model).  I(p) = |weight dn2 sum_k fc_k F_k(p)|^2 with F_k the
+ * FP32C mesh form factor of the rotated mesh (rot9 or NULL); rowfc: per-row Fresnel
+ * coefficients (nrow x 4); chi^2 = sum mask (scale I - counts)^2 / max(counts, 1).
+ * Outputs: chi2 (host double), grad_verts (nv x 3, may be NULL), intensity (N, may be
+ * NULL).  The grid must be a DWBA grid with real qz constant along rows. */
+int hgx_mesh_chi2_grad(hgx_ctx ctx, hgx_qgrid g, int nv, const double* verts, int nf,
+                       const int* faces, const double* rot9, const double* rowfc,
+                       double dn2_re, double dn2_im, double weight, const double* counts,
+                       const unsigned* mask, double scale, double* chi2, double* grad_verts,
+                       double* intensity);
+
 /* The FP32C numeric form factor for callers that cannot allocate device memory: code
  * running inside CUDA graph capture, inside another framework's memory pool or under a
  * fixed memory budget, where a cudaMalloc would fail, break the capture or synchronise the
