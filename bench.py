@@ -283,6 +283,41 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
     return out
 
 
+def mesh_grad_bench(ctx, grid, steps=2):
+    """Config 3, mesh part: chi^2 and the gradient with respect to all 25,002 x 3 vertex
+    coordinates of the 50,000-triangle star mesh on the 2048 x 2048 DWBA detector (forward
+    FP32C form factor + adjoint).  The reference's method (central differences) would need
+    1 + 2 x 75,006 forward runs; its cost is extrapolated from the forward time."""
+    from hipgisaxs_b200 import fitting, meshes, model
+    V, F = meshes.star_mesh(15.0, 250, 101, 8, 0.05, meshes.DEFAULT_SEED)
+    alpha_i = ALPHA_I_DEG * PI_REF / 180
+    k0 = k0_from_kev(ENERGY_KEV)
+    rowfc = model.propagation_coeffs(ctx, grid, [(4.88e-6, 7.37e-8, 0.0, -1)], k0, alpha_i, 0,
+                                     per_row=True)
+    dn2 = (-2 * 4.88e-6, -2 * 7.37e-8)
+    Vt, _ = meshes.star_mesh(15.0 * 1.02, 250, 101, 8, 0.05, meshes.DEFAULT_SEED + 1)
+    _, _, It = fitting.mesh_chi2_grad(ctx, grid, Vt, F, rowfc, dn2, None, None, 1.0, 1.0,
+                                      want_grad=False, want_intensity=True)
+    rng = np.random.default_rng(20240603)
+    scale = 1e4 / It.max()
+    counts = rng.poisson(scale * It).astype(np.float64)
+    fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale)
+    t = time.perf_counter()
+    for _ in range(steps):
+        chi, gv, _ = fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale)
+    dt = (time.perf_counter() - t) / steps
+    t = time.perf_counter()
+    fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale, want_grad=False)
+    dtf = time.perf_counter() - t
+    nparam = 3 * len(V)
+    return {"metric": "chi2+grad evals/s", "value": 1.0 / dt, "s_per_eval": dt,
+            "forward_only_s": dtf, "vertices": len(V), "triangles": len(F),
+            "gradient_components": nparam,
+            "central_differences_estimate_s": (1 + 2 * nparam) * dtf,
+            "note": "the central-difference gradient was not run: extrapolated from the timed "
+                    "forward (1 + 2 x 75,006 forward runs)"}
+
+
 def run_reference(args, rank):
     """The reference's own CPU implementation of the path on this host's cores."""
     if rank != 0:
@@ -448,6 +483,7 @@ def main():
     fit = None
     if not args.no_fitting:
         fit = fitting_bench(ctx, torch, dev, stream)
+        fit["mesh_vertices_2048sq"] = mesh_grad_bench(ctx, grid)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
