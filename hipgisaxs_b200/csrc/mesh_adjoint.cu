@@ -375,7 +375,8 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
   mesh_to_shape_kernel<<<(nf + 127) / 128, 128, 0, st>>>((const double*)dv, nv, (const int*)df, nf,
                                                          (double*)sd.p, c->d_err);
   HGX_TRY(F.reserve(sizeof(float2) * 4 * n));
-  HGX_TRY(ff_triangles_device(c, g, (const double*)sd.p, nf, R, HGX_F32C, F.p, HGX_C64, 0));
+  // the scalar row kernel (4 pixels/thread): the backward pass reads its triangle tiles
+  HGX_TRY(ff_triangles_device(c, g, (const double*)sd.p, nf, R, HGX_F32C, F.p, HGX_C64, 4));
   // 3. intensity, chi^2, seeds
   const int sblocks = (int)((n + 255) / 256);
   HGX_TRY(seeds.reserve(sizeof(float4) * 2 * n));

@@ -94,7 +94,9 @@ int hgx_qgrid_destroy(hgx_qgrid g);
 int hgx_ff_triangles_q(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
                        const double* rot9, int precision, void* ff, int ff_type);
 /* As hgx_ff_triangles_q with an explicit launch shape for the FP32 row kernel:
- * pixels_per_thread 1, 2 or 4 (0 = automatic).  Used by the launch-shape tuner. */
+ * pixels_per_thread 1, 2 or 4 selects the scalar kernel with that many pixels per thread;
+ * -2, -4 or -8 the packed FP32x2 kernel (paired real grids only); 0 = automatic (scalar, 4,
+ * fewer when the grid is too small to fill the GPU). */
 int hgx_ff_triangles_q_ex(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
                           const double* rot9, int precision, void* ff, int ff_type,
                           int pixels_per_thread);

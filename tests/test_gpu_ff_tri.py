@@ -39,7 +39,7 @@ def test_golden_fixtures(ctx, po, golden, golden_grid, grid, rot):
 
 
 @pytest.mark.parametrize("ntri", [1, 63, 64, 65, 200])
-@pytest.mark.parametrize("ppt", [1, 2, 4])
+@pytest.mark.parametrize("ppt", [1, 2, 4, -2, -4, -8])  # negative: packed FP32x2 kernel
 def test_ragged_triangle_counts_and_launch_shapes(ctx, po, golden_grid, ntri, ppt):
     rng = np.random.default_rng(ntri)
     G, _ = golden_grid("g16")
