@@ -7,6 +7,6 @@ libhgx.so).  This Python package is a thin host-side mirror of that ABI; the C++
 classes with the reference's signatures live in csrc/hig/.
 """
 from ._capi import HgxError, lib  # noqa: F401
-from .core import Context, QGrid, ff_triangles, ff_triangles_arrays, measure_peaks  # noqa: F401
+from .core import Context, QGrid, ff_triangles, ff_triangles_arrays, ff_tune, measure_peaks  # noqa: F401
 
-__all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "HgxError", "lib"]
+__all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "ff_tune", "HgxError", "lib"]

@@ -37,6 +37,7 @@ SIGNATURES = {
     "hgx_qgrid_destroy": (_i, [_vp]),
     "hgx_ff_triangles_q": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i]),
     "hgx_ff_triangles_q_ex": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i]),
+    "hgx_ff_tune": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "hgx_ff_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp]),
     "hgx_param_distribution": (_i, [_i, _d, _d, _d, _d, _i, _vp, _vp, _i, C.POINTER(_i)]),
     "hgx_ff_analytic": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp,
@@ -55,6 +56,10 @@ SIGNATURES = {
     "hgx_cyl_plain_forward": (_i, [_vp, _i, _vp, _vp]),
     "hgx_cyl_batch_info": (_i, [_vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]),
     "hgx_cyl_batch_destroy": (_i, [_vp]),
+    "hgx_cyl_shape_info": (_i, [_i, C.POINTER(_i), C.POINTER(_i)]),
+    "hgx_cyl_batch_set_shape": (_i, [_vp, _i]),
+    "hgx_cyl_batch_get_shape": (_i, [_vp, C.POINTER(_i)]),
+    "hgx_cyl_batch_tune": (_i, [_vp, _vp, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "hgx_mesh_to_shape_def": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "hgx_mesh_chi2_grad": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
                                 _vp, _vp, _vp]),

@@ -167,6 +167,22 @@ def ff_triangles(ctx: Context, grid: QGrid, shape_def, rot=None, precision="f32c
     return out
 
 
+TUNE_CANDIDATES = (4, 2, 1, -2, -4, -8)
+
+
+def ff_tune(ctx: Context, grid: QGrid, shape_def, rot=None, out_type="c64", reps=2):
+    """Autotune the FP32C kernel's launch shape on `grid` (hgx_ff_tune); later automatic
+    calls on this grid use the choice.  Returns (pixels_per_thread, ms, {candidate: ms})."""
+    psd, ksd = _in(shape_def, np.float64)
+    ntri = int((ksd.numel() if _is_tensor(ksd) else ksd.size) // 8)
+    r = _rot_arg(rot)
+    best, ms = C.c_int(), C.c_double()
+    times = np.zeros(len(TUNE_CANDIDATES))
+    check(lib().hgx_ff_tune(ctx.handle, grid.handle, psd, ntri, r.ctypes.data, CTYPE[out_type],
+                            int(reps), C.byref(best), C.byref(ms), times.ctypes.data))
+    return best.value, ms.value, {p: t for p, t in zip(TUNE_CANDIDATES, times) if t > 0}
+
+
 def measure_peaks(ctx: Context, sustained_ms: int = 0):
     """(FP32 TFLOP/s, SFU Gop/s) measured by the library's probe kernels."""
     f = C.c_double()

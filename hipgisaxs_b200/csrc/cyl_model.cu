@@ -38,9 +38,17 @@ int param_distribution_host(int stat, double pmin, double pmax, double mean, dou
                             int nvalues, std::vector<double>& dim, std::vector<double>& w);
 
 constexpr int CYL_MAXS = 64;
-constexpr int CYL_THREADS = 256;
-constexpr int CYL_PPT = 4;                         // pixels per thread per work item
-constexpr int CYL_TILE = CYL_THREADS * CYL_PPT;    // pixels per work item
+constexpr int CYL_THREADS = 256;                   // block of the row-table and final kernels
+// Tile shapes of the persistent pixel pass: threads per block x pixels per thread; one work
+// item is one tile of threads*ppt consecutive ROI pixels.  Shape 0 is the default; the
+// autotuner (hgx_cyl_batch_tune) times all of them on the batch's own ROIs.
+struct CylShape {
+  int threads, ppt;
+};
+constexpr CylShape CYL_SHAPES[] = {{256, 4}, {128, 1}, {128, 2}, {128, 4}, {256, 1},
+                                   {256, 2}, {256, 8}, {512, 1}, {512, 2}};
+constexpr int CYL_NSHAPES = sizeof(CYL_SHAPES) / sizeof(CYL_SHAPES[0]);
+constexpr int CYL_MIN_TILE = 128;                  // smallest threads*ppt above
 constexpr double PI_D = 3.141592653589793;
 
 // model parameter block of the C ABI (16 doubles)
@@ -163,7 +171,7 @@ struct BesselT<double> {
   static __device__ __forceinline__ double J1(double x) { return j1(x); }
 };
 
-template <typename T>
+template <int NT>
 __device__ __forceinline__ double block_sum5(double* v, double* sh) {
   // v[5] per thread -> sh[0..4] in thread 0; fixed tree order
 #pragma unroll
@@ -179,7 +187,7 @@ __device__ __forceinline__ double block_sum5(double* v, double* sh) {
   if (threadIdx.x < 32) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
-      double t = threadIdx.x < CYL_THREADS / 32 ? sh[threadIdx.x * 5 + q] : 0.0;
+      double t = threadIdx.x < NT / 32 ? sh[threadIdx.x * 5 + q] : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
       v[q] = t;
@@ -189,17 +197,17 @@ __device__ __forceinline__ double block_sum5(double* v, double* sh) {
   return v[0];
 }
 
-template <typename T>
-__global__ void __launch_bounds__(CYL_THREADS) cyl_pixels_kernel(CylArgs a) {
-  __shared__ double sh[(CYL_THREADS / 32) * 5];
+template <typename T, int NT, int PPT>
+__global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
+  __shared__ double sh[(NT / 32) * 5];
   for (long it = blockIdx.x; it < a.nitems; it += gridDim.x) {
     const int2 item = a.items[it];
     const CylCand& c = a.cands[item.x];
     const long npx = (long)c.nrows * c.ncols;
     double acc[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-    for (int j = 0; j < CYL_PPT; ++j) {
-      long idx = (long)item.y + threadIdx.x + (long)j * CYL_THREADS;
+    for (int j = 0; j < PPT; ++j) {
+      long idx = (long)item.y + threadIdx.x + (long)j * NT;
       if (idx >= npx) continue;
       int lr = (int)(idx / c.ncols), lc = (int)(idx - (long)lr * c.ncols);
       long p = (long)(c.row0 + lr) * a.grid_ncol + (c.col0 + lc);
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(CYL_THREADS) cyl_pixels_kernel(CylArgs a) {
       }
     }
     if (a.counts) {
-      block_sum5<T>(acc, sh);
+      block_sum5<NT>(acc, sh);
       if (threadIdx.x == 0)
 #pragma unroll
         for (int q = 0; q < 5; ++q) a.partial[5 * it + q] = acc[q];
@@ -275,10 +283,31 @@ __global__ void cyl_final_kernel(const CylCand* __restrict__ cands, const double
   for (long i = threadIdx.x; i < c.nitems; i += CYL_THREADS)
 #pragma unroll
     for (int q = 0; q < 5; ++q) acc[q] += partial[5 * (c.item0 + i) + q];
-  block_sum5<double>(acc, sh);
+  block_sum5<CYL_THREADS>(acc, sh);
   if (threadIdx.x == 0)
 #pragma unroll
     for (int q = 0; q < 5; ++q) out[5 * blockIdx.x + q] = acc[q];
+}
+
+// Launches tile shape `shape` of the pixel pass (a recursion over the shape table, so each
+// table row names its own instantiation); with `occ` set it returns the shape's resident
+// blocks per SM instead of launching.
+template <typename T, int I>
+static cudaError_t cyl_pixels_at(int shape, unsigned blocks, const CylArgs& a, cudaStream_t st,
+                                 int* occ) {
+  if constexpr (I < CYL_NSHAPES) {
+    if (shape == I) {
+      constexpr int NT = CYL_SHAPES[I].threads, PPT = CYL_SHAPES[I].ppt;
+      static_assert(NT % 32 == 0 && NT <= 1024 && NT * PPT >= CYL_MIN_TILE, "bad tile shape");
+      if (occ)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, cyl_pixels_kernel<T, NT, PPT>, NT, 0);
+      cyl_pixels_kernel<T, NT, PPT><<<blocks, NT, 0, st>>>(a);
+      return cudaGetLastError();
+    }
+    return cyl_pixels_at<T, I + 1>(shape, blocks, a, st, occ);
+  } else {
+    return cudaErrorInvalidValue;
+  }
 }
 
 // ------------------------------------------------- plain FP64 forward (baseline) ----
@@ -418,6 +447,7 @@ struct hgx_cyl_batch_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int persistent_blocks = 0;
+  int shape = 0;  // tile shape of the pixel pass (index into the shape table)
 };
 
 namespace hgx {
@@ -444,8 +474,10 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
   a.intensity = with_intensity ? (double*)b->d_inten.p : nullptr;
   a.partial = (double*)b->d_partial.p;
   long blocks = std::min<long>(b->nitems, (long)b->persistent_blocks);
-  if (b->precision == HGX_F64) cyl_pixels_kernel<double><<<(unsigned)blocks, CYL_THREADS, 0, st>>>(a);
-  else cyl_pixels_kernel<float><<<(unsigned)blocks, CYL_THREADS, 0, st>>>(a);
+  cudaError_t e = b->precision == HGX_F64
+                      ? cyl_pixels_at<double, 0>(b->shape, (unsigned)blocks, a, st, nullptr)
+                      : cyl_pixels_at<float, 0>(b->shape, (unsigned)blocks, a, st, nullptr);
+  if (e != cudaSuccess) return cuda_fail(e, "cyl_pixels_kernel launch");
   if (with_counts) {
     cyl_final_kernel<<<b->ncand, CYL_THREADS, 0, st>>>((const CylCand*)b->d_cands.p,
                                                       (const double*)b->d_partial.p,
@@ -454,6 +486,44 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
                              cudaMemcpyDeviceToHost, st));
   }
   HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+// Work items for tile shape `shape`: one per threads*ppt consecutive pixels of each ROI; sets
+// the candidates' item ranges, grows and fills the item and partial-sum buffers, sizes the
+// persistent grid from the shape's occupancy, and drops a captured graph (its launch shape
+// and buffers are stale).
+static int cyl_apply_shape(hgx_cyl_batch_s* b, int shape) {
+  if (shape < 0 || shape >= CYL_NSHAPES)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_cyl_batch: unknown tile shape");
+  const long tile = (long)CYL_SHAPES[shape].threads * CYL_SHAPES[shape].ppt;
+  std::vector<int2> items;
+  for (int i = 0; i < b->ncand; ++i) {
+    CylCand& h = b->h_cands[i];
+    long n = (long)b->rois[4 * i + 2] * b->rois[4 * i + 3];
+    h.item0 = (long)items.size();
+    for (long s = 0; s < n; s += tile) items.push_back(make_int2(i, (int)s));
+    h.nitems = (long)items.size() - h.item0;
+  }
+  cudaStream_t st = b->ctx->stream;
+  HGX_CUDA(cudaStreamSynchronize(st));
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  HGX_TRY(b->d_items.reserve(sizeof(int2) * items.size()));
+  HGX_TRY(b->d_partial.reserve(sizeof(double) * 5 * items.size()));
+  HGX_CUDA(cudaMemcpyAsync(b->d_items.p, items.data(), sizeof(int2) * items.size(),
+                           cudaMemcpyHostToDevice, st));
+  HGX_CUDA(cudaStreamSynchronize(st));  // `items` is pageable and about to go out of scope
+  int per_sm = 0;
+  CylArgs none{};
+  cudaError_t e = b->precision == HGX_F64 ? cyl_pixels_at<double, 0>(shape, 0, none, st, &per_sm)
+                                          : cyl_pixels_at<float, 0>(shape, 0, none, st, &per_sm);
+  if (e != cudaSuccess) return cuda_fail(e, "hgx_cyl_batch: occupancy query");
+  b->persistent_blocks = b->ctx->sm_count * std::max(1, per_sm);
+  b->nitems = (long)items.size();
+  b->shape = shape;
   return HGX_OK;
 }
 
@@ -512,7 +582,6 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
   if (cudaMallocHost(&b->h_cands, sizeof(CylCand) * ncand) != cudaSuccess ||
       cudaMallocHost(&b->h_out, sizeof(double) * 5 * ncand) != cudaSuccess)
     return bail(fail(HGX_ERR_NO_MEMORY, "hgx_cyl_batch_create: pinned host memory"));
-  std::vector<int2> items;
   long px = 0, rows = 0;
   for (int i = 0; i < ncand; ++i) {
     const int* r = rois + 4 * i;
@@ -522,28 +591,20 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
     h = CylCand();
     long n = (long)r[2] * r[3];
     h.px_off = px;
-    h.item0 = (long)items.size();
     h.rowtab0 = rows;
-    for (long s = 0; s < n; s += CYL_TILE) items.push_back(make_int2(i, (int)s));
-    h.nitems = (long)items.size() - h.item0;
     px += n;
     rows += r[2];
   }
   b->npx = px;
-  b->nitems = (long)items.size();
   b->nrowtab = rows;
   int s = HGX_OK;
-  if ((s = b->d_cands.reserve(sizeof(CylCand) * ncand)) || (s = b->d_items.reserve(sizeof(int2) * items.size())) ||
-      (s = b->d_tab.reserve(sizeof(RowTab) * rows)) || (s = b->d_partial.reserve(sizeof(double) * 5 * items.size())) ||
+  if ((s = b->d_cands.reserve(sizeof(CylCand) * ncand)) || (s = b->d_tab.reserve(sizeof(RowTab) * rows)) ||
       (s = b->d_out.reserve(sizeof(double) * 5 * ncand)) || (s = b->d_rowfc.reserve(sizeof(double2) * 4 * g->nrow)) ||
       (s = b->d_inten.reserve(sizeof(double) * px)))
     return bail(s);
   cudaStream_t st = c->stream;
-  cudaError_t e = cudaMemcpyAsync(b->d_items.p, items.data(), sizeof(int2) * items.size(),
-                                  cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(b->d_rowfc.p, rowfc, sizeof(double2) * 4 * g->nrow,
-                        is_device_ptr(rowfc) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+  cudaError_t e = cudaMemcpyAsync(b->d_rowfc.p, rowfc, sizeof(double2) * 4 * g->nrow,
+                                  is_device_ptr(rowfc) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && counts) {
     if ((s = b->d_counts.reserve(sizeof(double) * px))) return bail(s);
     e = cudaMemcpyAsync(b->d_counts.p, counts, sizeof(double) * px,
@@ -557,12 +618,7 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(cuda_fail(e, "hgx_cyl_batch_create: copies"));
   if (!mask) b->d_mask.release();
-  int per_sm = 0;
-  if (precision == HGX_F64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cyl_pixels_kernel<double>, CYL_THREADS, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cyl_pixels_kernel<float>, CYL_THREADS, 0);
-  b->persistent_blocks = c->sm_count * std::max(1, per_sm);
+  if ((s = cyl_apply_shape(b, 0))) return bail(s);
   *out = b;
   return HGX_OK;
 }
@@ -634,6 +690,74 @@ int hgx_cyl_plain_forward(hgx_cyl_batch_s* b, int cand, const double* model, dou
       b->grid->ncol, (double*)dI);
   HGX_CUDA(cudaGetLastError());
   HGX_TRY(finish_out(b->ctx, intensity, sizeof(double) * n, dI));
+  return hgx_synchronize(b->ctx);
+}
+
+// Tile-shape table of the pixel pass: threads per block and pixels per thread of `shape`;
+// HGX_ERR_INVALID_ARG past the end of the table (callers enumerate with it).
+int hgx_cyl_shape_info(int shape, int* threads, int* pixels_per_thread) {
+  if (shape < 0 || shape >= CYL_NSHAPES)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_cyl_shape_info: shape past the end of the table");
+  if (threads) *threads = CYL_SHAPES[shape].threads;
+  if (pixels_per_thread) *pixels_per_thread = CYL_SHAPES[shape].ppt;
+  return HGX_OK;
+}
+
+int hgx_cyl_batch_set_shape(hgx_cyl_batch_s* b, int shape) {
+  if (!b) return fail(HGX_ERR_INVALID_ARG, "hgx_cyl_batch_set_shape: null batch");
+  HGX_CUDA(cudaSetDevice(b->ctx->device));
+  return cyl_apply_shape(b, shape);
+}
+
+int hgx_cyl_batch_get_shape(hgx_cyl_batch_s* b, int* shape) {
+  if (!b || !shape) return fail(HGX_ERR_INVALID_ARG, "hgx_cyl_batch_get_shape: null argument");
+  *shape = b->shape;
+  return HGX_OK;
+}
+
+// The autotuner: for every tile shape, one untimed evaluation and then `reps` evaluations timed
+// together with CUDA events on the batch's stream (chi^2 + gradient when the batch has counts,
+// else the forward intensities), at these models and on this batch's ROIs; keeps the fastest
+// shape.  times_ms (may be NULL) receives the mean time of each shape, in table order.
+int hgx_cyl_batch_tune(hgx_cyl_batch_s* b, const double* models, int reps, int* best_shape,
+                       double* best_ms, double* times_ms) {
+  if (!b || !models) return fail(HGX_ERR_INVALID_ARG, "hgx_cyl_batch_tune: null argument");
+  if (reps < 1) reps = 1;
+  HGX_CUDA(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  HGX_CUDA(cudaStreamSynchronize(st));
+  HGX_TRY(cyl_set_models(b, models));
+  struct Events {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Events() {
+      for (auto x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  HGX_CUDA(cudaEventCreate(&ev.e[0]));
+  HGX_CUDA(cudaEventCreate(&ev.e[1]));
+  const bool chi = b->d_counts.p != nullptr;
+  int best = 0;
+  double bms = 0.0;
+  for (int sh = 0; sh < CYL_NSHAPES; ++sh) {
+    HGX_TRY(cyl_apply_shape(b, sh));
+    HGX_TRY(cyl_enqueue(b, chi, !chi));
+    HGX_CUDA(cudaEventRecord(ev.e[0], st));
+    for (int r = 0; r < reps; ++r) HGX_TRY(cyl_enqueue(b, chi, !chi));
+    HGX_CUDA(cudaEventRecord(ev.e[1], st));
+    HGX_CUDA(cudaEventSynchronize(ev.e[1]));
+    float ms = 0.f;
+    HGX_CUDA(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
+    double per = (double)ms / reps;
+    if (times_ms) times_ms[sh] = per;
+    if (sh == 0 || per < bms) {
+      best = sh;
+      bms = per;
+    }
+  }
+  HGX_TRY(cyl_apply_shape(b, best));
+  if (best_shape) *best_shape = best;
+  if (best_ms) *best_ms = bms;
   return hgx_synchronize(b->ctx);
 }
 

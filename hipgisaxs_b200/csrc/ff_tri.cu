@@ -765,6 +765,7 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
     HGX_CUDA(cudaGetLastError());
     return HGX_OK;
   }
+  if (want_p == 0) want_p = g->tuned_p;  // the autotuner's choice for this grid, if any
   const int ntiles = (ntri + TILE - 1) / TILE;
   // paired real DWBA blocks, packed FP32x2 kernel on request (want_p = -2, -4, -8 pixels per
   // thread).  Measured on a 2048 x 2048 detector with 50,000 triangles it runs at the speed of
@@ -872,6 +873,78 @@ int hgx_ff_triangles_q_ex(hgx_ctx c, hgx_qgrid g, const double* shape_def, int n
 int hgx_ff_triangles_q(hgx_ctx c, hgx_qgrid g, const double* shape_def, int ntri,
                        const double* rot9, int precision, void* ff, int ff_type) {
   return hgx_ff_triangles_q_ex(c, g, shape_def, ntri, rot9, precision, ff, ff_type, 0);
+}
+
+// The launch-shape autotuner of the FP32C row kernel.  Candidates, in this order: scalar
+// kernel with 4, 2, 1 pixels per thread, then (paired real grids only) the packed FP32x2
+// kernel with 2, 4, 8.  Each is run once untimed and then `reps` times between two CUDA
+// events on the context's stream, on the caller's triangles (the cost of every candidate is
+// linear in the triangle count, so a few thousand triangles rank them); the fastest is stored
+// in the grid and used by later calls that ask for the automatic shape.
+static const int TUNE_CANDIDATES[] = {4, 2, 1, -2, -4, -8};
+constexpr int TUNE_NCAND = sizeof(TUNE_CANDIDATES) / sizeof(TUNE_CANDIDATES[0]);
+
+int hgx_ff_tune(hgx_ctx c, hgx_qgrid g, const double* shape_def, int ntri, const double* rot9,
+                int ff_type, int reps, int* best_ppt, double* best_ms, double* times_ms) {
+  if (!c || !g || !shape_def) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_tune: null argument");
+  if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_tune: no triangles");
+  if (ff_type != HGX_C128 && ff_type != HGX_C64)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_tune: unknown output type");
+  if (g->ctx != c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_tune: grid of another context");
+  if (reps < 1) reps = 1;
+  if (times_ms)
+    for (int i = 0; i < TUNE_NCAND; ++i) times_ms[i] = 0.0;
+  if (g->mode == 0) {  // per-q-point kernel: one launch shape, nothing to choose
+    if (best_ppt) *best_ppt = 0;
+    if (best_ms) *best_ms = 0.0;
+    return HGX_OK;
+  }
+  HGX_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  const double* sd = shape_def;
+  DevBuf sdbuf, out;
+  if (!is_device_ptr(shape_def)) {
+    HGX_TRY(sdbuf.reserve(sizeof(double) * 8 * (size_t)ntri));
+    HGX_CUDA(cudaMemcpyAsync(sdbuf.p, shape_def, sizeof(double) * 8 * (size_t)ntri,
+                             cudaMemcpyHostToDevice, st));
+    sd = reinterpret_cast<const double*>(sdbuf.p);
+  }
+  const size_t esz = ff_type == HGX_C64 ? sizeof(float2) : sizeof(double2);
+  HGX_TRY(out.reserve(esz * (size_t)g->nqz));
+  struct Events {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    ~Events() {
+      for (auto x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  HGX_CUDA(cudaEventCreate(&ev.e[0]));
+  HGX_CUDA(cudaEventCreate(&ev.e[1]));
+  int best = 0;
+  double bms = 0.0;
+  for (int i = 0; i < TUNE_NCAND; ++i) {
+    const int p = TUNE_CANDIDATES[i];
+    if (p < 0 && g->mode != 1) continue;
+    HGX_TRY(ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, out.p, ff_type, p));
+    HGX_CUDA(cudaEventRecord(ev.e[0], st));
+    for (int r = 0; r < reps; ++r)
+      HGX_TRY(ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, out.p, ff_type, p));
+    HGX_CUDA(cudaEventRecord(ev.e[1], st));
+    HGX_CUDA(cudaEventSynchronize(ev.e[1]));
+    float ms = 0.f;
+    HGX_CUDA(cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]));
+    double per = (double)ms / reps;
+    if (times_ms) times_ms[i] = per;
+    if (best == 0 || per < bms) {
+      best = p;
+      bms = per;
+    }
+  }
+  HGX_TRY(hgx_synchronize(c));  // device errors of the timed launches
+  g->tuned_p = best;
+  if (best_ppt) *best_ppt = best;
+  if (best_ms) *best_ms = bms;
+  return HGX_OK;
 }
 
 int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, const double* qx,

@@ -71,6 +71,7 @@ struct hgx_qgrid_s {
   double2* rowqz = nullptr;      // nrow x nk: the row-constant qz of each block (modes 1, 2)
   double* qz_det = nullptr;      // nqy: detector qz (grids made by hgx_qgrid_create)
   double* alpha = nullptr;       // nrow exit angles (grids made by hgx_qgrid_create)
+  int tuned_p = 0;               // FP32 row-kernel launch shape chosen by hgx_ff_tune (0: none)
 };
 
 namespace hgx {

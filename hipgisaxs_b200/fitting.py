@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 from ._capi import F32C, F64, check, lib
-from .core import Context, QGrid
+from .core import Context, QGrid, _in
 
 MODEL_LEN = 16
 THETA = ("radius", "height", "lattice_a", "phi")
@@ -46,16 +46,15 @@ def mesh_chi2_grad(ctx: Context, grid: QGrid, verts, faces, rowfc, dn2, counts=N
     f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
     rf = np.ascontiguousarray(rowfc, dtype=np.complex128)
     r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64).reshape(9)
-    cnt = None if counts is None else np.ascontiguousarray(counts, dtype=np.float64)
-    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint32)
+    pc, cnt = _in(counts, np.float64)  # host arrays or device tensors
+    pm, mk = _in(mask, np.uint32)
     chi = C.c_double()
     gv = np.zeros((len(v), 3)) if want_grad else None
     inten = np.zeros(grid.nrow * grid.ncol) if want_intensity else None
     check(lib().hgx_mesh_chi2_grad(
         ctx.handle, grid.handle, len(v), v.ctypes.data, len(f), f.ctypes.data,
         None if r is None else r.ctypes.data, rf.ctypes.data, float(dn2[0]), float(dn2[1]),
-        float(weight), None if cnt is None else cnt.ctypes.data,
-        None if mk is None else mk.ctypes.data, float(scale), C.byref(chi),
+        float(weight), pc, pm, float(scale), C.byref(chi),
         None if gv is None else gv.ctypes.data, None if inten is None else inten.ctypes.data))
     return chi.value, gv, inten
 
@@ -83,8 +82,45 @@ class CylinderBatch:
         ctx._register(self)
         n1, n2 = C.c_long(), C.c_long()
         check(lib().hgx_cyl_batch_info(h, C.byref(n1), C.byref(n2)))
-        self.npx, self.nitems = n1.value, n2.value
+        self.npx = n1.value
         self.offsets = np.concatenate([[0], np.cumsum(r[:, 2].astype(np.int64) * r[:, 3])])
+
+    @property
+    def nitems(self):
+        """Work items of the current tile shape."""
+        n1, n2 = C.c_long(), C.c_long()
+        check(lib().hgx_cyl_batch_info(self._h, C.byref(n1), C.byref(n2)))
+        return n2.value
+
+    @staticmethod
+    def shapes():
+        """The tile-shape table: [(threads per block, pixels per thread), ...]."""
+        out, k = [], 0
+        while True:
+            t, p = C.c_int(), C.c_int()
+            if lib().hgx_cyl_shape_info(k, C.byref(t), C.byref(p)) != 0:
+                return out
+            out.append((t.value, p.value))
+            k += 1
+
+    @property
+    def shape(self):
+        s = C.c_int()
+        check(lib().hgx_cyl_batch_get_shape(self._h, C.byref(s)))
+        return s.value
+
+    @shape.setter
+    def shape(self, k):
+        check(lib().hgx_cyl_batch_set_shape(self._h, int(k)))
+
+    def tune(self, models, reps=3):
+        """Autotune the tile shape on this batch: (best shape, its ms, ms of every shape)."""
+        m = self._models(models)
+        best, ms = C.c_int(), C.c_double()
+        times = np.zeros(len(self.shapes()))
+        check(lib().hgx_cyl_batch_tune(self._h, m.ctypes.data, int(reps), C.byref(best),
+                                       C.byref(ms), times.ctypes.data))
+        return best.value, ms.value, times
 
     def _models(self, models):
         m = np.ascontiguousarray(np.asarray(models, dtype=np.float64).reshape(-1, MODEL_LEN))

@@ -100,6 +100,17 @@ int hgx_ff_triangles_q(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int nt
 int hgx_ff_triangles_q_ex(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
                           const double* rot9, int precision, void* ff, int ff_type,
                           int pixels_per_thread);
+/* The launch-shape autotuner of the FP32C kernel (no reference counterpart; the reference
+ * launches one fixed shape).  Times the candidate pixels_per_thread values 4, 2, 1 (scalar)
+ * and, on paired real grids, -2, -4, -8 (packed) on these triangles — one untimed launch,
+ * then `reps` launches between CUDA events each — and stores the fastest in the grid, where
+ * later calls with the automatic shape (hgx_ff_triangles_q, or pixels_per_thread 0) use it.
+ * Cost is linear in ntri for every candidate, so a few thousand triangles rank them.
+ * best_ppt, best_ms and times_ms (6 means in the order above; 0 for a candidate the grid
+ * does not take) may each be NULL.  Per-q-point grids have one shape: best_ppt = 0. */
+int hgx_ff_tune(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
+                const double* rot9, int ff_type, int reps, int* best_ppt, double* best_ms,
+                double* times_ms);
 /* The reference-shaped call: explicit q arrays, complex128 output, synchronous.
  * Returns HGX_ERR_INVALID_ARG for ntri < 1 (the reference returns 0 triangles). */
 int hgx_ff_triangles(hgx_ctx ctx, const double* shape_def, int ntri, int nqy, const double* qx,
@@ -216,6 +227,22 @@ int hgx_cyl_batch_forward(hgx_cyl_batch b, const double* models, double* intensi
 int hgx_cyl_plain_forward(hgx_cyl_batch b, int cand, const double* model, double* intensity);
 int hgx_cyl_batch_info(hgx_cyl_batch b, long* npx, long* nitems);
 int hgx_cyl_batch_destroy(hgx_cyl_batch b);
+/* Tile shapes of the batch's persistent pixel pass (no reference counterpart; the reference
+ * launches one fixed shape per kernel).  A work item is one tile of threads x
+ * pixels_per_thread consecutive pixels of a candidate's ROI; the persistent grid is the
+ * shape's resident blocks per SM x SM count.  hgx_cyl_shape_info describes table entry
+ * `shape` (HGX_ERR_INVALID_ARG past the end, for enumeration); set/get select and read the
+ * batch's shape (0 at creation).  Changing the shape drops the recorded CUDA graph; the
+ * next hgx_cyl_batch_eval records a new one. */
+int hgx_cyl_shape_info(int shape, int* threads, int* pixels_per_thread);
+int hgx_cyl_batch_set_shape(hgx_cyl_batch b, int shape);
+int hgx_cyl_batch_get_shape(hgx_cyl_batch b, int* shape);
+/* The autotuner: times every tile shape on this batch at these models (one untimed
+ * evaluation, then `reps` evaluations timed with CUDA events: chi^2 + gradient when the
+ * batch has counts, else forward intensities) and keeps the fastest.  best_shape, best_ms
+ * and times_ms (one mean per table entry, table order) may each be NULL. */
+int hgx_cyl_batch_tune(hgx_cyl_batch b, const double* models, int reps, int* best_shape,
+                       double* best_ms, double* times_ms);
 
 /* ------------------------------------------------------------ triangle meshes ---- */
 /* ObjectShapeReader::get_triangle_params / convert_to_shape

@@ -161,3 +161,24 @@ def test_errors_are_reported(ctx):
     g = hg.QGrid.from_arrays(ctx, np.zeros(4), np.zeros(4), np.ones(4, complex))
     with pytest.raises(hg.HgxError):
         hg.ff_triangles(ctx, g, np.zeros((0, 8)), None, "f32c")
+
+
+def test_launch_shape_autotuner(ctx, po, golden_grid):
+    """The tuner times the candidate shapes, stores the fastest in the grid, and automatic
+    calls afterwards give the result of that shape chosen by hand."""
+    G, _ = golden_grid("g16")
+    sd = tri_cloud(np.random.default_rng(12), 300)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    best, ms, times = hg.ff_tune(ctx, g, sd, None, "c128", reps=2)
+    assert best in (4, 2, 1, -2, -4, -8) and set(times) == {4, 2, 1, -2, -4, -8}
+    assert ms == times[best] == min(times.values())
+    auto = hg.ff_triangles(ctx, g, sd, None, "f32c")
+    hand = hg.ff_triangles(ctx, g, sd, None, "f32c", pixels_per_thread=best)
+    assert np.array_equal(auto, hand)
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext)
+    assert po.rel_err(auto, ref) < TOL32
+    # per-q-point grids have one shape
+    rng = np.random.default_rng(3)
+    gp = hg.QGrid.from_arrays(ctx, rng.uniform(-2, 2, 50), rng.uniform(-2, 2, 50),
+                              rng.uniform(0, 3, 150) + 0.01j)
+    assert gp.mode == 0 and hg.ff_tune(ctx, gp, sd)[0] == 0

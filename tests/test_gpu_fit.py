@@ -144,3 +144,40 @@ def test_batch_rejects_bad_input(ctx, po):
     fcc = np.array([[0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]])
     with pytest.raises(hg.HgxError):  # lattice vectors out of the plane
         fitting.CylinderBatch(ctx, g, rowfc, fcc, [[0, 0, 24, 32]]).forward([_model()])
+
+
+def test_tile_shapes_and_autotuner(ctx, po):
+    """Every tile shape gives the same intensities (bit-identical: per-pixel work does not
+    depend on the shape) and the same chi^2/gradient up to summation order; the tuner
+    returns a shape of the table, and evaluations after it match that shape set by hand."""
+    G, g, rowfc, abc = _setup(ctx, po, 128, 96)
+    rng = np.random.default_rng(5)
+    counts_full, s = _counts(_oracle_intensity(po, G, _model()), rng)
+    counts_full = counts_full.reshape(G.nrow, G.ncol)
+    rois = [[0, 0, 96, 128], [3, 9, 37, 61], [20, 30, 11, 5]]
+    counts = np.concatenate([counts_full[r0:r0 + nr, c0:c0 + nc].ravel() for r0, c0, nr, nc in rois])
+    models = [_model(5 * (1 + 0.02 * i), 10, 20 + 0.2 * i, 0.03 * i) for i in range(3)]
+    shapes = fitting.CylinderBatch.shapes()
+    assert len(shapes) >= 2 and all(t % 32 == 0 and p >= 1 for t, p in shapes)
+    batch = fitting.CylinderBatch(ctx, g, rowfc, abc, rois, counts, None, s, "f64")
+    assert batch.shape == 0
+    chi0, grad0 = batch.eval(models)
+    inten0 = batch.forward(models)
+    for k, (t, p) in enumerate(shapes):
+        batch.shape = k
+        assert batch.shape == k
+        assert batch.nitems == sum(-(-r[2] * r[3] // (t * p)) for r in rois)
+        for a, b in zip(batch.forward(models), inten0):
+            assert np.array_equal(a, b)
+        chi, grad = batch.eval(models)
+        np.testing.assert_allclose(chi, chi0, rtol=1e-12)
+        assert po.rel_err(grad, grad0) < 1e-12
+    best, ms, times = batch.tune(models, reps=2)
+    assert 0 <= best < len(shapes) and batch.shape == best
+    assert np.all(times > 0) and ms == times[best] == times.min()
+    chi_t, grad_t = batch.eval(models)
+    batch.shape = best
+    chi_s, grad_s = batch.eval(models)
+    assert np.array_equal(chi_t, chi_s) and np.array_equal(grad_t, grad_s)
+    with pytest.raises(hg.HgxError):
+        batch.shape = len(shapes)
