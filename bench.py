@@ -447,27 +447,6 @@ def main():
     ms_step = ms / args.steps
     value = world * evals * args.steps / (ms * 1e-3)
 
-    # FP64 plain kernel on the same inputs (the denominator of the FP32 speed-up)
-    f64 = None
-    if not args.no_f64:
-        out64 = torch.empty(4 * n, dtype=torch.complex128, device=dev)
-        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
-        a1.record(stream)
-        torch.cuda.synchronize()
-        ms64 = a0.elapsed_time(a1)
-        # accuracy of the timed FP32 output against the FP64 kernel (norm-wise)
-        d = (out.to(torch.complex128) - out64)
-        relerr = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(out64))
-        v64 = evals / (ms64 * 1e-3)
-        f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64,
-               "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr}
-        del out64
-
     # end to end through the reference-shaped C-ABI call with host (pinned) buffers
     e2e = None
     if not args.no_e2e:
@@ -496,6 +475,27 @@ def main():
                "h2d_bytes_per_step": int(sd.nbytes + 2 * 8 * n + 16 * 4 * n),
                "d2h_bytes_per_step": int(16 * 4 * n), "ms_per_step": mse,
                "path": "hgx_ff_triangles (reference-shaped, host buffers, complex128 out)"}
+
+    # FP64 plain kernel on the same inputs (the denominator of the FP32 speed-up)
+    f64 = None
+    if not args.no_f64:
+        out64 = torch.empty(4 * n, dtype=torch.complex128, device=dev)
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
+        a1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = a0.elapsed_time(a1)
+        # accuracy of the timed FP32 output against the FP64 kernel (norm-wise)
+        d = (out.to(torch.complex128) - out64)
+        relerr = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(out64))
+        v64 = evals / (ms64 * 1e-3)
+        f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64,
+               "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr}
+        del out64
 
     fit = None
     if not args.no_fitting:

@@ -12,7 +12,9 @@
 //
 // Precision: HGX_PRECISION=f64 in the environment selects the plain FP64 kernels; the
 // default is the FP32-compensated path (within 1e-5 norm-wise of FP64).
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <complex>
 #include <cstdlib>
 #include <cstring>
@@ -326,6 +328,197 @@ void StructureFactorG::get_sf(complex_t*& sf) {
   GridEntry* e = entry(this);
   if (!e || !sf) return;
   for (size_t i = 0; i < e->sf.size(); ++i) sf[i] = complex_t(e->sf[i].real(), e->sf[i].imag());
+}
+
+}  // namespace hig
+
+// ------------------------------------------------- HipGISAXSObjectiveFunctionG ----
+namespace hig {
+
+struct HipGISAXSObjectiveFunctionG::Impl {
+  CylinderLatticeSetup s;
+  hgx_ctx ctx = nullptr;  // the per-device context shared with the classes above
+  hgx_qgrid grid = nullptr;
+  std::vector<double> rowfc, abc9, counts;
+  std::vector<unsigned> mask;
+  hgx_cyl_batch one = nullptr;  // a single full-detector candidate
+  hgx_cyl_batch pop = nullptr;  // the population batch (rebuilt when its size changes)
+  int pop_n = 0;
+  real_t alpha = 0.0;
+  real_vec_t mean;
+  bool good = false;
+
+  ~Impl() {
+    if (pop) hgx_cyl_batch_destroy(pop);
+    if (one) hgx_cyl_batch_destroy(one);
+    if (grid) hgx_qgrid_destroy(grid);
+  }
+
+  // the 16-double model block of the hgx_cyl_batch functions
+  void model(const real_vec_t& x, double* m) const {
+    for (int i = 0; i < 16; ++i) m[i] = 0.0;
+    m[0] = x[0];
+    m[1] = x[1];
+    m[2] = x[2];
+    m[3] = x[3];
+    m[4] = s.spread;
+    m[5] = s.spread > 0 ? s.nsamples : 1;
+    for (int i = 0; i < 3; ++i) m[6 + i] = s.repet[i];
+    m[9] = s.dn2[0];
+    m[10] = s.dn2[1];
+    for (int i = 0; i < 3; ++i) m[11 + i] = s.center[i];
+    m[14] = s.weight;
+    m[15] = s.smooth_sampling ? 1.0 : 0.0;
+  }
+
+  hgx_cyl_batch make_batch(int n) {
+    const long npx = (long)s.nrow * s.ncol;
+    std::vector<int> rois(4 * (size_t)n);
+    std::vector<double> cnt((size_t)n * npx);
+    std::vector<unsigned> msk(mask.empty() ? 0 : (size_t)n * npx);
+    for (int i = 0; i < n; ++i) {
+      rois[4 * i + 0] = 0;
+      rois[4 * i + 1] = 0;
+      rois[4 * i + 2] = s.nrow;
+      rois[4 * i + 3] = s.ncol;
+      std::copy(counts.begin(), counts.end(), cnt.begin() + (size_t)i * npx);
+      if (!mask.empty()) std::copy(mask.begin(), mask.end(), msk.begin() + (size_t)i * npx);
+    }
+    hgx_cyl_batch b = nullptr;
+    if (!report(hgx_cyl_batch_create(ctx, grid, rowfc.data(), abc9.data(), n, rois.data(), cnt.data(),
+                                     msk.empty() ? nullptr : msk.data(), s.scale,
+                                     s.fp64 ? HGX_F64 : HGX_F32C, &b),
+                "objective batch"))
+      return nullptr;
+    return b;
+  }
+
+  // regularisation (alpha/2)||x - mean||^2 and its gradient alpha (x - mean)
+  real_t reg(const real_vec_t& x, real_vec_t* g) const {
+    real_t r = 0.0;
+    for (int i = 0; i < 4; ++i) {
+      real_t d = x[i] - (mean.size() == 4 ? mean[i] : 0.0);
+      r += d * d;
+      if (g) (*g)[i] += alpha * d;
+    }
+    return 0.5 * alpha * r;
+  }
+};
+
+HipGISAXSObjectiveFunctionG::HipGISAXSObjectiveFunctionG(const CylinderLatticeSetup& setup,
+                                                         const std::vector<real_t>& counts,
+                                                         const std::vector<unsigned int>& mask)
+    : impl_(new Impl()) {
+  Impl& m = *impl_;
+  m.s = setup;
+  const long npx = (long)setup.nrow * setup.ncol;
+  if (setup.nrow < 1 || setup.ncol < 1 || (long)counts.size() != npx ||
+      (!mask.empty() && (long)mask.size() != npx)) {
+    std::cerr << "hgx: objective: counts/mask do not match the detector size" << std::endl;
+    return;
+  }
+  m.ctx = context();
+  if (!m.ctx) return;
+  const double pi = 3.141592653589793;
+  const double k0 = 2 * pi / (1.23984 / setup.energy_kev);  // src/sim/hipgisaxs_main.cpp:144-158
+  const double ai = setup.alpha_i_deg * pi / 180.0;
+  if (!report(hgx_qgrid_create(m.ctx, setup.ncol, setup.nrow, setup.qy_min, setup.qz_min, setup.qy_max,
+                               setup.qz_max, ai, k0, 0.0, 0.0, &m.grid),
+              "objective q-grid"))
+    return;
+  const double delta = setup.substrate_delta, beta = setup.substrate_beta, thick = 0.0;
+  const int order = -1;
+  m.rowfc.assign(8 * (size_t)setup.nrow, 0.0);
+  if (!report(hgx_propagation_coeffs(m.ctx, m.grid, 1, &delta, &beta, &thick, &order, k0, ai, 0, nullptr,
+                                     m.rowfc.data(), 1),
+              "objective Fresnel coefficients"))
+    return;
+  const int type = setup.lattice == "cubic" ? 3 : setup.lattice == "hex" ? 7 : -1;
+  if (type < 0) {
+    std::cerr << "hgx: objective: lattice must be hex or cubic" << std::endl;
+    return;
+  }
+  m.abc9.assign(9, 0.0);
+  if (!report(hgx_lattice_vectors(type, "100", m.abc9.data(), nullptr), "objective lattice")) return;
+  m.counts = counts;
+  m.mask = mask;
+  m.one = m.make_batch(1);
+  m.good = m.one != nullptr;
+}
+
+HipGISAXSObjectiveFunctionG::~HipGISAXSObjectiveFunctionG() { delete impl_; }
+
+bool HipGISAXSObjectiveFunctionG::ok() const { return impl_->good; }
+
+std::vector<std::string> HipGISAXSObjectiveFunctionG::fit_param_keys() const {
+  return {"radius", "height", "lattice_a", "phi"};
+}
+
+bool HipGISAXSObjectiveFunctionG::set_regularization(real_t alpha) {
+  impl_->alpha = alpha;
+  return true;
+}
+
+bool HipGISAXSObjectiveFunctionG::set_param_mean(const real_vec_t& mean) {
+  if (mean.size() != 4) return false;
+  impl_->mean = mean;
+  return true;
+}
+
+unsigned int HipGISAXSObjectiveFunctionG::data_size() const {
+  return (unsigned)(impl_->s.nrow * impl_->s.ncol);
+}
+
+bool HipGISAXSObjectiveFunctionG::value_and_gradient(const real_vec_t& x, real_t& f, real_vec_t& g) {
+  Impl& m = *impl_;
+  if (!m.good || x.size() != 4) return false;
+  double mb[16], out[5];
+  m.model(x, mb);
+  if (!report(hgx_cyl_batch_eval(m.one, mb, out), "objective value_and_gradient")) return false;
+  g.assign(out + 1, out + 5);
+  f = out[0] + m.reg(x, &g);
+  return true;
+}
+
+real_vec_t HipGISAXSObjectiveFunctionG::operator()(const real_vec_t& x) {
+  real_t f = 0.0;
+  real_vec_t g;
+  if (!value_and_gradient(x, f, g) || !std::isfinite(f)) f = 1e8;  // the reference's stand-in
+  return real_vec_t(1, f);
+}
+
+bool HipGISAXSObjectiveFunctionG::evaluate(const std::vector<real_vec_t>& population, real_vec_t& f,
+                                           std::vector<real_vec_t>& g) {
+  Impl& m = *impl_;
+  const int n = (int)population.size();
+  if (!m.good || n < 1) return false;
+  for (const auto& x : population)
+    if (x.size() != 4) return false;
+  if (m.pop_n != n) {
+    if (m.pop) hgx_cyl_batch_destroy(m.pop);
+    m.pop = m.make_batch(n);
+    m.pop_n = m.pop ? n : 0;
+    if (!m.pop) return false;
+  }
+  std::vector<double> mb(16 * (size_t)n), out(5 * (size_t)n);
+  for (int i = 0; i < n; ++i) m.model(population[i], mb.data() + 16 * i);
+  if (!report(hgx_cyl_batch_eval(m.pop, mb.data(), out.data()), "objective evaluate")) return false;
+  f.resize(n);
+  g.assign(n, real_vec_t());
+  for (int i = 0; i < n; ++i) {
+    g[i].assign(out.begin() + 5 * i + 1, out.begin() + 5 * i + 5);
+    f[i] = out[5 * i] + m.reg(population[i], &g[i]);
+  }
+  return true;
+}
+
+bool HipGISAXSObjectiveFunctionG::simulate(const real_vec_t& x, real_vec_t& intensity) {
+  Impl& m = *impl_;
+  if (!m.good || x.size() != 4) return false;
+  double mb[16];
+  m.model(x, mb);
+  intensity.assign((size_t)m.s.nrow * m.s.ncol, 0.0);
+  return report(hgx_cyl_batch_forward(m.one, mb, intensity.data()), "objective simulate");
 }
 
 }  // namespace hig

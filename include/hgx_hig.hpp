@@ -31,6 +31,7 @@ namespace hig {
 
 typedef double real_t;                    // include/common/typedefs.hpp:47-65 (DOUBLEP)
 typedef std::complex<real_t> complex_t;
+typedef std::vector<real_t> real_vec_t;   // include/common/typedefs.hpp:66
 struct cucomplex_t {                      // layout of cuDoubleComplex
   double x, y;
 };
@@ -189,4 +190,72 @@ class StructureFactorG {
 
 }  // namespace hig
 #endif  // HGX_IN_REFERENCE_TREE
+
+namespace hig {
+
+// ---------------------------------------------------------- fitting front end ----
+// The objective of the reference's fitters (HipGISAXSObjectiveFunction,
+// include/analyzer/objective_func_hipgisaxs.hpp; operator() at
+// src/analyzer/objective_func_hipgisaxs.cpp:245-333) for one model family — cylinders on a
+// 2-D lattice over a substrate, in DWBA — evaluated on the GPU, with the two calls the
+// reference's fitters lack: the gradient by a hand-written adjoint (in place of LMVM's
+// central differences, src/analyzer/hipgisaxs_fit_lmvm.cpp:190-223) and a whole population
+// in one graph-captured launch (in place of PSO's one-particle-at-a-time loop,
+// src/analyzer/hipgisaxs_fit_pso.cpp:521-545).  A new class: the reference's own
+// HipGISAXSObjectiveFunction reads a HiG file and runs the full simulator.
+//
+// Fit parameters x = (radius, height, lattice constant, in-plane rotation phi [radians]).
+// Distance: chi^2 = sum mask (scale I(x) - counts)^2 / max(counts, 1), plus the reference's
+// regularisation (alpha/2) ||x - x_mean||^2 (objective_func_hipgisaxs.cpp:296-311).
+struct CylinderLatticeSetup {
+  int ncol = 1024, nrow = 1024;                       // detector pixels
+  real_t qy_min = -2.0, qz_min = 0.0, qy_max = 2.0, qz_max = 3.0;  // 1/nm
+  real_t alpha_i_deg = 0.20, energy_kev = 10.0;
+  real_t substrate_delta = 4.88e-6, substrate_beta = 7.37e-8;
+  std::string lattice = "hex";                        // "hex" or "cubic" (a, b in the plane)
+  real_t repet[3] = {20, 20, 1};
+  real_t spread = 0.05;                               // relative Gaussian size spread
+  int nsamples = 11;                                  // size samples over +-3 spread
+  bool smooth_sampling = true;                        // evenly spaced samples (smooth chi^2)
+  real_t dn2[2] = {-2 * 4.88e-6, -2 * 7.37e-8};       // particle contrast (complex)
+  real_t center[3] = {0, 0, 0};
+  real_t weight = 1.0;
+  real_t scale = 1.0;                                 // model-to-counts factor of the chi^2
+  bool fp64 = false;                                  // plain FP64 instead of FP32C
+};
+
+class HipGISAXSObjectiveFunctionG {
+ public:
+  // counts: nrow x ncol measured image (row 0 = top, as QGrid orders rows); mask: same
+  // size of 0/1, or empty for none.
+  HipGISAXSObjectiveFunctionG(const CylinderLatticeSetup& setup, const std::vector<real_t>& counts,
+                              const std::vector<unsigned int>& mask = std::vector<unsigned int>());
+  ~HipGISAXSObjectiveFunctionG();
+  HipGISAXSObjectiveFunctionG(const HipGISAXSObjectiveFunctionG&) = delete;
+  HipGISAXSObjectiveFunctionG& operator=(const HipGISAXSObjectiveFunctionG&) = delete;
+
+  bool ok() const;                                    // false when set-up failed
+  // the reference's call: the distance vector (one element: chi^2 + regularisation); a
+  // non-finite distance becomes 1e8 as in the reference
+  real_vec_t operator()(const real_vec_t& x);
+  // distance and its gradient with respect to x
+  bool value_and_gradient(const real_vec_t& x, real_t& f, real_vec_t& g);
+  // distances and gradients of a population in one launch
+  bool evaluate(const std::vector<real_vec_t>& population, real_vec_t& f,
+                std::vector<real_vec_t>& g);
+  // the model image at x (nrow x ncol)
+  bool simulate(const real_vec_t& x, real_vec_t& intensity);
+
+  int num_fit_params() const { return 4; }
+  std::vector<std::string> fit_param_keys() const;
+  bool set_regularization(real_t alpha);
+  bool set_param_mean(const real_vec_t& mean);        // x_mean of the regularisation
+  unsigned int data_size() const;
+
+ private:
+  struct Impl;
+  Impl* impl_;
+};
+
+}  // namespace hig
 #endif  // HGX_HIG_HPP
