@@ -29,6 +29,21 @@ def test_dropin_compiles_and_links(tmp_path):
     assert os.path.exists(_build(tmp_path))
 
 
+def test_dropin_compiles_inside_reference_tree():
+    """hig_dropin.cpp against the reference's own class declarations (-DHGX_IN_REFERENCE_TREE),
+    by the oracle Makefile's recipe; skipped where the reference sources are absent."""
+    env = dict(os.environ)
+    env.pop("CC", None)
+    env.pop("CXX", None)
+    ref = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                         capture_output=True, text=True, env=env).stdout.strip()
+    if not ref or not os.path.isdir(os.path.join(ref, "include")):
+        pytest.skip("reference sources not present")
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "dropin-check"],
+                       capture_output=True, text=True, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 @pytest.mark.gpu
 def test_dropin_matches_oracle(ctx, po, tmp_path):
     exe = _build(tmp_path)
