@@ -47,6 +47,22 @@ TRAFFIC_BYTES_PER_LAUNCH = 115.8e6
 TRAFFIC_SOURCE = "ncu capture at 1536x1536 (65.1 MB) scaled by pixels to 2048x2048"
 
 
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks (the slowest replica's time); x itself without a process
+    group.  Every rank must call it at the same point."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, units_per_rank, seconds_max):
+    """Whole-job rate of independent replicas: all ranks' units over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
+
+
 def k0_from_kev(e):
     return 2 * PI_REF / (1.23984 / e)
 
@@ -439,13 +455,9 @@ def main():
     barrier()
     clocks = clk.stop()
     ctx.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = ms / args.steps
-    value = world * evals * args.steps / (ms * 1e-3)
+    value = job_throughput(world, evals * args.steps, ms * 1e-3)
 
     # end to end through the reference-shaped C-ABI call with host (pinned) buffers
     e2e = None
@@ -466,12 +478,8 @@ def main():
             hg.ff_triangles_arrays(ctx, h_sd, h_qx, h_qy, h_qz, None, "f32c", out=h_out)
         b1.record(stream)
         torch.cuda.synchronize()
-        mse = b0.elapsed_time(b1) / k
-        if dist is not None:
-            t = torch.tensor([mse], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            mse = float(t.item())
-        e2e = {"value": world * evals / (mse * 1e-3), "unit": "evals/s",
+        mse = max_over_ranks(b0.elapsed_time(b1) / k, dist, dev)
+        e2e = {"value": job_throughput(world, evals, mse * 1e-3), "unit": "evals/s",
                "h2d_bytes_per_step": int(sd.nbytes + 2 * 8 * n + 16 * 4 * n),
                "d2h_bytes_per_step": int(16 * 4 * n), "ms_per_step": mse,
                "path": "hgx_ff_triangles (reference-shaped, host buffers, complex128 out)"}
