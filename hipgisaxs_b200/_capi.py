@@ -60,6 +60,11 @@ SIGNATURES = {
     "hgx_cyl_batch_set_shape": (_i, [_vp, _i]),
     "hgx_cyl_batch_get_shape": (_i, [_vp, C.POINTER(_i)]),
     "hgx_cyl_batch_tune": (_i, [_vp, _vp, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
+    "hgx_obj_load": (_i, [C.c_char_p, C.POINTER(_vp)]),
+    "hgx_mesh_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "hgx_mesh_read": (_i, [_vp, _vp, _vp]),
+    "hgx_mesh_destroy": (_i, [_vp]),
+    "hgx_read_shapes_file": (_i, [_vp, C.c_char_p, _vp, _i, C.POINTER(_i)]),
     "hgx_mesh_to_shape_def": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "hgx_mesh_chi2_grad": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
                                 _vp, _vp, _vp]),

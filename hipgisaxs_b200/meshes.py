@@ -143,3 +143,47 @@ def shape_def_from_mesh(V, F, keep_degenerate: bool = False):
     if not keep_degenerate:
         out = out[ok]
     return np.ascontiguousarray(out)
+
+
+def write_obj(path, verts, faces):
+    """Writes a mesh as Wavefront OBJ (1-based faces)."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+    with open(path, "w") as fh:
+        for x in v:
+            fh.write(f"v {x[0]:.17g} {x[1]:.17g} {x[2]:.17g}\n")
+        for t in f:
+            fh.write(f"f {t[0] + 1} {t[1] + 1} {t[2] + 1}\n")
+
+
+def load_obj(path):
+    """hgx_obj_load: (vertices[nv, 3], faces[nf, 3] 0-based, info) of an OBJ file; info has
+    the counts of 4-vertex faces left out (nquads) and larger faces skipped (nskipped)."""
+    import ctypes as C
+
+    from ._capi import check, lib
+    h = C.c_void_p()
+    check(lib().hgx_obj_load(str(path).encode(), C.byref(h)))
+    try:
+        nv, nf, nq, ns = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().hgx_mesh_info(h, C.byref(nv), C.byref(nf), C.byref(nq), C.byref(ns)))
+        v = np.zeros((nv.value, 3))
+        f = np.zeros((nf.value, 3), dtype=np.int32)
+        check(lib().hgx_mesh_read(h, v.ctypes.data, f.ctypes.data))
+    finally:
+        lib().hgx_mesh_destroy(h)
+    return v, f, {"nquads": nq.value, "nskipped": ns.value}
+
+
+def read_shapes_file(ctx, path):
+    """hgx_read_shapes_file: the (T, 8) shape_def of an .obj or raw .dat shape file (ctx may be
+    None for .dat files)."""
+    import ctypes as C
+
+    from ._capi import check, lib
+    h = None if ctx is None else ctx.handle
+    n = C.c_int()
+    check(lib().hgx_read_shapes_file(h, str(path).encode(), None, 0, C.byref(n)))
+    out = np.zeros((n.value, 8))
+    check(lib().hgx_read_shapes_file(h, str(path).encode(), out.ctypes.data, n.value, C.byref(n)))
+    return out

@@ -244,6 +244,31 @@ int hgx_cyl_batch_get_shape(hgx_cyl_batch b, int* shape);
 int hgx_cyl_batch_tune(hgx_cyl_batch b, const double* models, int reps, int* best_shape,
                        double* best_ms, double* times_ms);
 
+/* --------------------------------------------------------- shape-definition files ---- */
+/* Wavefront OBJ meshes without Boost (ObjectShapeReader::load_object,
+ * src/file/objectshape_reader.cpp:52-242): vertices ("v") and faces ("f" with items v, v/vt,
+ * v/vt/vn or v//vn, 1-based); other lines are ignored.  Triangles are kept in file order with
+ * 0-based indices; 4-vertex faces are counted (nquads) and left out, as the reference's
+ * converter leaves them out; larger faces are counted (nskipped).  Differences from the
+ * reference: lines of any length, tabs as separators, and a malformed, relative or
+ * out-of-range index returns HGX_ERR_INVALID_ARG instead of undefined behaviour.  Host only. */
+typedef struct hgx_mesh_s* hgx_mesh;
+int hgx_obj_load(const char* path, hgx_mesh* out);
+int hgx_mesh_info(hgx_mesh m, int* nv, int* nf, int* nquads, int* nskipped);
+/* verts: nv x 3 doubles, faces: nf x 3 ints (0-based); either may be NULL. */
+int hgx_mesh_read(hgx_mesh m, double* verts, int* faces);
+int hgx_mesh_destroy(hgx_mesh m);
+/* NumericFormFactor::read_shapes_file (src/ff/ff_num.cpp:985-1030): the shape_def rows
+ * (T x 8: s, n, c, pad) of an .obj file (triangles converted on the device with the
+ * get_triangle_params arithmetic, degenerate faces dropped as convert_to_shape drops them)
+ * or of a raw .dat file (7 values per triangle, RawShapeReader::load_raw).  The format is
+ * chosen by the extension (obj/Obj/OBJ, dat/Dat/DAT); HDF5 files are rejected, as by a
+ * reference build without its optional HDF5 support.  *ntri receives the triangle count;
+ * with shape_def NULL nothing else is written, otherwise shape_def must hold capacity >= *ntri
+ * rows (host memory).  ctx may be NULL for .dat files (no device work). */
+int hgx_read_shapes_file(hgx_ctx ctx, const char* path, double* shape_def, int capacity,
+                         int* ntri);
+
 /* ------------------------------------------------------------ triangle meshes ---- */
 /* ObjectShapeReader::get_triangle_params / convert_to_shape
  * (src/file/objectshape_reader.cpp:248-300) on the device: vertices nv x 3, faces nf x 3
