@@ -316,6 +316,98 @@ int orc_ff_approx_triangle(const double* sd, int ntri, int nqy, const double* qx
   return ntri;
 }
 
+/* FormFactorTriangle, src/ff/cpu/ff_tri_cpu.cpp:46-153: the exact Fourier transform of one
+ * triangle (vertices v1, v2, v3) at the rotated q-vector m, reduced to edges and vertices. */
+static double vabs3(const double* v) {
+  double n = 0.;
+  for (int i = 0; i < 3; ++i) n += v[i] * v[i];
+  return sqrt(n);
+}
+static void vcross3(const double* u, const double* v, double* w) {
+  w[0] = u[1] * v[2] - u[2] * v[1];
+  w[1] = u[2] * v[0] - u[0] * v[2];
+  w[2] = u[0] * v[1] - u[1] * v[0];
+}
+static cplx cdot3(const cplx* m, const double* v) {
+  cplx r = 0;
+  for (int i = 0; i < 3; ++i) r += rs(m[i], v[i]);
+  return r;
+}
+static cplx ff_triangle_exact(const cplx* m, const double* tri) {
+  const cplx unitc = cx(0.0, 1.0), n_unitc = cx(0.0, -1.0);
+  cplx ff = 0;
+  double q_sqr = 0.;
+  for (int i = 0; i < 3; ++i) q_sqr += cnorm(m[i]);
+  const double* vertex[3] = {tri, tri + 3, tri + 6};
+  double edge[3][3];
+  for (int i = 0; i < 3; ++i) {
+    edge[0][i] = vertex[1][i] - vertex[0][i];
+    edge[1][i] = vertex[2][i] - vertex[1][i];
+    edge[2][i] = vertex[0][i] - vertex[2][i];
+  }
+  double n_t[3];
+  vcross3(edge[0], edge[1], n_t);
+  double nabs = vabs3(n_t);
+  double t_area = 0.5 * nabs;
+  for (int i = 0; i < 3; ++i) n_t[i] = n_t[i] / nabs;
+  cplx q_dot_nt = cdot3(m, n_t);
+  double proj_tq = q_sqr - cnorm(q_dot_nt);
+  if (fabs(proj_tq) < TINY_REF) {  /* case 1 */
+    cplx q_dot_v = cdot3(m, vertex[0]);
+    return rdiv(rs(unitc * q_dot_nt, t_area), q_sqr) * cexp(n_unitc * q_dot_v);
+  }
+  for (int e = 0; e < 3; ++e) {
+    double n_e[3];
+    vcross3(edge[e], n_t, n_e);
+    double ea = vabs3(n_e);
+    for (int i = 0; i < 3; ++i) n_e[i] = n_e[i] / ea;
+    cplx q_dot_ne = cdot3(m, n_e);
+    double proj_eq = proj_tq - cnorm(q_dot_ne);
+    if (fabs(proj_eq) < TINY_REF) {  /* case 2 */
+      cplx q_dot_v = cdot3(m, vertex[e]);
+      double f0 = vabs3(edge[e]) / (q_sqr * proj_tq);
+      cplx c0 = -q_dot_nt * q_dot_ne;
+      cplx c1 = cexp(n_unitc * q_dot_v);
+      ff += rs(c0, f0) * c1;
+    } else {  /* case 3 */
+      double f0 = q_sqr * proj_tq * proj_eq;
+      cplx q_dot_v = cdot3(m, vertex[e]);
+      double el = vabs3(edge[e]);
+      double n_v[3] = {edge[e][0] / el, edge[e][1] / el, edge[e][2] / el};
+      cplx q_dot_nv = cdot3(m, n_v);
+      cplx c0 = n_unitc * q_dot_nt * q_dot_ne * q_dot_nv;
+      cplx c1 = cexp(n_unitc * q_dot_v);
+      ff += rdiv(c0 * c1, f0);
+      int ep = (e + 1) % 3;
+      q_dot_v = cdot3(m, vertex[ep]);
+      q_dot_nv = 0;
+      for (int i = 0; i < 3; ++i) q_dot_nv -= rs(m[i], n_v[i]);
+      c0 = n_unitc * q_dot_nt * q_dot_ne * q_dot_nv;
+      c1 = cexp(n_unitc * q_dot_v);
+      ff += rdiv(c0 * c1, f0);
+    }
+  }
+  return ff;
+}
+
+/* NumericFormFactorC::compute_exact_triangle, src/ff/cpu/ff_tri_cpu.cpp:157-196:
+ * tris: ntri x 9 doubles (v1, v2, v3, triangle_t of include/common/typedefs.hpp:102-106). */
+int orc_ff_exact_triangle(const double* tris, int ntri, int nqy, const double* qx,
+                          const double* qy, int nqz, const double* qz, const double* rot9,
+                          double* ff) {
+  if (ntri < 1) return 0;
+#pragma omp parallel for schedule(static)
+  for (int iz = 0; iz < nqz; ++iz) {
+    int iy = iz % nqy;
+    cplx m[3];
+    rotate(rot9, qx[iy], qy[iy], ld(qz, iz), m);
+    cplx acc = 0;
+    for (int t = 0; t < ntri; ++t) acc += ff_triangle_exact(m, tris + 9L * t);
+    st(ff, iz, acc);
+  }
+  return ntri;
+}
+
 /* src/file/objectshape_reader.cpp:275-300 */
 int orc_triangle_params(const double* v1, const double* v2, const double* v3, double* s,
                         double* n, double* c) {

@@ -49,6 +49,11 @@ void orc_rot_mul(const double* a, const double* b, double* out);
 int orc_ff_approx_triangle(const double* shape_def, int ntri, int nqy, const double* qx,
                            const double* qy, int nqz, const double* qz, const double* rot9,
                            double* ff);
+/* NumericFormFactorC::compute_exact_triangle (src/ff/cpu/ff_tri_cpu.cpp:46-196): tris is
+ * ntri x 9 (v1, v2, v3); ff nqz complex. */
+int orc_ff_exact_triangle(const double* tris, int ntri, int nqy, const double* qx,
+                          const double* qy, int nqz, const double* qz, const double* rot9,
+                          double* ff);
 /* ObjectShapeReader::get_triangle_params, src/file/objectshape_reader.cpp:275-300.
  * Returns 0 for a degenerate triangle (dropped by the reference). */
 int orc_triangle_params(const double* v1, const double* v2, const double* v3, double* s,

@@ -149,6 +149,32 @@ def ff_approx_triangle(shape_def, qx, qy, qz, rot=None, backend="port"):
     return out
 
 
+def ff_exact_triangle(tris, qx, qy, qz, rot=None, backend="port"):
+    """NumericFormFactorC::compute_exact_triangle on explicit arrays; tris: (T, 9) vertices
+    (v1, v2, v3) of each triangle."""
+    L = lib(backend)
+    tv = np.ascontiguousarray(tris, dtype=np.float64).reshape(-1, 9)
+    qx = np.ascontiguousarray(qx, dtype=np.float64)
+    qy = np.ascontiguousarray(qy, dtype=np.float64)
+    qz, qzf = _cbuf(qz)
+    r = np.ascontiguousarray(np.eye(3) if rot is None else rot, dtype=np.float64).reshape(9)
+    out = np.zeros(len(qz), dtype=np.complex128)
+    f = L.orc_ff_exact_triangle if backend == "port" else L.ref_ff_exact_triangle
+    rc = f(_p(tv), C.c_int(len(tv)), C.c_int(len(qx)), _p(qx), _p(qy), C.c_int(len(qz)),
+           _p(qzf), _p(r), _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"ff_exact_triangle failed rc={rc}")
+    return out
+
+
+def mesh_triangles(verts, faces):
+    """(T, 9) vertex triples of a mesh, as NumericFormFactor::compute2 builds triangle_t from
+    an OBJ mesh (src/ff/ff_num.cpp:66-80)."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(faces).reshape(-1, 3)
+    return np.ascontiguousarray(v[f].reshape(-1, 9))
+
+
 def mesh_to_shape_def(verts, faces):
     L = lib("port")
     v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)

@@ -185,6 +185,34 @@ int ref_ff_approx_triangle(const double* shape_def, int ntri, int nqy, const dou
   return (int)r;
 }
 
+int ref_ff_exact_triangle(const double* tris, int ntri, int nqy, const double* qx,
+                          const double* qy, int nqz, const double* qz, const double* rot9,
+                          double* ff) {
+  std::vector<triangle_t> tv(ntri);
+  for (int t = 0; t < ntri; ++t)
+    for (int k = 0; k < 3; ++k) {
+      tv[t].v1[k] = tris[9 * t + k];
+      tv[t].v2[k] = tris[9 * t + 3 + k];
+      tv[t].v3[k] = tris[9 * t + 6 + k];
+    }
+  std::vector<complex_t> qzc(nqz);
+  for (int i = 0; i < nqz; ++i) qzc[i] = complex_t(qz[2 * i], qz[2 * i + 1]);
+  std::vector<real_t> qxv(qx, qx + nqy), qyv(qy, qy + nqy);
+  RotMatrix_t rot = make_rot(rot9);
+  NumericFormFactorC cff;
+  complex_t* out = nullptr;
+  real_t t = 0;
+  unsigned r = cff.compute_exact_triangle(tv.data(), ntri, out, nqy, qxv.data(), qyv.data(), nqz,
+                                          qzc.data(), rot, t);
+  if (r == 0 || out == nullptr) return -1;
+  for (int i = 0; i < nqz; ++i) {
+    ff[2 * i] = out[i].real();
+    ff[2 * i + 1] = out[i].imag();
+  }
+  delete[] out;
+  return (int)r;
+}
+
 // AnalyticFormFactor::compute on the current singleton grid (extended qz).
 // params: nparam entries of (type, stat, min, max, mean, deviation, nvalues) as doubles.
 int ref_ff_analytic(int shape, int nparam, const double* params, double tau, double eta,

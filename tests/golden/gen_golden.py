@@ -91,8 +91,33 @@ def main():
             np.savez_compressed(os.path.join(HERE, f"fc_{lname}_{gname}.npz"),
                                 layers=np.array(layers, dtype=float), order=order, fc=fc,
                                 grid=gname)
+    exact_fixtures()
     print("golden fixtures written to", HERE)
 
 
+def exact_fixtures():
+    """The exact triangle form factor (NumericFormFactorC::compute_exact_triangle): a jittered
+    80-face icosphere plus 20 random triangles, on both grids, unrotated and rotated."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from hipgisaxs_b200 import meshes
+    rng = np.random.default_rng(20240605)
+    V, F = meshes.icosphere(6.0, 1)
+    V = V + rng.normal(scale=0.2, size=V.shape)
+    tris = np.vstack([po.mesh_triangles(V, F), rng.normal(scale=5.0, size=(20, 9))])
+    rots = {"id": np.eye(3),
+            "r3": po.rot_mul(po.rot_mul(po.rot_axis(2, 0.35), po.rot_axis(0, 0.12)),
+                             po.rot_axis(1, -0.2))}
+    for gname in ("g16", "g16abs"):
+        g = np.load(os.path.join(HERE, f"qgrid_{gname}.npz"))
+        for rname, R in rots.items():
+            ff = po.ff_exact_triangle(tris, g["qx"], g["qy"], g["qz_ext"], R, "ref")
+            np.savez_compressed(os.path.join(HERE, f"ffexact_{gname}_{rname}.npz"), tris=tris,
+                                rot=R, ff=ff, grid=gname)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["exact"]:
+        po.set_threads(4, "ref")
+        exact_fixtures()
+    else:
+        main()

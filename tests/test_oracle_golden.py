@@ -31,6 +31,14 @@ def test_ff_triangles(po, golden, golden_grid, name):
     np.testing.assert_allclose(ff, d["ff"], rtol=1e-13, atol=1e-13 * np.abs(d["ff"]).max())
 
 
+@pytest.mark.parametrize("name", _names("ffexact_"))
+def test_ff_exact_triangles(po, golden, golden_grid, name):
+    d = golden(name)
+    G, _ = golden_grid(str(d["grid"]))
+    ff = po.ff_exact_triangle(d["tris"], G.qx, G.qy, G.qz_ext, d["rot"], "port")
+    np.testing.assert_allclose(ff, d["ff"], rtol=1e-13, atol=1e-13 * np.abs(d["ff"]).max())
+
+
 @pytest.mark.parametrize("name", _names("ffana_"))
 def test_ff_analytic(po, golden, golden_grid, name):
     d = golden(name)
