@@ -4,9 +4,12 @@ The hot path of the reference simulator (tacaswell/hipgisaxs) — the triangulat
 form factor, the analytic form factors, the lattice structure factor and the four-term
 DWBA combination — as hand-written CUDA kernels behind a C ABI (include/hgx.h,
 libhgx.so).  This Python package is a thin host-side mirror of that ABI; the C++ drop-in
-classes with the reference's signatures live in csrc/hig/.
+classes with the reference's signatures are declared in include/hgx_hig.hpp and implemented
+in csrc/hig_dropin.cpp.
 """
 from ._capi import HgxError, lib  # noqa: F401
-from .core import Context, QGrid, ff_triangles, ff_triangles_arrays, ff_tune, measure_peaks  # noqa: F401
+from .core import (Context, QGrid, ff_exact_triangles, ff_triangles,  # noqa: F401
+                   ff_triangles_arrays, ff_tune, measure_peaks)
 
-__all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "ff_tune", "HgxError", "lib"]
+__all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "ff_exact_triangles",
+           "ff_tune", "HgxError", "lib"]

@@ -39,6 +39,8 @@ SIGNATURES = {
     "hgx_ff_triangles_q_ex": (_i, [_vp, _vp, _vp, _i, _vp, _i, _vp, _i, _i]),
     "hgx_ff_tune": (_i, [_vp, _vp, _vp, _i, _vp, _i, _i, C.POINTER(_i), C.POINTER(_d), _vp]),
     "hgx_ff_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp]),
+    "hgx_ff_exact_triangles_q": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i]),
+    "hgx_ff_exact_triangles": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp]),
     "hgx_param_distribution": (_i, [_i, _d, _d, _d, _d, _i, _vp, _vp, _i, C.POINTER(_i)]),
     "hgx_ff_analytic": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp,
                              _vp, _d, _d, _vp, _vp, _vp, _i]),

@@ -30,6 +30,12 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+# per-file extra flags.  ff_exact.cu: the exact triangle form factor follows the reference's
+# FP64 arithmetic without fused multiply-adds, because its edge and vertex terms cancel and
+# amplify any difference in rounding.
+FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"]}
+
+
 def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
                   if f.endswith(".cu") or f.endswith(".cpp"))
@@ -57,7 +63,8 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _needs(obj, [src] + headers):
-            cmd = [nvcc(), "-ccbin", "g++"] + flags + ["-c", src, "-o", obj]
+            cmd = [nvcc(), "-ccbin", "g++"] + flags + FILE_FLAGS.get(os.path.basename(src), []) + \
+                ["-c", src, "-o", obj]
             jobs.append(cmd)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         futs = {ex.submit(subprocess.run, cmd, capture_output=True, text=True, env=env): cmd

@@ -167,6 +167,21 @@ def ff_triangles(ctx: Context, grid: QGrid, shape_def, rot=None, precision="f32c
     return out
 
 
+def ff_exact_triangles(ctx: Context, grid: QGrid, tris, rot=None, out=None, out_type="c128"):
+    """Exact (polyhedral) triangle form factor on `grid` (hgx_ff_exact_triangles_q), FP64.
+
+    tris: (T, 9) float64 vertex triples (v1, v2, v3).  Returns `out`."""
+    pt, kt = _in(tris, np.float64)
+    ntri = int((kt.numel() if _is_tensor(kt) else kt.size) // 9)
+    r = _rot_arg(rot)
+    ct = CTYPE[out_type]
+    if out is None:
+        out = np.zeros(grid.nqz, dtype=np.complex64 if ct == C64 else np.complex128)
+    pout = out.data_ptr() if _is_tensor(out) else out.ctypes.data
+    check(lib().hgx_ff_exact_triangles_q(ctx.handle, grid.handle, pt, ntri, r.ctypes.data, pout, ct))
+    return out
+
+
 TUNE_CANDIDATES = (4, 2, 1, -2, -4, -8)
 
 

@@ -224,6 +224,37 @@ unsigned int NumericFormFactorG::compute_approx_triangle(std::vector<real_t>& sh
   return ntri;
 }
 
+// The exact triangle form factor (NumericFormFactor::compute2's path): FP64 always, as the
+// reference computes it; the triangles are the reference's triangle_t (9 reals each).
+unsigned int NumericFormFactorG::compute_exact_triangle(triangle_t* triangles, int num_triangles,
+                                                        cucomplex_t*& ff, int nqy, real_t* qx,
+                                                        real_t* qy, int nqz, cucomplex_t* qz,
+                                                        RotMatrix_t& rot, real_t& kernel_time) {
+  hgx_ctx c = context();
+  if (!c || !triangles || num_triangles < 1) return 0;
+  std::vector<double> tris(9 * (size_t)num_triangles);
+  for (int t = 0; t < num_triangles; ++t)
+    for (int k = 0; k < 3; ++k) {
+      tris[9 * t + k] = triangles[t].v1[k];
+      tris[9 * t + 3 + k] = triangles[t].v2[k];
+      tris[9 * t + 6 + k] = triangles[t].v3[k];
+    }
+  double r9[9];
+  rot_to_r9(rot, r9);
+  ff = new (std::nothrow) cucomplex_t[nqz];
+  if (!ff) return 0;
+  auto t0 = std::chrono::steady_clock::now();
+  int s = hgx_ff_exact_triangles(c, tris.data(), num_triangles, nqy, qx, qy, nqz,
+                                 reinterpret_cast<const double*>(qz), r9, reinterpret_cast<double*>(ff));
+  kernel_time = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (!report(s, "compute_exact_triangle")) {
+    delete[] ff;
+    ff = nullptr;
+    return 0;
+  }
+  return (unsigned)num_triangles;
+}
+
 // -------------------------------------------------------- AnalyticFormFactorG ----
 AnalyticFormFactorG::AnalyticFormFactorG(unsigned int nqy, unsigned int nqz) { init(nqy, nqz); }
 AnalyticFormFactorG::AnalyticFormFactorG() {}

@@ -117,6 +117,21 @@ int hgx_ff_triangles(hgx_ctx ctx, const double* shape_def, int ntri, int nqy, co
                      const double* qy, int nqz, const double* qz, const double* rot9,
                      int precision, double* ff);
 
+/* The exact (polyhedral) triangle form factor: FormFactorTriangle and
+ * NumericFormFactorC::compute_exact_triangle (src/ff/cpu/ff_tri_cpu.cpp:46-196), the path of
+ * NumericFormFactor::compute2 (src/ff/ff_num.cpp:47-178); GPU twin
+ * NumericFormFactorG::compute_exact_triangle (src/ff/gpu/ff_tri_gpu.cu:46-205, 210-...).
+ * tris: ntri x 9 doubles (v1, v2, v3 — triangle_t, include/common/typedefs.hpp:102-106),
+ * rot9 as above (NULL = identity), FP64 throughout, the reference's sign convention
+ * (e^{-i q.v}) and case thresholds.  A degenerate (zero-area) triangle contributes nothing;
+ * the reference divides by zero there.  ff: nqz complex of type ff_type. */
+int hgx_ff_exact_triangles_q(hgx_ctx ctx, hgx_qgrid g, const double* tris, int ntri,
+                             const double* rot9, void* ff, int ff_type);
+/* The reference-shaped call: explicit q arrays, complex128 output, synchronous. */
+int hgx_ff_exact_triangles(hgx_ctx ctx, const double* tris, int ntri, int nqy, const double* qx,
+                           const double* qy, int nqz, const double* qz, const double* rot9,
+                           double* ff);
+
 /* ------------------------------------------------------- analytic form factors ---- */
 /* AnalyticFormFactor::param_distribution (src/ff/ff_ana.cpp:235-284): the sample values
  * and weights of one shape parameter.  stat: StatisticType (0 null, 2 none, 4 gaussian,

@@ -32,6 +32,11 @@ namespace hig {
 typedef double real_t;                    // include/common/typedefs.hpp:47-65 (DOUBLEP)
 typedef std::complex<real_t> complex_t;
 typedef std::vector<real_t> real_vec_t;   // include/common/typedefs.hpp:66
+typedef struct Triangle {                 // include/common/typedefs.hpp:102-106
+  real_t v1[3];
+  real_t v2[3];
+  real_t v3[3];
+} triangle_t;
 struct cucomplex_t {                      // layout of cuDoubleComplex
   double x, y;
 };
@@ -113,6 +118,9 @@ class NumericFormFactorG {
   NumericFormFactorG(int, int, int) {}
   NumericFormFactorG() {}
   ~NumericFormFactorG() {}
+  unsigned int compute_exact_triangle(triangle_t* triangles, int num_triangles, cucomplex_t*& ff,
+                                      int nqy, real_t* qx, real_t* qy, int nqz, cucomplex_t* qz,
+                                      RotMatrix_t& rot, real_t& kernel_time);
   unsigned int compute_approx_triangle(std::vector<real_t>& shape_def, cucomplex_t*& ff, int nqy,
                                        real_t* qx, real_t* qy, int nqz, cucomplex_t* qz,
                                        RotMatrix_t& rot, real_t& kernel_time);

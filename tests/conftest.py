@@ -26,6 +26,39 @@ def _ensure_built():
 _ensure_built()
 
 
+def assert_exact_ff_close(po, got, tris, qx, qy, qz, rot=None, extra=0.0):
+    """Parity check of the exact (polyhedral) triangle form factor, point by point.  The
+    reference's formula adds edge and vertex terms of size O(1/(|q|^2 proj_t proj_e)) that
+    cancel to O(area) — at small |q| the cancellation is severe, so the reference's own result
+    moves by up to O(1) under a relative 1e-15 change of its inputs (its conditioning, not an
+    error of either implementation).  Each q-point may therefore differ from the oracle by 10x
+    the oracle's own spread under four seeded 1e-15 relative perturbations (two of the vertex
+    coordinates, two of the q-vectors), plus 1e-12 (plus `extra`, e.g. an output rounding)
+    times the rms of the result.  Returns the fraction of q-points whose spread exceeds 1e-12
+    of the rms."""
+    tris = np.asarray(tris, dtype=np.float64)
+    qx, qy = np.asarray(qx, dtype=np.float64), np.asarray(qy, dtype=np.float64)
+    qz = np.asarray(qz, dtype=np.complex128)
+    ref = po.ff_exact_triangle(tris, qx, qy, qz, rot)
+    spread = np.zeros(len(ref))
+    for seed in range(4):
+        r = np.random.default_rng(seed)
+        if seed < 2:
+            args = (tris * (1.0 + 1e-15 * r.standard_normal(tris.shape)), qx, qy, qz)
+        else:
+            args = (tris, qx * (1.0 + 1e-15 * r.standard_normal(qx.shape)),
+                    qy * (1.0 + 1e-15 * r.standard_normal(qy.shape)),
+                    qz * (1.0 + 1e-15 * r.standard_normal(qz.shape)))
+        spread = np.maximum(spread, np.abs(po.ff_exact_triangle(*args, rot) - ref))
+    rms = np.sqrt(np.mean(np.abs(ref) ** 2))
+    allowed = 10.0 * spread + (1e-12 + extra) * rms
+    err = np.abs(np.asarray(got, dtype=np.complex128) - ref)
+    bad = np.flatnonzero(err > allowed)
+    assert bad.size == 0, (f"{bad.size} of {len(ref)} q-points beyond the bound; worst "
+                           f"{np.max(err[bad] / allowed[bad]):.3g}x at q-point {bad[np.argmax(err[bad] / allowed[bad])]}")
+    return float(np.mean(spread > 1e-12 * rms))
+
+
 @pytest.fixture(scope="session")
 def po():
     import pyoracle

@@ -1,5 +1,5 @@
 // Exercises the drop-in GPU classes with the reference simulator's signatures:
-// NumericFormFactorG::compute_approx_triangle, AnalyticFormFactorG (init + compute_cylinder,
+// NumericFormFactorG::compute_approx_triangle and compute_exact_triangle, AnalyticFormFactorG (init + compute_cylinder,
 // compute_sphere), StructureFactorG (init, compute, get_sf).  Reads raw inputs from a
 // directory, writes raw outputs there; tests/test_gpu_dropin.py compares them with the oracle.
 #include <cstdio>
@@ -53,6 +53,22 @@ int main(int argc, char** argv) {
   if (nt != sd.size() / 8 || !ff) return 3;
   save(d + "/out_ff_tri.bin", reinterpret_cast<double*>(ff), 8 * (size_t)n);
   delete[] ff;
+
+  // exact triangle form factor (triangle_t vertex triples)
+  std::vector<double> tv9 = load(d + "/tris.bin");
+  std::vector<triangle_t> tris(tv9.size() / 9);
+  for (size_t k = 0; k < tris.size(); ++k)
+    for (int j = 0; j < 3; ++j) {
+      tris[k].v1[j] = tv9[9 * k + j];
+      tris[k].v2[j] = tv9[9 * k + 3 + j];
+      tris[k].v3[j] = tv9[9 * k + 6 + j];
+    }
+  cucomplex_t* ffe = nullptr;
+  unsigned ne = nff.compute_exact_triangle(tris.data(), (int)tris.size(), ffe, n, qx.data(), qy.data(),
+                                           4 * n, reinterpret_cast<cucomplex_t*>(ext.data()), rot, t);
+  if (ne != tris.size() || !ffe) return 9;
+  save(d + "/out_ff_exact.bin", reinterpret_cast<double*>(ffe), 8 * (size_t)n);
+  delete[] ffe;
 
   // analytic cylinder and sphere
   AnalyticFormFactorG aff;

@@ -7,7 +7,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, assert_exact_ff_close
 
 SRC = os.path.join(ROOT, "tests", "cpp", "test_dropin.cpp")
 LIBDIR = os.path.join(ROOT, "hipgisaxs_b200")
@@ -62,12 +62,15 @@ def test_dropin_matches_oracle(ctx, po, tmp_path):
     sd[:, 1:4] = nrm / np.linalg.norm(nrm, axis=1)[:, None]
     sd[:, 4:7] = rng.normal(scale=6.0, size=(T, 3))
     sd.tofile(d / "shape_def.bin")
+    tris = rng.normal(scale=4.0, size=(23, 9))
+    tris.tofile(d / "tris.bin")
     env = dict(os.environ, HGX_PRECISION="f64")
     r = subprocess.run([exe, str(d)], capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     rot = po.rot_mul(po.rot_axis(2, 0.3), po.rot_axis(0, 0.1))
     rd = lambda name: np.fromfile(d / name).view(np.complex128)
     assert po.rel_err(rd("out_ff_tri.bin"), po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext, rot)) < 1e-12
+    assert_exact_ff_close(po, rd("out_ff_exact.bin"), tris, G.qx, G.qy, G.qz_ext, rot)
     # the class receives explicit samples (radii 4.5, 5, 5.5; heights 9, 10), summed unweighted;
     # the oracle sums single-size cylinders (going through param_distribution would drop the
     # end values that its stepping lands on exactly)
