@@ -77,6 +77,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--no-fitting", action="store_true")
+    ap.add_argument("--no-exact", action="store_true")
     return ap.parse_args()
 
 
@@ -310,6 +311,52 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
     return out
 
 
+def exact_bench(ctx, torch, stream, sd_mesh, steps=2, n=512):
+    """The exact (polyhedral) triangle form factor, FP64: the 50,000-triangle star mesh on an
+    n x n DWBA detector of the headline's q-range (4 n^2 x 50,000 evaluations), device-resident
+    inputs, CUDA events; beside it the reference's own compute_exact_triangle (oracle/_ref,
+    all host threads) on whole detector rows of the same workload."""
+    import hipgisaxs_b200 as hg
+    from hipgisaxs_b200 import meshes
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    V, F = meshes.star_mesh(15.0, 250, 101, 8, 0.05, meshes.DEFAULT_SEED)
+    tris = po.mesh_triangles(V, F)
+    alpha_i = ALPHA_I_DEG * PI_REF / 180
+    g = hg.QGrid.create(ctx, n, n, QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z, alpha_i, k0_from_kev(ENERGY_KEV))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_tris = torch.tensor(tris, device=dev)
+    out = torch.empty(4 * n * n, dtype=torch.complex128, device=dev)
+    hg.ff_exact_triangles(ctx, g, d_tris, None, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        hg.ff_exact_triangles(ctx, g, d_tris, None, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    evals = 4.0 * n * n * len(tris)
+    res = {"metric": "q.triangle evals/s", "value": evals / (ms * 1e-3), "ms_per_step": ms,
+           "dtype": "f64", "workload": f"star mesh {len(tris)} triangles, {n}x{n} DWBA grid"}
+    if po.available("ref"):
+        r = g.read(qz_det=False, alpha=False)
+        ext = r["qz_ext"].reshape(4, n * n)
+        threads = po.set_threads(os.cpu_count() or 1, "ref")
+        rows = [n // 3, (2 * n) // 3]
+        idx = np.concatenate([np.arange(x * n, (x + 1) * n) for x in rows])
+        t = time.perf_counter()
+        po.ff_exact_triangle(tris, r["qx"][idx], r["qy"][idx], ext[:, idx].ravel(), None, "ref")
+        dt = time.perf_counter() - t
+        cev = 4.0 * len(idx) * len(tris)
+        res["cpu_reference"] = {"value": cev / dt, "cores": threads,
+                                "sample": f"{len(rows)} detector rows x 4 blocks x {len(tris)} "
+                                          f"triangles ({cev:.3e} evals, {dt:.1f} s)"}
+        res["speedup_vs_cpu_reference"] = res["value"] / res["cpu_reference"]["value"]
+    g.close()
+    return res
+
+
 def mesh_grad_bench(ctx, grid, steps=2):
     """Config 3, mesh part: chi^2 and the gradient with respect to all 25,002 x 3 vertex
     coordinates of the 50,000-triangle star mesh on the 2048 x 2048 DWBA detector (forward
@@ -510,6 +557,10 @@ def main():
         fit = fitting_bench(ctx, torch, dev, stream)
         fit["mesh_vertices_2048sq"] = mesh_grad_bench(ctx, grid)
 
+    exact = None
+    if not args.no_exact:
+        exact = exact_bench(ctx, torch, stream, sd)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         g = grid.read(qz_det=False, alpha=False)
@@ -544,6 +595,7 @@ def main():
                          "sfu": {"achieved_gops": sfu_rate, "peak_gops": peak_sfu,
                                  "frac": sfu_rate / peak_sfu}},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
+            "exact_triangle": exact,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
