@@ -802,6 +802,108 @@ int orc_lattice_vectors(int type, const char* hkl, double* a, double* b, double*
 }
 
 /* src/sf/sf.cpp:164-246 */
+/* StructureFactor::paracrystal1d / paracrystal2d_cubic / paracrystal2d_hex,
+ * src/sf/liquid.cpp:29-110, chosen as compute_structure_factor chooses them
+ * (src/sf/sf.cpp:116-151): dims 1, or dims 2 with lattice 3 (cubic) or 7 (hex). */
+int orc_sf_paracrystal(int dims, int lattice, double dx, double dy, double sx, double sy,
+                       double dom, int nqy, const double* qx, const double* qy, int nqz,
+                       double* sf) {
+  if (dims == 1) {
+    double exp_v1 = exp(-2. * dy / dom);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nqz; ++i) {
+      double q = qy[i % nqy];
+      double qysy = sy * q;
+      double exp_v2 = exp(-1.0 * qysy * qysy);
+      double exp_v3 = exp(-0.5 * qysy * qysy);
+      double tmp = (1. - exp_v2 * exp_v1) / (1. - 2. * exp_v3 * exp_v1 * cos(q * dy) + exp_v2 * exp_v1);
+      st(sf, i, cx(sqrt(tmp), 0.));
+    }
+    return nqz;
+  }
+  if (dims != 2 || (lattice != 3 && lattice != 7)) return -1;
+  double exp_v1x = exp(-2. * dx / dom);
+  double exp_v1y = exp(-2. * dy / dom);
+  const double C1 = 0.5 * sqrt(3.);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nqz; ++i) {
+    int j = i % nqy;
+    double x = qx[j], y = qy[j];
+    double qpar = sqrt(x * x + y * y);
+    double s1, s2;
+    if (lattice == 3) {
+      double cos_vx = cos(qpar * dx);
+      double cos_vy = cos(qpar * dy);
+      double qxsx = qpar * sx;
+      double exp_v2x = exp(-1. * qxsx * qxsx);
+      double exp_v3x = exp(-0.5 * qxsx * qxsx);
+      double qysy = qpar * sy;
+      double exp_v2y = exp(-1. * qysy * qysy);
+      double exp_v3y = exp(-0.5 * qysy * qysy);
+      s1 = (1. - exp_v2x * exp_v1x) / (1. - 2. * exp_v3x * exp_v1x * cos_vx + exp_v2x * exp_v1x);
+      s2 = (1. - exp_v2y * exp_v1y) / (1. - 2. * exp_v3y * exp_v1y * cos_vy + exp_v2y * exp_v1y);
+    } else {
+      double qpsx = qpar * sx;
+      double qpsy = qpar * sy;
+      double phi_x = cos(C1 * x * dx + 0.5 * y * dy);
+      double phi_y = cos(y * dy);
+      double exp_v2x = exp(-1. * qpsx * qpsx);
+      double exp_v2y = exp(-1. * qpsy * qpsy);
+      double exp_v3x = exp(-0.5 * qpsx * qpsx);
+      double exp_v3y = exp(-0.5 * qpsy * qpsy);
+      s1 = (1. - exp_v2x * exp_v1x) / (1. - 2. * exp_v3x * exp_v1x * phi_x + exp_v2x * exp_v1x);
+      s2 = (1. - exp_v2y * exp_v1y) / (1. - 2. * exp_v3y * exp_v1y * phi_y + exp_v2y * exp_v1y);
+    }
+    double tmp = fabs(s1 * s2);
+    st(sf, i, cx(sqrt(tmp), 0.));
+  }
+  return nqz;
+}
+
+/* StructureFactor::PYFcn, src/sf/liquid.cpp:112-125 */
+static double py_fcn(double alpha, double beta, double gamma, double x) {
+  double sinx = sin(x);
+  double cosx = cos(x);
+  double x2 = x * x;
+  double x3 = x2 * x;
+  double x4 = x3 * x;
+  double x5 = x4 * x;
+  double t1 = alpha * (sinx - x * cosx) / x2;
+  double t2 = beta * (2 * x * sinx + (2 - x2) * cosx - 2) / x3;
+  double t3 = gamma * (-x4 * cosx + 4 * ((3 * x2 - 6) * cosx + (x3 - 6 * x) * sinx + 6)) / x5;
+  return (t1 + t2 + t3);
+}
+
+/* StructureFactor::percus_yevik, src/sf/liquid.cpp:127-165: dims 2 uses |q_par|, dims 3 |q|
+ * with complex qz (and takes a fourth root, as the reference does); other dims leave zeros. */
+int orc_sf_percus_yevick(double dia, double volf, int dims, int nqy, const double* qx,
+                         const double* qy, int nqz, const double* qz, double* sf) {
+  double tmp0 = pow(1 - volf, 4);
+  double alpha = pow(1 + 2 * volf, 2) / tmp0;
+  double beta = -6 * volf * pow(1 + 0.5 * volf, 2) / tmp0;
+  double gamma = 0.5 * volf * alpha;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nqz; ++i) {
+    int j = i % nqy;
+    double x0 = qx[j], y0 = qy[j];
+    cplx out = 0;
+    if (dims == 2 || dims == 3) {
+      double qval = dims == 2 ? sqrt(x0 * x0 + y0 * y0)
+                              : sqrt(x0 * x0 + y0 * y0 + cnorm(ld(qz, i)));
+      if (qval < 1.0E-06) {
+        out = cx(alpha / 3. + beta / 4. + gamma, 0.);
+      } else {
+        double x = qval * dia;
+        double t = dims == 2 ? 1. / (1 + 24 * volf * py_fcn(alpha, beta, gamma, x) / x)
+                             : 1. / sqrt(1 + 24 * volf * py_fcn(alpha, beta, gamma, x) / x);
+        out = cx(sqrt(t), 0.);
+      }
+    }
+    st(sf, i, out);
+  }
+  return nqz;
+}
+
 int orc_sf_lattice(const double* abc9, const double* repet_in, const double* sc,
                    const double* center, const double* rot9, int nqy, const double* qx,
                    const double* qy, int nqz, const double* qz, double* sf) {

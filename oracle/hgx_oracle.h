@@ -84,6 +84,14 @@ int orc_sf_lattice(const double* abc9, const double* repet, const double* scalin
                    const double* center, const double* rot9, int nqy, const double* qx,
                    const double* qy, int nqz, const double* qz, double* sf);
 
+/* Paracrystal SFs, src/sf/liquid.cpp:29-110 (dims 1; dims 2 with lattice 3 cubic / 7 hex). */
+int orc_sf_paracrystal(int dims, int lattice, double dx, double dy, double sx, double sy,
+                       double dom, int nqy, const double* qx, const double* qy, int nqz,
+                       double* sf);
+/* Percus-Yevick SF, src/sf/liquid.cpp:112-165 (dims 2 or 3). */
+int orc_sf_percus_yevick(double dia, double volf, int dims, int nqy, const double* qx,
+                         const double* qy, int nqz, const double* qz, double* sf);
+
 /* DWBA combination, src/sim/hipgisaxs_main.cpp:1086-1100: I[i] += |w * sum_k fc sf ff|^2. */
 void orc_dwba_combine(int n, const double* fc, const double* sf, const double* ff,
                       double weight, double* intensity);

@@ -266,6 +266,58 @@ def sf_lattice(grid: Grid, abc, repet, scaling, center=(0, 0, 0), rot=None, back
     return out
 
 
+def sf_paracrystal(grid: Grid, dims, lattice, dx, dy, sx, sy, dom, backend=None):
+    """StructureFactor paracrystal branch on the grid's extended qz (4N values)."""
+    backend = backend or grid.backend
+    L = lib(backend)
+    out = np.zeros(4 * grid.n, dtype=np.complex128)
+    if backend == "port":
+        rc = L.orc_sf_paracrystal(C.c_int(dims), C.c_int(lattice), C.c_double(dx), C.c_double(dy),
+                                  C.c_double(sx), C.c_double(sy), C.c_double(dom), C.c_int(grid.n),
+                                  _p(grid.qx), _p(grid.qy), C.c_int(4 * grid.n),
+                                  _p(out.view(np.float64)))
+    else:
+        grid.activate()
+        rc = L.ref_sf_paracrystal(C.c_int(dims), C.c_int(lattice), C.c_double(dx), C.c_double(dy),
+                                  C.c_double(sx), C.c_double(sy), C.c_double(dom), C.c_int(1),
+                                  _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"sf_paracrystal failed rc={rc}")
+    return out
+
+
+def sf_percus_yevick(grid: Grid, dia, volf, dims, backend=None):
+    """StructureFactor Percus-Yevick branch on the grid's extended qz (4N values)."""
+    backend = backend or grid.backend
+    return (sf_percus_yevick_arrays(dia, volf, dims, grid.qx, grid.qy, grid.qz_ext)
+            if backend == "port" else _py_ref(grid, dia, volf, dims))
+
+
+def _py_ref(grid, dia, volf, dims):
+    L = lib("ref")
+    out = np.zeros(4 * grid.n, dtype=np.complex128)
+    grid.activate()
+    rc = L.ref_sf_percus_yevick(C.c_double(dia), C.c_double(volf), C.c_int(dims), C.c_int(1),
+                                _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"sf_percus_yevick failed rc={rc}")
+    return out
+
+
+def sf_percus_yevick_arrays(dia, volf, dims, qx, qy, qz):
+    """Port backend on explicit arrays (q-point i uses qx/qy[i % len(qx)])."""
+    L = lib("port")
+    qx = np.ascontiguousarray(qx, dtype=np.float64)
+    qy = np.ascontiguousarray(qy, dtype=np.float64)
+    qz, qzf = _cbuf(qz)
+    out = np.zeros(len(qz), dtype=np.complex128)
+    rc = L.orc_sf_percus_yevick(C.c_double(dia), C.c_double(volf), C.c_int(dims), C.c_int(len(qx)),
+                                _p(qx), _p(qy), C.c_int(len(qz)), _p(qzf), _p(out.view(np.float64)))
+    if rc <= 0:
+        raise RuntimeError(f"sf_percus_yevick failed rc={rc}")
+    return out
+
+
 def sf_lattice_arrays(abc, repet, scaling, center, rot, qx, qy, qz):
     """Port backend on explicit arrays (qz complex; q-point i uses qx/qy[i % len(qx)])."""
     L = lib("port")

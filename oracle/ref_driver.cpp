@@ -273,6 +273,55 @@ int ref_sf_lattice(const double* abc9, const double* repet, const double* scalin
   return n;
 }
 
+// StructureFactor::compute_structure_factor, paracrystal branch, on the singleton grid.
+int ref_sf_paracrystal(int dims, int lattice, double dx, double dy, double sx, double sy,
+                       double dom, int gisaxs, double* sf) {
+  auto pc = std::make_shared<Paracrystal>();
+  pc->putDims(dims);
+  pc->putDistXMean(dx);
+  pc->putDistYMean(dy);
+  pc->putDistXStddev(sx);
+  pc->putDistYStddev(sy);
+  pc->putDomainSize(dom);
+  Lattice lat;
+  lat.init();
+  lat.type((LatticeType)lattice);
+  StructureFactor s;
+  s.putStructureType(paracrystal_type);
+  RotMatrix_t rot;
+  vector3_t z(0, 0, 0);
+  if (!s.compute_structure_factor(gisaxs ? "gisaxs" : "saxs", z, &lat, z, z, rot, pc, nullptr)) return -2;
+  QGrid& g = QGrid::instance();
+  int n = gisaxs ? g.nqz_extended() : g.nqz();
+  for (int i = 0; i < n; ++i) {
+    sf[2 * i] = s[i].real();
+    sf[2 * i + 1] = s[i].imag();
+  }
+  return n;
+}
+
+// StructureFactor::compute_structure_factor, Percus-Yevick branch, on the singleton grid.
+int ref_sf_percus_yevick(double dia, double volf, int dims, int gisaxs, double* sf) {
+  auto py = std::make_shared<PercusYevick>();
+  py->putDims(dims);
+  py->putDiameter(dia);
+  py->putVolfract(volf);
+  Lattice lat;
+  lat.init();
+  StructureFactor s;
+  s.putStructureType(percusyevick_type);
+  RotMatrix_t rot;
+  vector3_t z(0, 0, 0);
+  if (!s.compute_structure_factor(gisaxs ? "gisaxs" : "saxs", z, &lat, z, z, rot, nullptr, py)) return -2;
+  QGrid& g = QGrid::instance();
+  int n = gisaxs ? g.nqz_extended() : g.nqz();
+  for (int i = 0; i < n; ++i) {
+    sf[2 * i] = s[i].real();
+    sf[2 * i + 1] = s[i].imag();
+  }
+  return n;
+}
+
 // RotMatrix_t(axis, angle) and products, for the rotation-composition checks.
 void ref_rotmatrix(int axis, double angle, double* r9) {
   RotMatrix_t r(axis, angle);

@@ -18,6 +18,13 @@ sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import pyoracle as po  # noqa: E402
 
 
+GRIDS = {
+    "g16": dict(ncol=16, nrow=12, region=(-1.0, 0.0, 1.0, 2.0), ai=0.16, e=10.0, dn2=(0, 0)),
+    "g16abs": dict(ncol=16, nrow=12, region=(-2.0, 0.0, 2.0, 3.0), ai=0.20, e=10.0,
+                   dn2=(2 * 3e-6, 2 * 2e-8)),
+}
+
+
 def tri_case(rng, T, scale):
     sd = np.zeros((T, 8))
     sd[:, 0] = rng.uniform(0.2, 3.0, T)
@@ -34,11 +41,7 @@ def main():
     rng = np.random.default_rng(20240601)
     out = {}
     # grids: a Born-like vacuum layer and a buried (absorbing) particle layer
-    grids = {
-        "g16": dict(ncol=16, nrow=12, region=(-1.0, 0.0, 1.0, 2.0), ai=0.16, e=10.0, dn2=(0, 0)),
-        "g16abs": dict(ncol=16, nrow=12, region=(-2.0, 0.0, 2.0, 3.0), ai=0.20, e=10.0,
-                       dn2=(2 * 3e-6, 2 * 2e-8)),
-    }
+    grids = GRIDS
     rots = {"id": np.eye(3),
             "r3": po.rot_mul(po.rot_mul(po.rot_axis(2, 0.35), po.rot_axis(0, 0.12)),
                              po.rot_axis(1, -0.2))}
@@ -92,6 +95,7 @@ def main():
                                 layers=np.array(layers, dtype=float), order=order, fc=fc,
                                 grid=gname)
     exact_fixtures()
+    liquid_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -115,9 +119,30 @@ def exact_fixtures():
                                 rot=R, ff=ff, grid=gname)
 
 
+LIQUID_CASES = {
+    "para1d": ("para", (1, 3, 0.0, 12.0, 0.0, 2.0, 200.0)),
+    "para2d_cubic": ("para", (2, 3, 10.0, 12.0, 1.5, 2.0, 300.0)),
+    "para2d_hex": ("para", (2, 7, 10.0, 12.0, 1.5, 2.0, 300.0)),
+    "py2d": ("py", (8.0, 0.3, 2)),
+    "py3d": ("py", (8.0, 0.3, 3)),
+}
+
+
+def liquid_fixtures():
+    """Paracrystal and Percus-Yevick structure factors (src/sf/liquid.cpp) on both grids."""
+    for gname, g in GRIDS.items():
+        G = po.Grid(g["ncol"], g["nrow"], *g["region"], g["ai"], g["e"], g["dn2"], backend="ref")
+        for cname, (kind, args) in LIQUID_CASES.items():
+            sf = po.sf_paracrystal(G, *args) if kind == "para" else po.sf_percus_yevick(G, *args)
+            np.savez_compressed(os.path.join(HERE, f"sfliq_{cname}_{gname}.npz"), kind=kind,
+                                args=np.array(args, dtype=float), sf=sf, grid=gname)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["exact"]:
         po.set_threads(4, "ref")
         exact_fixtures()
+    elif sys.argv[1:] == ["liquid"]:
+        liquid_fixtures()
     else:
         main()

@@ -39,6 +39,18 @@ def test_ff_exact_triangles(po, golden, golden_grid, name):
     np.testing.assert_allclose(ff, d["ff"], rtol=1e-13, atol=1e-13 * np.abs(d["ff"]).max())
 
 
+@pytest.mark.parametrize("name", _names("sfliq_"))
+def test_sf_liquid(po, golden, golden_grid, name):
+    d = golden(name)
+    G, _ = golden_grid(str(d["grid"]))
+    a = d["args"]
+    if str(d["kind"]) == "para":
+        sf = po.sf_paracrystal(G, int(a[0]), int(a[1]), *a[2:])
+    else:
+        sf = po.sf_percus_yevick(G, a[0], a[1], int(a[2]))
+    np.testing.assert_array_equal(sf, d["sf"])
+
+
 @pytest.mark.parametrize("name", _names("ffana_"))
 def test_ff_analytic(po, golden, golden_grid, name):
     d = golden(name)
