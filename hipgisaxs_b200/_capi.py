@@ -47,6 +47,8 @@ SIGNATURES = {
     "hgx_ff_analytic_params": (_i, [_vp, _vp, _i, _i, _vp, _d, _d, _vp, _vp, _vp, _i]),
     "hgx_lattice_vectors": (_i, [_i, C.c_char_p, _vp, _vp]),
     "hgx_sf_lattice": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "hgx_sf_paracrystal": (_i, [_vp, _vp, _i, _i, _d, _d, _d, _d, _d, _vp, _i]),
+    "hgx_sf_percus_yevick": (_i, [_vp, _vp, _d, _d, _i, _vp, _i]),
     "hgx_propagation_coeffs": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _i]),
     "hgx_dwba_combine": (_i, [_vp, C.c_long, _vp, _vp, _vp, _i, _d, _vp]),
     "hgx_abs_diff_square": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),

@@ -30,10 +30,10 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-# per-file extra flags.  ff_exact.cu: the exact triangle form factor follows the reference's
-# FP64 arithmetic without fused multiply-adds, because its edge and vertex terms cancel and
-# amplify any difference in rounding.
-FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"]}
+# per-file extra flags.  ff_exact.cu and sf_liquid.cu follow the reference's FP64 arithmetic
+# without fused multiply-adds: the exact triangle form factor's edge and vertex terms and the
+# Percus-Yevick function's terms cancel and amplify any difference in rounding.
+FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"], "sf_liquid.cu": ["-fmad=false"]}
 
 
 def _sources():

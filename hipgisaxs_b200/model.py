@@ -105,6 +105,26 @@ def sf_lattice(ctx: Context, grid: QGrid, abc, repet, scaling, center=(0, 0, 0),
     return out
 
 
+def sf_paracrystal(ctx: Context, grid: QGrid, dims, lattice="cubic", dist=(0.0, 0.0),
+                   sdev=(0.0, 0.0), domain=1.0, out=None, out_type="c128"):
+    """Paracrystal structure factor (hgx_sf_paracrystal): dims 1, or 2 on a cubic or hex
+    lattice; dist = (x, y) mean distances, sdev = (x, y) standard deviations."""
+    out = _out(out, grid.nqz, out_type)
+    check(lib().hgx_sf_paracrystal(ctx.handle, grid.handle, int(dims), LATTICE[lattice],
+                                   float(dist[0]), float(dist[1]), float(sdev[0]), float(sdev[1]),
+                                   float(domain), _ptr(out), CTYPE[out_type]))
+    return out
+
+
+def sf_percus_yevick(ctx: Context, grid: QGrid, diameter, volfract, dims=2, out=None,
+                     out_type="c128"):
+    """Percus-Yevick hard-sphere structure factor (hgx_sf_percus_yevick), dims 2 or 3."""
+    out = _out(out, grid.nqz, out_type)
+    check(lib().hgx_sf_percus_yevick(ctx.handle, grid.handle, float(diameter), float(volfract),
+                                     int(dims), _ptr(out), CTYPE[out_type]))
+    return out
+
+
 def propagation_coeffs(ctx: Context, grid: QGrid, layers, k0, alpha_i, particle_order=0,
                        alpha=None, per_row=False, out=None):
     """layers: (delta, beta, thickness, order) tuples, order -1 = substrate."""

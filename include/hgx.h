@@ -171,6 +171,22 @@ int hgx_sf_lattice(hgx_ctx ctx, hgx_qgrid g, const double* abc9, const double* r
                    const double* scaling, const double* center, const double* rot9, void* sf,
                    int sf_type);
 
+/* Paracrystal structure factors: StructureFactor::paracrystal1d / paracrystal2d_cubic /
+ * paracrystal2d_hex (src/sf/liquid.cpp:29-110), selected as compute_structure_factor selects
+ * them (src/sf/sf.cpp:116-151): dims 1, or dims 2 with lattice 3 (cubic) or 7 (hex);
+ * dist_x/dist_y the mean distances, sdev_x/sdev_y their standard deviations, domain the
+ * domain size (the 1-D form uses the y values and qy only).  FP64; sf: nqz complex (real
+ * values), q-point i uses qx/qy[i % nqy]. */
+int hgx_sf_paracrystal(hgx_ctx ctx, hgx_qgrid g, int dims, int lattice, double dist_x,
+                       double dist_y, double sdev_x, double sdev_y, double domain, void* sf,
+                       int sf_type);
+/* Percus-Yevick structure factor: StructureFactor::percus_yevik (src/sf/liquid.cpp:112-165):
+ * hard spheres of `diameter` at volume fraction `volfract`; dims 2 uses |q_par|, dims 3 |q|
+ * with the complex qz.  The reference's values are reproduced, including the fourth root of
+ * the 3-D form and the unrooted alpha/3 + beta/4 + gamma below |q| = 1e-6.  FP64. */
+int hgx_sf_percus_yevick(hgx_ctx ctx, hgx_qgrid g, double diameter, double volfract, int dims,
+                         void* sf, int sf_type);
+
 /* ---------------------------------------------------------------- DWBA terms ---- */
 /* MultiLayer::init + propagation_coeffs (src/model/multilayer.cpp:29-58,110-155), FP64:
  * user layers (delta, beta, thickness, order; order -1 = substrate; host arrays), the
