@@ -51,6 +51,8 @@ SIGNATURES = {
     "hgx_sf_percus_yevick": (_i, [_vp, _vp, _d, _d, _i, _vp, _i]),
     "hgx_propagation_coeffs": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _i]),
     "hgx_dwba_combine": (_i, [_vp, C.c_long, _vp, _vp, _vp, _i, _d, _vp]),
+    "hgx_dwba_mesh_grains": (_i, [_vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d,
+                                  _i, _vp]),
     "hgx_abs_diff_square": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_residual_vector": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_chi2": (_i, [_vp, C.c_long, _vp, _vp, _vp, _d, _vp]),

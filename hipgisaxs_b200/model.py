@@ -105,6 +105,30 @@ def sf_lattice(ctx: Context, grid: QGrid, abc, repet, scaling, center=(0, 0, 0),
     return out
 
 
+def dwba_mesh_grains(ctx: Context, grid: QGrid, shape_def, rots, centers, weights, abc, repet,
+                     scaling, fc, dn2, precision="f32c"):
+    """The grain loop of one structure (hgx_dwba_mesh_grains): sum over grains of
+    |w dn2 sum_k fc_k sf_k ff_k|^2 with each grain's rotation and unit-cell centre."""
+    from ._capi import F32C, F64
+    psd, ksd = _in(shape_def, np.float64)
+    ntri = int((ksd.numel() if _is_tensor(ksd) else ksd.size) // 8)
+    r = np.ascontiguousarray(np.asarray(rots, dtype=np.float64).reshape(-1, 9))
+    c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+    if not (len(r) == len(c) == len(w)):
+        raise ValueError("one rotation, centre and weight per grain")
+    abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
+    rp = np.ascontiguousarray(repet, dtype=np.float64)
+    sc = np.ascontiguousarray(scaling, dtype=np.float64)
+    pfc, kfc = _in(fc, np.complex128)
+    out = np.zeros(grid.nqy)
+    check(lib().hgx_dwba_mesh_grains(ctx.handle, grid.handle, psd, ntri, len(r), r.ctypes.data,
+                                     c.ctypes.data, w.ctypes.data, abc9.ctypes.data, rp.ctypes.data,
+                                     sc.ctypes.data, pfc, float(dn2[0]), float(dn2[1]),
+                                     F64 if precision == "f64" else F32C, out.ctypes.data))
+    return out
+
+
 def sf_paracrystal(ctx: Context, grid: QGrid, dims, lattice="cubic", dist=(0.0, 0.0),
                    sdev=(0.0, 0.0), domain=1.0, out=None, out_type="c128"):
     """Paracrystal structure factor (hgx_sf_paracrystal): dims 1, or 2 on a cubic or hex

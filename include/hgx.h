@@ -217,6 +217,22 @@ int hgx_residual_vector(hgx_ctx ctx, long n, const double* ref, const double* da
 int hgx_chi2(hgx_ctx ctx, long n, const double* model, const double* counts,
              const unsigned* mask, double scale, double* out);
 
+/* The grain loop of HipGISAXS::run_gisaxs (src/sim/hipgisaxs_main.cpp:794-1100) for one
+ * structure whose unit cell holds one triangulated particle, run on the device with no host
+ * round trip between grains: for each grain k, the form factor of shape_def (ntri x 8) rotated
+ * by rots[9k..] (the grain's composed rotation, :946-951, times the shape's own, :986), the
+ * lattice structure factor (abc9 unscaled lattice vectors, repet, scaling) at centre
+ * centers[3k..] and rotation rots[9k..] (:1050-1058), and
+ * intensity[i] += |weights[k] dn2 sum_j fc_j sf_j ff_j|^2 over the 4 DWBA blocks (:1086-1100).
+ * fc: 4N complex (hgx_propagation_coeffs); precision HGX_F32C or HGX_F64 for the form factor
+ * (the structure factor and combination are FP64).  intensity: N doubles, overwritten with the
+ * sum over grains.  The grid must be a DWBA grid (4 qz blocks). */
+int hgx_dwba_mesh_grains(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
+                         int ngrains, const double* rots, const double* centers,
+                         const double* weights, const double* abc9, const double* repet,
+                         const double* scaling, const double* fc, double dn2_re, double dn2_im,
+                         int precision, double* intensity);
+
 /* -------------------------------------------- fitting: chi^2 and its gradient ---- */
 /* A fused model for the fitting front end: cylinders on a 2-D lattice in DWBA (one grain,
  * as HipGISAXS::run_gisaxs computes it, src/sim/hipgisaxs_main.cpp:694-1100), its Poisson
