@@ -30,10 +30,12 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-# per-file extra flags.  ff_exact.cu and sf_liquid.cu follow the reference's FP64 arithmetic
-# without fused multiply-adds: the exact triangle form factor's edge and vertex terms and the
-# Percus-Yevick function's terms cancel and amplify any difference in rounding.
-FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"], "sf_liquid.cu": ["-fmad=false"]}
+# per-file extra flags.  ff_exact.cu, sf_liquid.cu and postproc.cu follow the reference's FP64
+# arithmetic without fused multiply-adds: the exact triangle form factor's edge and vertex
+# terms and the Percus-Yevick function's terms cancel and amplify any difference in rounding,
+# and the smearing sums then round as the reference's do (those kernels are memory-bound).
+FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"], "sf_liquid.cu": ["-fmad=false"],
+              "postproc.cu": ["-fmad=false"]}
 
 
 def _sources():

@@ -129,6 +129,29 @@ def dwba_mesh_grains(ctx: Context, grid: QGrid, shape_def, rots, centers, weight
     return out
 
 
+def gaussian_smearing(ctx: Context, image, sigma):
+    """Gaussian smearing of a (nrow, ncol) image (hgx_gaussian_smearing); returns a smeared
+    copy of a numpy image, or smears a contiguous device tensor in place and returns it."""
+    if _is_tensor(image):
+        nrow, ncol = image.shape
+        check(lib().hgx_gaussian_smearing(ctx.handle, image.data_ptr(), int(ncol), int(nrow),
+                                          float(sigma)))
+        return image
+    img = np.ascontiguousarray(image, dtype=np.float64).copy()
+    nrow, ncol = img.shape
+    check(lib().hgx_gaussian_smearing(ctx.handle, img.ctypes.data, int(ncol), int(nrow),
+                                      float(sigma)))
+    return img
+
+
+def normalize(ctx: Context, data):
+    """HipGISAXS::normalize of a copy of `data` (hgx_normalize): (normalised, flag)."""
+    d = np.ascontiguousarray(data, dtype=np.float64).copy()
+    ok = C.c_int()
+    check(lib().hgx_normalize(ctx.handle, d.ctypes.data, d.size, C.byref(ok)))
+    return d, bool(ok.value)
+
+
 def sf_paracrystal(ctx: Context, grid: QGrid, dims, lattice="cubic", dist=(0.0, 0.0),
                    sdev=(0.0, 0.0), domain=1.0, out=None, out_type="c128"):
     """Paracrystal structure factor (hgx_sf_paracrystal): dims 1, or 2 on a cubic or hex

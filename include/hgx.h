@@ -233,6 +233,19 @@ int hgx_dwba_mesh_grains(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int 
                          const double* scaling, const double* fc, double dn2_re, double dn2_im,
                          int precision, double* intensity);
 
+/* ------------------------------------------------------------ post-processing ---- */
+/* Gaussian smearing of a detector image in place (HipGISAXS::gaussian_smearing,
+ * src/sim/hipgisaxs_helpers.cpp:25-27, i.e. Convolutions::convolution_gaussian_2d,
+ * include/numerics/convolutions.hpp:127-174): image is nrow rows of ncol doubles; a
+ * horizontal then a vertical normalised pass over the window [i - r, i + r), r = ceil(6 sigma),
+ * with the reference's window arithmetic (right end excluded, weights indexed from the
+ * window's start).  sigma > 0 in pixels, 2 r + 1 <= 8193.  FP64, synchronous. */
+int hgx_gaussian_smearing(hgx_ctx ctx, double* image, int ncol, int nrow, double sigma);
+/* HipGISAXS::normalize (src/sim/hipgisaxs_main.cpp:1439-1450) in place: (x - min) /
+ * (max - min) for every element but the first (left as it is, as in the reference);
+ * *normalized = 0 and nothing changes when max - min < 1e-30.  Synchronous. */
+int hgx_normalize(hgx_ctx ctx, double* data, long n, int* normalized);
+
 /* -------------------------------------------- fitting: chi^2 and its gradient ---- */
 /* A fused model for the fitting front end: cylinders on a 2-D lattice in DWBA (one grain,
  * as HipGISAXS::run_gisaxs computes it, src/sim/hipgisaxs_main.cpp:694-1100), its Poisson

@@ -1009,3 +1009,67 @@ double orc_chi2(int n, const double* model, const double* counts, const unsigned
   }
   return s;
 }
+
+/* ------------------------------------------------------- post-processing ---- */
+
+/* Convolutions::gaussian, include/numerics/convolutions.hpp:122-124 */
+static double gauss1(int x, double sigma) {
+  return 1.0 / (sigma * sqrt(2 * PI_REF) * exp((x * x) / (2 * sigma * sigma)));
+}
+
+/* Convolutions::convolution_gaussian_2d, include/numerics/convolutions.hpp:127-174: two
+ * normalised passes (horizontal, then vertical) over the window [i - r, i + r) with
+ * r = ceil(6 sigma), the weights indexed from the window's start. data: ny rows of nx. */
+int orc_smear_gaussian(double* data, int nx, int ny, double sigma) {
+  int r = (int)ceil(6 * sigma);
+  int gn = 2 * r + 1;
+  double* gmap = (double*)malloc(sizeof(double) * gn);
+  double* conv = (double*)malloc(sizeof(double) * (size_t)nx * ny);
+  if (!gmap || !conv) {
+    free(gmap);
+    free(conv);
+    return -1;
+  }
+  for (int i = 0; i < gn; ++i) gmap[i] = gauss1(i - r, sigma);
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      double sum = 0.0, norm = 0.0;
+      int ibeg = i - r > 0 ? i - r : 0;
+      int iend = i + r < nx ? i + r : nx;
+      for (int k = ibeg; k < iend; ++k) {
+        sum += data[(size_t)j * nx + k] * gmap[k - ibeg];
+        norm += gmap[k - ibeg];
+      }
+      conv[(size_t)j * nx + i] = norm > TINY_REF ? sum / norm : 0;
+    }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nx; ++i)
+    for (int j = 0; j < ny; ++j) {
+      double sum = 0.0, norm = 0.0;
+      int jbeg = j - r > 0 ? j - r : 0;
+      int jend = j + r < ny ? j + r : ny;
+      for (int l = jbeg; l < jend; ++l) {
+        sum += conv[(size_t)l * nx + i] * gmap[l - jbeg];
+        norm += gmap[l - jbeg];
+      }
+      data[(size_t)j * nx + i] = norm > TINY_REF ? sum / norm : 0;
+    }
+  free(gmap);
+  free(conv);
+  return 0;
+}
+
+/* HipGISAXS::normalize, src/sim/hipgisaxs_main.cpp:1439-1450: (x - min)/(max - min) for
+ * every element but the first; returns 0 (and changes nothing) when max - min < 1e-30. */
+int orc_normalize(double* data, long n) {
+  double mn = data[0], mx = data[0];
+  for (long i = 1; i < n; ++i) {
+    mn = data[i] < mn ? data[i] : mn;
+    mx = data[i] > mx ? data[i] : mx;
+  }
+  double d = mx - mn;
+  if (d < 1e-30) return 0;
+  for (long i = 1; i < n; ++i) data[i] = (data[i] - mn) / d;
+  return 1;
+}

@@ -109,6 +109,12 @@ void orc_residual_vector(int n, const double* ref, const double* data, const uns
 double orc_chi2(int n, const double* model, const double* counts, const unsigned* mask,
                 double scale);
 
+/* Convolutions::convolution_gaussian_2d (include/numerics/convolutions.hpp:127-174), in place
+ * on ny rows of nx. */
+int orc_smear_gaussian(double* data, int nx, int ny, double sigma);
+/* HipGISAXS::normalize (src/sim/hipgisaxs_main.cpp:1439-1450), in place; 1 if normalised. */
+int orc_normalize(double* data, long n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -459,3 +459,23 @@ def rel_err(a, b):
     b = np.asarray(b)
     den = float(np.linalg.norm(b.ravel()))
     return float(np.linalg.norm((a - b).ravel())) / (den if den > 0 else 1.0)
+
+
+def smear_gaussian(image, sigma, backend="port"):
+    """Convolutions::convolution_gaussian_2d of a (nrow, ncol) image (a copy is returned)."""
+    L = lib(backend)
+    img = np.ascontiguousarray(image, dtype=np.float64).copy()
+    ny, nx = img.shape
+    f = L.orc_smear_gaussian if backend == "port" else L.ref_smear_gaussian
+    rc = f(_p(img), C.c_int(nx), C.c_int(ny), C.c_double(sigma))
+    if rc != 0:
+        raise RuntimeError("smear_gaussian failed")
+    return img
+
+
+def normalize(data):
+    """HipGISAXS::normalize (a copy; the first element is left as it is)."""
+    L = lib("port")
+    d = np.ascontiguousarray(data, dtype=np.float64).copy()
+    ok = L.orc_normalize(_p(d), C.c_long(d.size))
+    return d, bool(ok)

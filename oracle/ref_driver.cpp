@@ -25,6 +25,8 @@
 #include <model/layer.hpp>
 #include <model/shape.hpp>
 #include <model/structure.hpp>
+#include <common/constants.hpp>  // PI_, TINY_ used by convolutions.hpp
+#include <numerics/convolutions.hpp>
 #include <numerics/matrix.hpp>
 #include <ff/cpu/ff_num_cpu.hpp>
 #include <ff/ff_ana.hpp>
@@ -320,6 +322,17 @@ int ref_sf_percus_yevick(double dia, double volf, int dims, int gisaxs, double* 
     sf[2 * i + 1] = s[i].imag();
   }
   return n;
+}
+
+// Convolutions::convolution_gaussian_2d, as HipGISAXS::gaussian_smearing calls it
+// (src/sim/hipgisaxs_helpers.cpp:25-27): data of ny rows of nx, replaced in place.
+int ref_smear_gaussian(double* data, int nx, int ny, double sigma) {
+  real_t* buf = new real_t[(size_t)nx * ny];
+  for (size_t i = 0; i < (size_t)nx * ny; ++i) buf[i] = data[i];
+  if (!Convolutions::instance().convolution_gaussian_2d(buf, nx, ny, sigma)) return -1;
+  for (size_t i = 0; i < (size_t)nx * ny; ++i) data[i] = buf[i];
+  delete[] buf;
+  return 0;
 }
 
 // RotMatrix_t(axis, angle) and products, for the rotation-composition checks.

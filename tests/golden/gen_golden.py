@@ -96,6 +96,7 @@ def main():
                                 grid=gname)
     exact_fixtures()
     liquid_fixtures()
+    smear_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -138,11 +139,25 @@ def liquid_fixtures():
                                 args=np.array(args, dtype=float), sf=sf, grid=gname)
 
 
+def smear_fixtures():
+    """Convolutions::convolution_gaussian_2d on seeded images: narrow, wide (window larger than
+    the image) and a non-square image."""
+    rng = np.random.default_rng(20240606)
+    for name, shape, sigma in (("s07", (12, 16), 0.7), ("s20", (12, 16), 2.0),
+                               ("s35", (40, 48), 3.5)):
+        img = rng.random(shape) * 1e3
+        out = po.smear_gaussian(img, sigma, "ref")
+        np.savez_compressed(os.path.join(HERE, f"smear_{name}.npz"), image=img, sigma=sigma,
+                            smeared=out)
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["exact"]:
         po.set_threads(4, "ref")
         exact_fixtures()
     elif sys.argv[1:] == ["liquid"]:
         liquid_fixtures()
+    elif sys.argv[1:] == ["smear"]:
+        smear_fixtures()
     else:
         main()

@@ -51,6 +51,12 @@ def test_sf_liquid(po, golden, golden_grid, name):
     np.testing.assert_array_equal(sf, d["sf"])
 
 
+@pytest.mark.parametrize("name", _names("smear_"))
+def test_smearing(po, golden, name):
+    d = golden(name)
+    np.testing.assert_array_equal(po.smear_gaussian(d["image"], float(d["sigma"])), d["smeared"])
+
+
 @pytest.mark.parametrize("name", _names("ffana_"))
 def test_ff_analytic(po, golden, golden_grid, name):
     d = golden(name)

@@ -114,3 +114,25 @@ def test_chi2_definition(po):
     mask = np.array([1, 1, 0, 1], np.uint32)
     ref = (2 - 1) ** 2 / 1 + (4 - 0) ** 2 / 1 + (1 - 9) ** 2 / 9
     assert abs(po.chi2(m, c, mask, 2.0) - ref) < 1e-14
+
+
+def test_normalize_definition(po):
+    """HipGISAXS::normalize: (x - min)/(max - min) for all but the first element, which the
+    reference leaves as it is; a flat array is left unchanged."""
+    x = np.array([5.0, 2.0, 7.0, 4.5])
+    d, ok = po.normalize(x)
+    assert ok and d[0] == 5.0 and np.allclose(d[1:], (x[1:] - 2.0) / 5.0)
+    d, ok = po.normalize(np.full(5, 3.0))
+    assert not ok and np.all(d == 3.0)
+
+
+def test_smearing_preserves_constants_and_is_local(po):
+    """Normalised weights: a constant image stays constant; a point spreads no further than
+    ceil(6 sigma) pixels."""
+    img = np.full((20, 30), 2.5)
+    np.testing.assert_allclose(po.smear_gaussian(img, 1.3), img, rtol=1e-14)
+    pt = np.zeros((41, 41))
+    pt[20, 20] = 1.0
+    out = po.smear_gaussian(pt, 1.0)
+    nz = np.argwhere(out > 0)
+    assert nz.min() >= 20 - 6 and nz.max() <= 20 + 6
