@@ -56,6 +56,9 @@ SIGNATURES = {
     "hgx_abs_diff_square": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_residual_vector": (_i, [_vp, C.c_long, _vp, _vp, _vp, _vp]),
     "hgx_chi2": (_i, [_vp, C.c_long, _vp, _vp, _vp, _d, _vp]),
+    "hgx_dwba_analytic_grains": (_i, [_vp, _vp, _i, _i, _vp, _d, _d, _vp, _i, _vp, _vp, _vp, _vp,
+                                      _vp, _vp, _vp, _d, _d, _vp]),
+    "hgx_structure_sum": (_i, [_vp, _i, C.c_long, _vp, _vp, _vp]),
     "hgx_gaussian_smearing": (_i, [_vp, _vp, _i, _i, _d]),
     "hgx_normalize": (_i, [_vp, _vp, C.c_long, C.POINTER(_i)]),
     "hgx_cyl_batch_create": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _d, _i, C.POINTER(_vp)]),

@@ -129,6 +129,41 @@ def dwba_mesh_grains(ctx: Context, grid: QGrid, shape_def, rots, centers, weight
     return out
 
 
+def dwba_analytic_grains(ctx: Context, grid: QGrid, shape, params, rots, centers, weights, abc,
+                         repet, scaling, fc, dn2, tau=0.0, eta=0.0, transvec=(0, 0, 0)):
+    """The grain loop of one structure of analytic particles (hgx_dwba_analytic_grains)."""
+    P = params if isinstance(params, np.ndarray) else param_rows(params)
+    P = np.ascontiguousarray(P, dtype=np.float64)
+    tv = np.ascontiguousarray(transvec, dtype=np.float64)
+    r = np.ascontiguousarray(np.asarray(rots, dtype=np.float64).reshape(-1, 9))
+    c = np.ascontiguousarray(np.asarray(centers, dtype=np.float64).reshape(-1, 3))
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1))
+    if not (len(r) == len(c) == len(w)):
+        raise ValueError("one rotation, centre and weight per grain")
+    abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
+    rp = np.ascontiguousarray(repet, dtype=np.float64)
+    sc = np.ascontiguousarray(scaling, dtype=np.float64)
+    pfc, kfc = _in(fc, np.complex128)
+    out = np.zeros(grid.nqy)
+    check(lib().hgx_dwba_analytic_grains(ctx.handle, grid.handle, SHAPE[shape], len(P), P.ctypes.data,
+                                         float(tau), float(eta), tv.ctypes.data, len(r),
+                                         r.ctypes.data, c.ctypes.data, w.ctypes.data,
+                                         abc9.ctypes.data, rp.ctypes.data, sc.ctypes.data, pfc,
+                                         float(dn2[0]), float(dn2[1]), out.ctypes.data))
+    return out
+
+
+def structure_sum(ctx: Context, intensities, iratios):
+    """Sum over structures weighted by their (rescaled) iratios (hgx_structure_sum)."""
+    I = np.ascontiguousarray(intensities, dtype=np.float64)
+    I2 = I.reshape(len(I), -1)
+    r = np.ascontiguousarray(iratios, dtype=np.float64)
+    out = np.zeros(I2.shape[1])
+    check(lib().hgx_structure_sum(ctx.handle, len(I2), I2.shape[1], I2.ctypes.data, r.ctypes.data,
+                                  out.ctypes.data))
+    return out.reshape(I.shape[1:])
+
+
 def gaussian_smearing(ctx: Context, image, sigma):
     """Gaussian smearing of a (nrow, ncol) image (hgx_gaussian_smearing); returns a smeared
     copy of a numpy image, or smears a contiguous device tensor in place and returns it."""

@@ -233,6 +233,21 @@ int hgx_dwba_mesh_grains(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int 
                          const double* scaling, const double* fc, double dn2_re, double dn2_im,
                          int precision, double* intensity);
 
+/* As hgx_dwba_mesh_grains for a unit cell holding one analytic shape: the form factor of each
+ * grain is hgx_ff_analytic_params(shape, nparam, params, tau, eta, transvec) at rots[9k..]
+ * (AnalyticFormFactor::compute, src/ff/ff_ana.cpp:61-161), FP64. */
+int hgx_dwba_analytic_grains(hgx_ctx ctx, hgx_qgrid g, int shape, int nparam,
+                             const double* params, double tau, double eta,
+                             const double* transvec, int ngrains, const double* rots,
+                             const double* centers, const double* weights, const double* abc9,
+                             const double* repet, const double* scaling, const double* fc,
+                             double dn2_re, double dn2_im, double* intensity);
+/* The sum over structures of HipGISAXS::run_gisaxs with uncorrelated structures (its default,
+ * src/sim/hipgisaxs_main.cpp:1278-1293, 1352-1362): iratios rescaled to sum to 1 unless they
+ * already do; out[z] = sum_s intensities[s n + z] iratio_s.  intensities: nstruct x n. */
+int hgx_structure_sum(hgx_ctx ctx, int nstruct, long n, const double* intensities,
+                      const double* iratios, double* out);
+
 /* ------------------------------------------------------------ post-processing ---- */
 /* Gaussian smearing of a detector image in place (HipGISAXS::gaussian_smearing,
  * src/sim/hipgisaxs_helpers.cpp:25-27, i.e. Convolutions::convolution_gaussian_2d,

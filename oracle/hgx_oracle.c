@@ -1073,3 +1073,17 @@ int orc_normalize(double* data, long n) {
   for (long i = 1; i < n; ++i) data[i] = (data[i] - mn) / d;
   return 1;
 }
+
+/* HipGISAXS::run_gisaxs, uncorrelated structures (src/sim/hipgisaxs_main.cpp:1278-1293,
+ * 1352-1362): iratios rescaled unless they sum to 1; out[z] = sum_s I[s n + z] r_s. */
+void orc_structure_sum(int ns, long n, const double* img, const double* iratios, double* out) {
+  double r[256];
+  double rsum = 0.0;
+  for (int s = 0; s < ns && s < 256; ++s) rsum += iratios[s];
+  for (int s = 0; s < ns && s < 256; ++s) r[s] = rsum != 1.0 ? iratios[s] / rsum : iratios[s];
+  for (long z = 0; z < n; ++z) {
+    double sum = 0.0;
+    for (int s = 0; s < ns && s < 256; ++s) sum += img[(long)s * n + z] * r[s];
+    out[z] = sum;
+  }
+}

@@ -109,6 +109,9 @@ void orc_residual_vector(int n, const double* ref, const double* data, const uns
 double orc_chi2(int n, const double* model, const double* counts, const unsigned* mask,
                 double scale);
 
+/* HipGISAXS::run_gisaxs structure sum (src/sim/hipgisaxs_main.cpp:1278-1293, 1352-1362);
+ * at most 256 structures. */
+void orc_structure_sum(int ns, long n, const double* img, const double* iratios, double* out);
 /* Convolutions::convolution_gaussian_2d (include/numerics/convolutions.hpp:127-174), in place
  * on ny rows of nx. */
 int orc_smear_gaussian(double* data, int nx, int ny, double sigma);

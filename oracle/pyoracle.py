@@ -479,3 +479,12 @@ def normalize(data):
     d = np.ascontiguousarray(data, dtype=np.float64).copy()
     ok = L.orc_normalize(_p(d), C.c_long(d.size))
     return d, bool(ok)
+
+
+def structure_sum(intensities, iratios):
+    L = lib("port")
+    I = np.ascontiguousarray(intensities, dtype=np.float64).reshape(len(iratios), -1)
+    r = np.ascontiguousarray(iratios, dtype=np.float64)
+    out = np.zeros(I.shape[1])
+    L.orc_structure_sum(C.c_int(len(r)), C.c_long(I.shape[1]), _p(I), _p(r), _p(out))
+    return out

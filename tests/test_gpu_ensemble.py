@@ -59,3 +59,37 @@ def test_needs_a_dwba_grid(ctx, po):
     gb = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz + 0j)  # Born: one qz block
     with pytest.raises(hg.HgxError):
         model.dwba_mesh_grains(ctx, gb, sd, rots, centers, weights, abc, repet, scaling, fc, dn2)
+
+
+def test_structure_sum(ctx, po):
+    rng = np.random.default_rng(8)
+    I = rng.random((3, 20, 24))
+    for r in ([0.2, 0.3, 0.5], [1.0, 2.0, 5.0]):      # summing to 1, and rescaled
+        got = model.structure_sum(ctx, I, r)
+        ref = po.structure_sum(I, r).reshape(20, 24)
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_analytic_grain_loop_matches_oracle(ctx, po):
+    """Cylinders on a hex lattice with five grain orientations (the config-1 model with a
+    grain distribution) against the oracle's per-grain composition."""
+    rng = np.random.default_rng(9)
+    G = po.Grid(40, 30, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0)
+    ng = 5
+    rots = [po.rot_axis(2, a) for a in rng.uniform(-0.5, 0.5, ng)]
+    centers = rng.normal(scale=2.0, size=(ng, 3))
+    weights = rng.uniform(0.5, 1.5, ng)
+    abc = np.array(po.lattice_vectors("hex")[:3])
+    params = po.cylinder_params(5.0, 10.0, 0.05, 5)
+    tv = (0.5, -1.0, 0.0)
+    dn2 = (-2 * 4.88e-6, -2 * 7.37e-8)
+    fc = po.propagation_coeffs(G, [SUB], 0)
+    ref = np.zeros(G.n)
+    for R, c, w in zip(rots, centers, weights):
+        ff = po.ff_analytic(G, "cylinder", params, 0.0, 0.0, tv, R)
+        sf = po.sf_lattice(G, abc, (20, 20, 1), (20, 20, 20), c, R)
+        ref = po.dwba_combine(fc, sf, complex(*dn2) * ff, w, ref)
+    g = hg.QGrid.create(ctx, G.ncol, G.nrow, -2.0, 0.0, 2.0, 3.0, G.alpha_i, G.k0)
+    got = model.dwba_analytic_grains(ctx, g, "cylinder", params, rots, centers, weights, abc,
+                                     (20, 20, 1), (20, 20, 20), fc, dn2, transvec=tv)
+    assert po.rel_err(got, ref) < 1e-12

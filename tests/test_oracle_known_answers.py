@@ -136,3 +136,9 @@ def test_smearing_preserves_constants_and_is_local(po):
     out = po.smear_gaussian(pt, 1.0)
     nz = np.argwhere(out > 0)
     assert nz.min() >= 20 - 6 and nz.max() <= 20 + 6
+
+
+def test_structure_sum_rescales_iratios(po):
+    I = np.array([[1.0, 2.0], [3.0, 5.0]])
+    np.testing.assert_allclose(po.structure_sum(I, [1.0, 3.0]), 0.25 * I[0] + 0.75 * I[1])
+    np.testing.assert_allclose(po.structure_sum(I, [0.5, 0.5]), 0.5 * (I[0] + I[1]))
