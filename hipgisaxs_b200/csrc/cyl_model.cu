@@ -26,6 +26,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -49,6 +50,13 @@ constexpr CylShape CYL_SHAPES[] = {{256, 4}, {128, 1}, {128, 2}, {128, 4}, {256,
                                    {256, 2}, {256, 8}, {512, 1}, {512, 2}};
 constexpr int CYL_NSHAPES = sizeof(CYL_SHAPES) / sizeof(CYL_SHAPES[0]);
 constexpr int CYL_MIN_TILE = 128;                  // smallest threads*ppt above
+// Radial-sum tables of the FP32C pixel pass: per candidate, (fr, frR) of the sampled radii at
+// the nodes q_j = (j - 1) h, j = 0 .. CYL_NTAB - 1, h = (largest q_par of the grid) / CYL_QT;
+// the pixel pass interpolates them with 4-point Lagrange cubics (error ~ (h r)^4, about 1e-9
+// relative for r ~ 6 nm) instead of summing 2 Bessel functions per radius per pixel.  Both sums
+// depend on q_par only, which the in-plane rotation leaves unchanged.
+constexpr int CYL_QT = 1024;
+constexpr int CYL_NTAB = CYL_QT + 4;
 constexpr double PI_D = 3.141592653589793;
 
 // model parameter block of the C ABI (16 doubles)
@@ -67,6 +75,7 @@ struct CylCand {
   long item0, nitems;
   long rowtab0;      // offset of this candidate's rows in the row table
   double scale;
+  double rmin;       // smallest radius sample (the q_par -> 0 guard of the radial sums)
   double r[CYL_MAXS];
   double h[CYL_MAXS];
 };
@@ -143,6 +152,31 @@ __global__ void cyl_rows_kernel(const CylCand* __restrict__ cands,
   tab[c.rowtab0 + lr] = t;
 }
 
+// --------------------------------------------------------- radial-sum tables ----
+// One node per thread: (fr, frR) at q = |j - 1| h, as the pixel pass would sum them, except
+// that the q_par -> 0 guard takes the smooth limit (J1(x)/x -> 1/2, J0 -> 1) so that the
+// interpolation near q = 0 is right; pixels that meet the guard sum directly.
+__global__ void cyl_table_kernel(const CylCand* __restrict__ cands, double h, float2* __restrict__ table) {
+  const CylCand& c = cands[blockIdx.y];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= CYL_NTAB) return;
+  const float qp = (float)(fabs((double)(j - 1) * h));
+  float fr = 0.f, frR = 0.f;
+  for (int i = 0; i < c.nr; ++i) {
+    const float r = (float)c.r[i];
+    const float x = qp * r;
+    const float two_pi_r = (float)(2.0 * PI_D) * r;
+    if ((double)x * (double)x > 1.0e-13) {
+      fr += two_pi_r * r * j1f(x) / x;
+      frR += two_pi_r * r * j0f(x);
+    } else {
+      fr += two_pi_r * r * 0.5f;
+      frR += two_pi_r * r;
+    }
+  }
+  table[(long)blockIdx.y * CYL_NTAB + j] = make_float2(fr, frR / (float)c.R);
+}
+
 // --------------------------------------------------------------- pixel pass ----
 struct CylArgs {
   const CylCand* cands;
@@ -156,6 +190,8 @@ struct CylArgs {
   const unsigned* mask;  // may be NULL
   double* intensity;     // may be NULL
   double* partial;       // 5 doubles per item (chi2, dR, dH, da, dphi)
+  const float2* table;   // FP32C: CYL_NTAB (fr, frR) per candidate
+  double inv_h;          // 1 / node spacing of the table
 };
 
 template <typename T>
@@ -214,19 +250,39 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
       double qx = a.qx[p], qy = a.qy[p];
       double mx = c.cphi * qx - c.sphi * qy, my = c.sphi * qx + c.cphi * qy;
       double qpar = sqrt(mx * mx + my * my);
-      // radial sums (precision T)
+      // radial sums (precision T); FP32C interpolates the candidate's table except where a
+      // radius sample meets the reference's q_par -> 0 guard (then the terms are summed)
       T fr = 0, frR = 0;
-      const T qp = (T)qpar;
-      for (int i = 0; i < c.nr; ++i) {
-        T r = (T)c.r[i];
-        T x = qp * r;
-        if ((double)x * (double)x > 1.0e-13) {
-          T two_pi_r = (T)(2.0 * PI_D) * r;
-          fr += two_pi_r * r * BesselT<T>::J1(x) / x;
-          frR += two_pi_r * r * BesselT<T>::J0(x);
+      bool direct = true;
+      if constexpr (std::is_same<T, float>::value) {
+        if (qpar * qpar * c.rmin * c.rmin > 1.0e-13) {
+          direct = false;
+          const double u = qpar * a.inv_h + 1.0;
+          const int i0 = min(max((int)u, 1), CYL_NTAB - 3);
+          const float t = (float)(u - i0);
+          const float2* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
+          const float w0 = -t * (t - 1.f) * (t - 2.f) * (1.f / 6.f);
+          const float w1 = (t + 1.f) * (t - 1.f) * (t - 2.f) * 0.5f;
+          const float w2 = -(t + 1.f) * t * (t - 2.f) * 0.5f;
+          const float w3 = (t + 1.f) * t * (t - 1.f) * (1.f / 6.f);
+          const float2 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
+          fr = w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x;
+          frR = w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y;
         }
       }
-      frR /= (T)c.R;
+      if (direct) {
+        const T qp = (T)qpar;
+        for (int i = 0; i < c.nr; ++i) {
+          T r = (T)c.r[i];
+          T x = qp * r;
+          if ((double)x * (double)x > 1.0e-13) {
+            T two_pi_r = (T)(2.0 * PI_D) * r;
+            fr += two_pi_r * r * BesselT<T>::J1(x) / x;
+            frR += two_pi_r * r * BesselT<T>::J0(x);
+          }
+        }
+        frR /= (T)c.R;
+      }
       // lattice factors in FP64
       double tha = c.a * (c.ua[0] * mx + c.ua[1] * my);
       double thb = c.a * (c.ub[0] * mx + c.ub[1] * my);
@@ -419,6 +475,7 @@ int cyl_fill_cand(const double* m, const double* abc9, const int* roi, double sc
   c.nr = (int)rv.size();
   c.nh = (int)hv.size();
   for (int i = 0; i < c.nr; ++i) c.r[i] = rv[i];
+  c.rmin = c.nr > 0 ? *std::min_element(rv.begin(), rv.end()) : 0.0;
   for (int i = 0; i < c.nh; ++i) c.h[i] = hv[i];
   c.row0 = roi[0];
   c.col0 = roi[1];
@@ -448,6 +505,8 @@ struct hgx_cyl_batch_s {
   cudaGraphExec_t exec = nullptr;
   int persistent_blocks = 0;
   int shape = 0;  // tile shape of the pixel pass (index into the shape table)
+  hgx::DevBuf d_table;  // FP32C radial-sum tables
+  double table_h = 1.0;  // their node spacing
 };
 
 namespace hgx {
@@ -473,6 +532,11 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
   a.mask = with_counts ? (const unsigned*)b->d_mask.p : nullptr;
   a.intensity = with_intensity ? (double*)b->d_inten.p : nullptr;
   a.partial = (double*)b->d_partial.p;
+  a.table = (const float2*)b->d_table.p;
+  a.inv_h = 1.0 / b->table_h;
+  if (b->precision == HGX_F32C)
+    cyl_table_kernel<<<dim3((CYL_NTAB + 127) / 128, b->ncand), 128, 0, st>>>(
+        (const CylCand*)b->d_cands.p, b->table_h, (float2*)b->d_table.p);
   long blocks = std::min<long>(b->nitems, (long)b->persistent_blocks);
   cudaError_t e = b->precision == HGX_F64
                       ? cyl_pixels_at<double, 0>(b->shape, (unsigned)blocks, a, st, nullptr)
@@ -618,6 +682,17 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return bail(cuda_fail(e, "hgx_cyl_batch_create: copies"));
   if (!mask) b->d_mask.release();
+  if (precision == HGX_F32C) {
+    // node spacing of the radial-sum tables: the grid's largest q_par over CYL_QT intervals
+    std::vector<double> hx(g->nqy), hy(g->nqy);
+    e = cudaMemcpy(hx.data(), g->qx, sizeof(double) * g->nqy, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(hy.data(), g->qy, sizeof(double) * g->nqy, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "hgx_cyl_batch_create: read q-grid"));
+    double qm = 0.0;
+    for (int i = 0; i < g->nqy; ++i) qm = std::max(qm, sqrt(hx[i] * hx[i] + hy[i] * hy[i]));
+    b->table_h = (qm > 0.0 ? qm : 1.0) * (1.0 + 1e-9) / CYL_QT;
+    if ((s = b->d_table.reserve(sizeof(float2) * CYL_NTAB * (size_t)ncand))) return bail(s);
+  }
   if ((s = cyl_apply_shape(b, 0))) return bail(s);
   *out = b;
   return HGX_OK;
