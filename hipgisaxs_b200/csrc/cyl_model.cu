@@ -54,7 +54,9 @@ constexpr int CYL_MIN_TILE = 128;                  // smallest threads*ppt above
 // the nodes q_j = (j - 1) h, j = 0 .. CYL_NTAB - 1, h = (largest q_par of the grid) / CYL_QT;
 // the pixel pass interpolates them with 4-point Lagrange cubics (error ~ (h r)^4, about 1e-9
 // relative for r ~ 6 nm) instead of summing 2 Bessel functions per radius per pixel.  Both sums
-// depend on q_par only, which the in-plane rotation leaves unchanged.
+// depend on q_par only, which the in-plane rotation leaves unchanged.  Tables and interpolation
+// are FP64: the gradient sums over a detector cancel near an optimum, and FP32 radial sums
+// brought the batch's worst gradient error to 1e-5 of FP64.
 constexpr int CYL_QT = 1024;
 constexpr int CYL_NTAB = CYL_QT + 4;
 constexpr double PI_D = 3.141592653589793;
@@ -156,25 +158,25 @@ __global__ void cyl_rows_kernel(const CylCand* __restrict__ cands,
 // One node per thread: (fr, frR) at q = |j - 1| h, as the pixel pass would sum them, except
 // that the q_par -> 0 guard takes the smooth limit (J1(x)/x -> 1/2, J0 -> 1) so that the
 // interpolation near q = 0 is right; pixels that meet the guard sum directly.
-__global__ void cyl_table_kernel(const CylCand* __restrict__ cands, double h, float2* __restrict__ table) {
+__global__ void cyl_table_kernel(const CylCand* __restrict__ cands, double h, double2* __restrict__ table) {
   const CylCand& c = cands[blockIdx.y];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= CYL_NTAB) return;
-  const float qp = (float)(fabs((double)(j - 1) * h));
-  float fr = 0.f, frR = 0.f;
+  const double qp = fabs((double)(j - 1) * h);
+  double fr = 0.0, frR = 0.0;
   for (int i = 0; i < c.nr; ++i) {
-    const float r = (float)c.r[i];
-    const float x = qp * r;
-    const float two_pi_r = (float)(2.0 * PI_D) * r;
-    if ((double)x * (double)x > 1.0e-13) {
-      fr += two_pi_r * r * j1f(x) / x;
-      frR += two_pi_r * r * j0f(x);
+    const double r = c.r[i];
+    const double x = qp * r;
+    const double two_pi_r = 2.0 * PI_D * r;
+    if (x * x > 1.0e-13) {
+      fr += two_pi_r * r * j1(x) / x;
+      frR += two_pi_r * r * j0(x);
     } else {
-      fr += two_pi_r * r * 0.5f;
+      fr += two_pi_r * r * 0.5;
       frR += two_pi_r * r;
     }
   }
-  table[(long)blockIdx.y * CYL_NTAB + j] = make_float2(fr, frR / (float)c.R);
+  table[(long)blockIdx.y * CYL_NTAB + j] = make_double2(fr, frR / c.R);
 }
 
 // --------------------------------------------------------------- pixel pass ----
@@ -190,7 +192,7 @@ struct CylArgs {
   const unsigned* mask;  // may be NULL
   double* intensity;     // may be NULL
   double* partial;       // 5 doubles per item (chi2, dR, dH, da, dphi)
-  const float2* table;   // FP32C: CYL_NTAB (fr, frR) per candidate
+  const double2* table;  // FP32C: CYL_NTAB (fr, frR) per candidate
   double inv_h;          // 1 / node spacing of the table
 };
 
@@ -253,21 +255,22 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
       // radial sums (precision T); FP32C interpolates the candidate's table except where a
       // radius sample meets the reference's q_par -> 0 guard (then the terms are summed)
       T fr = 0, frR = 0;
+      double frt = 0.0, frRt = 0.0;  // interpolated (FP64 tables)
       bool direct = true;
       if constexpr (std::is_same<T, float>::value) {
         if (qpar * qpar * c.rmin * c.rmin > 1.0e-13) {
           direct = false;
           const double u = qpar * a.inv_h + 1.0;
           const int i0 = min(max((int)u, 1), CYL_NTAB - 3);
-          const float t = (float)(u - i0);
-          const float2* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
-          const float w0 = -t * (t - 1.f) * (t - 2.f) * (1.f / 6.f);
-          const float w1 = (t + 1.f) * (t - 1.f) * (t - 2.f) * 0.5f;
-          const float w2 = -(t + 1.f) * t * (t - 2.f) * 0.5f;
-          const float w3 = (t + 1.f) * t * (t - 1.f) * (1.f / 6.f);
-          const float2 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
-          fr = w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x;
-          frR = w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y;
+          const double t = u - i0;
+          const double2* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
+          const double w0 = -t * (t - 1.0) * (t - 2.0) * (1.0 / 6.0);
+          const double w1 = (t + 1.0) * (t - 1.0) * (t - 2.0) * 0.5;
+          const double w2 = -(t + 1.0) * t * (t - 2.0) * 0.5;
+          const double w3 = (t + 1.0) * t * (t - 1.0) * (1.0 / 6.0);
+          const double2 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
+          frt = w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x;
+          frRt = w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y;
         }
       }
       if (direct) {
@@ -283,6 +286,7 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
         }
         frR /= (T)c.R;
       }
+      const double FR = direct ? (double)fr : frt, FRR = direct ? (double)frR : frRt;
       // lattice factors in FP64
       double tha = c.a * (c.ua[0] * mx + c.ua[1] * my);
       double thb = c.a * (c.ub[0] * mx + c.ub[1] * my);
@@ -299,12 +303,12 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
       zd KQ = zd(c.K[0], c.K[1]) * zd(rt.Q);
       double SS = Sa * Sb;
       zd base = KQ * Pc;  // K Q Pc
-      zd A = base * ((double)fr * SS);
-      zd dA_R = base * ((double)frR * SS);
-      zd dA_H = (zd(c.K[0], c.K[1]) * zd(rt.QH)) * Pc * ((double)fr * SS);
-      zd dA_a = Pc * zd(c.K[0], c.K[1]) * (double)fr *
+      zd A = base * (FR * SS);
+      zd dA_R = base * (FRR * SS);
+      zd dA_H = (zd(c.K[0], c.K[1]) * zd(rt.QH)) * Pc * (FR * SS);
+      zd dA_a = Pc * zd(c.K[0], c.K[1]) * FR *
                 (zd(rt.Q) * ((dSa * tha / c.a) * Sb + Sa * (dSb * thb / c.a)) + zd(rt.Qa) * SS);
-      zd dA_p = KQ * (double)fr *
+      zd dA_p = KQ * FR *
                 (Pc * (dSa * dtha_dphi * Sb + Sa * dSb * dthb_dphi) + Pc * zd(0, dph) * SS);
       double I = A.x * A.x + A.y * A.y;
       if (a.intensity) a.intensity[c.px_off + idx] = I;
@@ -532,11 +536,11 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
   a.mask = with_counts ? (const unsigned*)b->d_mask.p : nullptr;
   a.intensity = with_intensity ? (double*)b->d_inten.p : nullptr;
   a.partial = (double*)b->d_partial.p;
-  a.table = (const float2*)b->d_table.p;
+  a.table = (const double2*)b->d_table.p;
   a.inv_h = 1.0 / b->table_h;
   if (b->precision == HGX_F32C)
     cyl_table_kernel<<<dim3((CYL_NTAB + 127) / 128, b->ncand), 128, 0, st>>>(
-        (const CylCand*)b->d_cands.p, b->table_h, (float2*)b->d_table.p);
+        (const CylCand*)b->d_cands.p, b->table_h, (double2*)b->d_table.p);
   long blocks = std::min<long>(b->nitems, (long)b->persistent_blocks);
   cudaError_t e = b->precision == HGX_F64
                       ? cyl_pixels_at<double, 0>(b->shape, (unsigned)blocks, a, st, nullptr)
@@ -691,7 +695,7 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
     double qm = 0.0;
     for (int i = 0; i < g->nqy; ++i) qm = std::max(qm, sqrt(hx[i] * hx[i] + hy[i] * hy[i]));
     b->table_h = (qm > 0.0 ? qm : 1.0) * (1.0 + 1e-9) / CYL_QT;
-    if ((s = b->d_table.reserve(sizeof(float2) * CYL_NTAB * (size_t)ncand))) return bail(s);
+    if ((s = b->d_table.reserve(sizeof(double2) * CYL_NTAB * (size_t)ncand))) return bail(s);
   }
   if ((s = cyl_apply_shape(b, 0))) return bail(s);
   *out = b;

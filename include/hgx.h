@@ -284,8 +284,9 @@ int hgx_normalize(hgx_ctx ctx, double* data, long n, int* normalized);
  * abc9: unscaled lattice vectors with a, b in the plane and c along z (hex, cubic).
  * rois: 4 ints per candidate (row0, col0, nrows, ncols); counts: the candidates' ROI images
  * concatenated (row-major), or NULL for forward-only batches; mask: same layout or NULL;
- * scale: the model-to-counts factor of the chi^2.  precision: HGX_F32C (FP32 Bessel sums,
- * FP64 lattice phases and reductions) or HGX_F64. */
+ * scale: the model-to-counts factor of the chi^2.  precision: HGX_F32C (the radial Bessel
+ * sums interpolated from per-candidate FP64 tables over q_par, FP64 lattice phases and
+ * reductions) or HGX_F64 (every Bessel function evaluated per pixel). */
 typedef struct hgx_cyl_batch_s* hgx_cyl_batch;
 int hgx_cyl_batch_create(hgx_ctx ctx, hgx_qgrid g, const double* rowfc, const double* abc9,
                          int ncand, const int* rois, const double* counts,
