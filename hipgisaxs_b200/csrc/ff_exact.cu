@@ -244,11 +244,12 @@ int hgx_ff_exact_triangles(hgx_ctx c, const double* tris, int ntri, int nqy, con
                            const double* qy, int nqz, const double* qz, const double* rot9,
                            double* ff) {
   if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_exact_triangles: no triangles");
+  if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_exact_triangles: null context");
+  HGX_CUDA(cudaSetDevice(c->device));
   hgx_qgrid g = nullptr;
-  HGX_TRY(hgx_qgrid_from_arrays(c, nqy, qx, qy, nqz, qz, 0, &g));
+  HGX_TRY(shaped_grid(c, nqy, qx, qy, nqz, qz, &g));
   int s = hgx_ff_exact_triangles_q(c, g, tris, ntri, rot9, ff, HGX_C128);
   if (s == HGX_OK) s = hgx_synchronize(c);
-  hgx_qgrid_destroy(g);
   return s;
 }
 

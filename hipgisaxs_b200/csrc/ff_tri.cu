@@ -857,10 +857,9 @@ int hgx_ff_triangles_q_ex(hgx_ctx c, hgx_qgrid g, const double* shape_def, int n
   const size_t esz = ff_type == HGX_C64 ? sizeof(float2) : sizeof(double2);
   const bool host_out = !is_device_ptr(ff);
   void* dout = ff;
-  DevBuf tmp;
-  if (host_out) {
-    HGX_TRY(tmp.reserve(esz * (size_t)g->nqz));
-    dout = tmp.p;
+  if (host_out) {  // the context's output staging (the call synchronises before returning)
+    HGX_TRY(c->shaped_out.reserve(esz * (size_t)g->nqz));
+    dout = c->shaped_out.p;
   }
   HGX_TRY(ff_triangles_device(c, g, sd, ntri, rot9, precision, dout, ff_type, pixels));
   if (host_out) {
@@ -951,11 +950,12 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
                      const double* qy, int nqz, const double* qz, const double* rot9,
                      int precision, double* ff) {
   if (ntri < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: no triangles");
+  if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: null context");
+  HGX_CUDA(cudaSetDevice(c->device));
   hgx_qgrid g = nullptr;
-  HGX_TRY(hgx_qgrid_from_arrays(c, nqy, qx, qy, nqz, qz, 0, &g));
+  HGX_TRY(shaped_grid(c, nqy, qx, qy, nqz, qz, &g));
   int s = hgx_ff_triangles_q(c, g, shape_def, ntri, rot9, precision, ff, HGX_C128);
   if (s == HGX_OK && is_device_ptr(ff)) s = hgx_synchronize(c);
-  hgx_qgrid_destroy(g);
   return s;
 }
 

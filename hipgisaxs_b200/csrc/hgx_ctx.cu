@@ -113,12 +113,74 @@ int finish_out(hgx_ctx c, void* p, size_t bytes, const void* dev) {
   return hgx_synchronize(c);
 }
 
+// Detector row length of a grid given as arrays: where qz of block 0 first changes (the QGrid
+// layout keeps qz constant along a row); 0 when that cannot be read.
+static int detect_ncol(hgx_qgrid g, const double* qz, int* ncol) {
+  *ncol = 0;
+  if (g->nk < 1) return HGX_OK;
+  std::vector<double> h;
+  const double* src = qz;
+  if (is_device_ptr(qz)) {
+    h.resize(2 * (size_t)g->nqy);
+    cudaError_t e = cudaMemcpyAsync(h.data(), qz, sizeof(double2) * g->nqy, cudaMemcpyDeviceToHost,
+                                    g->ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "q-grid: read qz");
+    src = h.data();
+  }
+  int n = 1;
+  while (n < g->nqy && src[2 * n] == src[0] && src[2 * n + 1] == src[1]) ++n;
+  *ncol = n;
+  return HGX_OK;
+}
+
+int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
+                hgx_qgrid* out) {
+  hgx_qgrid g = c->shaped;
+  if (g && g->nqy == nqy && g->nqz == nqz) {
+    cudaStream_t st = c->stream;
+    auto kind = [](const void* p) { return is_device_ptr(p) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; };
+    cudaError_t e = cudaMemcpyAsync(g->qx, qx, sizeof(double) * nqy, kind(qx), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->qy, qy, sizeof(double) * nqy, kind(qy), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->qz, qz, sizeof(double2) * nqz, kind(qz), st);
+    int s = e == cudaSuccess ? HGX_OK : cuda_fail(e, "q-grid refill: copy");
+    int ncol = 0;
+    if (s == HGX_OK) s = detect_ncol(g, qz, &ncol);
+    if (s == HGX_OK) {
+      g->ncol = ncol;
+      s = qgrid_finalize(g);
+    }
+    if (s == HGX_OK) {
+      *out = g;
+      return HGX_OK;
+    }
+    hgx_qgrid_destroy(g);  // leave no half-refilled grid behind
+    c->shaped = nullptr;
+    return s;
+  }
+  if (g) {
+    hgx_qgrid_destroy(g);
+    c->shaped = nullptr;
+  }
+  HGX_TRY(hgx_qgrid_from_arrays(c, nqy, qx, qy, nqz, qz, 0, &g));
+  c->shaped = g;
+  *out = g;
+  return HGX_OK;
+}
+
 int qgrid_finalize(hgx_qgrid g) {
   g->mode = 0;
   if (g->nk != 1 && g->nk != 4) return HGX_OK;
   if (g->ncol <= 0 || g->nqy % g->ncol != 0) return HGX_OK;
   g->nrow = g->nqy / g->ncol;
-  HGX_CUDA(cudaMalloc(&g->rowqz, sizeof(double2) * (size_t)g->nrow * g->nk));
+  const size_t need = (size_t)g->nrow * g->nk;
+  if (need > g->rowqz_cap) {
+    if (g->rowqz) cudaFree(g->rowqz);
+    g->rowqz = nullptr;
+    g->rowqz_cap = 0;
+    HGX_CUDA(cudaMalloc(&g->rowqz, sizeof(double2) * need));
+    g->rowqz_cap = need;
+  }
   HGX_TRY(g->ctx->scratch.reserve(256));
   unsigned* d_flags = reinterpret_cast<unsigned*>(g->ctx->scratch.p);
   cudaStream_t st = g->ctx->stream;
@@ -130,9 +192,7 @@ int qgrid_finalize(hgx_qgrid g) {
   unsigned flags = 0;
   HGX_CUDA(cudaMemcpyAsync(&flags, d_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   HGX_CUDA(cudaStreamSynchronize(st));
-  if (flags & 1u) {  // not row-constant: the per-q-point kernels handle it
-    cudaFree(g->rowqz);
-    g->rowqz = nullptr;
+  if (flags & 1u) {  // not row-constant: the per-q-point kernels handle it (row table unused)
     g->nrow = 0;
     g->mode = 0;
     return HGX_OK;
@@ -195,8 +255,10 @@ int hgx_destroy(hgx_ctx c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   if (c->d_err) cudaFree(c->d_err);
+  if (c->shaped) hgx_qgrid_destroy(c->shaped);
   c->scratch.release();
   c->staging.release();
+  c->shaped_out.release();
   delete c;
   return HGX_OK;
 }
@@ -254,18 +316,8 @@ int hgx_qgrid_from_arrays(hgx_ctx c, int nqy, const double* qx, const double* qy
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "hgx_qgrid_from_arrays: copy"));
   // detector row length: given, or found where qz of block 0 first changes
   if (ncol == 0 && g->nk >= 1) {
-    std::vector<double> h;
-    const double* src = qz;
-    if (is_device_ptr(qz)) {
-      h.resize(2 * (size_t)nqy);
-      e = cudaMemcpyAsync(h.data(), qz, sizeof(double2) * nqy, cudaMemcpyDeviceToHost, st);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e != cudaSuccess) return cleanup(cuda_fail(e, "hgx_qgrid_from_arrays: read qz"));
-      src = h.data();
-    }
-    int n = 1;
-    while (n < nqy && src[2 * n] == src[0] && src[2 * n + 1] == src[1]) ++n;
-    ncol = n;
+    int s0 = detect_ncol(g, qz, &ncol);
+    if (s0 != HGX_OK) return cleanup(s0);
   }
   g->ncol = ncol;
   int s = qgrid_finalize(g);

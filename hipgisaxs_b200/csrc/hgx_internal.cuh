@@ -58,6 +58,11 @@ struct hgx_ctx_s {
   hgx::DevBuf staging;        // device copies of host inputs
   int sm_count = 148;
   int max_smem_optin = 227 * 1024;
+  // the q-grid and device output of the reference-shaped calls (explicit host arrays in,
+  // host array out), kept between calls and refilled in place while the sizes stay the same,
+  // so that those calls allocate and free no device memory
+  hgx_qgrid_s* shaped = nullptr;
+  hgx::DevBuf shaped_out;
 };
 
 // -------------------------------------------------------------- the q-grid ----
@@ -71,12 +76,17 @@ struct hgx_qgrid_s {
   double2* rowqz = nullptr;      // nrow x nk: the row-constant qz of each block (modes 1, 2)
   double* qz_det = nullptr;      // nqy: detector qz (grids made by hgx_qgrid_create)
   double* alpha = nullptr;       // nrow exit angles (grids made by hgx_qgrid_create)
+  size_t rowqz_cap = 0;          // allocated entries of rowqz
   int tuned_p = 0;               // FP32 row-kernel launch shape chosen by hgx_ff_tune (0: none)
 };
 
 namespace hgx {
 // Prepares triangle tiles for the FP32 kernels (see ff_tri.cu).
 int qgrid_finalize(hgx_qgrid g);  // builds the row table and picks the mode
+// The context's grid for reference-shaped calls with these arrays: the kept one refilled in
+// place when nqy and nqz match, else a new one (the old one destroyed).
+int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
+                hgx_qgrid* out);
 }  // namespace hgx
 
 namespace hgx {
