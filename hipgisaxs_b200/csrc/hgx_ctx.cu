@@ -256,6 +256,7 @@ int hgx_destroy(hgx_ctx c) {
   cudaStreamSynchronize(c->stream);
   if (c->d_err) cudaFree(c->d_err);
   if (c->shaped) hgx_qgrid_destroy(c->shaped);
+  delete c->mesh;
   c->scratch.release();
   c->staging.release();
   c->shaped_out.release();

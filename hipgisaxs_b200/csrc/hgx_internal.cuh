@@ -49,6 +49,14 @@ struct DevBuf {
 
 }  // namespace hgx
 
+namespace hgx {
+// Device buffers of hgx_mesh_chi2_grad, kept by the context between calls (grow-only): large
+// cudaMalloc/cudaFree pairs per call cost tens to hundreds of milliseconds.
+struct MeshWork {
+  DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib, bwpart;
+};
+}  // namespace hgx
+
 // -------------------------------------------------------------- the context ----
 struct hgx_ctx_s {
   int device = 0;
@@ -63,6 +71,7 @@ struct hgx_ctx_s {
   // so that those calls allocate and free no device memory
   hgx_qgrid_s* shaped = nullptr;
   hgx::DevBuf shaped_out;
+  hgx::MeshWork* mesh = nullptr;  // work buffers of the mesh chi^2 and gradient
 };
 
 // -------------------------------------------------------------- the q-grid ----

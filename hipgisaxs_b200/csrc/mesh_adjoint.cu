@@ -363,7 +363,12 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
   static const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   const double* R = rot9 ? rot9 : eye;
   // inputs on the device
-  DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib;
+  if (!c->mesh) c->mesh = new (std::nothrow) MeshWork();
+  if (!c->mesh) return fail(HGX_ERR_NO_MEMORY, "hgx_mesh_chi2_grad: host allocation");
+  MeshWork& w = *c->mesh;
+  DevBuf &bv = w.bv, &bf = w.bf, &bfc = w.bfc, &bc = w.bc, &bm = w.bm, &sd = w.sd, &F = w.F,
+         &seeds = w.seeds, &part = w.part, &gtri = w.gtri, &vptr = w.vptr, &vfac = w.vfac,
+         &gvb = w.gvb, &Ib = w.Ib;
   const void *dv, *df, *dfc, *dc = nullptr, *dm = nullptr;
   HGX_TRY(stage_in(c, verts, sizeof(double) * 3 * nv, bv, &dv));
   HGX_TRY(stage_in(c, faces, sizeof(int) * 3 * nf, bf, &df));
@@ -412,7 +417,7 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
     const int rpc = (g->nrow + chunks - 1) / chunks;
     chunks = (g->nrow + rpc - 1) / rpc;
     HGX_TRY(gtri.reserve(sizeof(double) * 6 * nf));
-    DevBuf bwpart;
+    DevBuf& bwpart = w.bwpart;
     HGX_TRY(bwpart.reserve(sizeof(double) * 6 * (size_t)nf * chunks));
     BwArgs ba;
     ba.tiles = reinterpret_cast<const float*>(c->scratch.p);  // tiles left by the forward
