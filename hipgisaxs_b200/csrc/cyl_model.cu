@@ -510,6 +510,7 @@ struct hgx_cyl_batch_s {
   int persistent_blocks = 0;
   int shape = 0;  // tile shape of the pixel pass (index into the shape table)
   hgx::DevBuf d_table;  // FP32C radial-sum tables
+  hgx::DevBuf d_plain;  // the candidate record of hgx_cyl_plain_forward
   double table_h = 1.0;  // their node spacing
 };
 
@@ -758,7 +759,8 @@ int hgx_cyl_plain_forward(hgx_cyl_batch_s* b, int cand, const double* model, dou
   cudaStream_t st = b->ctx->stream;
   CylCand cnd;
   HGX_TRY(cyl_fill_cand(model, b->abc9, b->rois.data() + 4 * cand, b->scale, cnd));
-  DevBuf dc, dout;
+  DevBuf dout;
+  DevBuf& dc = b->d_plain;
   HGX_TRY(dc.reserve(sizeof(CylCand)));
   HGX_CUDA(cudaMemcpyAsync(dc.p, &cnd, sizeof(CylCand), cudaMemcpyHostToDevice, st));
   long n = (long)cnd.nrows * cnd.ncols;

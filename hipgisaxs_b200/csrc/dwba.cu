@@ -121,13 +121,14 @@ static int distance_entry(hgx_ctx c, int kind, long n, const double* ref, const 
   if (!c || !ref || !data || !out) return fail(HGX_ERR_INVALID_ARG, "distance: null argument");
   if (n < 1) return fail(HGX_ERR_INVALID_ARG, "distance: empty input");
   HGX_CUDA(cudaSetDevice(c->device));
-  DevBuf br, bd, bm, bo;
+  DevBuf br, bd, bm;
   const void *dr, *dd, *dm = nullptr;
   HGX_TRY(stage_in(c, ref, sizeof(double) * n, br, &dr));
   HGX_TRY(stage_in(c, data, sizeof(double) * n, bd, &dd));
   HGX_TRY(stage_in(c, mask, sizeof(unsigned) * n, bm, &dm));
-  void* dout = nullptr;
-  HGX_TRY(stage_out(c, out, sizeof(double), bo, &dout));
+  // a host result goes through the context's scratch, after the reduction's partial sums
+  HGX_TRY(c->scratch.reserve(sizeof(double) * (RED_BLOCKS + 1)));
+  void* dout = is_device_ptr(out) ? (void*)out : (void*)(reinterpret_cast<double*>(c->scratch.p) + RED_BLOCKS);
   HGX_TRY(distance_device(c, kind, n, (const double*)dr, (const double*)dd, (const unsigned*)dm,
                           scale, (double*)dout));
   HGX_TRY(finish_out(c, out, sizeof(double), dout));
