@@ -47,6 +47,24 @@ TRAFFIC_BYTES_PER_LAUNCH = 115.8e6
 TRAFFIC_SOURCE = "ncu capture at 1536x1536 (65.1 MB) scaled by pixels to 2048x2048"
 
 
+def hbm_view(ms_step):
+    """The row kernel against HBM bandwidth (MEASURED_PEAKS.json): its algorithmic bytes per
+    launch are the q-grid read once (qx, qy FP64) and the complex64 output written once; the
+    measured DRAM traffic is TRAFFIC_BYTES_PER_LAUNCH.  Far below 1: not memory-bound."""
+    n = NCOL * NROW
+    alg = 2 * 8 * n + 4 * 8 * n
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    achieved = alg / (ms_step * 1e-3) / 1e9
+    return {"bound": "hbm", "algorithmic_bytes": alg, "achieved": achieved, "unit": "GB/s",
+            "peak": peak, "frac": None if peak is None else achieved / peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)"}
+
+
 def max_over_ranks(x, dist, device):
     """The largest x over all ranks (the slowest replica's time); x itself without a process
     group.  Every rank must call it at the same point."""
@@ -600,7 +618,8 @@ def main():
                          "peak_source": "hgx_measure_peaks FFMA probe, sustained 2 s, same GPU",
                          "flop_per_pixel_triangle": FLOP_PER_PIXEL_TRI,
                          "sfu": {"achieved_gops": sfu_rate, "peak_gops": peak_sfu,
-                                 "frac": sfu_rate / peak_sfu}},
+                                 "frac": sfu_rate / peak_sfu},
+                         "hbm_view": hbm_view(ms_step)},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
             "exact_triangle": exact,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
