@@ -61,6 +61,7 @@ SIGNATURES = {
     "hgx_structure_sum": (_i, [_vp, _i, C.c_long, _vp, _vp, _vp]),
     "hgx_gaussian_smearing": (_i, [_vp, _vp, _i, _i, _d]),
     "hgx_normalize": (_i, [_vp, _vp, C.c_long, C.POINTER(_i)]),
+    "hgx_save_gisaxs": (_i, [_vp, _vp, _i, _i, C.c_char_p]),
     "hgx_cyl_batch_create": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _d, _i, C.POINTER(_vp)]),
     "hgx_cyl_batch_eval": (_i, [_vp, _vp, _vp]),
     "hgx_cyl_batch_forward": (_i, [_vp, _vp, _vp]),

@@ -7,6 +7,8 @@
 //    weights are those of an unclipped window shifted to the border.  Both as the reference.
 //  * normalize: HipGISAXS::normalize (src/sim/hipgisaxs_main.cpp:1439-1450), (x - min) /
 //    (max - min) over every element except the first, which the reference leaves unscaled.
+//  * save: HipGISAXS::save_gisaxs (src/sim/hipgisaxs_main.cpp:2250-2260), the ".out" text
+//    image: each value in the default stream format followed by a tab, one row per line.
 // FP64, compiled without fused multiply-adds (hipgisaxs_b200/build.py) so that every sum
 // rounds as the reference's does; both passes are bound by memory bandwidth.
 #include <cuda_runtime.h>
@@ -14,6 +16,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <fstream>
 #include <vector>
 
 #include "hgx_internal.cuh"
@@ -157,6 +160,30 @@ int hgx_normalize(hgx_ctx c, double* data, long n, int* normalized) {
   }
   if (normalized) *normalized = ok;
   return hgx_synchronize(c);
+}
+
+int hgx_save_gisaxs(hgx_ctx c, const double* image, int nrow, int ncol, const char* path) {
+  if (!image || !path || nrow < 1 || ncol < 1)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_save_gisaxs: null argument or empty image");
+  const size_t n = (size_t)nrow * ncol;
+  std::vector<double> h;
+  const double* src = image;
+  if (is_device_ptr(image)) {
+    if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_save_gisaxs: a device image needs a context");
+    HGX_CUDA(cudaSetDevice(c->device));
+    h.resize(n);
+    HGX_CUDA(cudaMemcpyAsync(h.data(), image, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    HGX_TRY(hgx_synchronize(c));
+    src = h.data();
+  }
+  std::ofstream f(path);
+  if (!f.is_open()) return fail(HGX_ERR_INVALID_ARG, std::string("hgx_save_gisaxs: cannot open ") + path);
+  for (int z = 0; z < nrow; ++z) {
+    for (int y = 0; y < ncol; ++y) f << src[(size_t)ncol * z + y] << "\t";
+    f << std::endl;
+  }
+  if (!f.good()) return fail(HGX_ERR_INVALID_ARG, std::string("hgx_save_gisaxs: write failed: ") + path);
+  return HGX_OK;
 }
 
 }  // extern "C"

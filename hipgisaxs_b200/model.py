@@ -153,6 +153,19 @@ def dwba_analytic_grains(ctx: Context, grid: QGrid, shape, params, rots, centers
     return out
 
 
+def save_gisaxs(path, image, ctx: Context = None):
+    """Writes a (nrow, ncol) image as the reference's ".out" text (hgx_save_gisaxs)."""
+    if _is_tensor(image):
+        nrow, ncol = image.shape
+        ptr, keep = image.data_ptr(), image
+    else:
+        keep = np.ascontiguousarray(image, dtype=np.float64)
+        nrow, ncol = keep.shape
+        ptr = keep.ctypes.data
+    check(lib().hgx_save_gisaxs(None if ctx is None else ctx.handle, ptr, int(nrow), int(ncol),
+                                str(path).encode()))
+
+
 def structure_sum(ctx: Context, intensities, iratios):
     """Sum over structures weighted by their (rescaled) iratios (hgx_structure_sum)."""
     I = np.ascontiguousarray(intensities, dtype=np.float64)

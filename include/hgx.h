@@ -260,6 +260,11 @@ int hgx_gaussian_smearing(hgx_ctx ctx, double* image, int ncol, int nrow, double
  * (max - min) for every element but the first (left as it is, as in the reference);
  * *normalized = 0 and nothing changes when max - min < 1e-30.  Synchronous. */
 int hgx_normalize(hgx_ctx ctx, double* data, long n, int* normalized);
+/* HipGISAXS::save_gisaxs (src/sim/hipgisaxs_main.cpp:2250-2260): the ".out" text image, each
+ * value in the default C++ stream format (6 significant digits) followed by a tab, one
+ * detector row per line.  image: nrow x ncol doubles, host memory or device memory of ctx's
+ * GPU (ctx may be NULL for a host image). */
+int hgx_save_gisaxs(hgx_ctx ctx, const double* image, int nrow, int ncol, const char* path);
 
 /* -------------------------------------------- fitting: chi^2 and its gradient ---- */
 /* A fused model for the fitting front end: cylinders on a 2-D lattice in DWBA (one grain,

@@ -31,3 +31,14 @@ def test_lattice_vectors_reject_unknown():
     from hipgisaxs_b200 import HgxError
     with pytest.raises(HgxError):
         model.lattice_vectors("cubic", "111")
+
+
+def test_save_gisaxs_matches_the_stream_format(tmp_path):
+    """The ".out" text of HipGISAXS::save_gisaxs: default C++ stream formatting (6 significant
+    digits, %g-like), a tab after every value, one row per line."""
+    from hipgisaxs_b200 import model
+    img = np.array([[1.0, 2.5e-7, 123456789.0], [0.0, -3.25, 1e5], [7e-5, 42.0, 1.0 / 3.0]])
+    p = tmp_path / "img.out"
+    model.save_gisaxs(p, img)
+    expect = "".join("".join(f"{v:g}\t" for v in row) + "\n" for row in img)
+    assert p.read_text() == expect
