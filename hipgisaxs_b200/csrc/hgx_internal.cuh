@@ -96,6 +96,9 @@ int qgrid_finalize(hgx_qgrid g);  // builds the row table and picks the mode
 // place when nqy and nqz match, else a new one (the old one destroyed).
 int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
                 hgx_qgrid* out);
+// Lattice vectors a, b, c (abc9) and basis offset t3 of a lattice type (LatticeType code) and
+// hkl string; false when the type has no vectors for that hkl (sf.cu).
+bool lattice_table(int type, const std::string& hkl, double* abc9, double* t3);
 }  // namespace hgx
 
 namespace hgx {

@@ -76,31 +76,30 @@ __global__ void __launch_bounds__(128) sf_lattice_kernel(SfArgs a) {
 
 using namespace hgx;
 
-extern "C" {
+namespace hgx {
 
 // Lattice::construct_vectors, src/model/structure.cpp:86-182 (ca = 1, gamma = 0 as the
 // reference's Lattice constructor sets them).  type: LatticeType (include/common/enums.hpp:56-65).
-int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3) {
-  if (!abc9) return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: null output");
+// False for an unknown type or an hkl the type has no vectors for.
+bool lattice_table(int type, const std::string& h, double* abc9, double* t3) {
   const double sqrt3 = sqrt(3.0);
-  std::string h = hkl ? hkl : "100";
   double a[3] = {0}, b[3] = {0}, c[3] = {0}, t[3] = {0};
   auto set = [](double* v, double x, double y, double z) { v[0] = x; v[1] = y; v[2] = z; };
   switch (type) {
     case 3:  // cubic
       if (h == "100") { set(a, 1, 0, 0); set(b, 0, 1, 0); set(c, 0, 0, 1); }
       else if (h == "110") { set(a, 1, 0, 0); set(b, 0., 1.4142, 0); set(c, 0., 0.7071, 0.7071); }
-      else return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: invalid lattice type and hkl");
+      else return false;
       break;
     case 2:  // bcc
       if (h == "100") { set(a, 1., 0., 0.); set(b, 0., 1., 0.); set(c, 0.5, 0.5, 0.5); }
       else if (h == "110") { set(a, 1.0, 0.0, 0); set(b, 0.5, 0.7071, 0); set(c, 0.0, 0.7071, 0.7071); }
-      else return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: invalid lattice type and hkl");
+      else return false;
       break;
     case 4:  // fcc
       if (h == "100") { set(a, 0.0, 0.5, 0.5); set(b, 0.5, 0.0, 0.5); set(c, 0.5, 0.5, 0.0); }
       else if (h == "111") { set(a, 1., 0., 0); set(b, 0.5, 0.866, -0.); set(c, 1., 0.5773, 0.866); }
-      else return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: invalid lattice type and hkl");
+      else return false;
       break;
     case 5:  // fco
       set(a, 1, 0, 0); set(b, 0.5, tan(0.0) / 2.0, 0); set(c, 0, 0, 1.0); set(t, 0.5, 0, 0.5);
@@ -112,7 +111,7 @@ int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3) {
       set(a, 1, 0, 0); set(b, 0.5, sqrt3 / 2.0, 0); set(c, 0, 0, 1);
       break;
     default:
-      return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: unknown lattice type");
+      return false;
   }
   for (int i = 0; i < 3; ++i) {
     abc9[i] = a[i];
@@ -120,6 +119,18 @@ int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3) {
     abc9[6 + i] = c[i];
     if (t3) t3[i] = t[i];
   }
+  return true;
+}
+
+}  // namespace hgx
+
+extern "C" {
+
+int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3) {
+  if (!abc9) return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: null output");
+  if (type < 2 || type > 7) return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: unknown lattice type");
+  if (!lattice_table(type, hkl ? hkl : "100", abc9, t3))
+    return fail(HGX_ERR_INVALID_ARG, "hgx_lattice_vectors: invalid lattice type and hkl");
   return HGX_OK;
 }
 

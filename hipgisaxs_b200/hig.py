@@ -1,0 +1,139 @@
+"""HiG input files: HiGInput (include/config/hig_input.hpp) over the C reader (hgx_hig_read).
+
+    inp = read_hig("cylinders.hig")
+    inp.shapes["s1"]["params"]["radius"]["min"]
+    k0, alpha_i, freq = inp.beam()
+    grid = inp.qgrid(ctx)          # QGrid::create + create_qz_extended on the device
+
+The description is the reader's JSON (hgx_hig_json) as plain dicts; the accessor methods
+carry the reference's names (scattering_alphai, param_resolution, ...).  Parsing is host
+work and needs no GPU; qgrid() builds device arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+
+from ._capi import check, lib
+from .core import Context, QGrid
+
+
+class HiGInput:
+    """A HiG file read by hgx_hig_read (HiGInput::construct_input_config)."""
+
+    def __init__(self, path: str):
+        h = C.c_void_p()
+        check(lib().hgx_hig_read(os.fsencode(path), C.byref(h)))
+        self._h = h
+        self.path = path
+        n = C.c_size_t()
+        check(lib().hgx_hig_json(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value + 1)
+        check(lib().hgx_hig_json(self._h, buf, n.value + 1, C.byref(n)))
+        self.data = json.loads(buf.value.decode())
+
+    # the blocks of the file
+    @property
+    def shapes(self):
+        return self.data["shapes"]
+
+    @property
+    def layers(self):
+        """{order: layer}, sorted by order as the reference's std::map keeps them."""
+        return {int(k): v for k, v in sorted(self.data["layers"].items(), key=lambda kv: int(kv[0]))}
+
+    @property
+    def unitcells(self):
+        return self.data["unitcells"]
+
+    @property
+    def structures(self):
+        return self.data["structures"]
+
+    @property
+    def scattering(self):
+        return self.data["scattering"]
+
+    @property
+    def detector(self):
+        return self.data["detector"]
+
+    @property
+    def compute(self):
+        return self.data["computation"]
+
+    @property
+    def fit_params(self):
+        return self.data["fitparams"]
+
+    @property
+    def algorithms(self):
+        return self.data["algorithms"]
+
+    # accessors with the reference's names (include/config/hig_input.hpp:170-260)
+    def scattering_alphai(self):
+        return tuple(self.scattering["alphai"])
+
+    def scattering_inplanerot(self):
+        return tuple(self.scattering["inplanerot"])
+
+    def scattering_tilt(self):
+        return tuple(self.scattering["tilt"])
+
+    def photon_energy(self):
+        return self.scattering["photon_value"], self.scattering["photon_unit"]
+
+    def param_resolution(self):
+        return [int(v) for v in self.compute["resolution"]]
+
+    def param_output_minpoint(self):
+        return tuple(self.compute["minpoint"])
+
+    def param_output_maxpoint(self):
+        return tuple(self.compute["maxpoint"])
+
+    def param_output_type(self):
+        return self.compute["region_type"]
+
+    def num_structures(self):
+        return len(self.structures)
+
+    def substrate_refindex(self):
+        sub = self.layers.get(-1)
+        return (sub["refindex"][0], sub["refindex"][1]) if sub else (0.0, 0.0)
+
+    def fit_param_keys(self):
+        return sorted(self.fit_params)
+
+    # device set-up of HipGISAXS::init
+    def beam(self):
+        """(k0 in 1/nm, alpha_i in radians, frequency) as HipGISAXS::init computes them."""
+        k0, ai, fr = C.c_double(), C.c_double(), C.c_double()
+        check(lib().hgx_hig_beam(self._h, C.byref(k0), C.byref(ai), C.byref(fr)))
+        return k0.value, ai.value, fr.value
+
+    def qgrid(self, ctx: Context, dn2=(0.0, 0.0)) -> QGrid:
+        """The computation block's q-space grid with its DWBA extension for dn2 (device)."""
+        h = C.c_void_p()
+        check(lib().hgx_hig_qgrid(ctx.handle, self._h, float(dn2[0]), float(dn2[1]), C.byref(h)))
+        return QGrid(ctx, h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hgx_hig_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_hig(path: str) -> HiGInput:
+    return HiGInput(path)

@@ -386,6 +386,28 @@ int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int nqy, const d
                              const double* qy, int nqz, const double* qz, const double* rot9,
                              void* ff, int ff_type, void* stream);
 
+/* -------------------------------------------------------------- HiG input files ---- */
+/* A simulation description read from a HiG file: HiGInput::construct_input_config
+ * (src/config/hig_input.cpp:61-104, tokenizer src/file/read_oo_input.cpp, keywords
+ * include/config/token_mapper.hpp).  Files the reference reads are read to the same values,
+ * `include = "file"` splicing and the reference's carry-over quirks included; a file it
+ * rejects is rejected (HGX_ERR_INVALID_ARG, the message names file and line).  Host only. */
+typedef struct hgx_hig_s* hgx_hig;
+int hgx_hig_read(const char* path, hgx_hig* out);
+/* The whole description as JSON (shapes, layers, unitcells, structures, scattering, detector,
+ * computation, fitting).  buf may be NULL to ask for the size: *len receives the length
+ * without the terminating NUL; with buf, cap must be > *len. */
+int hgx_hig_json(hgx_hig h, char* buf, size_t cap, size_t* len);
+int hgx_hig_destroy(hgx_hig h);
+/* The beam of HipGISAXS::init (src/sim/hipgisaxs_main.cpp:146-160): wave number k0 (1/nm)
+ * from the photon energy ("ev" or "kev"), incidence angle alphai.min in radians, frequency.
+ * Any output may be NULL. */
+int hgx_hig_beam(hgx_hig h, double* k0, double* alpha_i, double* freq);
+/* QGrid::create for the computation block's q-space output region and resolution
+ * (src/model/qgrid.cpp:30-101) at the file's beam, then create_qz_extended with
+ * dn2 = dn2_re + i dn2_im (the layer's 1 - n^2): a DWBA grid, built on the device. */
+int hgx_hig_qgrid(hgx_ctx ctx, hgx_hig h, double dn2_re, double dn2_im, hgx_qgrid* out);
+
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA
  * throughput (TFLOP/s, an FMA counted as 2 FLOP) and SFU __sinf throughput (Gop/s),
