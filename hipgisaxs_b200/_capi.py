@@ -86,6 +86,8 @@ SIGNATURES = {
     "hgx_hig_destroy": (_i, [_vp]),
     "hgx_hig_beam": (_i, [_vp, C.POINTER(_d), C.POINTER(_d), C.POINTER(_d)]),
     "hgx_hig_qgrid": (_i, [_vp, _vp, _d, _d, C.POINTER(_vp)]),
+    "hgx_hig_image_size": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
+    "hgx_hig_compute_gisaxs": (_i, [_vp, _vp, _i, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }
 

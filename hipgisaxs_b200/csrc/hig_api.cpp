@@ -9,11 +9,6 @@
 #include "hgx_internal.cuh"
 #include "hig_config.hpp"
 
-struct hgx_hig_s {
-  hgx::hig::Input in;
-  std::string json;  // built on first request
-};
-
 using namespace hgx;
 
 extern "C" {

@@ -195,3 +195,9 @@ bool photon_k0(const Scattering& s, double* k0, double* freq);
 
 }  // namespace hig
 }  // namespace hgx
+
+// the handle behind hgx_hig (include/hgx.h)
+struct hgx_hig_s {
+  hgx::hig::Input in;
+  std::string json;  // built on first request
+};

@@ -1,0 +1,382 @@
+// HipGISAXS::compute_gisaxs for a HiG description, on the device
+// (src/sim/hipgisaxs_main.cpp:630-685 and run_gisaxs, :694-1440).
+//
+// For every structure: the grains of its ensemble (a regular grid of centres,
+// spatial_distribution :1702-1867; one orientation per grain, orientation_distribution
+// :1869-2010), for every grain the form factor of the unit cell (every element's shape at
+// every location, weighted by dn2 = (1 - n^2)_layer - (1 - n^2)_shape, :976-1015), the
+// structure factor (lattice, paracrystal or Percus-Yevick, :1045-1058) and the DWBA sum
+// I += |w sum_k fc_k sf_k ff_k|^2 (:1086-1100); the structures' intensities are then summed
+// with their iratios (:1352-1362, 1417-1431).  Structures and the elements of a unit cell are
+// taken in key order; the reference walks unordered maps, whose order is unspecified (only
+// the rounding of the sums depends on it).  The grid, the Fresnel coefficients and every
+// per-grain array stay on the device; the host only walks the description.
+//
+// As in the reference: the particles sit in layer order 0 (the vacuum: the grain's layer
+// order is never assigned, src/model/structure.cpp:389-398), so the DWBA grid is built with
+// dn2 = 0 and the Fresnel coefficients for order 0; a custom (mesh) shape ignores its
+// location (FormFactor::compute_form_factor passes no translation to the numeric form
+// factor, src/ff/ff.cpp:40-48) but is added once per location; orientations drawn by the
+// "range" and "random" statistics come from the C library's rand(), in the reference's
+// order.  The reference subtracts single_layer_thickness_, a member it never assigns, from
+// the grain translation's z (:871-875); it is taken as 0 here.
+//
+// Configurations whose reference result is not determined by the input are refused with
+// HGX_ERR_INVALID_ARG: clock-seeded random grain positions, the Mersenne-Twister sampled
+// scaling distributions, repetition distributions, gaussian/cauchy/bragg orientations (whose
+// sampling is commented out or needs the q-grid singleton), structure correlations other
+// than none, sliced layers (nslices > 1), SAXS, and angle scans (more than one alpha_i, phi
+// or tilt: compute_gisaxs itself refuses those).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdlib.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "hgx_internal.cuh"
+#include "hig_config.hpp"
+
+namespace hgx {
+
+namespace {
+
+constexpr double PI = 3.141592653589793;  // PI_, include/common/constants.hpp:29
+
+// ff += dn2 * eff over n complex values, each product and sum rounded once (no fused
+// multiply-add), as the reference's complex arithmetic rounds them
+__global__ void add_scaled_kernel(long n, double dre, double dim, const double2* __restrict__ eff,
+                                  double2* __restrict__ ff) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 e = eff[i];
+  double2 f = ff[i];
+  const double re = __dsub_rn(__dmul_rn(dre, e.x), __dmul_rn(dim, e.y));
+  const double im = __dadd_rn(__dmul_rn(dre, e.y), __dmul_rn(dim, e.x));
+  f.x = __dadd_rn(f.x, re);
+  f.y = __dadd_rn(f.y, im);
+  ff[i] = f;
+}
+
+// RotMatrix_t(axis, angle) and its product (include/numerics/matrix.hpp:43-117)
+struct Rot {
+  double m[9];
+  static Rot axis(int ax, double a) {
+    const double c = cos(a), s = sin(a);
+    Rot r;
+    switch (ax) {
+      case 0: { const double v[9] = {1., 0., 0., 0., c, -s, 0., s, c}; for (int i = 0; i < 9; ++i) r.m[i] = v[i]; break; }
+      case 1: { const double v[9] = {c, 0., -s, 0., 1., 0., s, 0., c}; for (int i = 0; i < 9; ++i) r.m[i] = v[i]; break; }
+      case 2: { const double v[9] = {c, -s, 0., s, c, 0., 0., 0., 1.}; for (int i = 0; i < 9; ++i) r.m[i] = v[i]; break; }
+      default: { const double v[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}; for (int i = 0; i < 9; ++i) r.m[i] = v[i]; }
+    }
+    return r;
+  }
+  Rot operator*(const Rot& b) const {
+    Rot r;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < 3; ++k) acc += m[i * 3 + k] * b.m[j + 3 * k];
+        r.m[i * 3 + j] = acc;
+      }
+    return r;
+  }
+  void apply(const double* v, double* out) const {
+    for (int i = 0; i < 3; ++i) out[i] = m[3 * i] * v[0] + m[3 * i + 1] * v[1] + m[3 * i + 2] * v[2];
+  }
+};
+
+int shape_code(const std::string& name) {  // ShapeName, include/common/enums.hpp:24-43
+  if (name == "box") return 2;
+  if (name == "cube") return 3;
+  if (name == "cylinder") return 4;
+  if (name == "sphere") return 5;
+  if (name == "prism3") return 8;
+  if (name == "prism6") return 9;
+  if (name == "pyramid") return 14;
+  return -1;
+}
+int param_code(const std::string& t) {  // ShapeParamType, enums.hpp:45-54
+  if (t == "radius") return 2;
+  if (t == "xsize") return 3;
+  if (t == "ysize") return 4;
+  if (t == "height") return 5;
+  if (t == "edge") return 6;
+  if (t == "baseangle") return 7;
+  return 1;
+}
+int stat_code(const std::string& s) {  // StatisticType, enums.hpp:74-84
+  if (s == "null") return 0;
+  if (s == "none") return 2;
+  if (s == "cauchy") return 3;
+  if (s == "gaussian") return 4;
+  if (s == "random") return 5;
+  if (s == "range") return 6;
+  if (s == "t") return 7;
+  if (s == "uniform") return 8;
+  return 1;
+}
+int lattice_code(const std::string& t) {
+  if (t == "bcc") return 2;
+  if (t == "cubic") return 3;
+  if (t == "fcc") return 4;
+  if (t == "fco") return 5;
+  if (t == "hcp") return 6;
+  if (t == "hex") return 7;
+  return 1;
+}
+
+bool file_exists(const std::string& p) {
+  FILE* f = fopen(p.c_str(), "rb");
+  if (!f) return false;
+  fclose(f);
+  return true;
+}
+
+// how many values an angle scan takes (HipGISAXS::compute_gisaxs, :640-660)
+int scan_count(double mn, double mx, double step, bool clamp_max) {
+  if (clamp_max && mx < mn) mx = mn;
+  if ((clamp_max && mn == mx) || step == 0) return 1;
+  return (int)((mx - mn) / step + 1);
+}
+
+}  // namespace
+
+// The grain centres of spatial_distribution's "regular" branch (:1765-1828) with the unit
+// cell size cell_ = 0 (the reference never assigns it) and tz = 0: d[3][ngrains].
+static void regular_centres(const hig::Structure& s, std::vector<double>& d, int& ngr) {
+  const double nd[3] = {s.maxgrains[0], s.maxgrains[1], s.maxgrains[2]};
+  const int n0 = (int)nd[0], n1 = (int)nd[1], n2 = (int)nd[2];
+  ngr = (int)(nd[0] * nd[1] * nd[2]);
+  d.assign(3 * (size_t)ngr, 0.0);
+  std::vector<double> dx(n0), dy(n1), dz(n2);
+  const double sc[3] = {s.spacing[0], s.spacing[1], s.spacing[2]};  // cell_ + spacing
+  double val = 0, step = sc[0], mx = sc[0] * (nd[0] - 1);
+  for (int i = 0; i < n0; ++i, val += step) dx[i] = val - mx / 2;
+  val = 0, step = sc[1], mx = sc[1] * (nd[1] - 1);
+  for (int i = 0; i < n1; ++i, val += step) dy[i] = val - mx / 2;
+  val = 0, step = sc[2];
+  for (int i = 0; i < n2; ++i, val += step) dz[i] = val + 0.0;
+  double* d1 = d.data();
+  double* d2 = d1 + ngr;
+  double* d3 = d2 + ngr;
+  for (int x = 0; x < n0; ++x)
+    for (int yz = 0; yz < n1 * n2; ++yz) d1[n1 * n2 * x + yz] = dx[x];
+  for (int x = 0; x < n0; ++x)
+    for (int y = 0; y < n1; ++y)
+      for (int z = 0; z < n2; ++z) d2[n1 * n2 * x + n2 * y + z] = dy[y];
+  for (int xy = 0; xy < n0 * n1; ++xy)
+    for (int z = 0; z < n2; ++z) d3[n2 * xy + z] = dz[z];
+}
+
+// rotation_rotN() of a structure: (axis - 'x', first angle, second angle), zeros for axis 'n'
+static void rotation_of(const hig::Rotation& r, double out[3]) {
+  if (r.axis == 'n') { out[0] = out[1] = out[2] = 0; return; }
+  out[0] = (double)((char)r.axis - 'x');
+  out[1] = r.angles[0];
+  out[2] = r.angles[1];
+}
+
+// orientation_distribution (:1869-1960) for single, range and random: nn[3][ngr] radians
+static int orientations(const hig::Structure& s, int ngr, std::vector<double>& nn) {
+  double r[3][3];
+  rotation_of(s.rot1, r[0]);
+  rotation_of(s.rot2, r[1]);
+  rotation_of(s.rot3, r[2]);
+  nn.assign(3 * (size_t)ngr, 0.0);
+  const std::string& st = s.orientation_stat;
+  if (st == "single") {
+    for (int k = 0; k < 3; ++k)
+      for (int x = 0; x < ngr; ++x) nn[k * ngr + x] = r[k][1] * PI / 180;
+  } else if (st == "random") {
+    for (int x = 0; x < 3 * ngr; ++x) nn[x] = (double(rand()) / RAND_MAX) * 2 * PI;
+  } else if (st == "range") {
+    for (int k = 0; k < 3; ++k) {
+      const double dr = fabs(r[k][2] - r[k][1]);
+      for (int x = 0; x < ngr; ++x) nn[k * ngr + x] = (r[k][1] + (double(rand()) / RAND_MAX) * dr) * PI / 180;
+    }
+  } else {
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: structure '" + s.key +
+                                         "': orientation statistic '" + st + "' is not supported");
+  }
+  return HGX_OK;
+}
+
+}  // namespace hgx
+
+using namespace hgx;
+
+extern "C" {
+
+int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_image_size: null handle");
+  if (nrow) *nrow = h->in.compute.resolution[1];
+  if (ncol) *ncol = h->in.compute.resolution[0];
+  return HGX_OK;
+}
+
+int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
+  if (!c || !h || !image) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: null argument");
+  if (precision != HGX_F64 && precision != HGX_F32C)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: unknown precision");
+  const hig::Input& in = h->in;
+  const hig::Scattering& sc = in.scattering;
+  const hig::Compute& cp = in.compute;
+  auto refuse = [](const std::string& why) {
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: " + why);
+  };
+  if (scan_count(sc.alphai[0], sc.alphai[1], sc.alphai[2], true) > 1 ||
+      scan_count(sc.inplanerot[0], sc.inplanerot[1], sc.inplanerot[2], false) > 1 ||
+      scan_count(sc.tilt[0], sc.tilt[1], sc.tilt[2], false) > 1)
+    return refuse("more than one alpha_i, phi or tilt (the reference's compute_gisaxs refuses scans)");
+  if (sc.expt != "gisaxs") return refuse("experiment '" + sc.expt + "': only gisaxs (DWBA) is supported");
+  if (cp.nslices > 1) return refuse("sliced layers (nslices > 1) are not supported");
+  if (cp.structcorrelation != "null" && cp.structcorrelation != "nGnE")
+    return refuse("structure correlation '" + cp.structcorrelation + "' is not supported");
+  if (in.structures.empty()) return refuse("the description has no structure");
+  for (const auto& kv : in.structures) {
+    const hig::Structure& s = kv.second;
+    if (s.distribution != "regular")
+      return refuse("structure '" + s.key + "': ensemble distribution '" + s.distribution + "' is not supported");
+    if (s.repetition_dist) return refuse("structure '" + s.key + "': repetition distributions are not supported");
+    for (int k = 0; k < 3; ++k)
+      if (s.scaling_stat[k] != "none")
+        return refuse("structure '" + s.key + "': scaling distributions are not supported");
+    if (!in.unitcells.count(s.unitcell_key))
+      return refuse("structure '" + s.key + "': unknown unit cell '" + s.unitcell_key + "'");
+    if (s.maxgrains[0] < 1 || s.maxgrains[1] < 1 || s.maxgrains[2] < 1)
+      return refuse("structure '" + s.key + "': maxgrains must be >= 1");
+  }
+  HGX_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+
+  // beam, grid (vacuum layer: dn2 = 0) and Fresnel coefficients for layer order 0
+  double k0, alpha_i;
+  HGX_TRY(hgx_hig_beam(h, &k0, &alpha_i, nullptr));
+  const double phi = sc.inplanerot[0] * PI / 180;
+  hgx_qgrid g = nullptr;
+  HGX_TRY(hgx_hig_qgrid(c, h, 0.0, 0.0, &g));
+  struct GridGuard { hgx_qgrid g; ~GridGuard() { hgx_qgrid_destroy(g); } } guard{g};
+  const long n = (long)g->nqy;
+  const long nq = (long)g->nqz;  // 4n
+  std::vector<double> ld, lb, lt;
+  std::vector<int> lo;
+  for (const auto& kv : in.layers) {
+    ld.push_back(kv.second.refindex.delta);
+    lb.push_back(kv.second.refindex.beta);
+    lt.push_back(kv.second.thickness);
+    lo.push_back(kv.second.order);
+  }
+  DevBuf bfc, bff, beff, bsf, bI;
+  HGX_TRY(bfc.reserve(sizeof(double2) * nq));
+  HGX_TRY(bff.reserve(sizeof(double2) * nq));
+  HGX_TRY(beff.reserve(sizeof(double2) * nq));
+  HGX_TRY(bsf.reserve(sizeof(double2) * nq));
+  const int nstruct = (int)in.structures.size();
+  HGX_TRY(bI.reserve(sizeof(double) * n * nstruct));
+  HGX_TRY(hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(),
+                                 k0, alpha_i, 0, nullptr, (double*)bfc.p, 0));
+  HGX_CUDA(cudaMemsetAsync(bI.p, 0, sizeof(double) * n * nstruct, st));
+
+  // custom shapes: triangle tuples read once, kept on the device
+  std::map<std::string, std::pair<DevBuf, int>> meshes;
+  const std::string dir = in.path.rfind('/') == std::string::npos ? "" : in.path.substr(0, in.path.rfind('/') + 1);
+  for (const auto& kv : in.shapes) {
+    const hig::Shape& sh = kv.second;
+    if (sh.name != "custom") continue;
+    std::string path = sh.name_str;
+    if (!file_exists(path) && !path.empty() && path[0] != '/' && file_exists(dir + path)) path = dir + path;
+    int ntri = 0;
+    HGX_TRY(hgx_read_shapes_file(c, path.c_str(), nullptr, 0, &ntri));
+    if (ntri < 1) return refuse("shape file '" + path + "' has no triangles");
+    std::vector<double> sd(8 * (size_t)ntri);
+    HGX_TRY(hgx_read_shapes_file(c, path.c_str(), sd.data(), ntri, &ntri));
+    auto& m = meshes[kv.first];
+    HGX_TRY(m.first.reserve(sizeof(double) * sd.size()));
+    HGX_CUDA(cudaMemcpyAsync(m.first.p, sd.data(), sizeof(double) * sd.size(), cudaMemcpyHostToDevice, st));
+    m.second = ntri;
+    HGX_CUDA(cudaStreamSynchronize(st));
+  }
+
+  const Rot rot_phi = Rot::axis(2, phi);  // rot_ = RotMatrix_t(2, phi)
+  const unsigned blocks = (unsigned)((nq + 255) / 256);
+  int si = 0;
+  for (const auto& skv : in.structures) {  // in key order (the reference: unordered_map order)
+    const hig::Structure& s = skv.second;
+    const hig::Unitcell& uc = in.unitcells.at(s.unitcell_key);
+    std::vector<double> dd, nn;
+    int ngr = 0;
+    regular_centres(s, dd, ngr);
+    HGX_TRY(orientations(s, ngr, nn));
+    double r1[3], r2[3], r3[3];
+    rotation_of(s.rot1, r1);
+    rotation_of(s.rot2, r2);
+    rotation_of(s.rot3, r3);
+    const int ax1 = (int)r1[0], ax2 = (int)r2[0], ax3 = (int)r3[0];
+    const double abc9[9] = {s.lattice.a[0], s.lattice.a[1], s.lattice.a[2], s.lattice.b[0], s.lattice.b[1],
+                            s.lattice.b[2], s.lattice.c[0], s.lattice.c[1], s.lattice.c[2]};
+    const double repet[3] = {s.repetition[0], s.repetition[1], s.repetition[2]};
+    const double scaling[3] = {s.scaling_mean[0], s.scaling_mean[1], s.scaling_mean[2]};
+    double* Is = (double*)bI.p + (size_t)si * n;
+    for (int gi = 0; gi < ngr; ++gi) {
+      const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
+                      Rot::axis(ax1, nn[gi]);
+      const double ddv[3] = {dd[gi], dd[gi + ngr], dd[gi + 2 * ngr]};
+      double center[3];
+      rot.apply(ddv, center);
+      for (int k = 0; k < 3; ++k) center[k] += s.transvec[k];
+      // the unit cell's form factor
+      HGX_CUDA(cudaMemsetAsync(bff.p, 0, sizeof(double2) * nq, st));
+      for (const auto& ekv : uc.elements) {  // in shape-key order
+        const std::string& skey = ekv.first;
+        auto shp = in.shapes.find(skey);
+        if (shp == in.shapes.end()) return refuse("unit cell '" + uc.key + "': unknown shape '" + skey + "'");
+        const hig::Shape& sh = shp->second;
+        const Rot srot = ((rot * Rot::axis(0, sh.xrot)) * Rot::axis(1, sh.yrot)) * Rot::axis(2, sh.zrot);
+        const double dre = 0.0 - 2 * sh.refindex.delta, dim = 0.0 - 2 * sh.refindex.beta;
+        std::vector<double> prm;
+        for (const auto& pk : sh.params) {
+          const hig::ShapeParam& p = pk.second;
+          const double row[7] = {(double)param_code(p.type), (double)stat_code(p.stat), p.min, p.max,
+                                 p.p1, p.p2, (double)p.nvalues};
+          prm.insert(prm.end(), row, row + 7);
+        }
+        const int code = shape_code(sh.name);
+        if (sh.name != "custom" && code < 0)
+          return refuse("shape '" + sh.key + "': '" + sh.name + "' has no analytic form factor here");
+        for (const hig::vec3& loc : ekv.second) {
+          if (sh.name == "custom") {
+            const auto& m = meshes.at(skey);
+            HGX_TRY(hgx_ff_triangles_q(c, g, (const double*)m.first.p, m.second, srot.m, precision,
+                                       beff.p, HGX_C128));
+          } else {
+            const double tv[3] = {loc[0], loc[1], loc[2]};
+            HGX_TRY(hgx_ff_analytic_params(c, g, code, (int)(prm.size() / 7), prm.data(), 0.0, 0.0, tv,
+                                           srot.m, beff.p, HGX_C128));
+          }
+          add_scaled_kernel<<<blocks, 256, 0, st>>>(nq, dre, dim, (const double2*)beff.p, (double2*)bff.p);
+          HGX_CUDA(cudaGetLastError());
+        }
+      }
+      // the grain's structure factor
+      if (s.type == "paracrystal") {
+        HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1],
+                                   s.pc_dist[0], s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
+      } else if (s.type == "percusyevick") {
+        HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
+      } else {
+        HGX_TRY(hgx_sf_lattice(c, g, abc9, repet, scaling, center, rot.m, bsf.p, HGX_C128));
+      }
+      HGX_TRY(hgx_dwba_combine(c, n, (const double*)bfc.p, (const double*)bsf.p, bff.p, HGX_C128, 1.0, Is));
+    }
+    ++si;
+  }
+  std::vector<double> ratios;
+  for (const auto& kv : in.structures) ratios.push_back(kv.second.iratio);
+  HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), image));
+  return hgx_synchronize(c);
+}
+
+}  // extern "C"

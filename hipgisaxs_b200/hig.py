@@ -15,8 +15,10 @@ import ctypes as C
 import json
 import os
 
+import numpy as np
+
 from ._capi import check, lib
-from .core import Context, QGrid
+from .core import PRECISION, Context, QGrid, _is_tensor
 
 
 class HiGInput:
@@ -118,6 +120,24 @@ class HiGInput:
         h = C.c_void_p()
         check(lib().hgx_hig_qgrid(ctx.handle, self._h, float(dn2[0]), float(dn2[1]), C.byref(h)))
         return QGrid(ctx, h)
+
+    def image_size(self):
+        """(nrow, ncol) of the detector image (computation.resolution)."""
+        r, c = C.c_int(), C.c_int()
+        check(lib().hgx_hig_image_size(self._h, C.byref(r), C.byref(c)))
+        return r.value, c.value
+
+    def compute_gisaxs(self, ctx: Context, precision: str = "f64", out=None):
+        """HipGISAXS::compute_gisaxs on the device (hgx_hig_compute_gisaxs): the nrow x ncol
+        intensity image of every structure's grains, summed with the iratios.  `out`: a
+        float64 numpy array or CUDA tensor of nrow*ncol values (allocated when None).
+        precision "f32c" computes mesh form factors in compensated FP32."""
+        nrow, ncol = self.image_size()
+        if out is None:
+            out = np.zeros((nrow, ncol))
+        ptr = out.data_ptr() if _is_tensor(out) else out.ctypes.data
+        check(lib().hgx_hig_compute_gisaxs(ctx.handle, self._h, PRECISION[precision], C.c_void_p(ptr)))
+        return out
 
     @property
     def handle(self):

@@ -407,6 +407,19 @@ int hgx_hig_beam(hgx_hig h, double* k0, double* alpha_i, double* freq);
  * (src/model/qgrid.cpp:30-101) at the file's beam, then create_qz_extended with
  * dn2 = dn2_re + i dn2_im (the layer's 1 - n^2): a DWBA grid, built on the device. */
 int hgx_hig_qgrid(hgx_ctx ctx, hgx_hig h, double dn2_re, double dn2_im, hgx_qgrid* out);
+/* The detector image size of the description (computation.resolution): nrow x ncol. */
+int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
+/* HipGISAXS::compute_gisaxs (src/sim/hipgisaxs_main.cpp:630-685, run_gisaxs :694-1440) on
+ * the device: for every structure and every grain of its ensemble, the unit cell's form
+ * factor (analytic shapes at each location, mesh shapes from their .obj/.dat file), the
+ * structure factor (lattice, paracrystal or Percus-Yevick) and the DWBA intensity with the
+ * layer stack's Fresnel coefficients; the structures summed with their iratios.  image:
+ * nrow x ncol doubles (host or device).  precision: HGX_F64, or HGX_F32C for the mesh form
+ * factors.  Supported: GISAXS, one alpha_i/phi/tilt, nslices <= 1, no structure correlation,
+ * regular grain grids, "single", "range" and "random" orientations (drawn with the C
+ * library's rand() in the reference's order), no scaling or repetition distributions; other
+ * descriptions return HGX_ERR_INVALID_ARG naming the feature. */
+int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
 
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA

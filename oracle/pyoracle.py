@@ -488,3 +488,140 @@ def structure_sum(intensities, iratios):
     out = np.zeros(I.shape[1])
     L.orc_structure_sum(C.c_int(len(r)), C.c_long(I.shape[1]), _p(I), _p(r), _p(out))
     return out
+
+
+def _libc_rand():
+    libc = C.CDLL(None)
+    libc.rand.restype = C.c_int
+    return libc.rand
+
+
+RAND_MAX = 2147483647  # glibc
+
+
+def _read_obj_shape_def(path):
+    """A Wavefront OBJ's vertices and triangles (v / f lines; f items v, v/vt, v/vt/vn, v//vn)
+    turned into shape_def rows (mesh_to_shape_def)."""
+    V, F = [], []
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "v":
+                V.append([float(x) for x in t[1:4]])
+            elif t[0] == "f" and len(t) == 4:
+                F.append([int(x.split("/")[0]) - 1 for x in t[1:4]])
+    return mesh_to_shape_def(np.array(V), np.array(F, dtype=np.int32))
+
+
+def compute_gisaxs(hig, hig_dir=".", rand=None):
+    """HipGISAXS::compute_gisaxs / run_gisaxs (src/sim/hipgisaxs_main.cpp:630-1440) for the
+    configurations hgx_hig_compute_gisaxs supports, composed from this oracle's pinned pieces
+    (QGrid, MultiLayer::propagation_coeffs, the analytic and numeric form factors, the
+    structure factors, the DWBA combination and the structure sum).  `hig`: the reader's
+    JSON model (dict).  Orientations drawn by "range"/"random" call `rand` (default: the C
+    library's rand()) in the reference's order.  Returns the nrow x ncol image (FP64)."""
+    rand = rand or _libc_rand()
+    sc, cp = hig["scattering"], hig["computation"]
+    value, unit = sc["photon_value"], sc["photon_unit"]
+    kev = value / 1000 if unit == "ev" else value  # HipGISAXS::init, :146-160
+    ncol, nrow = int(cp["resolution"][0]), int(cp["resolution"][1])
+    (ymin, zmin), (ymax, zmax) = cp["minpoint"], cp["maxpoint"]
+    G = Grid(ncol, nrow, ymin, zmin, ymax, zmax, sc["alphai"][0], kev, (0.0, 0.0))
+    layers = [(l["refindex"][0], l["refindex"][1], l["thickness"], l["order"])
+              for _, l in sorted(hig["layers"].items(), key=lambda kv: int(kv[0]))]
+    fc = propagation_coeffs(G, layers, 0)  # particle layer order 0 (:779-785)
+    pi = 3.141592653589793
+    rot_phi = rot_axis(2, sc["inplanerot"][0] * pi / 180)
+    meshes = {}
+    for key, sh in hig["shapes"].items():
+        if sh["name"] == "custom":
+            p = sh["name_str"]
+            if not os.path.exists(p) and not os.path.isabs(p):
+                p = os.path.join(hig_dir, p)
+            meshes[key] = _read_obj_shape_def(p)
+    intens = []
+    for skey, s in hig["structures"].items():  # key order, as the product walks them
+        uc = hig["unitcells"][s["unitcell_key"]]
+        # spatial_distribution "regular" (:1765-1828), cell_ = 0, tz = 0
+        nd = [float(v) for v in s["maxgrains"]]
+        n0, n1, n2 = int(nd[0]), int(nd[1]), int(nd[2])
+        ngr = int(nd[0] * nd[1] * nd[2])
+        sp = s["spacing"]
+        axes = []
+        for k in range(3):
+            n_k, st = (n0, n1, n2)[k], sp[k]
+            mx = st * (nd[k] - 1)
+            vals, val = [], 0.0
+            for _ in range(n_k):
+                vals.append(val - mx / 2 if k < 2 else val + 0.0)
+                val += st
+            axes.append(vals)
+        d = np.zeros((3, ngr))
+        for x in range(n0):
+            for y in range(n1):
+                for z in range(n2):
+                    g = n1 * n2 * x + n2 * y + z
+                    d[0, g], d[1, g], d[2, g] = axes[0][x], axes[1][y], axes[2][z]
+        # orientation_distribution (:1869-1960)
+        rots = []
+        for name in ("rot1", "rot2", "rot3"):
+            r = s[name]
+            rots.append((0.0, 0.0, 0.0) if r["axis"] == "n" else
+                        (float(ord(r["axis"]) - ord("x")), r["angles"][0], r["angles"][1]))
+        nn = np.zeros((3, ngr))
+        stat = s["orientation_stat"]
+        if stat == "single":
+            for k in range(3):
+                nn[k, :] = rots[k][1] * pi / 180
+        elif stat == "random":
+            for x in range(3 * ngr):
+                nn.reshape(-1)[x] = (float(rand()) / RAND_MAX) * 2 * pi
+        elif stat == "range":
+            for k in range(3):
+                dr = abs(rots[k][2] - rots[k][1])
+                for x in range(ngr):
+                    nn[k, x] = (rots[k][1] + (float(rand()) / RAND_MAX) * dr) * pi / 180
+        else:
+            raise ValueError(stat)
+        lat = s["lattice"]
+        abc = np.array([lat["a"], lat["b"], lat["c"]])
+        I = np.zeros(G.n)
+        for gi in range(ngr):
+            rot = rot_mul(rot_mul(rot_mul(rot_phi, rot_axis(int(rots[2][0]), nn[2, gi])),
+                                  rot_axis(int(rots[1][0]), nn[1, gi])),
+                          rot_axis(int(rots[0][0]), nn[0, gi]))
+            dv = d[:, gi]
+            center = np.array([rot[i, 0] * dv[0] + rot[i, 1] * dv[1] + rot[i, 2] * dv[2]
+                               for i in range(3)]) + np.array(s["transvec"])
+            ff = np.zeros(4 * G.n, dtype=np.complex128)
+            for ekey in uc:
+                sh = hig["shapes"][ekey]
+                zr, yr, xr = sh["rot"]
+                srot = rot_mul(rot_mul(rot_mul(rot, rot_axis(0, xr)), rot_axis(1, yr)), rot_axis(2, zr))
+                dn2 = complex(0.0 - 2 * sh["refindex"][0], 0.0 - 2 * sh["refindex"][1])
+                params = [{"type": p["type"], "stat": p["stat"], "min": p["min"], "max": p["max"],
+                           "mean": p["p1"], "deviation": p["p2"], "nvalues": p["nvalues"]}
+                          for p in sh["params"].values()]
+                for loc in uc[ekey]:
+                    if sh["name"] == "custom":
+                        eff = ff_approx_triangle(meshes[ekey], G.qx, G.qy, G.qz_ext, srot)
+                    else:
+                        eff = ff_analytic(G, sh["name"], params, transvec=loc, rot=srot)
+                    ff = ff + dn2 * eff
+            if s["type"] == "paracrystal":
+                pc = s["paracrystal"]
+                sf = sf_paracrystal(G, pc["dims"], LATTICE.get(lat["type"], 1), pc.get("xmean", 0.0),
+                                    pc.get("ymean", 0.0), pc.get("xstddev", 0.0),
+                                    pc.get("ystddev", 0.0), pc.get("domain", 0.0))
+            elif s["type"] == "percusyevick":
+                py = s["percusyevick"]
+                sf = sf_percus_yevick(G, py["diameter"], py["volfraction"], py["dims"])
+            else:
+                sf = sf_lattice(G, abc, s["repetition"], s["scaling_mean"], center, rot)
+            I = dwba_combine(fc, sf, ff, 1.0, I)
+        intens.append(I)
+    ratios = [s["iratio"] for s in hig["structures"].values()]
+    img = structure_sum(np.array(intens), ratios)
+    return img.reshape(nrow, ncol)
