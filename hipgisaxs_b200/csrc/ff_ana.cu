@@ -14,92 +14,11 @@
 #include <string>
 #include <vector>
 
+#include "ana_sf.cuh"
 #include "cplx.cuh"
 #include "hgx_internal.cuh"
 
 namespace hgx {
-
-constexpr double PI_REF = 3.141592653589793;  // PI_, include/common/constants.hpp
-constexpr double CUTINY_REF = 1.0e-13;
-constexpr int ANA_MAXV = 64;  // samples per dimension
-
-// ShapeName values (include/common/enums.hpp:24-43)
-enum { SH_BOX = 2, SH_CUBE = 3, SH_CYLINDER = 4, SH_SPHERE = 5, SH_PRISM3 = 8, SH_PRISM6 = 9,
-       SH_PYRAMID = 14 };
-
-struct Dist {
-  int n;
-  double v[ANA_MAXV];
-  double w[ANA_MAXV];
-};
-
-struct AnaArgs {
-  int shape;
-  Dist d[4];
-  double tau, eta, tv[3];
-  Rot9d R;
-  const double* qx;
-  const double* qy;
-  const double2* qz;
-  int nqy, nqz;
-  void* out;
-  int out_c64;
-};
-
-// hig::sinc, include/numerics/numeric_utils.hpp:54-63 (free function)
-__device__ __forceinline__ zd sinc_free(zd x) {
-  if (cabs_(x) > 1.0E-14) return csin_(x) / x;
-  zd x2 = x * x;
-  return (1.0 - x2 / 6.0) + (x2 * x * x) / 120.0;
-}
-// AnalyticFormFactor::sinc, src/ff/ff_ana.cpp:222-227 (member)
-__device__ __forceinline__ zd sinc_member(zd v) {
-  if (fabs(v.x) <= 1e-14 && fabs(v.y) <= 1e-14) return zd(1.0, 0.0);
-  return csin_(v) / v;
-}
-// AnalyticFormFactor::fq_inv, src/ff/ff_ana.cpp:190-196
-__device__ __forceinline__ zd fq_inv(zd value, double y) {
-  zd t = (cexp_((zd(0, 1) * value) * y / 2.0) * 2.0) * csin_(value * y / 2.0) / value;
-  if (cabs_(t) <= 1e-14) t = zd(y, 0);
-  return t;
-}
-__device__ __forceinline__ zd trans_phase(const zd* m, const double* tv) {
-  zd t = m[0] * tv[0] + m[1] * tv[1] + m[2] * tv[2];
-  return cexp_(zd(-t.y, t.x));
-}
-
-// ff_ana_sphere.cpp:33-45
-__device__ zd ff_sphere_one(zd qx, zd qy, zd qz, double radius) {
-  zd qval = csqrt_(qx * qx + qy * qy + qz * qz);
-  if (cabs_(qval) < 2.2250738585072014e-308) return zd(0, 0);
-  zd qR = qval * radius;
-  zd qR3 = qR * qR * qR;
-  zd t1 = conj(qR3) / norm2(qR3);
-  zd c0 = (csin_(qR) - qR * ccos_(qR)) * t1;
-  zd c1 = cexp_((zd(0, 1) * qz) * radius);
-  double f0 = 4 * PI_REF * radius * radius * radius;
-  return (c0 * f0) * c1;
-}
-
-// ff_ana_pyramid.cpp:35-78 (angle in degrees)
-__device__ zd ff_pyramid_one(zd qx, zd qy, zd qz, double L, double W, double H, double angle) {
-  double a = angle * PI_REF / 180.;
-  double tan_a = tan(a);
-  if ((2 * H / L >= tan_a) || (2 * H / W >= tan_a)) return zd(0, 0);
-  zd tmp = qx * qy;
-  if (cabs_(tmp) < 1.0E-20) return zd(0, 0);
-  const zd PJ(0, 1), NJ(0, -1);
-  zd q1 = ((qx - qy) / tan_a + qz) * 0.5;
-  zd q2 = ((qx - qy) / tan_a - qz) * 0.5;
-  zd q3 = ((qx + qy) / tan_a + qz) * 0.5;
-  zd q4 = ((qx + qy) / tan_a - qz) * 0.5;
-  zd s1 = sinc_free(q1 * H) * cexp_((NJ * q1) * H), s2 = sinc_free(q2 * H) * cexp_((PJ * q2) * H);
-  zd s3 = sinc_free(q3 * H) * cexp_((NJ * q3) * H), s4 = sinc_free(q4 * H) * cexp_((PJ * q4) * H);
-  zd k1 = s1 + s2, k2 = s1 * NJ + s2 * PJ, k3 = s3 + s4, k4 = s3 * NJ + s4 * PJ;
-  zd am = (qx * L - qy * W) * 0.5, ap = (qx * L + qy * W) * 0.5;
-  zd t1 = k1 * ccos_(am), t2 = k2 * csin_(am), t3 = k3 * ccos_(ap), t4 = k4 * csin_(ap);
-  return (H / tmp) * (t1 + t2 - t3 - t4);
-}
 
 template <typename OUT>
 __device__ __forceinline__ void put(void* out, long i, zd v);
@@ -112,6 +31,18 @@ __device__ __forceinline__ void put<float2>(void* out, long i, zd v) {
   reinterpret_cast<float2*>(out)[i] = make_float2((float)v.x, (float)v.y);
 }
 
+struct AnaArgs {
+  AnaShape s;
+  double tv[3];
+  Rot9d R;
+  const double* qx;
+  const double* qy;
+  const double2* qz;
+  int nqy, nqz;
+  void* out;
+  int out_c64;
+};
+
 template <typename OUT>
 __global__ void __launch_bounds__(128) ff_analytic_kernel(const AnaArgs* __restrict__ ap) {
   const AnaArgs& a = *ap;
@@ -120,106 +51,7 @@ __global__ void __launch_bounds__(128) ff_analytic_kernel(const AnaArgs* __restr
   long iy = iz % a.nqy;
   zd m[3];
   rotate_q(a.R, a.qx[iy], a.qy[iy], zd(a.qz[iz]), m);
-  zd out(0, 0);
-  const Dist& X = a.d[0];
-  const Dist& Y = a.d[1];
-  const Dist& Z = a.d[2];
-  const Dist& B = a.d[3];
-  switch (a.shape) {
-    case SH_CYLINDER: {  // ff_ana_cylinder.cpp:34-42,100-117
-      zd qpar = csqrt_(m[0] * m[0] + m[1] * m[1]);
-      zd fr(0, 0), gh(0, 0);
-      for (int i = 0; i < X.n; ++i) {
-        double r = X.v[i];
-        zd t1 = qpar * r;
-        if (norm2(t1) > CUTINY_REF) fr += (zd(j1(t1.x), 0.0) * conj(t1) / norm2(t1)) * (2. * PI_REF * r * r);
-      }
-      for (int i = 0; i < Z.n; ++i) {
-        double h = Z.v[i];
-        gh += (sinc_free((m[2] * 0.5) * h) * h) * cexp_(((zd(0, 0.5)) * m[2]) * h);
-      }
-      out = fr * gh * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_SPHERE: {  // ff_ana_sphere.cpp:95-107
-      zd acc(0, 0);
-      for (int i = 0; i < X.n; ++i) acc += ff_sphere_one(m[0], m[1], m[2], X.v[i]) * X.w[i];
-      out = acc * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_BOX: {  // ff_ana_box.cpp:35-42,96-125
-      zd sx(0, 0), sy(0, 0), sz(0, 0);
-      for (int i = 0; i < X.n; ++i) sx += sinc_free((m[0] * 0.5) * X.v[i]) * (X.v[i] * X.w[i]);
-      for (int i = 0; i < Y.n; ++i) sy += sinc_free((m[1] * 0.5) * Y.v[i]) * (Y.v[i] * Y.w[i]);
-      for (int i = 0; i < Z.n; ++i)
-        sz += (cexp_((zd(0, 0.5) * m[2]) * Z.v[i]) * sinc_free((m[2] * 0.5) * Z.v[i])) *
-              (Z.v[i] * Z.w[i]);
-      out = sx * sy * sz * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_CUBE: {  // ff_ana_cube.cpp:35-42,87-107
-      zd acc(0, 0);
-      for (int i = 0; i < X.n; ++i) {
-        double L = X.v[i];
-        zd e = cexp_((zd(0, 0.5) * m[2]) * L);
-        zd s = sinc_free((m[0] * 0.5) * L) * sinc_free((m[1] * 0.5) * L) * sinc_free((m[2] * 0.5) * L);
-        acc += ((e * (L * L * L)) * s) * X.w[i];
-      }
-      out = acc * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_PRISM3: {  // ff_ana_prism.cpp:82-108 (unweighted)
-      const double sqrt3 = sqrt(3.0);
-      zd t1 = m[0] * (m[0] * m[0] - (m[1] * 3.0) * m[1]);
-      zd t2 = m[2] + (m[0] * sin(a.eta) + m[1] * cos(a.eta)) * tan(a.tau);
-      zd sl(0, 0), sh(0, 0);
-      for (int i = 0; i < X.n; ++i) {
-        double L = X.v[i];
-        zd t4 = m[0] * cexp_(((zd(0, 1) * m[1]) * L) * sqrt3);
-        zd t5 = m[0] * ccos_(m[0] * L);
-        zd t6 = (zd(0, sqrt3) * m[1]) * csin_(m[0] * L);
-        zd t3 = (m[1] * L) / sqrt3;
-        zd t9 = cexp_(zd(t3.y, -t3.x)) * (2.0 * sqrt3);
-        sl += (t9 / t1) * (t4 - t5 - t6);
-      }
-      for (int i = 0; i < Z.n; ++i) sh += fq_inv(t2, Z.v[i]);
-      out = sl * sh * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_PRISM6: {  // ff_ana_prism6.cpp:80-98 (unweighted)
-      const double sqrt3 = sqrt(3.0);
-      zd qm = (m[0] * sin(a.eta) + m[1] * cos(a.eta)) * tan(a.tau);
-      zd t1 = (4.0 * sqrt3) / ((m[1] * 3.0) * m[1] - m[0] * m[0]);
-      zd sl(0, 0), sh(0, 0);
-      for (int i = 0; i < X.n; ++i) {
-        double L = X.v[i];
-        zd rmqx = (m[0] * L) / sqrt3, rmqy = m[1] * L;
-        zd t2 = rmqy * rmqy * sinc_member(rmqx) * sinc_member(rmqy);
-        zd t3 = ccos_(rmqx * 2.0);
-        zd t4 = ccos_(rmqy) * ccos_(rmqx);
-        sl += t2 + t3 - t4;
-      }
-      for (int i = 0; i < Z.n; ++i) sh += fq_inv(m[2] + qm, Z.v[i]);
-      out = t1 * sl * sh * trans_phase(m, a.tv);
-      break;
-    }
-    case SH_PYRAMID: {  // ff_ana_pyramid.cpp:118-139
-      zd acc(0, 0);
-      for (int i = 0; i < X.n; ++i)
-        for (int j = 0; j < Y.n; ++j)
-          for (int h = 0; h < Z.n; ++h)
-            for (int b = 0; b < B.n; ++b) {
-              double prob = X.w[i] * Y.w[j] * Z.w[h] * B.w[b];
-              acc += ff_pyramid_one(m[0], m[1], m[2], X.v[i], Y.v[j], Z.v[h], B.v[b]) * prob;
-            }
-      zd t1 = m[0] * a.tv[0] + m[1] * a.tv[1] + m[2] * a.tv[2];
-      out = acc * cexp_(zd(0, 1) * t1);
-      break;
-    }
-    default:
-      break;
-  }
-  put<OUT>(a.out, iz, out);
+  put<OUT>(a.out, iz, ff_analytic_eval(a.s, m, a.tv));
 }
 
 // ------------------------------------------------------------------- host side ----
@@ -274,6 +106,88 @@ static int fill_dist(Dist& d, int n, const double* v, const double* w, const cha
   return HGX_OK;
 }
 
+static int check_dims(const AnaShape& a) {
+  const int n1 = a.d[0].n, n2 = a.d[1].n, n3 = a.d[2].n;
+  switch (a.shape) {
+    case SH_BOX:
+      if (!n1 || !n2 || !n3) return fail(HGX_ERR_INVALID_ARG, "box needs x, y and height");
+      break;
+    case SH_CUBE:
+    case SH_SPHERE:
+      if (!n1) return fail(HGX_ERR_INVALID_ARG, "cube/sphere need dimension 1");
+      break;
+    case SH_CYLINDER:
+    case SH_PRISM3:
+      if (!n1 || !n3) return fail(HGX_ERR_INVALID_ARG, "cylinder/prism3 need dimensions 1 and 3");
+      break;
+    case SH_PRISM6:
+    case SH_PYRAMID:
+      break;
+    default:
+      return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: shape not implemented by the reference");
+  }
+  return HGX_OK;
+}
+
+// The reference's parameter routing (the compute_* switch statements of
+// src/ff/ff_ana_*.cpp) plus param_distribution: HiG-style parameters (7 doubles each:
+// ShapeParamType, StatisticType, min, max, mean, deviation, nvalues) -> the sampled dimensions
+// of an AnaShape, checked as hgx_ff_analytic checks them.
+int ana_shape_from_params(int shape, int nparam, const double* params, double tau, double eta,
+                          AnaShape& out) {
+  if (nparam < 0 || (nparam > 0 && !params))
+    return fail(HGX_ERR_INVALID_ARG, "analytic shape: bad parameter list");
+  enum { P_RADIUS = 2, P_XSIZE = 3, P_YSIZE = 4, P_HEIGHT = 5, P_EDGE = 6, P_BASEANGLE = 7 };
+  std::vector<double> v[4], w[4];
+  for (int i = 0; i < nparam; ++i) {
+    const double* p = params + 7 * i;
+    int type = (int)p[0];
+    std::vector<int> dims;
+    switch (shape) {
+      case SH_BOX:
+        if (type == P_EDGE) dims = {0, 1, 2};
+        else if (type == P_XSIZE) dims = {0};
+        else if (type == P_YSIZE) dims = {1};
+        else if (type == P_HEIGHT) dims = {2};
+        break;
+      case SH_CUBE:
+        if (type == P_HEIGHT) dims = {0};
+        break;
+      case SH_CYLINDER:
+        if (type == P_RADIUS) dims = {0};
+        else if (type == P_HEIGHT) dims = {2};
+        break;
+      case SH_SPHERE:
+        if (type == P_RADIUS) dims = {0};
+        else if (type == P_EDGE || type == P_XSIZE || type == P_YSIZE || type == P_HEIGHT)
+          dims = {2};
+        break;
+      case SH_PRISM3:
+      case SH_PRISM6:
+        if (type == P_EDGE) dims = {0};
+        else if (type == P_HEIGHT) dims = {2};
+        break;
+      case SH_PYRAMID:
+        if (type == P_XSIZE) dims = {0};
+        else if (type == P_YSIZE) dims = {1};
+        else if (type == P_HEIGHT) dims = {2};
+        else if (type == P_BASEANGLE) dims = {3};
+        break;
+      default:
+        return fail(HGX_ERR_INVALID_ARG, "analytic shape: shape not implemented by the reference");
+    }
+    for (int d : dims)
+      HGX_TRY(param_distribution_host((int)p[1], p[2], p[3], p[4], p[5], (int)p[6], v[d], w[d]));
+  }
+  out.shape = shape;
+  for (int k = 0; k < 4; ++k)
+    HGX_TRY(fill_dist(out.d[k], (int)v[k].size(), v[k].empty() ? nullptr : v[k].data(),
+                      w[k].empty() ? nullptr : w[k].data(), "a parameter distribution"));
+  out.tau = tau;
+  out.eta = eta;
+  return check_dims(out);
+}
+
 int ff_analytic_launch(hgx_ctx c, hgx_qgrid g, const AnaArgs& host_args, void* out, int ff_type) {
   // the argument block (about 4 KB) goes to device scratch so the kernel can index it freely
   AnaArgs a = host_args;
@@ -325,31 +239,14 @@ int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
   if (ff_type != HGX_C128 && ff_type != HGX_C64)
     return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: unknown output type");
   AnaArgs a;  // about 4 KB; filled here, copied to device scratch by ff_analytic_launch
-  a.shape = shape;
-  HGX_TRY(fill_dist(a.d[0], n1, v1, w1, "dimension 1"));
-  HGX_TRY(fill_dist(a.d[1], n2, v2, w2, "dimension 2"));
-  HGX_TRY(fill_dist(a.d[2], n3, v3, w3, "dimension 3"));
-  HGX_TRY(fill_dist(a.d[3], n4, v4, w4, "dimension 4"));
-  switch (shape) {
-    case SH_BOX:
-      if (!n1 || !n2 || !n3) return fail(HGX_ERR_INVALID_ARG, "box needs x, y and height");
-      break;
-    case SH_CUBE:
-    case SH_SPHERE:
-      if (!n1) return fail(HGX_ERR_INVALID_ARG, "cube/sphere need dimension 1");
-      break;
-    case SH_CYLINDER:
-    case SH_PRISM3:
-      if (!n1 || !n3) return fail(HGX_ERR_INVALID_ARG, "cylinder/prism3 need dimensions 1 and 3");
-      break;
-    case SH_PRISM6:
-    case SH_PYRAMID:
-      break;
-    default:
-      return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: shape not implemented by the reference");
-  }
-  a.tau = tau;
-  a.eta = eta;
+  a.s.shape = shape;
+  HGX_TRY(fill_dist(a.s.d[0], n1, v1, w1, "dimension 1"));
+  HGX_TRY(fill_dist(a.s.d[1], n2, v2, w2, "dimension 2"));
+  HGX_TRY(fill_dist(a.s.d[2], n3, v3, w3, "dimension 3"));
+  HGX_TRY(fill_dist(a.s.d[3], n4, v4, w4, "dimension 4"));
+  HGX_TRY(check_dims(a.s));
+  a.s.tau = tau;
+  a.s.eta = eta;
   for (int i = 0; i < 3; ++i) a.tv[i] = transvec ? transvec[i] : 0.0;
   static const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   for (int i = 0; i < 9; ++i) a.R.r[i] = rot9 ? rot9[i] : eye[i];
@@ -377,49 +274,12 @@ int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
 int hgx_ff_analytic_params(hgx_ctx c, hgx_qgrid g, int shape, int nparam, const double* params,
                            double tau, double eta, const double* transvec, const double* rot9,
                            void* ff, int ff_type) {
-  if (nparam < 0 || (nparam > 0 && !params))
-    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic_params: bad parameter list");
-  enum { P_RADIUS = 2, P_XSIZE = 3, P_YSIZE = 4, P_HEIGHT = 5, P_EDGE = 6, P_BASEANGLE = 7 };
+  AnaShape s;
+  HGX_TRY(ana_shape_from_params(shape, nparam, params, tau, eta, s));
   std::vector<double> v[4], w[4];
-  for (int i = 0; i < nparam; ++i) {
-    const double* p = params + 7 * i;
-    int type = (int)p[0];
-    std::vector<int> dims;
-    switch (shape) {
-      case SH_BOX:
-        if (type == P_EDGE) dims = {0, 1, 2};
-        else if (type == P_XSIZE) dims = {0};
-        else if (type == P_YSIZE) dims = {1};
-        else if (type == P_HEIGHT) dims = {2};
-        break;
-      case SH_CUBE:
-        if (type == P_HEIGHT) dims = {0};
-        break;
-      case SH_CYLINDER:
-        if (type == P_RADIUS) dims = {0};
-        else if (type == P_HEIGHT) dims = {2};
-        break;
-      case SH_SPHERE:
-        if (type == P_RADIUS) dims = {0};
-        else if (type == P_EDGE || type == P_XSIZE || type == P_YSIZE || type == P_HEIGHT)
-          dims = {2};
-        break;
-      case SH_PRISM3:
-      case SH_PRISM6:
-        if (type == P_EDGE) dims = {0};
-        else if (type == P_HEIGHT) dims = {2};
-        break;
-      case SH_PYRAMID:
-        if (type == P_XSIZE) dims = {0};
-        else if (type == P_YSIZE) dims = {1};
-        else if (type == P_HEIGHT) dims = {2};
-        else if (type == P_BASEANGLE) dims = {3};
-        break;
-      default:
-        return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic_params: shape not implemented by the reference");
-    }
-    for (int d : dims)
-      HGX_TRY(param_distribution_host((int)p[1], p[2], p[3], p[4], p[5], (int)p[6], v[d], w[d]));
+  for (int k = 0; k < 4; ++k) {
+    v[k].assign(s.d[k].v, s.d[k].v + s.d[k].n);
+    w[k].assign(s.d[k].w, s.d[k].w + s.d[k].n);
   }
   auto ptr = [](std::vector<double>& x) { return x.empty() ? nullptr : x.data(); };
   return hgx_ff_analytic(c, g, shape, (int)v[0].size(), ptr(v[0]), ptr(w[0]), (int)v[1].size(),

@@ -257,6 +257,8 @@ int hgx_destroy(hgx_ctx c) {
   if (c->d_err) cudaFree(c->d_err);
   if (c->shaped) hgx_qgrid_destroy(c->shaped);
   delete c->mesh;
+  if (c->hig && c->hig->grid) hgx_qgrid_destroy(c->hig->grid);
+  delete c->hig;
   c->scratch.release();
   c->staging.release();
   c->shaped_out.release();

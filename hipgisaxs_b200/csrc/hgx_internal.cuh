@@ -55,6 +55,13 @@ namespace hgx {
 struct MeshWork {
   DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib, bwpart;
 };
+// Work of hgx_hig_compute_gisaxs, kept by the context between calls: the last description's
+// q-grid (rebuilt when its region, beam or resolution changes) and grow-only buffers.
+struct HigWork {
+  hgx_qgrid grid = nullptr;
+  double key[8] = {0};
+  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er;
+};
 }  // namespace hgx
 
 // -------------------------------------------------------------- the context ----
@@ -72,6 +79,7 @@ struct hgx_ctx_s {
   hgx_qgrid_s* shaped = nullptr;
   hgx::DevBuf shaped_out;
   hgx::MeshWork* mesh = nullptr;  // work buffers of the mesh chi^2 and gradient
+  hgx::HigWork* hig = nullptr;    // work of the HiG-driven simulation
 };
 
 // -------------------------------------------------------------- the q-grid ----

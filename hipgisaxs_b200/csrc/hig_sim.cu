@@ -32,9 +32,11 @@
 #include <stdlib.h>
 
 #include <map>
+#include <new>
 #include <string>
 #include <vector>
 
+#include "ana_sf.cuh"
 #include "hgx_internal.cuh"
 #include "hig_config.hpp"
 
@@ -58,6 +60,94 @@ __global__ void add_scaled_kernel(long n, double dre, double dim, const double2*
   f.y = __dadd_rn(f.y, im);
   ff[i] = f;
 }
+
+// The fused grain loop (structures whose unit cell holds analytic shapes only): a quad of
+// threads per pixel loops over the grains and evaluates, for its DWBA block, every element's
+// form factor at its own rotation and location and the grain's structure factor; the quad
+// forms the DWBA sum and accumulates |sum|^2 in a register.  The per-grain form-factor and
+// structure-factor arrays of the step-by-step path (4N complex each, written and read back
+// per grain) never exist: per grain the kernel reads a few dozen parameters.  The arithmetic
+// is the step-by-step path's (the same device functions, the same order of sums), so the two
+// agree to rounding.
+struct FusedElem {
+  double loc[3];
+  double dre, dim;  // dn2 of the element's shape
+};
+
+struct FusedArgs {
+  const AnaShape* shapes;  // one per element-location
+  const FusedElem* elems;
+  int nelem;
+  const double* grains;    // per grain: rotation (9), centre (3)
+  const double* elem_rot;  // per grain and element-location: rotation (9)
+  int g0, g1;              // grains of this launch
+  SfLat lat;               // lattice vectors and repetitions (centre set per grain)
+  const double2* sfbuf;    // grain-independent structure factor (4N), or NULL for the lattice
+  const double* qx;
+  const double* qy;
+  const double2* qz;
+  const double2* fc;
+  long n;
+  double* out;             // N intensities, accumulated
+};
+
+// Four threads per pixel, one per DWBA block k: each evaluates fc_k sf_k ff_k and the quad
+// adds the four terms in the order k = 0..3 (shuffles), as the step-by-step combination does.
+// SHAPE: the one analytic shape of every element (0: any).
+template <int SHAPE>
+__global__ void __launch_bounds__(128) grain_dwba_kernel(FusedArgs a) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = t >> 2;
+  const int k = (int)(t & 3);
+  const bool live = i < a.n;  // every lane takes part in the shuffles
+  const long ii = live ? i : 0;
+  const double qx = a.qx[ii], qy = a.qy[ii];
+  const zd qz(a.qz[k * a.n + ii]);
+  const zd fc(a.fc[k * a.n + ii]);
+  const int base = (threadIdx.x & 31) & ~3;
+  double acc = (live && k == 0) ? a.out[i] : 0.0;
+  for (int g = a.g0; g < a.g1; ++g) {
+    const double* gp = a.grains + 12 * (long)g;
+    zd ff(0, 0);
+    for (int e = 0; e < a.nelem; ++e) {
+      const double* er = a.elem_rot + 9 * ((long)g * a.nelem + e);
+      Rot9d Re;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) Re.r[r] = er[r];
+      zd m[3];
+      rotate_q(Re, qx, qy, qz, m);
+      const zd eff = ff_analytic_eval<SHAPE>(a.shapes[e], m, a.elems[e].loc);
+      const double dre = a.elems[e].dre, dim = a.elems[e].dim;
+      ff.x = __dadd_rn(ff.x, __dsub_rn(__dmul_rn(dre, eff.x), __dmul_rn(dim, eff.y)));
+      ff.y = __dadd_rn(ff.y, __dadd_rn(__dmul_rn(dre, eff.y), __dmul_rn(dim, eff.x)));
+    }
+    zd s;
+    if (a.sfbuf) {
+      s = zd(a.sfbuf[k * a.n + ii]);
+    } else {
+      Rot9d R;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) R.r[r] = gp[r];
+      SfLat L = a.lat;
+      L.center[0] = gp[9];
+      L.center[1] = gp[10];
+      L.center[2] = gp[11];
+      zd m[3];
+      rotate_q(R, qx, qy, qz, m);
+      s = sf_lattice_eval(L, m);
+    }
+    const zd term = fc * s * ff;
+    zd sum(0, 0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      sum += zd(__shfl_sync(0xffffffffu, term.x, base + j), __shfl_sync(0xffffffffu, term.y, base + j));
+    sum = 1.0 * sum;
+    acc += sum.x * sum.x + sum.y * sum.y;
+  }
+  if (live && k == 0) a.out[i] = acc;
+}
+
+constexpr int FUSED_GRAINS_PER_LAUNCH = 64;  // keeps each launch to tens of milliseconds
 
 // RotMatrix_t(axis, angle) and its product (include/numerics/matrix.hpp:43-117)
 struct Rot {
@@ -204,6 +294,120 @@ static int orientations(const hig::Structure& s, int ngr, std::vector<double>& n
   return HGX_OK;
 }
 
+
+// The fused path for one structure: element-location and grain tables on the device, the
+// structure factor once when it does not depend on the grain, then the grain kernel in
+// launches of FUSED_GRAINS_PER_LAUNCH grains (the grains in order, so the sums run as in the
+// step-by-step path).
+static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Structure& s, const hig::Unitcell& uc,
+                           const hig::Input& in, const Rot& rot_phi, const std::vector<double>& dd,
+                           const std::vector<double>& nn, int ngr, int ax1, int ax2, int ax3,
+                           const double* abc9, const double* repet, const double* scaling,
+                           const double2* fc, double* Is) {
+  cudaStream_t st = c->stream;
+  std::vector<AnaShape> shapes;
+  std::vector<FusedElem> elems;
+  std::vector<const hig::Shape*> owner;
+  for (const auto& ekv : uc.elements) {  // in shape-key order, locations in file order
+    const hig::Shape& sh = in.shapes.at(ekv.first);
+    std::vector<double> prm;
+    for (const auto& pk : sh.params) {
+      const hig::ShapeParam& p = pk.second;
+      const double row[7] = {(double)param_code(p.type), (double)stat_code(p.stat), p.min, p.max,
+                             p.p1, p.p2, (double)p.nvalues};
+      prm.insert(prm.end(), row, row + 7);
+    }
+    AnaShape as;
+    HGX_TRY(ana_shape_from_params(shape_code(sh.name), (int)(prm.size() / 7), prm.data(), 0.0, 0.0, as));
+    for (const hig::vec3& loc : ekv.second) {
+      FusedElem fe;
+      for (int k = 0; k < 3; ++k) fe.loc[k] = loc[k];
+      fe.dre = 0.0 - 2 * sh.refindex.delta;
+      fe.dim = 0.0 - 2 * sh.refindex.beta;
+      shapes.push_back(as);
+      elems.push_back(fe);
+      owner.push_back(&sh);
+    }
+  }
+  const int nelem = (int)elems.size();
+  std::vector<double> gt(12 * (size_t)ngr), er(9 * (size_t)ngr * (nelem > 0 ? nelem : 1));
+  for (int gi = 0; gi < ngr; ++gi) {
+    const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
+                    Rot::axis(ax1, nn[gi]);
+    const double ddv[3] = {dd[gi], dd[gi + ngr], dd[gi + 2 * ngr]};
+    double center[3];
+    rot.apply(ddv, center);
+    for (int k = 0; k < 3; ++k) center[k] += s.transvec[k];
+    for (int r = 0; r < 9; ++r) gt[12 * (size_t)gi + r] = rot.m[r];
+    for (int k = 0; k < 3; ++k) gt[12 * (size_t)gi + 9 + k] = center[k];
+    for (int e = 0; e < nelem; ++e) {
+      const hig::Shape& sh = *owner[e];
+      const Rot srot = ((rot * Rot::axis(0, sh.xrot)) * Rot::axis(1, sh.yrot)) * Rot::axis(2, sh.zrot);
+      for (int r = 0; r < 9; ++r) er[9 * ((size_t)gi * nelem + e) + r] = srot.m[r];
+    }
+  }
+  DevBuf &bshapes = w.shapes, &belems = w.elems, &bgt = w.gt, &ber = w.er, &bsf = w.sf;
+  if (nelem > 0) {
+    HGX_TRY(bshapes.reserve(sizeof(AnaShape) * nelem));
+    HGX_TRY(belems.reserve(sizeof(FusedElem) * nelem));
+    HGX_CUDA(cudaMemcpyAsync(bshapes.p, shapes.data(), sizeof(AnaShape) * nelem, cudaMemcpyHostToDevice, st));
+    HGX_CUDA(cudaMemcpyAsync(belems.p, elems.data(), sizeof(FusedElem) * nelem, cudaMemcpyHostToDevice, st));
+  }
+  HGX_TRY(bgt.reserve(sizeof(double) * gt.size()));
+  HGX_TRY(ber.reserve(sizeof(double) * er.size()));
+  HGX_CUDA(cudaMemcpyAsync(bgt.p, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice, st));
+  HGX_CUDA(cudaMemcpyAsync(ber.p, er.data(), sizeof(double) * er.size(), cudaMemcpyHostToDevice, st));
+  FusedArgs a;
+  a.shapes = (const AnaShape*)bshapes.p;
+  a.elems = (const FusedElem*)belems.p;
+  a.nelem = nelem;
+  a.grains = (const double*)bgt.p;
+  a.elem_rot = (const double*)ber.p;
+  for (int k = 0; k < 3; ++k) {  // as hgx_sf_lattice scales and clamps them (sf.cu)
+    a.lat.la[k] = abc9[k] * scaling[0];
+    a.lat.lb[k] = abc9[3 + k] * scaling[1];
+    a.lat.lc[k] = abc9[6 + k] * scaling[2];
+    a.lat.rep[k] = repet[k] < 1 ? 1 : repet[k];
+    a.lat.center[k] = 0.0;
+  }
+  a.sfbuf = nullptr;
+  if (s.type == "paracrystal") {
+    HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1], s.pc_dist[0],
+                               s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
+    a.sfbuf = (const double2*)bsf.p;
+  } else if (s.type == "percusyevick") {
+    HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
+    a.sfbuf = (const double2*)bsf.p;
+  }
+  a.qx = g->qx;
+  a.qy = g->qy;
+  a.qz = g->qz;
+  a.fc = fc;
+  a.n = (long)g->nqy;
+  a.out = Is;
+  const unsigned blocks = (unsigned)((4 * a.n + 127) / 128);
+  int one = nelem > 0 ? shapes[0].shape : 0;  // the shape every element shares, if any
+  for (int e = 1; e < nelem; ++e)
+    if (shapes[e].shape != one) one = 0;
+  for (int g0 = 0; g0 < ngr; g0 += FUSED_GRAINS_PER_LAUNCH) {
+    a.g0 = g0;
+    a.g1 = g0 + FUSED_GRAINS_PER_LAUNCH < ngr ? g0 + FUSED_GRAINS_PER_LAUNCH : ngr;
+    switch (one) {
+      case SH_CYLINDER: grain_dwba_kernel<SH_CYLINDER><<<blocks, 128, 0, st>>>(a); break;
+      case SH_SPHERE: grain_dwba_kernel<SH_SPHERE><<<blocks, 128, 0, st>>>(a); break;
+      case SH_BOX: grain_dwba_kernel<SH_BOX><<<blocks, 128, 0, st>>>(a); break;
+      case SH_CUBE: grain_dwba_kernel<SH_CUBE><<<blocks, 128, 0, st>>>(a); break;
+      case SH_PRISM3: grain_dwba_kernel<SH_PRISM3><<<blocks, 128, 0, st>>>(a); break;
+      case SH_PRISM6: grain_dwba_kernel<SH_PRISM6><<<blocks, 128, 0, st>>>(a); break;
+      case SH_PYRAMID: grain_dwba_kernel<SH_PYRAMID><<<blocks, 128, 0, st>>>(a); break;
+      default: grain_dwba_kernel<0><<<blocks, 128, 0, st>>>(a); break;
+    }
+    HGX_CUDA(cudaGetLastError());
+  }
+  // the tables stay in the context's buffers; the next structure rewrites them in stream order
+  return HGX_OK;
+}
+
 }  // namespace hgx
 
 using namespace hgx;
@@ -256,9 +460,22 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   double k0, alpha_i;
   HGX_TRY(hgx_hig_beam(h, &k0, &alpha_i, nullptr));
   const double phi = sc.inplanerot[0] * PI / 180;
-  hgx_qgrid g = nullptr;
-  HGX_TRY(hgx_hig_qgrid(c, h, 0.0, 0.0, &g));
-  struct GridGuard { hgx_qgrid g; ~GridGuard() { hgx_qgrid_destroy(g); } } guard{g};
+  if (!c->hig) {
+    c->hig = new (std::nothrow) HigWork;
+    if (!c->hig) return fail(HGX_ERR_NO_MEMORY, "hgx_hig_compute_gisaxs: out of host memory");
+  }
+  HigWork& w = *c->hig;
+  const double key[8] = {(double)cp.resolution[0], (double)cp.resolution[1], cp.minpoint[0], cp.minpoint[1],
+                         cp.maxpoint[0], cp.maxpoint[1], alpha_i, k0};
+  bool same = w.grid != nullptr;
+  for (int k = 0; k < 8 && same; ++k) same = w.key[k] == key[k];
+  if (!same) {  // the grid of this description (vacuum layer: dn2 = 0)
+    if (w.grid) hgx_qgrid_destroy(w.grid);
+    w.grid = nullptr;
+    HGX_TRY(hgx_hig_qgrid(c, h, 0.0, 0.0, &w.grid));
+    for (int k = 0; k < 8; ++k) w.key[k] = key[k];
+  }
+  hgx_qgrid g = w.grid;
   const long n = (long)g->nqy;
   const long nq = (long)g->nqz;  // 4n
   std::vector<double> ld, lb, lt;
@@ -269,7 +486,7 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     lt.push_back(kv.second.thickness);
     lo.push_back(kv.second.order);
   }
-  DevBuf bfc, bff, beff, bsf, bI;
+  DevBuf &bfc = w.fc, &bff = w.ff, &beff = w.eff, &bsf = w.sf, &bI = w.I;
   HGX_TRY(bfc.reserve(sizeof(double2) * nq));
   HGX_TRY(bff.reserve(sizeof(double2) * nq));
   HGX_TRY(beff.reserve(sizeof(double2) * nq));
@@ -320,6 +537,20 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     const double repet[3] = {s.repetition[0], s.repetition[1], s.repetition[2]};
     const double scaling[3] = {s.scaling_mean[0], s.scaling_mean[1], s.scaling_mean[2]};
     double* Is = (double*)bI.p + (size_t)si * n;
+    bool all_analytic = true;
+    for (const auto& ekv : uc.elements) {
+      auto shp = in.shapes.find(ekv.first);
+      if (shp == in.shapes.end()) return refuse("unit cell '" + uc.key + "': unknown shape '" + ekv.first + "'");
+      if (shp->second.name == "custom") all_analytic = false;
+      else if (shape_code(shp->second.name) < 0)
+        return refuse("shape '" + shp->second.key + "': '" + shp->second.name + "' has no analytic form factor here");
+    }
+    if (all_analytic) {
+      HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, abc9, repet, scaling,
+                              (const double2*)bfc.p, Is));
+      ++si;
+      continue;
+    }
     for (int gi = 0; gi < ngr; ++gi) {
       const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
                       Rot::axis(ax1, nn[gi]);
@@ -375,7 +606,13 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   }
   std::vector<double> ratios;
   for (const auto& kv : in.structures) ratios.push_back(kv.second.iratio);
-  HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), image));
+  if (is_device_ptr(image)) {
+    HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), image));
+  } else {
+    HGX_TRY(w.img.reserve(sizeof(double) * n));
+    HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), (double*)w.img.p));
+    HGX_CUDA(cudaMemcpyAsync(image, w.img.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  }
   return hgx_synchronize(c);
 }
 

@@ -14,15 +14,14 @@
 
 #include <string>
 
+#include "ana_sf.cuh"
 #include "cplx.cuh"
 #include "hgx_internal.cuh"
 
 namespace hgx {
 
 struct SfArgs {
-  double la[3], lb[3], lc[3];
-  double rep[3];
-  double center[3];
+  SfLat L;
   Rot9d R;
   const double* qx;
   const double* qy;
@@ -31,8 +30,6 @@ struct SfArgs {
   void* out;
 };
 
-__device__ __forceinline__ zd times_i(zd s) { return zd(-s.y, s.x); }  // (0,1) * s
-
 template <typename OUT>
 __global__ void __launch_bounds__(128) sf_lattice_kernel(SfArgs a) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -40,32 +37,7 @@ __global__ void __launch_bounds__(128) sf_lattice_kernel(SfArgs a) {
   long j = i % a.nqy;
   zd m[3];
   rotate_q(a.R, a.qx[j], a.qy[j], zd(a.qz[i]), m);
-  const double eps = DBL_EPSILON;
-  const zd one(1.0, 0.0);
-
-  zd e_iqa = cexp_(times_i(m[0] * a.la[0] + m[1] * a.la[1] + m[2] * a.la[2]));
-  zd Xa = one - cpow_std(e_iqa, a.rep[0]);
-  zd Ya = one - e_iqa;
-  zd sa = (fabs(Ya.y) > eps || fabs(Ya.x) > eps) ? Xa / Ya : zd(a.rep[0], 0.0);
-  sa = cpow_std(e_iqa, (1.0 - a.rep[0]) / 2.0) * sa;
-
-  zd iqb = times_i(m[0] * a.lb[0] + m[1] * a.lb[1] + a.lb[2] * a.lb[2]);
-  zd iqNb = iqb * a.rep[1];
-  zd e_iqb = cexp_(iqb);
-  zd Xb = one - cexp_(iqNb);
-  zd Yb = one - e_iqb;
-  zd sb = (fabs(Yb.y) > eps || fabs(Yb.x) > eps) ? Xb / Yb : zd(a.rep[1], 0.0);
-  sb = cpow_std(e_iqb, (1.0 - a.rep[1]) / 2.0) * sb;
-
-  zd e_iqc = cexp_(times_i(m[0] * a.lc[0] + m[1] * a.lc[1] + m[2] * a.lc[2]));
-  zd Xc = one - cpow_std(e_iqc, a.rep[2]);
-  zd Yc = one - e_iqc;
-  zd sc = (fabs(Yc.y) > eps || fabs(Yc.x) > eps) ? Xc / Yc : zd(a.rep[2], 0.0);
-  sc = cpow_std(e_iqc, (1.0 - a.rep[2]) / 2.0) * sc;
-
-  zd t3 = m[0] * a.center[0] + m[1] * a.center[1] + m[2] * a.center[2];
-  t3 = cexp_(zd(-t3.y, t3.x));
-  zd v = t3 * sa * sb * sc;
+  const zd v = sf_lattice_eval(a.L, m);
   if (sizeof(OUT) == sizeof(double2))
     reinterpret_cast<double2*>(a.out)[i] = v.d2();
   else
@@ -144,11 +116,11 @@ int hgx_sf_lattice(hgx_ctx c, hgx_qgrid g, const double* abc9, const double* rep
     return fail(HGX_ERR_INVALID_ARG, "hgx_sf_lattice: unknown output type");
   SfArgs a;
   for (int i = 0; i < 3; ++i) {
-    a.la[i] = abc9[i] * scaling[0];
-    a.lb[i] = abc9[3 + i] * scaling[1];
-    a.lc[i] = abc9[6 + i] * scaling[2];
-    a.rep[i] = repet[i] < 1 ? 1 : repet[i];  // sf.cpp:164-166
-    a.center[i] = center ? center[i] : 0.0;
+    a.L.la[i] = abc9[i] * scaling[0];
+    a.L.lb[i] = abc9[3 + i] * scaling[1];
+    a.L.lc[i] = abc9[6 + i] * scaling[2];
+    a.L.rep[i] = repet[i] < 1 ? 1 : repet[i];  // sf.cpp:164-166
+    a.L.center[i] = center ? center[i] : 0.0;
   }
   static const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   for (int i = 0; i < 9; ++i) a.R.r[i] = rot9 ? rot9[i] : eye[i];
