@@ -96,6 +96,7 @@ def parse():
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--no-fitting", action="store_true")
     ap.add_argument("--no-exact", action="store_true")
+    ap.add_argument("--no-hig", action="store_true")
     return ap.parse_args()
 
 
@@ -382,6 +383,74 @@ def exact_bench(ctx, torch, stream, sd_mesh, steps=2, n=512):
     return res
 
 
+# An ensemble simulation driven by a HiG description of the size of the reference's
+# hcp-cylinder example: 600 x 300 detector, 25 x 25 grains with z-rotations drawn over
+# [0, 180] degrees, an hcp lattice of 100 x 10 x 2 cells, DWBA over a substrate.
+HIG_ENSEMBLE = """hipGisaxsInput = {
+	shape = { key = "cyl", name = "cylinder", refindex = { delta = 8.5E-06, beta = 3.1E-07 },
+		param = { type = "radius", min = 5 }, param = { type = "height", min = 150 } },
+	unitcell = { key = "u1", element = { shape:key = "cyl", locations = [[0 0 0]] } },
+	layer = { key = "substr", order = -1, refindex = { delta = 9.1E-06, beta = 2.5E-07 } },
+	structure = { key = "st1",
+		grain = { unitcell:key = "u1", lattice = { type = "hcp" }, repetition = [100 10 2], scaling = 50 },
+		ensemble = { maxgrains = [NG NG 1],
+			orientations = { stat = "range", rot1 = { axis = "z", angles = [0 180] } } } },
+	instrumentation = { scattering = { alphai = { min = 0.175 }, photon = { value = 7350, unit = "ev" } },
+		detector = { pixelsize = 0.172, sdd = 4128.62, directbeam = [ 489.9 843.1 ] } },
+	computation = { runname = "ensemble", outputregion = { type = "qspace", minpoint = [ -1 0 ], maxpoint = [ 1 1 ] },
+		resolution = [ 600 300 ] }
+}
+"""
+
+
+def hig_bench(ctx, steps=3, ng=25):
+    """HipGISAXS::compute_gisaxs of HIG_ENSEMBLE through hgx_hig_compute_gisaxs (host image
+    out, the call synchronous), timed by the host clock; beside it the oracle's composition
+    of the same simulation on one grain (all host threads), scaled to the grain count."""
+    import ctypes
+    import tempfile
+    from hipgisaxs_b200.hig import read_hig
+    libc = ctypes.CDLL(None)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "ensemble.hig")
+        with open(path, "w") as f:
+            f.write(HIG_ENSEMBLE.replace("NG", str(ng)))
+        d = read_hig(path)
+        nrow, ncol = d.image_size()
+        img = np.zeros((nrow, ncol))
+        libc.srand(1)
+        d.compute_gisaxs(ctx, out=img)
+        ts = []
+        for _ in range(steps):
+            libc.srand(1)
+            t = time.perf_counter()
+            d.compute_gisaxs(ctx, out=img)
+            ts.append(time.perf_counter() - t)
+        ms = 1e3 * min(ts)
+        grains = ng * ng
+        res = {"metric": "simulations/s", "value": 1e3 / ms, "ms_per_simulation": ms,
+               "ms_per_grain": ms / grains, "grains": grains, "pixels": nrow * ncol,
+               "q_grain_evals_per_s": 4.0 * nrow * ncol * grains / (ms * 1e-3), "dtype": "f64",
+               "path": "hgx_hig_compute_gisaxs (fused grain kernel), host image out",
+               "workload": f"cylinders on an hcp lattice, {grains} grains, {ncol}x{nrow} DWBA"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        one = os.path.join(tmp, "one.hig")
+        with open(one, "w") as f:
+            f.write(HIG_ENSEMBLE.replace("NG", "1"))
+        d1 = read_hig(one)
+        threads = po.set_threads(os.cpu_count() or 1, "port")
+        libc.srand(1)
+        t = time.perf_counter()
+        po.compute_gisaxs(d1.data, tmp)
+        dt = time.perf_counter() - t
+        res["cpu_oracle"] = {"s_per_grain": dt, "estimate_s": dt * grains, "cores": threads,
+                             "kind": "port",
+                             "sample": f"the same description with 1 grain ({dt:.2f} s), x {grains}"}
+        res["speedup_vs_cpu_oracle"] = dt * grains / (ms * 1e-3)
+    return res
+
+
 def mesh_grad_bench(ctx, grid, steps=2):
     """Config 3, mesh part: chi^2 and the gradient with respect to all 25,002 x 3 vertex
     coordinates of the 50,000-triangle star mesh on the 2048 x 2048 DWBA detector (forward
@@ -586,6 +655,10 @@ def main():
     if not args.no_exact:
         exact = exact_bench(ctx, torch, stream, sd)
 
+    hig = None
+    if not args.no_hig and rank == 0 and world == 1:
+        hig = hig_bench(ctx)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         g = grid.read(qz_det=False, alpha=False)
@@ -621,7 +694,7 @@ def main():
                                  "frac": sfu_rate / peak_sfu},
                          "hbm_view": hbm_view(ms_step)},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
-            "exact_triangle": exact,
+            "exact_triangle": exact, "hig_simulation": hig,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
