@@ -31,8 +31,11 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
+#include <array>
 #include <map>
 #include <new>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -69,6 +72,12 @@ __global__ void add_scaled_kernel(long n, double dre, double dim, const double2*
 // per grain) never exist: per grain the kernel reads a few dozen parameters.  The arithmetic
 // is the step-by-step path's (the same device functions, the same order of sums), so the two
 // agree to rounding.
+// One structure-factor evaluation of a grain: scaled lattice vectors, repetitions, weight.
+struct ScaleEntry {
+  double la[3], lb[3], lc[3], rep[3];
+  double w;
+};
+
 struct FusedElem {
   double loc[3];
   double dre, dim;  // dn2 of the element's shape
@@ -81,7 +90,8 @@ struct FusedArgs {
   const double* grains;    // per grain: rotation (9), centre (3)
   const double* elem_rot;  // per grain and element-location: rotation (9)
   int g0, g1;              // grains of this launch
-  SfLat lat;               // lattice vectors and repetitions (centre set per grain)
+  const ScaleEntry* scales;  // per grain: nscale structure-factor evaluations
+  int nscale;
   const double2* sfbuf;    // grain-independent structure factor (4N), or NULL for the lattice
   const double* qx;
   const double* qy;
@@ -121,28 +131,36 @@ __global__ void __launch_bounds__(128) grain_dwba_kernel(FusedArgs a) {
       ff.x = __dadd_rn(ff.x, __dsub_rn(__dmul_rn(dre, eff.x), __dmul_rn(dim, eff.y)));
       ff.y = __dadd_rn(ff.y, __dadd_rn(__dmul_rn(dre, eff.y), __dmul_rn(dim, eff.x)));
     }
-    zd s;
-    if (a.sfbuf) {
-      s = zd(a.sfbuf[k * a.n + ii]);
-    } else {
-      Rot9d R;
+    Rot9d R;
 #pragma unroll
-      for (int r = 0; r < 9; ++r) R.r[r] = gp[r];
-      SfLat L = a.lat;
-      L.center[0] = gp[9];
-      L.center[1] = gp[10];
-      L.center[2] = gp[11];
-      zd m[3];
-      rotate_q(R, qx, qy, qz, m);
-      s = sf_lattice_eval(L, m);
+    for (int r = 0; r < 9; ++r) R.r[r] = gp[r];
+    zd mr[3];
+    rotate_q(R, qx, qy, qz, mr);
+    const ScaleEntry* sp = a.scales + (long)g * a.nscale;
+    for (int si = 0; si < a.nscale; ++si) {
+      zd sfv;
+      if (a.sfbuf) {
+        sfv = zd(a.sfbuf[k * a.n + ii]);
+      } else {
+        SfLat L;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          L.la[d] = sp[si].la[d];
+          L.lb[d] = sp[si].lb[d];
+          L.lc[d] = sp[si].lc[d];
+          L.rep[d] = sp[si].rep[d];
+          L.center[d] = gp[9 + d];
+        }
+        sfv = sf_lattice_eval(L, mr);
+      }
+      const zd term = fc * sfv * ff;
+      zd sum(0, 0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        sum += zd(__shfl_sync(0xffffffffu, term.x, base + j), __shfl_sync(0xffffffffu, term.y, base + j));
+      sum = sp[si].w * sum;
+      acc += sum.x * sum.x + sum.y * sum.y;
     }
-    const zd term = fc * s * ff;
-    zd sum(0, 0);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-      sum += zd(__shfl_sync(0xffffffffu, term.x, base + j), __shfl_sync(0xffffffffu, term.y, base + j));
-    sum = 1.0 * sum;
-    acc += sum.x * sum.x + sum.y * sum.y;
   }
   if (live && k == 0) a.out[i] = acc;
 }
@@ -234,6 +252,132 @@ int scan_count(double mn, double mx, double step, bool clamp_max) {
 
 }  // namespace
 
+// woo::MTRandomNumberGenerator (include/woo/random/woo_mtrandom.hpp): a 64-bit Mersenne
+// Twister seeded with 0, rand() = (x - min) / (max - min) in doubles.
+struct MtRand {
+  std::mt19937_64 gen{0};
+  double min_ = (double)std::mt19937_64::min(), max_ = (double)std::mt19937_64::max();
+  double rand() { return (double)(gen() - min_) / (max_ - min_); }
+};
+
+// HipGISAXS::gaussian and ::cauchy (include/sim/hipgisaxs_main.hpp:151-172)
+static double weight_gaussian(double x, double mean, double sigma) {
+  const double tiny = 2.2250738585072014e-308, sqrt_2pi = 2.506628;  // TINY_, SQRT_2PI_
+  if (sigma < tiny) return (x - mean < tiny) ? 1.0 : 0.0;
+  return (1.0 / (sigma * sqrt_2pi) * exp(-(x - mean) * (x - mean) / (2 * sigma * sigma)));
+}
+static double weight_cauchy(double x, double l, double sc) {
+  const double tiny = 2.2250738585072014e-308;
+  if (sc > tiny) return 1.0 / (PI * sc * (1.0 + ((x - l) / sc) * ((x - l) / sc)));
+  return (x - l > tiny) ? 0.0 : 1.0;
+}
+
+// The grain-scaling and repetition loops of run_gisaxs (:815-870, :1017-1040) with
+// construct_scaling_distribution (:2179-2226), construct_repetition_distribution (:2100-2176)
+// and generate_repetition_range (:2089-2098): for every grain the list of (scaling, repetition,
+// weight) its structure factor is evaluated with, in the reference's order.  Reproduced as
+// written: the samples of all three axes share one sample vector indexed as if each axis had
+// samples.size() / 3 of them; each repetition axis draws from a fresh generator; with a
+// repetition distribution the repetition list is zipped to its shortest axis and indexed by
+// grain, and the scaling loop runs max(#scalings, #repetitions) times.  Where the reference
+// reads past its sample vector (a repetition distribution with an undistributed scaling, in the
+// branch its grain_scaling_is_dist() takes by undefined behaviour) the undistributed branch is
+// taken.  Returns false (with a message) where the reference's own steps fail.
+static bool scale_plan(const hig::Structure& s, int ngr, std::vector<ScaleEntry>& plan, int& nscale,
+                       std::string& why) {
+  // scaling samples
+  std::vector<double> samples, weights;
+  bool any_dist = false, dist_branch = false;
+  int nv[3];
+  for (int i = 0; i < 3; ++i) {
+    const bool is_dist = s.scaling_stat[i] != "none";
+    any_dist = any_dist || is_dist;
+    nv[i] = (!is_dist || s.scaling_stddev[i] == 0) ? 1 : s.scaling_nsamples[i];
+    if (s.scaling_stddev[i] > 0) dist_branch = true;  // grain_scaling_is_dist()
+  }
+  MtRand rng;
+  const double width = 4;
+  const int max_nvals = std::max(nv[0], std::max(nv[1], nv[2]));
+  for (int i = 0; i < 3; ++i) {
+    const std::string& st = s.scaling_stat[i];
+    const double mean = s.scaling_mean[i];
+    const double sd = st != "none" ? s.scaling_stddev[i] : 0.0;
+    if (st == "none") {
+      samples.push_back(mean);
+      weights.push_back(1.0);
+    } else if (st == "gaussian" || st == "cauchy") {
+      if (!(sd > 0)) {
+        why = "a " + st + " scaling distribution needs stddev > 0 (the reference divides by zero)";
+        return false;
+      }
+      const double mn = mean - width * sd;
+      const double dx = (2 * width) * sd / (max_nvals + 1);
+      for (int j = 0; j < max_nvals; ++j) {
+        const double t = mn + j * dx + rng.rand() * dx;
+        samples.push_back(t);
+        weights.push_back(st == "gaussian" ? weight_gaussian(t, mean, sd) : weight_cauchy(t, mean, sd));
+      }
+    } else {
+      why = "scaling statistic '" + st + "' (the reference samples only gaussian and cauchy)";
+      return false;
+    }
+  }
+  (void)any_dist;
+  // repetitions
+  std::vector<std::array<double, 3>> repeats;
+  if (s.repetition_dist) {
+    const int nrep = samples.size() > 1 ? (int)samples.size() : ngr;
+    const hig::Repetition* axes[3] = {&s.xrep, &s.yrep, &s.zrep};
+    std::vector<unsigned> vals[3];
+    for (int a = 0; a < 3; ++a) {
+      const hig::Repetition& r = *axes[a];
+      if (r.stat == "none") {
+        vals[a].push_back(r.min);
+      } else if (r.stat == "range") {
+        MtRand rr;  // a fresh generator for every axis
+        for (int i = 0; i < nrep; ++i) vals[a].push_back((unsigned)(r.min + rr.rand() * (double)(r.max - r.min)));
+      } else {
+        why = "repetition statistic '" + r.stat + "' (the reference supports none and range)";
+        return false;
+      }
+    }
+    const size_t sizes = std::min(std::min(vals[0].size(), vals[1].size()), vals[2].size());
+    for (size_t i = 0; i < sizes; ++i) repeats.push_back({{(double)vals[0][i], (double)vals[1][i], (double)vals[2][i]}});
+  } else {
+    repeats.push_back({{s.repetition[0], s.repetition[1], s.repetition[2]}});
+  }
+  const int num_scaling = (int)samples.size() / 3, num_repeats = (int)repeats.size();
+  if (num_scaling == num_repeats) nscale = num_scaling;
+  else if (num_scaling == 1) nscale = num_repeats;
+  else if (num_repeats == 1) nscale = num_scaling;
+  else {
+    why = "scaling and repetition sample counts differ (the reference refuses this)";
+    return false;
+  }
+  plan.resize((size_t)ngr * nscale);
+  for (int g = 0; g < ngr; ++g)
+    for (int i = 0; i < nscale; ++i) {
+      double sc[3], w;
+      if (dist_branch) {
+        for (int k = 0; k < 3; ++k) sc[k] = samples[i + num_scaling * k];
+        w = weights[i];
+      } else {
+        for (int k = 0; k < 3; ++k) sc[k] = samples[k];
+        w = weights[0];
+      }
+      const std::array<double, 3>& rp = repeats[s.repetition_dist ? g % num_repeats : 0];
+      ScaleEntry& e = plan[(size_t)g * nscale + i];
+      for (int k = 0; k < 3; ++k) {  // scaled and clamped as hgx_sf_lattice does (sf.cu)
+        e.la[k] = s.lattice.a[k] * sc[0];
+        e.lb[k] = s.lattice.b[k] * sc[1];
+        e.lc[k] = s.lattice.c[k] * sc[2];
+        e.rep[k] = rp[k] < 1 ? 1 : rp[k];
+      }
+      e.w = 1.0 * w;  // gauss_weight (1 for the supported orientations) * scaling weight
+    }
+  return true;
+}
+
 // The grain centres of spatial_distribution's "regular" branch (:1765-1828) with the unit
 // cell size cell_ = 0 (the reference never assigns it) and tz = 0: d[3][ngrains].
 static void regular_centres(const hig::Structure& s, std::vector<double>& d, int& ngr) {
@@ -302,8 +446,8 @@ static int orientations(const hig::Structure& s, int ngr, std::vector<double>& n
 static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Structure& s, const hig::Unitcell& uc,
                            const hig::Input& in, const Rot& rot_phi, const std::vector<double>& dd,
                            const std::vector<double>& nn, int ngr, int ax1, int ax2, int ax3,
-                           const double* abc9, const double* repet, const double* scaling,
-                           const double2* fc, double* Is) {
+                           const std::vector<ScaleEntry>& plan, int nscale, const double2* fc,
+                           double* Is) {
   cudaStream_t st = c->stream;
   std::vector<AnaShape> shapes;
   std::vector<FusedElem> elems;
@@ -346,7 +490,7 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
       for (int r = 0; r < 9; ++r) er[9 * ((size_t)gi * nelem + e) + r] = srot.m[r];
     }
   }
-  DevBuf &bshapes = w.shapes, &belems = w.elems, &bgt = w.gt, &ber = w.er, &bsf = w.sf;
+  DevBuf &bshapes = w.shapes, &belems = w.elems, &bgt = w.gt, &ber = w.er, &bsf = w.sf, &bsc = w.sc;
   if (nelem > 0) {
     HGX_TRY(bshapes.reserve(sizeof(AnaShape) * nelem));
     HGX_TRY(belems.reserve(sizeof(FusedElem) * nelem));
@@ -357,19 +501,16 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
   HGX_TRY(ber.reserve(sizeof(double) * er.size()));
   HGX_CUDA(cudaMemcpyAsync(bgt.p, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice, st));
   HGX_CUDA(cudaMemcpyAsync(ber.p, er.data(), sizeof(double) * er.size(), cudaMemcpyHostToDevice, st));
+  HGX_TRY(bsc.reserve(sizeof(ScaleEntry) * plan.size()));
+  HGX_CUDA(cudaMemcpyAsync(bsc.p, plan.data(), sizeof(ScaleEntry) * plan.size(), cudaMemcpyHostToDevice, st));
   FusedArgs a;
   a.shapes = (const AnaShape*)bshapes.p;
   a.elems = (const FusedElem*)belems.p;
   a.nelem = nelem;
   a.grains = (const double*)bgt.p;
   a.elem_rot = (const double*)ber.p;
-  for (int k = 0; k < 3; ++k) {  // as hgx_sf_lattice scales and clamps them (sf.cu)
-    a.lat.la[k] = abc9[k] * scaling[0];
-    a.lat.lb[k] = abc9[3 + k] * scaling[1];
-    a.lat.lc[k] = abc9[6 + k] * scaling[2];
-    a.lat.rep[k] = repet[k] < 1 ? 1 : repet[k];
-    a.lat.center[k] = 0.0;
-  }
+  a.scales = (const ScaleEntry*)bsc.p;
+  a.nscale = nscale;
   a.sfbuf = nullptr;
   if (s.type == "paracrystal") {
     HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1], s.pc_dist[0],
@@ -444,10 +585,6 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     const hig::Structure& s = kv.second;
     if (s.distribution != "regular")
       return refuse("structure '" + s.key + "': ensemble distribution '" + s.distribution + "' is not supported");
-    if (s.repetition_dist) return refuse("structure '" + s.key + "': repetition distributions are not supported");
-    for (int k = 0; k < 3; ++k)
-      if (s.scaling_stat[k] != "none")
-        return refuse("structure '" + s.key + "': scaling distributions are not supported");
     if (!in.unitcells.count(s.unitcell_key))
       return refuse("structure '" + s.key + "': unknown unit cell '" + s.unitcell_key + "'");
     if (s.maxgrains[0] < 1 || s.maxgrains[1] < 1 || s.maxgrains[2] < 1)
@@ -532,10 +669,10 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     rotation_of(s.rot2, r2);
     rotation_of(s.rot3, r3);
     const int ax1 = (int)r1[0], ax2 = (int)r2[0], ax3 = (int)r3[0];
-    const double abc9[9] = {s.lattice.a[0], s.lattice.a[1], s.lattice.a[2], s.lattice.b[0], s.lattice.b[1],
-                            s.lattice.b[2], s.lattice.c[0], s.lattice.c[1], s.lattice.c[2]};
-    const double repet[3] = {s.repetition[0], s.repetition[1], s.repetition[2]};
-    const double scaling[3] = {s.scaling_mean[0], s.scaling_mean[1], s.scaling_mean[2]};
+    std::vector<ScaleEntry> plan;
+    int nscale = 0;
+    std::string why;
+    if (!scale_plan(s, ngr, plan, nscale, why)) return refuse("structure '" + s.key + "': " + why);
     double* Is = (double*)bI.p + (size_t)si * n;
     bool all_analytic = true;
     for (const auto& ekv : uc.elements) {
@@ -546,7 +683,7 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
         return refuse("shape '" + shp->second.key + "': '" + shp->second.name + "' has no analytic form factor here");
     }
     if (all_analytic) {
-      HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, abc9, repet, scaling,
+      HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, plan, nscale,
                               (const double2*)bfc.p, Is));
       ++si;
       continue;
@@ -591,16 +728,21 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
           HGX_CUDA(cudaGetLastError());
         }
       }
-      // the grain's structure factor
-      if (s.type == "paracrystal") {
-        HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1],
-                                   s.pc_dist[0], s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
-      } else if (s.type == "percusyevick") {
-        HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
-      } else {
-        HGX_TRY(hgx_sf_lattice(c, g, abc9, repet, scaling, center, rot.m, bsf.p, HGX_C128));
+      // the grain's structure factors and intensity terms, one per scaling/repetition sample
+      for (int k = 0; k < nscale; ++k) {
+        const ScaleEntry& e = plan[(size_t)gi * nscale + k];
+        if (s.type == "paracrystal") {
+          HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1],
+                                     s.pc_dist[0], s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
+        } else if (s.type == "percusyevick") {
+          HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
+        } else {
+          const double abc9[9] = {e.la[0], e.la[1], e.la[2], e.lb[0], e.lb[1], e.lb[2], e.lc[0], e.lc[1], e.lc[2]};
+          const double one[3] = {1.0, 1.0, 1.0};
+          HGX_TRY(hgx_sf_lattice(c, g, abc9, e.rep, one, center, rot.m, bsf.p, HGX_C128));
+        }
+        HGX_TRY(hgx_dwba_combine(c, n, (const double*)bfc.p, (const double*)bsf.p, bff.p, HGX_C128, e.w, Is));
       }
-      HGX_TRY(hgx_dwba_combine(c, n, (const double*)bfc.p, (const double*)bsf.p, bff.p, HGX_C128, 1.0, Is));
     }
     ++si;
   }

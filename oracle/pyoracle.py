@@ -515,6 +515,89 @@ def _read_obj_shape_def(path):
     return mesh_to_shape_def(np.array(V), np.array(F, dtype=np.int32))
 
 
+def _weight_gaussian(x, mean, sigma):
+    """HipGISAXS::gaussian (include/sim/hipgisaxs_main.hpp:151-156)."""
+    tiny, sqrt_2pi = 2.2250738585072014e-308, 2.506628
+    if sigma < tiny:
+        return 1.0 if x - mean < tiny else 0.0
+    return 1.0 / (sigma * sqrt_2pi) * math.exp(-(x - mean) * (x - mean) / (2 * sigma * sigma))
+
+
+def _weight_cauchy(x, l, sc):
+    """HipGISAXS::cauchy (include/sim/hipgisaxs_main.hpp:169-172)."""
+    tiny = 2.2250738585072014e-308
+    if sc > tiny:
+        return 1.0 / (3.141592653589793 * sc * (1.0 + ((x - l) / sc) * ((x - l) / sc)))
+    return 0.0 if x - l > tiny else 1.0
+
+
+def scale_plan(s, ngr):
+    """run_gisaxs's scaling and repetition loops (src/sim/hipgisaxs_main.cpp:815-870,
+    1017-1040) with construct_scaling_distribution (:2179-2226), construct_repetition_
+    distribution (:2100-2176) and generate_repetition_range (:2089-2098): per grain the list
+    of (a, b, c scaled, repetitions, weight) in the reference's order."""
+    stat, mean, sd0, ns = s["scaling_stat"], s["scaling_mean"], s["scaling_stddev"], s["scaling_nsamples"]
+    nv = [1 if (stat[i] == "none" or sd0[i] == 0) else int(ns[i]) for i in range(3)]
+    dist_branch = any(sd0[i] > 0 for i in range(3))  # grain_scaling_is_dist()
+    rnd = woo_mt_rand()
+    width, max_nvals = 4, max(nv)
+    samples, weights = [], []
+    for i in range(3):
+        sd = sd0[i] if stat[i] != "none" else 0.0
+        if stat[i] == "none":
+            samples.append(mean[i]); weights.append(1.0)
+        elif stat[i] in ("gaussian", "cauchy"):
+            mn = mean[i] - width * sd
+            dx = (2 * width) * sd / (max_nvals + 1)
+            for j in range(max_nvals):
+                t = mn + j * dx + rnd() * dx
+                samples.append(t)
+                weights.append(_weight_gaussian(t, mean[i], sd) if stat[i] == "gaussian"
+                               else _weight_cauchy(t, mean[i], sd))
+        else:
+            raise ValueError(stat[i])
+    if s["repetition_dist"]:
+        nrep = len(samples) if len(samples) > 1 else ngr
+        vals = []
+        for ax in ("xrepetition", "yrepetition", "zrepetition"):
+            r = s[ax]
+            if r["stat"] == "none":
+                vals.append([r["min"]])
+            else:
+                rr = woo_mt_rand()  # a fresh generator per axis
+                vals.append([int(r["min"] + rr() * float(r["max"] - r["min"])) for _ in range(nrep)])
+        sizes = min(len(v) for v in vals)
+        repeats = [(float(vals[0][i]), float(vals[1][i]), float(vals[2][i])) for i in range(sizes)]
+    else:
+        repeats = [tuple(s["repetition"])]
+    num_scaling, num_repeats = len(samples) // 3, len(repeats)
+    if num_scaling == num_repeats:
+        nscale = num_scaling
+    elif num_scaling == 1:
+        nscale = num_repeats
+    elif num_repeats == 1:
+        nscale = num_scaling
+    else:
+        raise ValueError("scaling and repetition counts differ")
+    lat = s["lattice"]
+    plan = []
+    for g in range(ngr):
+        row = []
+        for i in range(nscale):
+            if dist_branch:
+                sc = [samples[i + num_scaling * k] for k in range(3)]
+                w = weights[i]
+            else:
+                sc = samples[:3]
+                w = weights[0]
+            rp = repeats[g % num_repeats if s["repetition_dist"] else 0]
+            abc = np.array([[v * sc[0] for v in lat["a"]], [v * sc[1] for v in lat["b"]],
+                            [v * sc[2] for v in lat["c"]]])
+            row.append((abc, [1.0 if x < 1 else x for x in rp], 1.0 * w))
+        plan.append(row)
+    return plan
+
+
 def compute_gisaxs(hig, hig_dir=".", rand=None):
     """HipGISAXS::compute_gisaxs / run_gisaxs (src/sim/hipgisaxs_main.cpp:630-1440) for the
     configurations hgx_hig_compute_gisaxs supports, composed from this oracle's pinned pieces
@@ -586,7 +669,7 @@ def compute_gisaxs(hig, hig_dir=".", rand=None):
         else:
             raise ValueError(stat)
         lat = s["lattice"]
-        abc = np.array([lat["a"], lat["b"], lat["c"]])
+        plan = scale_plan(s, ngr)
         I = np.zeros(G.n)
         for gi in range(ngr):
             rot = rot_mul(rot_mul(rot_mul(rot_phi, rot_axis(int(rots[2][0]), nn[2, gi])),
@@ -610,18 +693,64 @@ def compute_gisaxs(hig, hig_dir=".", rand=None):
                     else:
                         eff = ff_analytic(G, sh["name"], params, transvec=loc, rot=srot)
                     ff = ff + dn2 * eff
-            if s["type"] == "paracrystal":
-                pc = s["paracrystal"]
-                sf = sf_paracrystal(G, pc["dims"], LATTICE.get(lat["type"], 1), pc.get("xmean", 0.0),
-                                    pc.get("ymean", 0.0), pc.get("xstddev", 0.0),
-                                    pc.get("ystddev", 0.0), pc.get("domain", 0.0))
-            elif s["type"] == "percusyevick":
-                py = s["percusyevick"]
-                sf = sf_percus_yevick(G, py["diameter"], py["volfraction"], py["dims"])
-            else:
-                sf = sf_lattice(G, abc, s["repetition"], s["scaling_mean"], center, rot)
-            I = dwba_combine(fc, sf, ff, 1.0, I)
+            for abc, rp, w in plan[gi]:
+                if s["type"] == "paracrystal":
+                    pc = s["paracrystal"]
+                    sf = sf_paracrystal(G, pc["dims"], LATTICE.get(lat["type"], 1), pc.get("xmean", 0.0),
+                                        pc.get("ymean", 0.0), pc.get("xstddev", 0.0),
+                                        pc.get("ystddev", 0.0), pc.get("domain", 0.0))
+                elif s["type"] == "percusyevick":
+                    py = s["percusyevick"]
+                    sf = sf_percus_yevick(G, py["diameter"], py["volfraction"], py["dims"])
+                else:
+                    sf = sf_lattice(G, abc, rp, (1.0, 1.0, 1.0), center, rot)
+                I = dwba_combine(fc, sf, ff, w, I)
         intens.append(I)
     ratios = [s["iratio"] for s in hig["structures"].values()]
     img = structure_sum(np.array(intens), ratios)
     return img.reshape(nrow, ncol)
+
+
+class MT19937_64:
+    """The 64-bit Mersenne Twister of Matsumoto and Nishimura (std::mt19937_64: n = 312,
+    m = 156, r = 31 and the standard's tempering constants), restated from the published
+    algorithm."""
+
+    N, M = 312, 156
+    MATRIX_A = 0xB5026F5AA96619E9
+    UM, LM = 0xFFFFFFFF80000000, 0x7FFFFFFF
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed=0):
+        self.mt = [0] * self.N
+        self.mt[0] = seed & self.MASK
+        for i in range(1, self.N):
+            x = self.mt[i - 1]
+            self.mt[i] = (6364136223846793005 * (x ^ (x >> 62)) + i) & self.MASK
+        self.i = self.N
+
+    def __call__(self):
+        if self.i >= self.N:
+            mt = self.mt
+            for k in range(self.N):
+                x = (mt[k] & self.UM) | (mt[(k + 1) % self.N] & self.LM)
+                y = x >> 1
+                if x & 1:
+                    y ^= self.MATRIX_A
+                mt[k] = mt[(k + self.M) % self.N] ^ y
+            self.i = 0
+        y = self.mt[self.i]
+        self.i += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & self.MASK
+
+
+def woo_mt_rand():
+    """woo::MTRandomNumberGenerator (include/woo/random/woo_mtrandom.hpp): seed 0, rand() =
+    (x - min) / (max - min) in doubles."""
+    g = MT19937_64(0)
+    mx = float((1 << 64) - 1)
+    return lambda: (float(g()) - 0.0) / (mx - 0.0)

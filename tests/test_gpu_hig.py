@@ -29,7 +29,7 @@ def test_hig_qgrid_matches_oracle(ctx, po, name):
 
 
 SIM = ["sim_cylinders_hcp.hig", "sim_two_structures.hig", "paracrystal.hig", "percus_yevick.hig",
-       "include_main.hig"]
+       "include_main.hig", "sim_scaling.hig", "sim_scaling_mixed.hig", "sim_repetition.hig"]
 
 
 def _srand(seed):
@@ -83,8 +83,10 @@ def test_compute_gisaxs_device_output(ctx, po):
     (('stat = "range"', 'stat = "gaussian"'), "orientation statistic"),
     (("spacing = [ 150 150 0 ],", 'spacing = [ 150 150 0 ], distribution = "random",'), "distribution"),
     (("alphai = { min = 0.175 }", "alphai = { min = 0.1, max = 0.2, step = 0.05 }"), "alpha_i"),
-    (('scaling = 24,', 'scaling = 24, lattice = { a = { mean = 2, stddev = 0.1, stat = "gaussian" } },'),
-     "scaling distributions"),
+    (('scaling = 24,', 'scaling = 24, lattice = { a = { mean = 2, stddev = 0.1, stat = "uniform" } },'),
+     "scaling statistic"),
+    (('repetition = [ 6 4 2 ]', 'repetitiondist = { xrepetition = { stat = "gaussian", min = 2, max = 5 } }'),
+     "repetition statistic"),
 ])
 def test_compute_gisaxs_refuses_unsupported(ctx, tmp_path, edit, words):
     from hipgisaxs_b200 import HgxError
