@@ -18,15 +18,17 @@
 // location (FormFactor::compute_form_factor passes no translation to the numeric form
 // factor, src/ff/ff.cpp:40-48) but is added once per location; orientations drawn by the
 // "range" and "random" statistics come from the C library's rand(), in the reference's
-// order.  The reference subtracts single_layer_thickness_, a member it never assigns, from
-// the grain translation's z (:871-875); it is taken as 0 here.
+// order, while "gaussian", "normal" and "cauchy" step evenly over each axis's range and weight
+// the grains; grain scalings and repetitions are sampled with the reference's seeded 64-bit
+// Mersenne Twister.  The reference subtracts single_layer_thickness_, a member it never
+// assigns, from the grain translation's z (:871-875), and spaces the grains by cell_, which it
+// never assigns either; both are taken as 0 here.
 //
-// Configurations whose reference result is not determined by the input are refused with
-// HGX_ERR_INVALID_ARG: clock-seeded random grain positions, the Mersenne-Twister sampled
-// scaling distributions, repetition distributions, gaussian/cauchy/bragg orientations (whose
-// sampling is commented out or needs the q-grid singleton), structure correlations other
-// than none, sliced layers (nslices > 1), SAXS, and angle scans (more than one alpha_i, phi
-// or tilt: compute_gisaxs itself refuses those).
+// Refused with HGX_ERR_INVALID_ARG, naming the feature: clock-seeded random grain positions,
+// "bragg" orientations (the reference's search reads q-grid extents it never sets and fails),
+// structure correlations other than none (the reference indexes its single grain image as if
+// it held one per grain), sliced layers (nslices > 1), SAXS, and angle scans (more than one
+// alpha_i, phi or tilt: compute_gisaxs itself refuses those).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdlib.h>
@@ -105,7 +107,7 @@ struct FusedArgs {
 // adds the four terms in the order k = 0..3 (shuffles), as the step-by-step combination does.
 // SHAPE: the one analytic shape of every element (0: any).
 template <int SHAPE>
-__global__ void __launch_bounds__(128) grain_dwba_kernel(FusedArgs a) {
+__global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 : 5) grain_dwba_kernel(FusedArgs a) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long i = t >> 2;
   const int k = (int)(t & 3);
@@ -283,8 +285,8 @@ static double weight_cauchy(double x, double l, double sc) {
 // reads past its sample vector (a repetition distribution with an undistributed scaling, in the
 // branch its grain_scaling_is_dist() takes by undefined behaviour) the undistributed branch is
 // taken.  Returns false (with a message) where the reference's own steps fail.
-static bool scale_plan(const hig::Structure& s, int ngr, std::vector<ScaleEntry>& plan, int& nscale,
-                       std::string& why) {
+static bool scale_plan(const hig::Structure& s, int ngr, const std::vector<double>& gw,
+                       std::vector<ScaleEntry>& plan, int& nscale, std::string& why) {
   // scaling samples
   std::vector<double> samples, weights;
   bool any_dist = false, dist_branch = false;
@@ -373,7 +375,7 @@ static bool scale_plan(const hig::Structure& s, int ngr, std::vector<ScaleEntry>
         e.lc[k] = s.lattice.c[k] * sc[2];
         e.rep[k] = rp[k] < 1 ? 1 : rp[k];
       }
-      e.w = 1.0 * w;  // gauss_weight (1 for the supported orientations) * scaling weight
+      e.w = gw[g] * w;  // gauss_weight * scaling_wght (:1045)
     }
   return true;
 }
@@ -413,13 +415,20 @@ static void rotation_of(const hig::Rotation& r, double out[3]) {
   out[2] = r.angles[1];
 }
 
-// orientation_distribution (:1869-1960) for single, range and random: nn[3][ngr] radians
-static int orientations(const hig::Structure& s, int ngr, std::vector<double>& nn) {
+// orientation_distribution (:1869-2085): nn[3][ngr] radians and the grain weights gw[ngr]
+// (run_gisaxs applies the product of the three axes' weights for "gaussian" and "cauchy",
+// :946-951; for "normal", the same angles, it does not).  "range"/"random" draw with the C
+// library's rand(); "gaussian"/"normal"/"cauchy" step each axis evenly over its range (the
+// reference's random sampling of them is commented out) and weight by the distribution.
+static int orientations(const hig::Structure& s, int ngr, std::vector<double>& nn, std::vector<double>& gw) {
+  const double tiny = 2.2250738585072014e-308;  // TINY_
   double r[3][3];
   rotation_of(s.rot1, r[0]);
   rotation_of(s.rot2, r[1]);
   rotation_of(s.rot3, r[2]);
+  const hig::Rotation* rot[3] = {&s.rot1, &s.rot2, &s.rot3};
   nn.assign(3 * (size_t)ngr, 0.0);
+  std::vector<double> wg(3 * (size_t)ngr, 1.0);
   const std::string& st = s.orientation_stat;
   if (st == "single") {
     for (int k = 0; k < 3; ++k)
@@ -431,13 +440,50 @@ static int orientations(const hig::Structure& s, int ngr, std::vector<double>& n
       const double dr = fabs(r[k][2] - r[k][1]);
       for (int x = 0; x < ngr; ++x) nn[k * ngr + x] = (r[k][1] + (double(rand()) / RAND_MAX) * dr) * PI / 180;
     }
+  } else if (st == "gaussian" || st == "normal") {
+    for (int k = 0; k < 3; ++k) {
+      double dr = fabs(r[k][2] - r[k][1]);
+      if (dr > tiny) {
+        dr /= ngr;
+        for (int x = 0; x < ngr; ++x) {
+          const double t = r[k][1] + x * dr;
+          nn[k * ngr + x] = t * PI / 180;
+          wg[k * ngr + x] = weight_gaussian(t, rot[k]->mean, rot[k]->sd);
+        }
+      } else {
+        for (int x = 0; x < ngr; ++x) nn[k * ngr + x] = r[k][1] * PI / 180;
+      }
+    }
+  } else if (st == "cauchy") {
+    for (int k = 0; k < 3; ++k) {
+      if (ngr == 1 && fabs(r[k][2] - r[k][1]) > 0)
+        return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: structure '" + s.key +
+                                             "': cauchy orientations over a range need more than one grain "
+                                             "(the reference divides the range by ngrains - 1)");
+      const double dr = fabs(r[k][2] - r[k][1]) / (ngr - 1);
+      if (dr > tiny) {
+        for (int x = 0; x < ngr; ++x) {
+          const double t = r[k][1] + x * dr;
+          nn[k * ngr + x] = t * PI / 180;
+          wg[k * ngr + x] = weight_cauchy(t, rot[k]->location, rot[k]->scale);
+        }
+      } else {
+        for (int x = 0; x < ngr; ++x) nn[k * ngr + x] = r[k][1] * PI / 180;
+      }
+    }
+  } else if (st == "bragg") {
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: structure '" + s.key +
+                                         "': bragg orientations are not supported (the reference's Bragg search "
+                                         "reads q-grid extents it never sets, finds no angle and fails)");
   } else {
     return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: structure '" + s.key +
                                          "': orientation statistic '" + st + "' is not supported");
   }
+  gw.assign(ngr, 1.0);
+  if (st == "gaussian" || st == "cauchy")
+    for (int g = 0; g < ngr; ++g) gw[g] = wg[g] * wg[ngr + g] * wg[2 * ngr + g];
   return HGX_OK;
 }
-
 
 // The fused path for one structure: element-location and grain tables on the device, the
 // structure factor once when it does not depend on the grain, then the grain kernel in
@@ -660,10 +706,10 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   for (const auto& skv : in.structures) {  // in key order (the reference: unordered_map order)
     const hig::Structure& s = skv.second;
     const hig::Unitcell& uc = in.unitcells.at(s.unitcell_key);
-    std::vector<double> dd, nn;
+    std::vector<double> dd, nn, gw;
     int ngr = 0;
     regular_centres(s, dd, ngr);
-    HGX_TRY(orientations(s, ngr, nn));
+    HGX_TRY(orientations(s, ngr, nn, gw));
     double r1[3], r2[3], r3[3];
     rotation_of(s.rot1, r1);
     rotation_of(s.rot2, r2);
@@ -672,7 +718,7 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     std::vector<ScaleEntry> plan;
     int nscale = 0;
     std::string why;
-    if (!scale_plan(s, ngr, plan, nscale, why)) return refuse("structure '" + s.key + "': " + why);
+    if (!scale_plan(s, ngr, gw, plan, nscale, why)) return refuse("structure '" + s.key + "': " + why);
     double* Is = (double*)bI.p + (size_t)si * n;
     bool all_analytic = true;
     for (const auto& ekv : uc.elements) {

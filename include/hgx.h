@@ -416,8 +416,9 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * layer stack's Fresnel coefficients; the structures summed with their iratios.  image:
  * nrow x ncol doubles (host or device).  precision: HGX_F64, or HGX_F32C for the mesh form
  * factors.  Supported: GISAXS, one alpha_i/phi/tilt, nslices <= 1, no structure correlation,
- * regular grain grids, "single", "range" and "random" orientations (drawn with the C
- * library's rand() in the reference's order), no scaling or repetition distributions; other
+ * regular grain grids; "single", "range", "random" (drawn with the C library's rand() in the
+ * reference's order), "gaussian", "normal" and "cauchy" orientations; gaussian/cauchy grain
+ * scalings and ranged repetitions (the reference's seeded Mersenne Twister).  Other
  * descriptions return HGX_ERR_INVALID_ARG naming the feature. */
 int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
 

@@ -531,7 +531,7 @@ def _weight_cauchy(x, l, sc):
     return 0.0 if x - l > tiny else 1.0
 
 
-def scale_plan(s, ngr):
+def scale_plan(s, ngr, gw=None):
     """run_gisaxs's scaling and repetition loops (src/sim/hipgisaxs_main.cpp:815-870,
     1017-1040) with construct_scaling_distribution (:2179-2226), construct_repetition_
     distribution (:2100-2176) and generate_repetition_range (:2089-2098): per grain the list
@@ -593,7 +593,7 @@ def scale_plan(s, ngr):
             rp = repeats[g % num_repeats if s["repetition_dist"] else 0]
             abc = np.array([[v * sc[0] for v in lat["a"]], [v * sc[1] for v in lat["b"]],
                             [v * sc[2] for v in lat["c"]]])
-            row.append((abc, [1.0 if x < 1 else x for x in rp], 1.0 * w))
+            row.append((abc, [1.0 if x < 1 else x for x in rp], (1.0 if gw is None else gw[g]) * w))
         plan.append(row)
     return plan
 
@@ -654,6 +654,7 @@ def compute_gisaxs(hig, hig_dir=".", rand=None):
             rots.append((0.0, 0.0, 0.0) if r["axis"] == "n" else
                         (float(ord(r["axis"]) - ord("x")), r["angles"][0], r["angles"][1]))
         nn = np.zeros((3, ngr))
+        wg = np.ones((3, ngr))
         stat = s["orientation_stat"]
         if stat == "single":
             for k in range(3):
@@ -666,10 +667,27 @@ def compute_gisaxs(hig, hig_dir=".", rand=None):
                 dr = abs(rots[k][2] - rots[k][1])
                 for x in range(ngr):
                     nn[k, x] = (rots[k][1] + (float(rand()) / RAND_MAX) * dr) * pi / 180
+        elif stat in ("gaussian", "normal", "cauchy"):
+            # evenly stepped angles, weighted by the distribution (:1920-2082)
+            tiny = 2.2250738585072014e-308
+            robj = (s["rot1"], s["rot2"], s["rot3"])
+            for k in range(3):
+                span = abs(rots[k][2] - rots[k][1])
+                dr = span / ngr if stat != "cauchy" else (span / (ngr - 1) if ngr > 1 else float("nan"))
+                if dr > tiny:
+                    for x in range(ngr):
+                        t = rots[k][1] + x * dr
+                        nn[k, x] = t * pi / 180
+                        wg[k, x] = (_weight_cauchy(t, robj[k]["location"], robj[k]["scale"]) if stat == "cauchy"
+                                    else _weight_gaussian(t, robj[k]["mean"], robj[k]["sd"]))
+                else:
+                    nn[k, :] = rots[k][1] * pi / 180
         else:
             raise ValueError(stat)
+        gw = [wg[0, g] * wg[1, g] * wg[2, g] if stat in ("gaussian", "cauchy") else 1.0
+              for g in range(ngr)]
         lat = s["lattice"]
-        plan = scale_plan(s, ngr)
+        plan = scale_plan(s, ngr, gw)
         I = np.zeros(G.n)
         for gi in range(ngr):
             rot = rot_mul(rot_mul(rot_mul(rot_phi, rot_axis(int(rots[2][0]), nn[2, gi])),

@@ -29,7 +29,8 @@ def test_hig_qgrid_matches_oracle(ctx, po, name):
 
 
 SIM = ["sim_cylinders_hcp.hig", "sim_two_structures.hig", "paracrystal.hig", "percus_yevick.hig",
-       "include_main.hig", "sim_scaling.hig", "sim_scaling_mixed.hig", "sim_repetition.hig"]
+       "include_main.hig", "sim_scaling.hig", "sim_scaling_mixed.hig", "sim_repetition.hig",
+       "sim_orientations.hig"]
 
 
 def _srand(seed):
@@ -80,7 +81,7 @@ def test_compute_gisaxs_device_output(ctx, po):
 @pytest.mark.gpu
 @pytest.mark.parametrize("edit,words", [
     (("resolution = [ 48 32 ]", "resolution = [ 48 32 ], nslices = 3"), "nslices"),
-    (('stat = "range"', 'stat = "gaussian"'), "orientation statistic"),
+    (('stat = "range"', 'stat = "bragg"'), "bragg orientations"),
     (("spacing = [ 150 150 0 ],", 'spacing = [ 150 150 0 ], distribution = "random",'), "distribution"),
     (("alphai = { min = 0.175 }", "alphai = { min = 0.1, max = 0.2, step = 0.05 }"), "alpha_i"),
     (('scaling = 24,', 'scaling = 24, lattice = { a = { mean = 2, stddev = 0.1, stat = "uniform" } },'),
