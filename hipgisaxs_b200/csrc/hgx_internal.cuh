@@ -60,7 +60,7 @@ struct MeshWork {
 struct HigWork {
   hgx_qgrid grid = nullptr;
   double key[8] = {0};
-  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc;
+  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj;
 };
 }  // namespace hgx
 

@@ -3,6 +3,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <iterator>
 #include <new>
 #include <string>
 
@@ -53,6 +54,56 @@ int hgx_hig_beam(hgx_hig h, double* k0, double* alpha_i, double* freq) {
   return HGX_OK;
 }
 
+int hgx_hig_update_param(hgx_hig h, const char* variable, double value) {
+  if (!h || !variable) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_update_param: null argument");
+  std::string err;
+  if (!hig::update_param(h->in, variable, value, err)) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_update_param: " + err);
+  h->json.clear();
+  return HGX_OK;
+}
+
+int hgx_hig_fit_count(hgx_hig h, int* n) {
+  if (!h || !n) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_count: null argument");
+  *n = (int)h->in.fit_params.size();
+  return HGX_OK;
+}
+
+int hgx_hig_fit_param(hgx_hig h, int i, char* key, size_t key_cap, char* variable, size_t var_cap,
+                      double* range3, double* init) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_param: null handle");
+  if (i < 0 || i >= (int)h->in.fit_params.size())
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_param: index out of range");
+  auto it = h->in.fit_params.begin();
+  std::advance(it, i);
+  const hig::FitParam& p = it->second;
+  if (key) {
+    if (key_cap <= p.key.size()) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_param: key buffer too small");
+    memcpy(key, p.key.c_str(), p.key.size() + 1);
+  }
+  if (variable) {
+    if (var_cap <= p.variable.size()) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_param: variable buffer too small");
+    memcpy(variable, p.variable.c_str(), p.variable.size() + 1);
+  }
+  if (range3)
+    for (int k = 0; k < 3; ++k) range3[k] = p.range[k];
+  if (init) *init = p.init;
+  return HGX_OK;
+}
+
+int hgx_hig_fit_update(hgx_hig h, const double* x, int n) {
+  if (!h || (n > 0 && !x)) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_update: null argument");
+  if (n != (int)h->in.fit_params.size())
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_update: one value per fit parameter expected");
+  int i = 0;
+  for (const auto& kv : h->in.fit_params) {  // in key order, as fit_param_keys() lists them
+    std::string err;
+    if (!hig::update_param(h->in, kv.second.variable, x[i++], err))
+      return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_update: " + err);
+  }
+  h->json.clear();
+  return HGX_OK;
+}
+
 int hgx_hig_qgrid(hgx_ctx ctx, hgx_hig h, double dn2_re, double dn2_im, hgx_qgrid* out) {
   if (!ctx || !h || !out) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_qgrid: null argument");
   const hig::Compute& c = h->in.compute;
@@ -65,4 +116,41 @@ int hgx_hig_qgrid(hgx_ctx ctx, hgx_hig h, double dn2_re, double dn2_im, hgx_qgri
                           c.maxpoint[0], c.maxpoint[1], alpha_i, k0, dn2_re, dn2_im, out);
 }
 
+int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
+                      const unsigned* mask, int metric, double reg_alpha, double* dist, long* ndist) {
+  if (!ctx || !h || !ref || !dist) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective: null argument");
+  if (is_device_ptr(dist)) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective: dist must be host memory");
+  // HipGISAXSObjectiveFunction::operator() (src/analyzer/objective_func_hipgisaxs.cpp:263-320):
+  // the parameters in key order, the simulation, the distance, the regularisation
+  HGX_TRY(hgx_hig_fit_update(h, x, nx));
+  int nrow = 0, ncol = 0;
+  HGX_TRY(hgx_hig_image_size(h, &nrow, &ncol));
+  const long n = (long)nrow * ncol;
+  HGX_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->hig) {
+    ctx->hig = new (std::nothrow) HigWork;
+    if (!ctx->hig) return fail(HGX_ERR_NO_MEMORY, "hgx_hig_objective: out of host memory");
+  }
+  DevBuf& img = ctx->hig->obj;
+  HGX_TRY(img.reserve(sizeof(double) * n));
+  HGX_TRY(hgx_hig_compute_gisaxs(ctx, h, HGX_F64, (double*)img.p));
+  const bool residual = metric == 4 || metric == 5;  // the residual-vector measures
+  HGX_TRY(hgx_fit_distance(ctx, metric, n, ref, (const double*)img.p, mask, dist));
+  const long nd = residual ? n : 1;
+  double pmean = 0.0;
+  int i = 0;
+  for (const auto& kv : h->in.fit_params) {
+    const double mean = (kv.second.range[1] - kv.second.range[0]) / 2.0 + kv.second.range[0];
+    double t = x[i++] - mean;
+    t *= t;
+    pmean += t;
+  }
+  const double reg = (reg_alpha / 2) * pmean;
+  const double reg_dist = reg / nd;
+  for (long k = 0; k < nd; ++k) dist[k] = isfinite(dist[k]) ? dist[k] + reg_dist : 1e8;
+  if (ndist) *ndist = nd;
+  return HGX_OK;
+}
+
 }  // extern "C"
+

@@ -56,6 +56,7 @@ struct Rotation {                  // Rotation, include/model/structure.hpp:166-
   char axis = 'n';
   vec2 angles{{0.0, 0.0}};
   double mean = 0.0, sd = 0.0, location = 0.0, scale = 0.0;
+  bool mean_set = false;           // an anglemean was given: angles_min no longer moves the mean
 };
 
 struct Lattice {                   // Lattice, include/model/structure.hpp:88-160
@@ -77,6 +78,7 @@ struct Structure {                 // Structure, include/model/structure.hpp:481
   std::string type = "default";    // default, paracrystal, percusyevick
   // grain
   std::string unitcell_key;
+  RefIndex grain_refindex;         // Grain::refindex_, settable by a fit, unused by the simulation
   std::string layer_key = "air";
   int layer_order = 0;             // never set from layer:key by the reference's reader
   Lattice lattice;
@@ -181,6 +183,10 @@ struct Input {
   bool reference_data_set = false;
   std::vector<FitAlgorithm> algorithms;
 };
+
+// HiGInput::update_params for one parameter variable (src/config/hig_input.cpp:2712-2830 and
+// the update_param methods of the model classes), e.g. "shape['s1']:param['radius']:min".
+bool update_param(Input& in, const std::string& variable, double value, std::string& err);
 
 // Reads a HiG file (HiGInput::construct_input_config).  Returns false with a message naming the
 // line on a syntax or semantic error.

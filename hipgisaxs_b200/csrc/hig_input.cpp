@@ -728,7 +728,7 @@ struct Builder {
     for (const Node& e : n.kids) {
       if (e.key == "axis") { std::string a; if (!string(e, a)) return false; r.axis = a.empty() ? '\0' : a[0]; }
       else if (e.key == "angles") { if (!vec(e, r.angles)) return false; }
-      else if (e.key == "anglemean") { if (!number(e, r.mean)) return false; }
+      else if (e.key == "anglemean") { if (!number(e, r.mean)) return false; r.mean_set = true; }
       else if (e.key == "anglesd") { if (!number(e, r.sd)) return false; }
       else if (e.key == "anglelocation") { if (!number(e, r.location)) return false; }
       else if (e.key == "anglescale") { if (!number(e, r.scale)) return false; }
@@ -1045,6 +1045,279 @@ bool read_input(const std::string& path, Input& out, std::string& err) {
   if (!ps.file(root)) { err = ps.err; return false; }
   Builder b(out, lx);
   if (!b.top(root)) { err = b.err; return false; }
+  return true;
+}
+
+// ---------------------------------------------------------------- parameter updates ----
+
+namespace {
+
+// extract_first_keyword / extract_keyword_name_and_key (src/utils/string_utils.cpp:23-90)
+void first_keyword(const std::string& str, std::string& kw, std::string& rest) {
+  const size_t pos = str.find(':');
+  kw = str.substr(0, pos);
+  rest = pos == std::string::npos ? "" : str.substr(pos + 1);
+}
+bool name_and_key(const std::string& kw, std::string& name, std::string& key) {
+  const size_t pos = kw.find('[');
+  if (pos == std::string::npos) { name = kw; key = ""; return true; }
+  name = kw.substr(0, pos);
+  std::string rem = kw.substr(pos + 1);
+  if (rem.empty() || rem.back() != ']') return false;
+  rem.pop_back();
+  if (rem.size() < 2 || rem.front() != '\'' || rem.back() != '\'') return false;
+  key = rem.substr(1, rem.size() - 2);
+  return true;
+}
+// "x"/"0", "y"/"1", "z"/"2" -> 0, 1, 2; -1 otherwise
+int coordinate(const std::string& c) {
+  if (c == "x" || c == "0") return 0;
+  if (c == "y" || c == "1") return 1;
+  if (c == "z" || c == "2") return 2;
+  return -1;
+}
+
+struct Updater {
+  Input& in;
+  std::string err;
+  bool bad(const std::string& m) { err = m; return false; }
+
+  bool shape_param(ShapeParam& p, const std::string& rest, double v) {  // shape.cpp:114-150
+    std::string kw, r2, name, key;
+    first_keyword(rest, kw, r2);
+    if (!name_and_key(kw, name, key)) return bad("malformed keyword '" + kw + "'");
+    if (name == "min") p.min = v;
+    else if (name == "max") p.max = v;
+    else if (name == "p1") p.p1 = v;
+    else if (name == "p2") p.p2 = v;
+    else if (name == "nvalues") p.nvalues = (int)v;
+    else if (name == "stat") {}
+    else return bad("'" + name + "' is not a shape parameter field");
+    return true;
+  }
+
+  bool shape(Shape& s, const std::string& rest, double v) {  // Shape::update_param, shape.cpp:190-247
+    std::string kw, r2, name, key, coord, r3;
+    first_keyword(rest, kw, r2);
+    if (!name_and_key(kw, name, key)) return bad("malformed keyword '" + kw + "'");
+    if (name == "key" || name == "name" || name == "originvec") {  // all three set originvec
+      first_keyword(r2, coord, r3);
+      const int c = coordinate(coord);
+      if (c < 0) return bad("'" + coord + "' is not a coordinate");
+      s.originvec[c] = v;
+    } else if (name == "zrot") {
+      s.zrot = v;  // radians: the update takes the value as it is
+    } else if (name == "yrot") {
+      s.yrot = v;
+    } else if (name == "xrot") {
+      return bad("'xrot' cannot be updated (the reference falls through into the parameter "
+                 "branch and throws)");
+    } else if (name == "param") {
+      auto it = s.params.find(key);
+      if (it == s.params.end()) return bad("shape '" + s.key + "' has no parameter '" + key + "'");
+      return shape_param(it->second, r2, v);
+    } else {
+      return bad("'" + name + "' cannot be updated in a shape");
+    }
+    return true;
+  }
+
+  bool layer(Layer& l, const std::string& rest, double v) {  // Layer::update_param, layer.cpp
+    std::string kw, r2, kw2, r3;
+    first_keyword(rest, kw, r2);
+    if (kw == "key" || kw == "order") return true;
+    if (kw == "thickness") { l.thickness = v; return true; }
+    if (kw == "refindex") {
+      first_keyword(r2, kw2, r3);
+      if (kw2 == "beta") { l.refindex.beta = v; return true; }
+      if (kw2 == "delta") { l.refindex.delta = v; return true; }
+      return bad("'" + kw2 + "' is not a refindex field");
+    }
+    return bad("'" + kw + "' cannot be updated in a layer");
+  }
+
+  bool rotation(Rotation& r, const std::string& name, const std::string& key, const std::string& rest,
+                double v) {  // GrainOrientations::update_param, structure.cpp:237-330
+    if (key != std::string(1, r.axis)) return bad("'" + name + "' is about axis '" + std::string(1, r.axis) + "'");
+    std::string kw2, r2;
+    first_keyword(rest, kw2, r2);
+    if (kw2 == "min" || kw2 == "0") {
+      r.angles[0] = v;
+      if (!r.mean_set) r.mean = v;  // Rotation::angles_min
+    } else if (kw2 == "max" || kw2 == "1") {
+      if (name == "rot2") {  // the reference sets rot2's minimum here
+        r.angles[0] = v;
+        if (!r.mean_set) r.mean = v;
+      } else {
+        r.angles[1] = v;
+      }
+    } else if (kw2 == "anglelocation") r.location = v;
+    else if (kw2 == "anglemean") { r.mean = v; r.mean_set = true; }
+    else if (kw2 == "anglescale") r.scale = v;
+    else if (kw2 == "anglesd") r.sd = v;
+    else return bad("'" + kw2 + "' is not an orientation field");
+    return true;
+  }
+
+  bool structure(Structure& s, const std::string& rest, double v) {  // structure.cpp:486-820
+    std::string kw, r2, kw2, r3, kw3, r4, kw4, r5;
+    first_keyword(rest, kw, r2);
+    if (kw == "key") return true;
+    if (kw == "iratio") { s.iratio = v; return true; }
+    if (kw == "grain") {
+      first_keyword(r2, kw2, r3);
+      if (kw2 == "refindex") {
+        first_keyword(r3, kw3, r4);
+        if (kw3 == "delta") { s.grain_refindex.delta = v; return true; }
+        if (kw3 == "beta") { s.grain_refindex.beta = v; return true; }
+        return bad("'" + kw3 + "' is not a refindex field");
+      }
+      if (kw2 == "lattice") {
+        first_keyword(r3, kw3, r4);
+        if (kw3 == "a" || kw3 == "b" || kw3 == "c") {
+          first_keyword(r4, kw4, r5);
+          const int c = coordinate(kw4);
+          if (c < 0) return bad("'" + kw4 + "' is not a coordinate");
+          vec3& vec = kw3 == "a" ? s.lattice.a : kw3 == "b" ? s.lattice.b : s.lattice.c;
+          vec[c] = v;
+          return true;
+        }
+        if (kw3 == "type" || kw3 == "hkl") return true;  // immutable: a warning, no change
+        if (kw3 == "abangle") { s.lattice.abangle = v; return true; }
+        if (kw3 == "caratio") { s.lattice.caratio = v; return true; }
+        return bad("'" + kw3 + "' cannot be updated in a lattice");
+      }
+      if (kw2 == "scaling") {
+        if (r3.empty()) { s.scaling_mean = {{v, v, v}}; return true; }
+        first_keyword(r3, kw3, r4);
+        if (kw3 == "a" || kw3 == "b" || kw3 == "c") {
+          const int ax = kw3[0] - 'a';
+          first_keyword(r4, kw4, r5);
+          if (kw4 == "mean") s.scaling_mean[ax] = v;
+          else if (kw4 == "stddev") s.scaling_stddev[ax] = v;
+          else if (kw4 == "nsamples") s.scaling_nsamples[ax] = (int)v;
+          else return bad("'" + kw4 + "' is not a scaling field");
+          return true;
+        }
+        return bad("'" + kw3 + "' is not a scaling axis");
+      }
+      if (kw2 == "transvec" || kw2 == "repetition") {
+        first_keyword(r3, kw3, r4);
+        const int c = coordinate(kw3);
+        if (c < 0) return bad("'" + kw3 + "' is not a coordinate");
+        (kw2 == "transvec" ? s.transvec : s.repetition)[c] = v;
+        return true;
+      }
+      return bad("'" + kw2 + "' cannot be updated in a grain");
+    }
+    if (kw == "ensemble") {
+      first_keyword(r2, kw2, r3);
+      if (kw2 == "spacing" || kw2 == "maxgrains") {
+        first_keyword(r3, kw3, r4);
+        // x/0, y/1, and z only by name: the reference tests "1" again instead of "2"
+        const int c = (kw3 == "x" || kw3 == "0") ? 0 : (kw3 == "y" || kw3 == "1") ? 1 : kw3 == "z" ? 2 : -1;
+        if (c < 0) return bad("'" + kw3 + "' is not a coordinate here");
+        (kw2 == "spacing" ? s.spacing : s.maxgrains)[c] = v;
+        return true;
+      }
+      if (kw2 == "orientations") {
+        first_keyword(r3, kw3, r4);
+        std::string name, key;
+        if (!name_and_key(kw3, name, key)) return bad("malformed keyword '" + kw3 + "'");
+        if (name == "rot1") return rotation(s.rot1, name, key, r4, v);
+        if (name == "rot2") return rotation(s.rot2, name, key, r4, v);
+        if (name == "rot3") return rotation(s.rot3, name, key, r4, v);
+        return bad("'" + name + "' cannot be updated in orientations");
+      }
+      if (kw2 == "distribution") return true;
+      return bad("'" + kw2 + "' cannot be updated in an ensemble");
+    }
+    return bad("'" + kw + "' cannot be updated in a structure");
+  }
+
+  bool range(vec3& r, const std::string& rest, double v) {
+    std::string kw, r2;
+    first_keyword(rest, kw, r2);
+    if (kw == "min") r[0] = v;
+    else if (kw == "max") r[1] = v;
+    else if (kw == "step") r[2] = v;
+    else return bad("'" + kw + "' is not min, max or step");
+    return true;
+  }
+
+  bool scattering(const std::string& rest, double v) {  // inst_scattering.cpp:36-120
+    Scattering& sc = in.scattering;
+    std::string kw, r2, kw2, r3;
+    first_keyword(rest, kw, r2);
+    if (kw == "expt" || kw == "polarization" || kw == "smearing") return true;
+    if (kw == "alphai") return range(sc.alphai, r2, v);
+    if (kw == "inplanerot") return range(sc.inplanerot, r2, v);
+    if (kw == "tilt") return range(sc.tilt, r2, v);
+    if (kw == "photon") {
+      first_keyword(r2, kw2, r3);
+      if (kw2 == "value") { sc.photon_value = v; return true; }
+      if (kw2 == "unit") return true;
+      return bad("'" + kw2 + "' is not a photon field");
+    }
+    if (kw == "coherence") { sc.coherence = v; return true; }
+    if (kw == "spotarea") { sc.spotarea = v; return true; }
+    return bad("'" + kw + "' cannot be updated in scattering");
+  }
+
+  bool detector(const std::string& rest, double v) {  // inst_detector.cpp:35-60
+    std::string kw, r2;
+    first_keyword(rest, kw, r2);
+    if (kw == "origin" || kw == "totalpixels" || kw == "directbeam") return true;
+    if (kw == "pixelsize") { in.detector.pixelsize = v; return true; }
+    if (kw == "sdd") { in.detector.sdd = v; return true; }
+    return bad("'" + kw + "' cannot be updated in the detector");
+  }
+
+  bool top(const std::string& var, double v) {  // HiGInput::update_params, hig_input.cpp:2712-2830
+    std::string kw, rest, name, key, kw2, r2;
+    if (var.empty()) return bad("empty parameter variable");
+    first_keyword(var, kw, rest);
+    if (!name_and_key(kw, name, key)) return bad("malformed keyword '" + kw + "'");
+    if (name == "shape") {
+      auto it = in.shapes.find(key);
+      if (it == in.shapes.end()) return bad("no shape '" + key + "'");
+      return shape(it->second, rest, v);
+    }
+    if (name == "layer") {
+      auto lk = in.layer_keys.find(key);
+      if (lk == in.layer_keys.end() || !in.layers.count(lk->second)) return bad("no layer '" + key + "'");
+      return layer(in.layers[lk->second], rest, v);
+    }
+    if (name == "structure") {
+      auto it = in.structures.find(key);
+      if (it == in.structures.end()) return bad("no structure '" + key + "'");
+      return structure(it->second, rest, v);
+    }
+    if (name == "instrumentation") {
+      first_keyword(rest, kw2, r2);
+      if (kw2 == "scattering") return scattering(r2, v);
+      if (kw2 == "detector") return detector(r2, v);
+      return bad("'" + kw2 + "' cannot be updated in instrumentation");
+    }
+    if (name == "computation") {  // ComputeParams::update_param: nothing changes
+      first_keyword(rest, kw2, r2);
+      if (kw2 == "pathprefix" || kw2 == "runname" || kw2 == "method" || kw2 == "outputregion" ||
+          kw2 == "resolution" || kw2 == "nslices")
+        return true;
+      return bad("'" + kw2 + "' cannot be updated in computation");
+    }
+    return bad("'" + name + "' is not an updatable block");
+  }
+};
+
+}  // namespace
+
+bool update_param(Input& in, const std::string& variable, double value, std::string& err) {
+  Updater u{in, ""};
+  if (!u.top(variable, value)) {
+    err = "parameter '" + variable + "': " + u.err;
+    return false;
+  }
   return true;
 }
 

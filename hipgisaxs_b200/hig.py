@@ -18,7 +18,12 @@ import os
 import numpy as np
 
 from ._capi import check, lib
-from .core import PRECISION, Context, QGrid, _is_tensor
+from .core import PRECISION, Context, QGrid, _in, _is_tensor
+
+# the fitting block's distance metrics (hgx_fit_metric)
+METRICS = {"sqrt_unit_l2": 0, "sqrt_c_l2": 1, "cbrt_unit_l2": 2, "cbrt_c_l2": 3,
+           "sqrt_unit_l2_residual": 4, "sqrt_c_l2_residual": 5, "sqrt_unit_l1": 6,
+           "cbrt_unit_l1": 7}
 
 
 class HiGInput:
@@ -29,6 +34,9 @@ class HiGInput:
         check(lib().hgx_hig_read(os.fsencode(path), C.byref(h)))
         self._h = h
         self.path = path
+        self._reload()
+
+    def _reload(self):
         n = C.c_size_t()
         check(lib().hgx_hig_json(self._h, None, 0, C.byref(n)))
         buf = C.create_string_buffer(n.value + 1)
@@ -139,6 +147,45 @@ class HiGInput:
         check(lib().hgx_hig_compute_gisaxs(ctx.handle, self._h, PRECISION[precision], C.c_void_p(ptr)))
         return out
 
+    # fitting (HiGInput::update_params, HipGISAXSObjectiveFunction)
+    def fit_keys(self):
+        """The fit parameters' keys in the order of an x vector (fit_param_keys)."""
+        n = C.c_int()
+        check(lib().hgx_hig_fit_count(self._h, C.byref(n)))
+        keys = []
+        for i in range(n.value):
+            k = C.create_string_buffer(256)
+            check(lib().hgx_hig_fit_param(self._h, i, k, 256, None, 0, None, None))
+            keys.append(k.value.decode())
+        return keys
+
+    def update_param(self, variable: str, value: float):
+        """Sets one parameter by its variable name, e.g. "shape['s1']:param['radius']:min"."""
+        check(lib().hgx_hig_update_param(self._h, variable.encode(), float(value)))
+        self._reload()
+
+    def fit_update(self, x):
+        """Sets every fit parameter: x[i] for fit_keys()[i]."""
+        xa = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        check(lib().hgx_hig_fit_update(self._h, xa.ctypes.data, int(xa.size)))
+        self._reload()
+
+    def objective(self, ctx: Context, x, ref, mask=None, metric="sqrt_unit_l2", reg_alpha=0.0):
+        """HipGISAXSObjectiveFunction::operator()(x) on the device: the distance between the
+        simulation at x and `ref` (nrow x ncol), regularised; a numpy array of 1 value, or one
+        per pixel for the residual metrics."""
+        xa = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        pr, kr = _in(ref, np.float64)
+        pm, km = (None, None) if mask is None else _in(mask, np.uint32)
+        nrow, ncol = self.image_size()
+        dist = np.zeros(nrow * ncol)
+        nd = C.c_long()
+        check(lib().hgx_hig_objective(ctx.handle, self._h, xa.ctypes.data, int(xa.size), pr, pm,
+                                      METRICS.get(metric, metric), float(reg_alpha),
+                                      dist.ctypes.data, C.byref(nd)))
+        self._reload()
+        return dist[:nd.value].copy()
+
     @property
     def handle(self):
         return self._h
@@ -157,3 +204,15 @@ class HiGInput:
 
 def read_hig(path: str) -> HiGInput:
     return HiGInput(path)
+
+
+def fit_distance(ctx: Context, metric, ref, data, mask=None):
+    """hgx_fit_distance: the fitter's distance measure (name or number) between two images."""
+    m = METRICS.get(metric, metric)
+    pr, kr = _in(ref, np.float64)
+    pd, kd = _in(data, np.float64)
+    n = int(kr.numel() if _is_tensor(kr) else kr.size)
+    pm, km = (None, None) if mask is None else _in(mask, np.uint32)
+    out = np.zeros(n if m in (4, 5) else 1)
+    check(lib().hgx_fit_distance(ctx.handle, int(m), n, pr, pd, pm, out.ctypes.data))
+    return out

@@ -422,6 +422,48 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * descriptions return HGX_ERR_INVALID_ARG naming the feature. */
 int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
 
+/* The fitting block of a HiG description: parameters in key order (the order of
+ * HiGInput::fit_param_keys, which the reference's fitters use for their x vectors). */
+int hgx_hig_fit_count(hgx_hig h, int* n);
+/* Parameter i: key, variable (e.g. "shape['s1']:param['radius']:min"), range (min, max,
+ * step) and init; any output may be NULL. */
+int hgx_hig_fit_param(hgx_hig h, int i, char* key, size_t key_cap, char* variable, size_t var_cap,
+                      double* range3, double* init);
+/* HiGInput::update_params (src/config/hig_input.cpp:2712-2830) for one variable, with the
+ * update_param methods of the model classes and their quirks (a rotation's value is taken in
+ * radians; "rot2['..']:max" sets rot2's minimum; "spacing:2" is not accepted, "spacing:z" is;
+ * "xrot" is refused where the reference throws). */
+int hgx_hig_update_param(hgx_hig h, const char* variable, double value);
+/* All fit parameters at once: x[i] for the i-th key (nx = hgx_hig_fit_count). */
+int hgx_hig_fit_update(hgx_hig h, const double* x, int nx);
+
+/* ------------------------------------------------------------- fitting metrics ---- */
+/* The distance measures of the reference's HiG-driven fitter
+ * (include/analyzer/distance_functions.hpp:387-844, chosen by the fitting block's
+ * distancemetric, src/analyzer/hipgisaxs_fit_main.cpp:82-104): square- or cube-rooted images,
+ * unit-vector (L2 or L1) or c-normalised, masked.  out: 1 value, or n per-pixel values for the
+ * residual forms.  mask may be NULL (all pixels).  FP64, deterministic order. */
+typedef enum {
+  HGX_METRIC_SQRT_UNIT_L2 = 0,
+  HGX_METRIC_SQRT_C_L2 = 1,
+  HGX_METRIC_CBRT_UNIT_L2 = 2,
+  HGX_METRIC_CBRT_C_L2 = 3,
+  HGX_METRIC_SQRT_UNIT_L2_RESIDUAL = 4,
+  HGX_METRIC_SQRT_C_L2_RESIDUAL = 5,
+  HGX_METRIC_SQRT_UNIT_L1 = 6,
+  HGX_METRIC_CBRT_UNIT_L1 = 7
+} hgx_fit_metric;
+int hgx_fit_distance(hgx_ctx ctx, int metric, long n, const double* ref, const double* data,
+                     const unsigned* mask, double* out);
+/* HipGISAXSObjectiveFunction::operator() (src/analyzer/objective_func_hipgisaxs.cpp:263-320)
+ * for a HiG description: set the fit parameters to x (key order), simulate
+ * (hgx_hig_compute_gisaxs, FP64), measure the distance to ref (nrow x ncol) under mask, add
+ * the regularisation (reg_alpha/2) |x - mean|^2 spread over the distance vector (mean = the
+ * middle of each parameter's range; a non-finite entry becomes 1e8).  dist: host memory for
+ * 1 value, or nrow*ncol for the residual forms; *ndist receives the count. */
+int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
+                      const unsigned* mask, int metric, double reg_alpha, double* dist, long* ndist);
+
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA
  * throughput (TFLOP/s, an FMA counted as 2 FLOP) and SFU __sinf throughput (Gop/s),

@@ -1087,3 +1087,80 @@ void orc_structure_sum(int ns, long n, const double* img, const double* iratios,
     out[z] = sum;
   }
 }
+
+/* The fitter's distance measures (include/analyzer/distance_functions.hpp:387-844), numbered
+ * as hgx_fit_distance numbers them, in the reference's sequential order: the masked norms
+ * (DistanceMeasure::norm_l1/norm_l2/vec_dot, :31-55), then the terms.  Returns the number of
+ * values written to out (1, or n for the residual forms), -1 for an unknown metric. */
+static double fit_tr(int metric, double x) {
+  return (metric == 2 || metric == 3 || metric == 7) ? cbrt(x) : sqrt(x);
+}
+
+long orc_fit_distance(int metric, long n, const double* ref, const double* dat, const unsigned* mask,
+                      double* out) {
+  if (metric < 0 || metric > 7) return -1;
+  const int l1 = metric == 6 || metric == 7;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (long i = 0; i < n; ++i) {
+    const double m = mask ? (double)mask[i] : 1.0;
+    const double tr = fit_tr(metric, ref[i]), td = fit_tr(metric, dat[i]);
+    if (l1) {
+      a += m * fabs(tr);
+      b += m * fabs(td);
+    } else {
+      const double rr = tr * tr, dd = td * td, rd = fabs(td * tr);
+      a += m * (isnan(rr) ? 0 : rr);
+      b += m * (isnan(dd) ? 0 : dd);
+      c += m * (isnan(rd) ? 0 : rd);
+    }
+  }
+  const double ref_norm = l1 ? a : sqrt(a), dat_norm = l1 ? b : sqrt(b);
+  const double cc = c / (dat_norm * dat_norm);
+  double sum = 0.0;
+  for (long i = 0; i < n; ++i) {
+    const double m = mask ? (double)mask[i] : 1.0;
+    const double tr = fit_tr(metric, ref[i]), td = fit_tr(metric, dat[i]);
+    double t, nd, nr;
+    switch (metric) {
+      case 0:
+        nd = td / dat_norm; nr = tr / ref_norm;
+        t = m * fabs(nr - nd);
+        t = isfinite(t) ? t : 0.0;
+        sum += t * t;
+        break;
+      case 1:
+        nd = cc * td; nr = tr;
+        t = m * fabs(nr - nd);
+        t = isfinite(t) ? t : 0.0;
+        sum += t * t;
+        break;
+      case 2:
+        nd = td / dat_norm; nr = tr / ref_norm;
+        t = m * (nd - nr);
+        sum += t * t;
+        break;
+      case 3:
+        nd = cc * td; nr = tr;
+        t = m * fabs(nr - nd);
+        sum += t * t;
+        break;
+      case 4:
+        nd = td / dat_norm; nr = tr / ref_norm;
+        t = m * fabs(nd - nr);
+        out[i] = t * t;
+        break;
+      case 5:
+        nd = cc * td; nr = tr;
+        t = m * fabs(nr - nd);
+        out[i] = t * t;
+        break;
+      default:
+        nd = td / dat_norm; nr = tr / ref_norm;
+        sum += m * fabs(nd - nr);
+        break;
+    }
+  }
+  if (metric == 4 || metric == 5) return n;
+  out[0] = sum;
+  return 1;
+}

@@ -118,6 +118,11 @@ int orc_smear_gaussian(double* data, int nx, int ny, double sigma);
 /* HipGISAXS::normalize (src/sim/hipgisaxs_main.cpp:1439-1450), in place; 1 if normalised. */
 int orc_normalize(double* data, long n);
 
+/* The fitter's distance measures (distance_functions.hpp:387-844), numbered as
+ * hgx_fit_distance numbers them.  Returns the count written to out (1 or n), -1 on error. */
+long orc_fit_distance(int metric, long n, const double* ref, const double* dat, const unsigned* mask,
+                      double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -772,3 +772,26 @@ def woo_mt_rand():
     g = MT19937_64(0)
     mx = float((1 << 64) - 1)
     return lambda: (float(g()) - 0.0) / (mx - 0.0)
+
+
+FIT_METRICS = {"sqrt_unit_l2": 0, "sqrt_c_l2": 1, "cbrt_unit_l2": 2, "cbrt_c_l2": 3,
+               "sqrt_unit_l2_residual": 4, "sqrt_c_l2_residual": 5, "sqrt_unit_l1": 6,
+               "cbrt_unit_l1": 7}
+
+
+def fit_distance(metric, ref, data, mask=None, backend="port"):
+    """The fitter's distance measure `metric` (name or number): an array of 1 value, or n for
+    the residual forms."""
+    m = FIT_METRICS.get(metric, metric)
+    L = lib(backend)
+    r = np.ascontiguousarray(ref, dtype=np.float64).ravel()
+    d = np.ascontiguousarray(data, dtype=np.float64).ravel()
+    mk = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint32).ravel()
+    out = np.zeros(r.size)
+    f = L.orc_fit_distance if backend == "port" else L.ref_fit_distance
+    f.restype = C.c_long
+    k = f(C.c_int(int(m)), C.c_long(r.size), _p(r), _p(d),
+          None if mk is None else mk.ctypes.data_as(_up), _p(out))
+    if k < 0:
+        raise ValueError(f"fit_distance({metric}) failed")
+    return out[:k].copy()

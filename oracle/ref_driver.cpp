@@ -11,6 +11,7 @@
 //   NumericFormFactorC::compute_approx_triangle (src/ff/cpu/ff_tri_cpu.cpp:200-246)
 //   AnalyticFormFactor::compute (src/ff/ff_ana.cpp:61-161)
 //   StructureFactor::compute_structure_factor (src/sf/sf.cpp:85-285)
+//   the fitter's distance measures (include/analyzer/distance_functions.hpp:387-844)
 #include <complex>
 #include <cstring>
 #include <map>
@@ -31,6 +32,7 @@
 #include <ff/cpu/ff_num_cpu.hpp>
 #include <ff/ff_ana.hpp>
 #include <sf/sf.hpp>
+#include <analyzer/distance_functions.hpp>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -348,4 +350,34 @@ void ref_rotmatrix(int axis, double angle, double* r9) {
   }
 }
 
+// The fitter's distance measures, chosen as hgx_fit_distance numbers them: 0 sqrt_unit_l2,
+// 1 sqrt_c_l2, 2 cbrt_unit_l2, 3 cbrt_c_l2, 4 sqrt_unit_l2_residual, 5 sqrt_c_l2_residual,
+// 6 sqrt_unit_l1, 7 cbrt_unit_l1.  Returns the number of values written to out, -1 on error.
+long ref_fit_distance(int metric, long n, const double* ref, const double* dat, const unsigned* mask,
+                      double* out) {
+  std::unique_ptr<DistanceMeasure> d;
+  switch (metric) {
+    case 0: d.reset(new SqrtUnitVectorNormL2DistanceSquare()); break;
+    case 1: d.reset(new SqrtCNormL2DistanceSquare()); break;
+    case 2: d.reset(new CbrtUnitVectorNormL2DistanceSquare()); break;
+    case 3: d.reset(new CbrtCNormL2DistanceSquare()); break;
+    case 4: d.reset(new SqrtUnitVectorNormL2DistanceSquareResidualVector()); break;
+    case 5: d.reset(new SqrtCNormL2DistanceSquareResidualVector()); break;
+    case 6: d.reset(new SqrtUnitVectorNormL1Distance()); break;
+    case 7: d.reset(new CbrtUnitVectorNormL1Distance()); break;
+    default: return -1;
+  }
+  std::vector<real_t> r(ref, ref + n), x(dat, dat + n);
+  std::vector<unsigned> m(n, 1);
+  if (mask) m.assign(mask, mask + n);
+  real_t* rp = r.data();
+  real_t* xp = x.data();
+  unsigned* mp = m.data();
+  std::vector<real_t> dist;
+  if (!(*d)(rp, xp, mp, (unsigned)n, dist)) return -1;
+  for (size_t i = 0; i < dist.size(); ++i) out[i] = dist[i];
+  return (long)dist.size();
+}
+
 }  // extern "C"
+

@@ -470,4 +470,40 @@ long ref_hig_json(const char* path, char* buf, long cap) {
   return (long)out.size();
 }
 
+// As ref_hig_json, after HiGInput::update_params with the fit parameters keys[i] = vals[i]
+// (the keys of the file's fitting block).  -3 when update_params refused.
+long ref_hig_json_updated(const char* path, const char** keys, const double* vals, int n, char* buf,
+                          long cap) {
+  static std::string out;
+  {
+    HiGInput in;
+    in.init();
+    std::streambuf* old = std::cerr.rdbuf();
+    std::ostringstream sink;
+    std::cerr.rdbuf(sink.rdbuf());
+    std::streambuf* old_out = std::cout.rdbuf();
+    std::cout.rdbuf(sink.rdbuf());
+    InputReader::instance().input_stream_.clear();
+    bool ok = in.construct_input_config(path);
+    if (ok) {
+      map_t m;
+      for (int i = 0; i < n; ++i) m[keys[i]] = vals[i];
+      ok = in.update_params(m);
+      if (!ok) {
+        std::cerr.rdbuf(old);
+        std::cout.rdbuf(old_out);
+        return -3;
+      }
+    }
+    std::cerr.rdbuf(old);
+    std::cout.rdbuf(old_out);
+    if (!ok) return -1;
+    out = dump(in);
+  }
+  if ((long)out.size() + 1 > cap) return -2;
+  memcpy(buf, out.c_str(), out.size() + 1);
+  return (long)out.size();
+}
+
 }  // extern "C"
+

@@ -99,3 +99,51 @@ def test_compute_gisaxs_refuses_unsupported(ctx, tmp_path, edit, words):
     with pytest.raises(HgxError) as e:
         d.compute_gisaxs(ctx)
     assert words in str(e.value)
+
+
+@pytest.mark.gpu
+def test_fit_distance_matches_oracle(ctx, po):
+    """hgx_fit_distance against the oracle's restatement (itself the reference's classes, bit
+    for bit): 1e-12 relative for the sums (the device sums run in another order)."""
+    from hipgisaxs_b200.hig import METRICS, fit_distance
+    rng = np.random.default_rng(9)
+    n = 70_001
+    ref = rng.gamma(2.0, 3.0, n)
+    dat = rng.gamma(2.0, 3.0, n)
+    ref[:10] = 0
+    dat[10:20] = 0
+    mask = (rng.random(n) > 0.1).astype(np.uint32)
+    for name in METRICS:
+        for mk in (None, mask):
+            got = fit_distance(ctx, name, ref, dat, mk)
+            want = po.fit_distance(name, ref, dat, mk)
+            assert got.shape == want.shape, name
+            # per-pixel residual terms |n_d - n_r|^2 cancel where model and reference agree:
+            # there the norms' summation order shows, so they are held to 1e-12 of the largest
+            np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max(),
+                                       err_msg=name)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("metric", ["sqrt_unit_l2", "sqrt_c_l2", "cbrt_c_l2", "sqrt_unit_l2_residual"])
+def test_objective_matches_oracle(ctx, po, metric):
+    """HipGISAXSObjectiveFunction::operator()(x) for a HiG fitting block: the parameters set in
+    key order, the simulation, the distance to a reference image and the regularisation,
+    against the oracle's composition of the same steps."""
+    d = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    assert d.fit_keys() == ["radius", "spacing", "twist"]
+    d.fit_update([5.0, 25.0, 12.0])
+    ref_img = po.compute_gisaxs(d.data, HIG)
+    mask = np.ones(ref_img.size, dtype=np.uint32)
+    mask[::7] = 0
+    x = [4.2, 21.0, 3.0]
+    alpha = 0.5
+    got = d.objective(ctx, x, ref_img, mask, metric, alpha)
+    # the oracle on the same updated description
+    img = po.compute_gisaxs(d.data, HIG)
+    want = po.fit_distance(metric, ref_img, img, mask)
+    means = [(7 + 3) / 2.0, (30 + 18) / 2.0, (30 + 0) / 2.0]
+    reg = (alpha / 2) * sum((xi - m) ** 2 for xi, m in zip(x, means))
+    want = np.where(np.isfinite(want), want + reg / want.size, 1e8)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=0)

@@ -211,3 +211,70 @@ def test_reference_examples_live():
         assert n > 0, path
         d = model_diff(read_hig(path).data, json.loads(buf.value.decode()))
         assert not d, path + "\n" + "\n".join(d)
+
+
+def test_fit_update_matches_reference():
+    """HiGInput::update_params for 51 variables of every form (shape parameters and origin,
+    layers, lattice, scaling, translation, repetition, ensemble, orientations, instrument,
+    no-op fields and the reference's quirks), against the reference's own update."""
+    path = os.path.join(HIG, "fit_update.hig")
+    d = read_hig(path)
+    keys = d.fit_keys()
+    assert keys == sorted(keys) and len(keys) == 51
+    d.fit_update([1.5 + 0.25 * i for i in range(len(keys))])
+    with open(path[:-4] + ".updated.ref.json") as f:
+        ref = json.load(f)
+    diff = model_diff(d.data, ref)
+    assert not diff, "\n".join(diff)
+    s = d.structures["st1"]
+    assert d.shapes["cyl"]["originvec"][2] == 1.5 + 0.25 * 7   # "key:z" sets the origin
+    assert s["rot2"]["angles"][0] == 1.5 + 0.25 * 32           # rot2's "max" sets its minimum
+    assert s["rot3"]["mean"] == 1.5 + 0.25 * 33                # anglemean, then min leaves it
+
+
+def test_update_param_errors():
+    d = read_hig(os.path.join(HIG, "fit_update.hig"))
+    for var in ("shape['cyl']:xrot", "shape['nope']:zrot", "structure['st1']:ensemble:spacing:2",
+                "structure['st1']:ensemble:orientations:rot1['x']:min", "shape[cyl]:zrot",
+                "shape['cyl']:param['width']:min", "detector:sdd"):
+        with pytest.raises(HgxError):
+            d.update_param(var, 1.0)
+    d.update_param("shape['cyl']:zrot", 0.25)  # radians, as the reference takes them
+    assert d.shapes["cyl"]["rot"][0] == 0.25
+
+
+def test_fit_metrics_restatement_is_the_reference():
+    """The oracle's restatement of the fitter's eight distance measures against the
+    reference's classes (distance_functions.hpp), bit for bit, with masks, zeros and NaNs."""
+    import numpy as np
+    import pyoracle as po
+    if not po.available("ref"):
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(5)
+    n = 4000
+    ref = rng.gamma(2.0, 3.0, n)
+    dat = rng.gamma(2.0, 3.0, n)
+    ref[:10] = 0
+    dat[10:20] = 0
+    ref[20:25] = -1.0
+    mask = (rng.random(n) > 0.1).astype(np.uint32)
+    for name in po.FIT_METRICS:
+        for mk in (None, mask):
+            a = po.fit_distance(name, ref, dat, mk, "port")
+            b = po.fit_distance(name, ref, dat, mk, "ref")
+            assert np.array_equal(a, b, equal_nan=True), name
+
+
+def test_fit_update_live_against_reference():
+    _, lib = _reference_tree()
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gen_hig", os.path.join(HIG, "gen_hig_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    path = os.path.join(HIG, "fit_update.hig")
+    d = read_hig(path)
+    keys = d.fit_keys()
+    vals = [0.75 - 0.5 * i for i in range(len(keys))]
+    d.fit_update(vals)
+    diff = model_diff(d.data, gen.ref_updated(path, keys, vals))
+    assert not diff, "\n".join(diff)
