@@ -93,6 +93,8 @@ SIGNATURES = {
     "hgx_hig_update_param": (_i, [_vp, C.c_char_p, _d]),
     "hgx_hig_fit_update": (_i, [_vp, _vp, _i]),
     "hgx_fit_distance": (_i, [_vp, _i, C.c_long, _vp, _vp, _vp, _vp]),
+    "hgx_read_image": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long), C.POINTER(_i), C.POINTER(_i)]),
+    "hgx_read_mask": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long)]),
     "hgx_hig_objective": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, C.POINTER(C.c_long)]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
 }

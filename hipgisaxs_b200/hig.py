@@ -216,3 +216,24 @@ def fit_distance(ctx: Context, metric, ref, data, mask=None):
     out = np.zeros(n if m in (4, 5) else 1)
     check(lib().hgx_fit_distance(ctx.handle, int(m), n, pr, pd, pm, out.ctypes.data))
     return out
+
+
+def read_image(path: str):
+    """hgx_read_image: a reference image (text or EDF) as (values, ncol, nrow); values may hold
+    a last row more than ncol x nrow counts, as the reference's text reader leaves it."""
+    cnt, nc, nr = C.c_long(), C.c_int(), C.c_int()
+    check(lib().hgx_read_image(os.fsencode(path), None, 0, C.byref(cnt), C.byref(nc), C.byref(nr)))
+    data = np.zeros(cnt.value)
+    check(lib().hgx_read_image(os.fsencode(path), data.ctypes.data, cnt.value, C.byref(cnt),
+                               C.byref(nc), C.byref(nr)))
+    return data, nc.value, nr.value
+
+
+def read_mask(path: str):
+    """hgx_read_mask: a fit mask (text or EDF) as uint32 values."""
+    cnt = C.c_long()
+    check(lib().hgx_read_mask(os.fsencode(path), None, 0, C.byref(cnt)))
+    m = np.zeros(cnt.value, dtype=np.uint32)
+    check(lib().hgx_read_mask(os.fsencode(path), m.ctypes.data, cnt.value, C.byref(cnt)))
+    return m
+

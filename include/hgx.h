@@ -437,6 +437,17 @@ int hgx_hig_update_param(hgx_hig h, const char* variable, double value);
 /* All fit parameters at once: x[i] for the i-th key (nx = hgx_hig_fit_count). */
 int hgx_hig_fit_update(hgx_hig h, const double* x, int nx);
 
+/* A fit's reference image and mask as the reference reads them
+ * (src/analyzer/objective_func_hipgisaxs.cpp:83-205): the type by extension (edf/EDF: EDF,
+ * src/file/edf_reader.cpp; txt/TXT/dat/DAT/out/OUT: text, ImageData::read,
+ * src/analyzer/ImageData.cpp:79-104, whose row count leaves out a last line without a newline).
+ * *count receives the number of values read (it exceeds ncol x nrow by that last line); data
+ * may be NULL to ask for the sizes, otherwise capacity must hold every value.  Masks: the unsigned integers of
+ * a text file (a last value followed directly by the end of the file is dropped, as the
+ * reference drops it) or an EDF image's values.  Host only. */
+int hgx_read_image(const char* path, double* data, long capacity, long* count, int* ncol, int* nrow);
+int hgx_read_mask(const char* path, unsigned* mask, long capacity, long* count);
+
 /* ------------------------------------------------------------- fitting metrics ---- */
 /* The distance measures of the reference's HiG-driven fitter
  * (include/analyzer/distance_functions.hpp:387-844, chosen by the fitting block's

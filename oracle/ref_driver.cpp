@@ -33,6 +33,8 @@
 #include <ff/ff_ana.hpp>
 #include <sf/sf.hpp>
 #include <analyzer/distance_functions.hpp>
+#include <analyzer/ImageData.hpp>
+#include <file/edf_reader.hpp>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -377,6 +379,31 @@ long ref_fit_distance(int metric, long n, const double* ref, const double* dat, 
   if (!(*d)(rp, xp, mp, (unsigned)n, dist)) return -1;
   for (size_t i = 0; i < dist.size(); ++i) out[i] = dist[i];
   return (long)dist.size();
+}
+
+// A reference image as the reference reads it: ImageData::read for text files
+// (src/analyzer/ImageData.cpp:79-104), EDFReader for .edf (src/file/edf_reader.cpp).
+// Returns the value count, -1 when the file cannot be read, -2 when cap is too small.
+long ref_read_image(const char* path, int edf, double* data, long cap, int* ncol, int* nrow) {
+  std::vector<double> v;
+  if (edf) {
+    EDFReader r(path);  // exits the process on a file it cannot read: call it on good files only
+    real_t* d = nullptr;
+    unsigned ny = 0, nz = 0;
+    if (!r.get_data(d, ny, nz)) return -1;
+    v.assign(d, d + (size_t)ny * nz);
+    *ncol = (int)ny;
+    *nrow = (int)nz;
+  } else {
+    ImageData img;
+    if (!img.read(path)) return -1;
+    v.assign(img.data(), img.data() + img.size());
+    *ncol = (int)img.n_par();
+    *nrow = (int)img.n_ver();
+  }
+  if ((long)v.size() > cap) return -2;
+  for (size_t i = 0; i < v.size(); ++i) data[i] = v[i];
+  return (long)v.size();
 }
 
 }  // extern "C"
