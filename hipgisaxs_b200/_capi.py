@@ -90,6 +90,9 @@ SIGNATURES = {
     "hgx_hig_compute_gisaxs": (_i, [_vp, _vp, _i, _vp]),
     "hgx_hig_fit_count": (_i, [_vp, C.POINTER(_i)]),
     "hgx_hig_fit_param": (_i, [_vp, _i, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, _vp, _vp]),
+    "hgx_hig_fit_reference": (_i, [_vp, _i, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, _vp, _vp]),
+    "hgx_hig_fit_algorithm_count": (_i, [_vp, C.POINTER(_i)]),
+    "hgx_hig_fit_algorithm": (_i, [_vp, _i, C.c_char_p, C.c_size_t, _vp, _vp, _vp]),
     "hgx_hig_update_param": (_i, [_vp, C.c_char_p, _d]),
     "hgx_hig_fit_update": (_i, [_vp, _vp, _i]),
     "hgx_fit_distance": (_i, [_vp, _i, C.c_long, _vp, _vp, _vp, _vp]),

@@ -90,6 +90,55 @@ int hgx_hig_fit_param(hgx_hig h, int i, char* key, size_t key_cap, char* variabl
   return HGX_OK;
 }
 
+namespace {
+int put_str(const std::string& v, char* buf, size_t cap, const char* what) {
+  if (!buf) return HGX_OK;
+  if (cap <= v.size()) return fail(HGX_ERR_INVALID_ARG, std::string(what) + ": buffer too small");
+  memcpy(buf, v.c_str(), v.size() + 1);
+  return HGX_OK;
+}
+}  // namespace
+
+int hgx_hig_fit_reference(hgx_hig h, int i, char* path, size_t path_cap, char* mask, size_t mask_cap,
+                          int* npar, int* nperp) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_reference: null handle");
+  if (!h->in.reference_data_set || i != 0)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_reference: no referencedata block of that index");
+  const hig::FitReferenceData& r = h->in.reference_data;
+  HGX_TRY(put_str(r.path_set ? r.path : std::string(), path, path_cap, "hgx_hig_fit_reference"));
+  HGX_TRY(put_str(r.mask_set ? r.mask : std::string(), mask, mask_cap, "hgx_hig_fit_reference"));
+  if (npar) *npar = (int)r.npoints_parallel;
+  if (nperp) *nperp = (int)r.npoints_perpendicular;
+  return HGX_OK;
+}
+
+int hgx_hig_fit_algorithm_count(hgx_hig h, int* n) {
+  if (!h || !n) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_algorithm_count: null argument");
+  *n = (int)h->in.algorithms.size();
+  return HGX_OK;
+}
+
+int hgx_hig_fit_algorithm(hgx_hig h, int i, char* name, size_t name_cap, int* metric, double* tolerance,
+                          double* regularization) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_algorithm: null handle");
+  if (i < 0 || i >= (int)h->in.algorithms.size())
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_algorithm: index out of range");
+  const hig::FitAlgorithm& a = h->in.algorithms[i];
+  HGX_TRY(put_str(a.name, name, name_cap, "hgx_hig_fit_algorithm"));
+  if (metric) {
+    static const char* const names[] = {"sqrt_unit_l2", "sqrt_c_l2", "cbrt_unit_l2", "cbrt_c_l2",
+                                        "sqrt_unit_l2_residual", "sqrt_c_l2_residual",
+                                        "sqrt_unit_l1", "cbrt_unit_l1"};
+    *metric = -1;
+    if (a.metric_set)
+      for (int k = 0; k < 8; ++k)
+        if (a.distance_metric == names[k]) *metric = k;
+  }
+  if (tolerance) *tolerance = a.tolerance;
+  if (regularization) *regularization = a.regularization;
+  return HGX_OK;
+}
+
 int hgx_hig_fit_update(hgx_hig h, const double* x, int n) {
   if (!h || (n > 0 && !x)) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_update: null argument");
   if (n != (int)h->in.fit_params.size())

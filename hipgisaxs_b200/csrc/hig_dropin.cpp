@@ -19,6 +19,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
+#include <map>
+#include <stdexcept>
+#include <string>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -46,8 +49,7 @@ struct GridEntry {
 };
 std::unordered_map<const void*, GridEntry> g_grids;
 
-hgx_ctx context() {
-  const int dev = current_device();
+hgx_ctx context_on(int dev) {
   std::lock_guard<std::mutex> lk(g_mu);
   auto it = g_ctx.find(dev);
   if (it != g_ctx.end()) return it->second;
@@ -59,6 +61,8 @@ hgx_ctx context() {
   g_ctx[dev] = c;
   return c;
 }
+
+hgx_ctx context() { return context_on(current_device()); }
 
 int precision() {
   const char* p = std::getenv("HGX_PRECISION");
@@ -551,5 +555,353 @@ bool HipGISAXSObjectiveFunctionG::simulate(const real_vec_t& x, real_vec_t& inte
   intensity.assign((size_t)m.s.nrow * m.s.ncol, 0.0);
   return report(hgx_cyl_batch_forward(m.one, mb, intensity.data()), "objective simulate");
 }
+
+}  // namespace hig
+
+// ------------------------------------------------------------------- HipGISAXSG ----
+namespace hig {
+
+struct HipGISAXSG::Impl {
+  int device = 0;
+  hgx_ctx ctx = nullptr;
+  hgx_hig h = nullptr;
+  int nrow = 0, ncol = 0;
+  double k0 = 0.0;
+  bool ready = false;
+  std::string err;
+
+  ~Impl() {
+    if (h) hgx_hig_destroy(h);
+  }
+  bool check(int status, const char* where) {
+    if (status == HGX_OK) return true;
+    err = hgx_last_error();
+    std::cerr << "hgx: " << where << ": " << err << std::endl;
+    return false;
+  }
+  bool refuse(const std::string& msg) {
+    err = msg;
+    std::cerr << "hgx: " << msg << std::endl;
+    return false;
+  }
+  // the fit parameters in key order (HiGInput::fit_param_keys and its parallel lists)
+  struct Param {
+    std::string key, variable;
+    double range[3], init;
+  };
+  std::vector<Param> params() const {
+    std::vector<Param> out;
+    int n = 0;
+    if (!h || hgx_hig_fit_count(h, &n) != HGX_OK) return out;
+    for (int i = 0; i < n; ++i) {
+      char key[512], var[1024];
+      Param p;
+      if (hgx_hig_fit_param(h, i, key, sizeof(key), var, sizeof(var), p.range, &p.init) != HGX_OK) break;
+      p.key = key;
+      p.variable = var;
+      out.push_back(p);
+    }
+    return out;
+  }
+};
+
+HipGISAXSG::HipGISAXSG(int device) : impl_(new Impl) { impl_->device = device; }
+HipGISAXSG::~HipGISAXSG() { delete impl_; }
+
+bool HipGISAXSG::construct_input(const char* filename) {
+  if (impl_->h) hgx_hig_destroy(impl_->h);
+  impl_->h = nullptr;
+  impl_->ready = false;
+  if (!filename) return impl_->refuse("construct_input: no file name");
+  return impl_->check(hgx_hig_read(filename, &impl_->h), "construct_input");
+}
+
+// HipGISAXS::init (src/sim/hipgisaxs_main.cpp): the beam and the detector image's size; the
+// q-grid and Fresnel coefficients are built on the device by the first compute_gisaxs
+bool HipGISAXSG::init() {
+  Impl& m = *impl_;
+  if (!m.h) return m.refuse("init: no input (construct_input first)");
+  double ai = 0.0, fr = 0.0;
+  if (!m.check(hgx_hig_beam(m.h, &m.k0, &ai, &fr), "init")) return false;
+  if (!m.check(hgx_hig_image_size(m.h, &m.nrow, &m.ncol), "init")) return false;
+  m.ctx = context_on(m.device);
+  if (!m.ctx) return m.refuse(std::string("init: no device context: ") + hgx_last_error());
+  m.ready = true;
+  return true;
+}
+
+bool HipGISAXSG::compute_gisaxs(real_t*& final_data) {
+  Impl& m = *impl_;
+  if (!m.ready && !init()) return false;
+  if (!m.check(hgx_hig_image_size(m.h, &m.nrow, &m.ncol), "compute_gisaxs")) return false;
+  const size_t n = (size_t)m.nrow * m.ncol;
+  bool owned = false;
+  if (!final_data) {
+    final_data = new (std::nothrow) real_t[n];
+    if (!final_data) return m.refuse("compute_gisaxs: out of host memory");
+    owned = true;
+  }
+  static_assert(sizeof(real_t) == sizeof(double), "the HiG simulation computes in double");
+  if (!m.check(hgx_hig_compute_gisaxs(m.ctx, m.h, precision(), reinterpret_cast<double*>(final_data)),
+               "compute_gisaxs")) {
+    if (owned) {
+      delete[] final_data;
+      final_data = nullptr;
+    }
+    return false;
+  }
+  return true;
+}
+
+// HiGInput::update_params (src/config/hig_input.cpp:2712-2830): fit keys -> values; an
+// unknown key throws std::out_of_range, as the reference's map lookup does
+bool HipGISAXSG::update_params(const std::map<std::string, real_t>& values) {
+  Impl& m = *impl_;
+  if (!m.h) return m.refuse("update_params: no input");
+  const std::vector<Impl::Param> ps = m.params();
+  for (const auto& kv : values) {
+    const Impl::Param* p = nullptr;
+    for (const auto& q : ps)
+      if (q.key == kv.first) p = &q;
+    if (!p) throw std::out_of_range("update_params: no fit parameter with key '" + kv.first + "'");
+    if (!m.check(hgx_hig_update_param(m.h, p->variable.c_str(), kv.second), "update_params")) return false;
+  }
+  return true;
+}
+
+bool HipGISAXSG::update_param(const std::string& variable, real_t value) {
+  Impl& m = *impl_;
+  if (!m.h) return m.refuse("update_param: no input");
+  return m.check(hgx_hig_update_param(m.h, variable.c_str(), value), "update_param");
+}
+
+bool HipGISAXSG::gaussian_smearing(real_t*& data, real_t sigma) {
+  Impl& m = *impl_;
+  if (!m.ready && !init()) return false;
+  return m.check(hgx_gaussian_smearing(m.ctx, reinterpret_cast<double*>(data), m.ncol, m.nrow, sigma),
+                 "gaussian_smearing");
+}
+
+bool HipGISAXSG::normalize(real_t*& data, unsigned int size) {
+  Impl& m = *impl_;
+  if (!m.ready && !init()) return false;
+  int done = 0;
+  if (!m.check(hgx_normalize(m.ctx, reinterpret_cast<double*>(data), (long)size, &done), "normalize"))
+    return false;
+  return done != 0;  // false when max - min < 1e-30, as in the reference
+}
+
+bool HipGISAXSG::save_gisaxs(real_t* final_data, std::string filename) {
+  Impl& m = *impl_;
+  if (!m.ready && !init()) return false;
+  return m.check(hgx_save_gisaxs(m.ctx, reinterpret_cast<const double*>(final_data), m.nrow, m.ncol,
+                                 filename.c_str()),
+                 "save_gisaxs");
+}
+
+unsigned int HipGISAXSG::nrow() const { return (unsigned)impl_->nrow; }
+unsigned int HipGISAXSG::ncol() const { return (unsigned)impl_->ncol; }
+real_t HipGISAXSG::k0() const { return impl_->k0; }
+const char* HipGISAXSG::last_error() const { return impl_->err.c_str(); }
+
+std::vector<std::string> HipGISAXSG::fit_param_keys() const {
+  std::vector<std::string> keys;
+  for (const auto& p : impl_->params()) keys.push_back(p.key);
+  return keys;
+}
+
+// ------------------------------------------------------- HiGObjectiveFunctionG ----
+struct HiGObjectiveFunctionG::Impl {
+  HipGISAXSG sim;
+  unsigned n_par = 0, n_ver = 0;
+  int metric = -1;
+  real_t alpha = 0.0;
+  std::vector<double> ref;
+  std::vector<unsigned> mask;  // empty: every pixel
+  bool good = false;
+  explicit Impl(int device) : sim(device) {}
+};
+
+namespace {
+const char* const kMetricNames[] = {"sqrt_unit_l2", "sqrt_c_l2", "cbrt_unit_l2", "cbrt_c_l2",
+                                    "sqrt_unit_l2_residual", "sqrt_c_l2_residual", "sqrt_unit_l1",
+                                    "cbrt_unit_l1"};
+}  // namespace
+
+HiGObjectiveFunctionG::HiGObjectiveFunctionG(const char* hig_file, int device) : impl_(new Impl(device)) {
+  Impl& m = *impl_;
+  if (!m.sim.construct_input(hig_file) || !m.sim.init()) return;
+  m.n_par = m.sim.ncol();
+  m.n_ver = m.sim.nrow();
+  int nalg = 0;
+  if (hgx_hig_fit_algorithm_count(m.sim.impl_->h, &nalg) == HGX_OK && nalg > 0)
+    hgx_hig_fit_algorithm(m.sim.impl_->h, 0, nullptr, 0, &m.metric, nullptr, nullptr);
+  // set_mean_data: every fit parameter at the middle of its range (the image the reference
+  // computes there is not used by its operator(), so it is not computed here)
+  std::map<std::string, real_t> mean;
+  for (const auto& p : m.sim.impl_->params()) mean[p.key] = (p.range[1] - p.range[0]) / 2.0 + p.range[0];
+  if (!m.sim.update_params(mean)) return;
+  m.good = true;
+}
+
+HiGObjectiveFunctionG::~HiGObjectiveFunctionG() { delete impl_; }
+
+bool HiGObjectiveFunctionG::ok() const { return impl_->good; }
+
+// HipGISAXSObjectiveFunction::set_reference_data, read_mask_data, read_edf_mask_data
+// (src/analyzer/objective_func_hipgisaxs.cpp:116-205)
+bool HiGObjectiveFunctionG::set_reference_data(int i) {
+  Impl& m = *impl_;
+  HipGISAXSG::Impl& s = *m.sim.impl_;
+  if (!m.good) return s.refuse("set_reference_data: the objective did not initialise");
+  char path[4096], maskp[4096];
+  if (!s.check(hgx_hig_fit_reference(s.h, i, path, sizeof(path), maskp, sizeof(maskp), nullptr, nullptr),
+               "set_reference_data"))
+    return false;
+  long count = 0;
+  int nc = 0, nr = 0;
+  if (!s.check(hgx_read_image(path, nullptr, 0, &count, &nc, &nr), "set_reference_data")) return false;
+  std::vector<double> img((size_t)std::max(count, 1L));
+  if (!s.check(hgx_read_image(path, img.data(), (long)img.size(), &count, &nc, &nr), "set_reference_data"))
+    return false;
+  if ((unsigned)nc != m.n_par || (unsigned)nr != m.n_ver)
+    return s.refuse("set_reference_data: the reference image is " + std::to_string(nc) + " x " +
+                    std::to_string(nr) + ", the detector " + std::to_string(m.n_par) + " x " +
+                    std::to_string(m.n_ver) + " (re-gridding the simulation to the reference's region "
+                    "is not supported)");
+  const size_t n = (size_t)m.n_par * m.n_ver;
+  img.resize(n);  // a text image may carry a last, uncounted row
+  std::vector<unsigned> msk;
+  const std::string mp = maskp;
+  if (!mp.empty()) {  // EDF or text by the extension, as the reference reads it
+    long mc = 0;
+    if (!s.check(hgx_read_mask(mp.c_str(), nullptr, 0, &mc), "set_reference_data")) return false;
+    msk.resize((size_t)std::max(mc, 1L));
+    if (!s.check(hgx_read_mask(mp.c_str(), msk.data(), (long)msk.size(), &mc), "set_reference_data")) return false;
+    msk.resize((size_t)mc);
+    if (msk.size() != n)
+      return s.refuse("set_reference_data: mask and reference data sizes differ (" + std::to_string(n) +
+                      " != " + std::to_string(msk.size()) + ")");
+  }
+  m.ref.swap(img);
+  m.mask.swap(msk);
+  return true;
+}
+
+bool HiGObjectiveFunctionG::set_reference_data(const real_vec_t& ref, const std::vector<unsigned int>& mask) {
+  Impl& m = *impl_;
+  const size_t n = (size_t)m.n_par * m.n_ver;
+  if (!m.good) return m.sim.impl_->refuse("set_reference_data: the objective did not initialise");
+  if (ref.size() != n || (!mask.empty() && mask.size() != n))
+    return m.sim.impl_->refuse("set_reference_data: " + std::to_string(n) + " values expected");
+  m.ref.assign(ref.begin(), ref.end());
+  m.mask.assign(mask.begin(), mask.end());
+  return true;
+}
+
+// simulate_and_set_ref (src/analyzer/objective_func_hipgisaxs.cpp:336-374); the mask is kept
+bool HiGObjectiveFunctionG::simulate_and_set_ref(const real_vec_t& x) {
+  Impl& m = *impl_;
+  if (!m.good) return m.sim.impl_->refuse("simulate_and_set_ref: the objective did not initialise");
+  if (!x.empty()) {
+    const std::vector<std::string> keys = m.sim.fit_param_keys();
+    if (x.size() > keys.size()) return m.sim.impl_->refuse("simulate_and_set_ref: more values than fit parameters");
+    std::map<std::string, real_t> vals;
+    for (size_t i = 0; i < x.size(); ++i) vals[keys[i]] = x[i];
+    if (!m.sim.update_params(vals)) return false;
+  }
+  std::vector<real_t> img((size_t)m.n_par * m.n_ver);
+  real_t* p = img.data();
+  if (!m.sim.compute_gisaxs(p)) return false;
+  m.ref.assign(img.begin(), img.end());
+  return true;
+}
+
+bool HiGObjectiveFunctionG::set_distance_metric(const std::string& name) {
+  for (int k = 0; k < 8; ++k)
+    if (name == kMetricNames[k]) {
+      impl_->metric = k;
+      return true;
+    }
+  return impl_->sim.impl_->refuse("set_distance_metric: unknown metric '" + name + "'");
+}
+
+bool HiGObjectiveFunctionG::set_regularization(real_t alpha) {
+  impl_->alpha = alpha;
+  return true;
+}
+
+// operator() (src/analyzer/objective_func_hipgisaxs.cpp:263-334) through hgx_hig_objective
+real_vec_t HiGObjectiveFunctionG::operator()(const real_vec_t& x) {
+  Impl& m = *impl_;
+  HipGISAXSG::Impl& s = *m.sim.impl_;
+  if (!m.good) {
+    s.refuse("operator(): the objective did not initialise");
+    return real_vec_t();
+  }
+  if (m.ref.empty()) {
+    s.refuse("operator(): no reference data (set_reference_data first)");
+    return real_vec_t();
+  }
+  if (m.metric < 0) {
+    s.refuse("operator(): no distance metric (none in the fitting block; set_distance_metric)");
+    return real_vec_t();
+  }
+  std::vector<double> xd(x.begin(), x.end());
+  std::vector<double> dist((size_t)m.n_par * m.n_ver);
+  long nd = 0;
+  if (!s.check(hgx_hig_objective(s.ctx, s.h, xd.data(), (int)xd.size(), m.ref.data(),
+                                 m.mask.empty() ? nullptr : m.mask.data(), m.metric, m.alpha, dist.data(), &nd),
+               "operator()"))
+    return real_vec_t();
+  return real_vec_t(dist.begin(), dist.begin() + nd);
+}
+
+int HiGObjectiveFunctionG::num_fit_params() const { return (int)impl_->sim.impl_->params().size(); }
+
+std::vector<std::string> HiGObjectiveFunctionG::fit_param_keys() const { return impl_->sim.fit_param_keys(); }
+
+std::vector<std::pair<real_t, real_t>> HiGObjectiveFunctionG::fit_param_limits() const {
+  std::vector<std::pair<real_t, real_t>> out;
+  for (const auto& p : impl_->sim.impl_->params()) out.emplace_back(p.range[0], p.range[1]);
+  return out;
+}
+
+real_vec_t HiGObjectiveFunctionG::fit_param_step_values() const {
+  real_vec_t out;
+  for (const auto& p : impl_->sim.impl_->params()) out.push_back(p.range[2]);
+  return out;
+}
+
+real_vec_t HiGObjectiveFunctionG::fit_param_init_values() const {
+  real_vec_t out;
+  for (const auto& p : impl_->sim.impl_->params()) out.push_back(p.init);
+  return out;
+}
+
+// HiGInput::param_space_mean (include/config/hig_input.hpp:322-325); an unknown key throws
+// std::out_of_range as the reference's map lookup does
+real_t HiGObjectiveFunctionG::param_space_mean(const std::string& key) const {
+  for (const auto& p : impl_->sim.impl_->params())
+    if (p.key == key) return (p.range[1] - p.range[0]) / 2.0 + p.range[0];
+  throw std::out_of_range("param_space_mean: no fit parameter with key '" + key + "'");
+}
+
+real_t HiGObjectiveFunctionG::analysis_tolerance(int n) const {
+  double t = 0.0;
+  hgx_hig_fit_algorithm(impl_->sim.impl_->h, n, nullptr, 0, nullptr, &t, nullptr);
+  return t;
+}
+
+real_t HiGObjectiveFunctionG::analysis_regularization(int n) const {
+  double r = 0.0;
+  hgx_hig_fit_algorithm(impl_->sim.impl_->h, n, nullptr, 0, nullptr, nullptr, &r);
+  return r;
+}
+
+unsigned int HiGObjectiveFunctionG::n_par() const { return impl_->n_par; }
+unsigned int HiGObjectiveFunctionG::n_ver() const { return impl_->n_ver; }
+unsigned int HiGObjectiveFunctionG::data_size() const { return impl_->n_par * impl_->n_ver; }
+HipGISAXSG& HiGObjectiveFunctionG::simulator() { return impl_->sim; }
 
 }  // namespace hig

@@ -159,6 +159,29 @@ class HiGInput:
             keys.append(k.value.decode())
         return keys
 
+    def fit_reference(self):
+        """The referencedata block: {"path", "mask", "npar", "nperp"} (reference_data_path,
+        reference_data_mask; paths as written, "" when not given)."""
+        p, m = C.create_string_buffer(4096), C.create_string_buffer(4096)
+        npar, nperp = C.c_int(), C.c_int()
+        check(lib().hgx_hig_fit_reference(self._h, 0, p, 4096, m, 4096, C.byref(npar), C.byref(nperp)))
+        return {"path": p.value.decode(), "mask": m.value.decode(), "npar": npar.value,
+                "nperp": nperp.value}
+
+    def fit_algorithms(self):
+        """The analysis algorithms in file order: [{"name", "metric", "tolerance",
+        "regularization"}], metric an hgx_fit_metric number (-1: none of them)."""
+        n = C.c_int()
+        check(lib().hgx_hig_fit_algorithm_count(self._h, C.byref(n)))
+        out = []
+        for i in range(n.value):
+            nm = C.create_string_buffer(64)
+            met, tol, reg = C.c_int(), C.c_double(), C.c_double()
+            check(lib().hgx_hig_fit_algorithm(self._h, i, nm, 64, C.byref(met), C.byref(tol), C.byref(reg)))
+            out.append({"name": nm.value.decode(), "metric": met.value, "tolerance": tol.value,
+                        "regularization": reg.value})
+        return out
+
     def update_param(self, variable: str, value: float):
         """Sets one parameter by its variable name, e.g. "shape['s1']:param['radius']:min"."""
         check(lib().hgx_hig_update_param(self._h, variable.encode(), float(value)))

@@ -437,6 +437,22 @@ int hgx_hig_update_param(hgx_hig h, const char* variable, double value);
 /* All fit parameters at once: x[i] for the i-th key (nx = hgx_hig_fit_count). */
 int hgx_hig_fit_update(hgx_hig h, const double* x, int nx);
 
+/* The fitting block's reference data (HiGInput::reference_data_path / reference_data_mask,
+ * include/config/hig_input.hpp:327-328; FitReferenceData, include/config/temp_helpers.hpp:26-62):
+ * one referencedata block, i = 0.  The image and mask paths as written ("" when not given;
+ * the reference opens them relative to the working directory) and the npoints counts (0 when
+ * not given).  Any output may be NULL. */
+int hgx_hig_fit_reference(hgx_hig h, int i, char* path, size_t path_cap, char* mask, size_t mask_cap,
+                          int* npar, int* nperp);
+/* The fitting block's analysis algorithms in file order (HiGInput::analysis_algo,
+ * analysis_distance_metric, analysis_tolerance, analysis_regularization,
+ * include/config/hig_input.hpp:338-345): the name ("pso", "lmvm", "pounders", "bruteforce",
+ * "none_pounders", "error" for an unknown one), the distance metric as an hgx_fit_metric (-1
+ * when not given or not one of them), tolerance and regularization.  Any output may be NULL. */
+int hgx_hig_fit_algorithm_count(hgx_hig h, int* n);
+int hgx_hig_fit_algorithm(hgx_hig h, int i, char* name, size_t name_cap, int* metric, double* tolerance,
+                          double* regularization);
+
 /* A fit's reference image and mask as the reference reads them
  * (src/analyzer/objective_func_hipgisaxs.cpp:83-205): the type by extension (edf/EDF: EDF,
  * src/file/edf_reader.cpp; txt/TXT/dat/DAT/out/OUT: text, ImageData::read,

@@ -12,6 +12,7 @@
 #define HGX_HIG_HPP
 
 #include <complex>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -259,6 +260,81 @@ class HipGISAXSObjectiveFunctionG {
   bool set_regularization(real_t alpha);
   bool set_param_mean(const real_vec_t& mean);        // x_mean of the regularisation
   unsigned int data_size() const;
+
+ private:
+  struct Impl;
+  Impl* impl_;
+};
+
+
+// --------------------------------------------------------- HiG-driven simulation ----
+// HipGISAXS (include/sim/hipgisaxs_main.hpp, src/sim/hipgisaxs_main.cpp) for the path built
+// here: read a HiG description, simulate it on the GPU (hgx_hig_compute_gisaxs), update
+// parameters, post-process.  The method names are the reference's; the class name carries the
+// G of the GPU classes so that it can sit beside the reference's own HipGISAXS.
+class HipGISAXSG {
+ public:
+  explicit HipGISAXSG(int device = 0);
+  ~HipGISAXSG();
+  HipGISAXSG(const HipGISAXSG&) = delete;
+  HipGISAXSG& operator=(const HipGISAXSG&) = delete;
+
+  bool construct_input(const char* filename);        // HiGInput::construct_input_config
+  bool init();                                       // beam and q-grid (HipGISAXS::init)
+  // the nrow x ncol image of all structures; `final_data` is allocated with new[] when NULL
+  bool compute_gisaxs(real_t*& final_data);
+  bool update_params(const std::map<std::string, real_t>& params);  // fit keys -> values
+  bool update_param(const std::string& variable, real_t value);      // a variable name
+  bool gaussian_smearing(real_t*& data, real_t sigma);               // in place
+  bool normalize(real_t*& data, unsigned int size);                  // in place
+  bool save_gisaxs(real_t* final_data, std::string filename);        // the .out text
+  unsigned int nrow() const;
+  unsigned int ncol() const;
+  real_t k0() const;
+  std::vector<std::string> fit_param_keys() const;
+  const char* last_error() const;                    // the library's message after a false
+
+ private:
+  struct Impl;
+  Impl* impl_;
+  friend class HiGObjectiveFunctionG;
+};
+
+// HipGISAXSObjectiveFunction (src/analyzer/objective_func_hipgisaxs.cpp,
+// include/analyzer/objective_func_hipgisaxs.hpp) for a HiG file: the fitting block's parameters
+// (key order), its reference data and mask (read by extension as the reference reads them),
+// the distance metric of its first algorithm, the regularisation.  As in the reference, the
+// constructor sets every fit parameter to the middle of its range (set_mean_data) and the
+// regularisation starts at 0; operator() returns one distance, or one per pixel for the
+// residual metrics, each plus its share of (alpha/2)|x - mean|^2 (a non-finite one becomes 1e8).
+class HiGObjectiveFunctionG {
+ public:
+  HiGObjectiveFunctionG(const char* hig_file, int device = 0);
+  ~HiGObjectiveFunctionG();
+  HiGObjectiveFunctionG(const HiGObjectiveFunctionG&) = delete;
+  HiGObjectiveFunctionG& operator=(const HiGObjectiveFunctionG&) = delete;
+
+  bool ok() const;
+  // the fitting block's reference data and mask (i = 0); false when the image's size differs
+  // from the detector's (the reference then re-grids its simulation, which is not done here)
+  bool set_reference_data(int i);
+  bool set_reference_data(const real_vec_t& ref, const std::vector<unsigned int>& mask);
+  bool simulate_and_set_ref(const real_vec_t& x);    // the simulation at x as the reference
+  bool set_distance_metric(const std::string& name);  // sqrt_unit_l2, sqrt_c_l2, ...
+  bool set_regularization(real_t alpha);
+  real_vec_t operator()(const real_vec_t& x);        // empty on failure
+  int num_fit_params() const;
+  std::vector<std::string> fit_param_keys() const;
+  std::vector<std::pair<real_t, real_t>> fit_param_limits() const;
+  real_vec_t fit_param_step_values() const;
+  real_vec_t fit_param_init_values() const;
+  real_t param_space_mean(const std::string& key) const;
+  real_t analysis_tolerance(int n) const;
+  real_t analysis_regularization(int n) const;
+  unsigned int n_par() const;                        // detector columns
+  unsigned int n_ver() const;                        // detector rows
+  unsigned int data_size() const;
+  HipGISAXSG& simulator();
 
  private:
   struct Impl;
