@@ -88,9 +88,14 @@ SIGNATURES = {
     "hgx_hig_qgrid": (_i, [_vp, _vp, _d, _d, C.POINTER(_vp)]),
     "hgx_hig_image_size": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
     "hgx_hig_compute_gisaxs": (_i, [_vp, _vp, _i, _vp]),
+    "hgx_hig_output_names": (_i, [_vp, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t]),
+    "hgx_hig_scan_size": (_i, [_vp, _vp, _vp, _vp]),
+    "hgx_hig_scan_point": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "hgx_hig_compute_scan_point": (_i, [_vp, _vp, _i, _i, _vp]),
     "hgx_hig_fit_count": (_i, [_vp, C.POINTER(_i)]),
     "hgx_hig_fit_param": (_i, [_vp, _i, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, _vp, _vp]),
     "hgx_hig_fit_reference": (_i, [_vp, _i, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t, _vp, _vp]),
+    "hgx_hig_override_qregion": (_i, [_vp, _i, _i, _i]),
     "hgx_hig_fit_algorithm_count": (_i, [_vp, C.POINTER(_i)]),
     "hgx_hig_fit_algorithm": (_i, [_vp, _i, C.c_char_p, C.c_size_t, _vp, _vp, _vp]),
     "hgx_hig_update_param": (_i, [_vp, C.c_char_p, _d]),

@@ -34,8 +34,11 @@ def nvcc() -> str:
 # arithmetic without fused multiply-adds: the exact triangle form factor's edge and vertex
 # terms and the Percus-Yevick function's terms cancel and amplify any difference in rounding,
 # and the smearing sums then round as the reference's do (those kernels are memory-bound).
+# qgrid.cu likewise: QGrid::create's 2theta is acos(t) with t just below 1 near qy = 0, where
+# a one-ulp change of t (a contracted cos_af^2 + cos_ai^2) moves 2theta by up to ~1e-9
+# relative; the grid is built once per description.
 FILE_FLAGS = {"ff_exact.cu": ["-fmad=false"], "sf_liquid.cu": ["-fmad=false"],
-              "postproc.cu": ["-fmad=false"]}
+              "postproc.cu": ["-fmad=false"], "qgrid.cu": ["-fmad=false"]}
 
 
 def _sources():

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -55,12 +56,22 @@ namespace hgx {
 struct MeshWork {
   DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib, bwpart;
 };
+// A custom shape's triangle tuples on the device, with the file's identity when it was read.
+struct MeshTuples {
+  DevBuf tri;  // ntri x 8 doubles (read_shapes_file layout)
+  int ntri = 0;
+  long long size = -1, mtime_ns = -1;
+};
 // Work of hgx_hig_compute_gisaxs, kept by the context between calls: the last description's
-// q-grid (rebuilt when its region, beam or resolution changes) and grow-only buffers.
+// q-grid (rebuilt when its region, beam or resolution changes), the custom shapes' triangle
+// tuples (re-read only when the file's size or modification time changes) and grow-only
+// buffers.
 struct HigWork {
   hgx_qgrid grid = nullptr;
   double key[8] = {0};
+  double ext_alpha = 0.0;  // the incidence angle the grid's qz blocks were extended for
   DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj;
+  std::map<std::string, MeshTuples> meshes;  // by resolved path
 };
 }  // namespace hgx
 
@@ -100,6 +111,9 @@ struct hgx_qgrid_s {
 namespace hgx {
 // Prepares triangle tiles for the FP32 kernels (see ff_tri.cu).
 int qgrid_finalize(hgx_qgrid g);  // builds the row table and picks the mode
+// Recomputes the DWBA qz blocks of a grid made by hgx_qgrid_create for another incidence
+// angle (the detector qx, qy, qz and exit angles stay), then the row table (qgrid.cu).
+int qgrid_reextend(hgx_qgrid g, double alpha_i, double k0, double dn2_re, double dn2_im);
 // The context's grid for reference-shaped calls with these arrays: the kept one refilled in
 // place when nqy and nqz match, else a new one (the old one destroyed).
 int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,

@@ -112,6 +112,36 @@ int hgx_hig_fit_reference(hgx_hig h, int i, char* path, size_t path_cap, char* m
   return HGX_OK;
 }
 
+// HipGISAXS::override_qregion (src/sim/hipgisaxs_main.cpp:236-277) with QGrid::update
+// (src/model/qgrid.cpp:133-197), whose arithmetic is QGrid::create's for the given size and
+// region: the computation block takes the reference data's fit region and the image's size
+int hgx_hig_override_qregion(hgx_hig h, int ny, int nz, int i) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_override_qregion: null handle");
+  if (ny < 1 || nz < 1) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_override_qregion: empty size");
+  if (!h->in.reference_data_set || i != 0)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_override_qregion: no referencedata block of that index");
+  hig::Compute& c = h->in.compute;
+  if (c.region_type == "pixels" || c.region_type == "angles")  // "not yet implemented" there
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_override_qregion: only a qspace output region can be overridden");
+  if (c.region_type != "qspace")
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_override_qregion: unknown output region type");
+  const hig::FitReferenceData& r = h->in.reference_data;
+  c.resolution[0] = ny;
+  c.resolution[1] = nz;
+  c.minpoint = r.region_min;
+  c.maxpoint = r.region_max;
+  h->json.clear();
+  return HGX_OK;
+}
+
+int hgx_hig_output_names(hgx_hig h, char* pathprefix, size_t prefix_cap, char* runname, size_t run_cap) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_output_names: null handle");
+  const hig::Compute& c = h->in.compute;
+  HGX_TRY(put_str(c.pathprefix, pathprefix, prefix_cap, "hgx_hig_output_names"));
+  HGX_TRY(put_str(c.runname_set ? c.runname : std::string(), runname, run_cap, "hgx_hig_output_names"));
+  return HGX_OK;
+}
+
 int hgx_hig_fit_algorithm_count(hgx_hig h, int* n) {
   if (!h || !n) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_fit_algorithm_count: null argument");
   *n = (int)h->in.algorithms.size();

@@ -23,10 +23,13 @@
 #include <stdexcept>
 #include <string>
 #include <mutex>
+#include <sstream>
 #include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <sys/stat.h>
+#include <time.h>
 
 #include "hgx_hig.hpp"
 
@@ -563,6 +566,7 @@ namespace hig {
 
 struct HipGISAXSG::Impl {
   int device = 0;
+  std::string outdir;
   hgx_ctx ctx = nullptr;
   hgx_hig h = nullptr;
   int nrow = 0, ncol = 0;
@@ -699,6 +703,65 @@ bool HipGISAXSG::save_gisaxs(real_t* final_data, std::string filename) {
                  "save_gisaxs");
 }
 
+namespace {
+// ComputeParams::timestamp (src/model/compute_params.cpp:68-78)
+std::string run_timestamp() {
+  time_t raw;
+  time(&raw);
+  char buf[16];
+  strftime(buf, sizeof(buf), "%Y%m%d_%H%M%S", localtime(&raw));
+  return buf;
+}
+// a value as std::stringstream << writes it (6 significant digits), for the file names
+std::string angle_text(double v) {
+  std::ostringstream o;
+  o << v;
+  return o.str();
+}
+}  // namespace
+
+// HipGISAXS::init's output directory and run_all_gisaxs's loops (src/sim/hipgisaxs_main.cpp:
+// 160-170, 283-613); each point is hgx_hig_compute_scan_point, the sums run in point order
+bool HipGISAXSG::run_all_gisaxs(int, int, int) {
+  Impl& m = *impl_;
+  if (!init()) return false;
+  char prefix[4096], run[4096];
+  if (!m.check(hgx_hig_output_names(m.h, prefix, sizeof(prefix), run, sizeof(run)), "run_all_gisaxs")) return false;
+  const std::string rn = run[0] ? std::string(run) + "_" + run_timestamp() : "run_" + run_timestamp();
+  m.outdir = std::string(prefix) + "/" + rn;
+  if (mkdir(m.outdir.c_str(), 0755) != 0) return m.refuse("run_all_gisaxs: could not create output directory " + m.outdir);
+  int na = 0, np = 0, nt = 0;
+  if (!m.check(hgx_hig_scan_size(m.h, &na, &np, &nt), "run_all_gisaxs")) return false;
+  const size_t n = (size_t)m.nrow * m.ncol;
+  std::vector<double> img(n), sum(n);
+  int p = 0;
+  for (int i = 0; i < na; ++i) {
+    double a = 0.0;
+    std::fill(sum.begin(), sum.end(), 0.0);
+    for (int j = 0; j < np; ++j)
+      for (int k = 0; k < nt; ++k, ++p) {
+        double f = 0.0, t = 0.0;
+        if (!m.check(hgx_hig_scan_point(m.h, p, &a, &f, &t), "run_all_gisaxs")) return false;
+        if (!m.check(hgx_hig_compute_scan_point(m.ctx, m.h, precision(), p, img.data()), "run_all_gisaxs"))
+          return false;
+        const std::string name = m.outdir + "/gisaxs_ai=" + angle_text(a) + "_rot=" + angle_text(f) + "_tilt=" +
+                                 angle_text(t) + ".out";
+        if (!m.check(hgx_save_gisaxs(m.ctx, img.data(), m.nrow, m.ncol, name.c_str()), "run_all_gisaxs"))
+          return false;
+        if (np > 1 || nt > 1)
+          for (size_t q = 0; q < n; ++q) sum[q] = sum[q] + img[q];
+      }
+    if ((np > 1 || nt > 1) && np * nt > 0) {
+      const std::string name = m.outdir + "/gisaxs_ai=" + angle_text(a) + "_averaged.out";
+      if (!m.check(hgx_save_gisaxs(m.ctx, sum.data(), m.nrow, m.ncol, name.c_str()), "run_all_gisaxs"))
+        return false;
+    }
+  }
+  return true;
+}
+
+const std::string& HipGISAXSG::output_dir() const { return impl_->outdir; }
+
 unsigned int HipGISAXSG::nrow() const { return (unsigned)impl_->nrow; }
 unsigned int HipGISAXSG::ncol() const { return (unsigned)impl_->ncol; }
 real_t HipGISAXSG::k0() const { return impl_->k0; }
@@ -764,11 +827,16 @@ bool HiGObjectiveFunctionG::set_reference_data(int i) {
   std::vector<double> img((size_t)std::max(count, 1L));
   if (!s.check(hgx_read_image(path, img.data(), (long)img.size(), &count, &nc, &nr), "set_reference_data"))
     return false;
-  if ((unsigned)nc != m.n_par || (unsigned)nr != m.n_ver)
-    return s.refuse("set_reference_data: the reference image is " + std::to_string(nc) + " x " +
-                    std::to_string(nr) + ", the detector " + std::to_string(m.n_par) + " x " +
-                    std::to_string(m.n_ver) + " (re-gridding the simulation to the reference's region "
-                    "is not supported)");
+  if ((unsigned)nc != m.n_par || (unsigned)nr != m.n_ver) {
+    // the reference warns and re-grids its simulation to the image (override_qregion)
+    std::cerr << "hgx: set_reference_data: the reference image is " << nc << " x " << nr
+              << ", the simulation " << m.n_par << " x " << m.n_ver
+              << "; the simulation takes the reference data's region" << std::endl;
+    if (!s.check(hgx_hig_override_qregion(s.h, nc, nr, i), "set_reference_data")) return false;
+    if (!s.check(hgx_hig_image_size(s.h, &s.nrow, &s.ncol), "set_reference_data")) return false;
+    m.n_par = (unsigned)nc;
+    m.n_ver = (unsigned)nr;
+  }
   const size_t n = (size_t)m.n_par * m.n_ver;
   img.resize(n);  // a text image may carry a last, uncounted row
   std::vector<unsigned> msk;

@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdlib.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <array>
@@ -599,16 +600,12 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
 
 using namespace hgx;
 
-extern "C" {
-
-int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol) {
-  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_image_size: null handle");
-  if (nrow) *nrow = h->in.compute.resolution[1];
-  if (ncol) *ncol = h->in.compute.resolution[0];
-  return HGX_OK;
-}
-
-int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
+namespace {
+// HipGISAXS::run_gisaxs (src/sim/hipgisaxs_main.cpp:694-1440) at incidence angle alpha_deg and
+// in-plane rotation phi_deg (degrees, as the reference's scan loops hold them; the tilt is not
+// used by run_gisaxs).  The detector grid is QGrid::create's at the description's first
+// alpha_i (HipGISAXS::init); qz_extended and the Fresnel coefficients take alpha_deg.
+int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi_deg, double* image) {
   if (!c || !h || !image) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: null argument");
   if (precision != HGX_F64 && precision != HGX_F32C)
     return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: unknown precision");
@@ -618,10 +615,6 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   auto refuse = [](const std::string& why) {
     return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: " + why);
   };
-  if (scan_count(sc.alphai[0], sc.alphai[1], sc.alphai[2], true) > 1 ||
-      scan_count(sc.inplanerot[0], sc.inplanerot[1], sc.inplanerot[2], false) > 1 ||
-      scan_count(sc.tilt[0], sc.tilt[1], sc.tilt[2], false) > 1)
-    return refuse("more than one alpha_i, phi or tilt (the reference's compute_gisaxs refuses scans)");
   if (sc.expt != "gisaxs") return refuse("experiment '" + sc.expt + "': only gisaxs (DWBA) is supported");
   if (cp.nslices > 1) return refuse("sliced layers (nslices > 1) are not supported");
   if (cp.structcorrelation != "null" && cp.structcorrelation != "nGnE")
@@ -640,9 +633,10 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   cudaStream_t st = c->stream;
 
   // beam, grid (vacuum layer: dn2 = 0) and Fresnel coefficients for layer order 0
-  double k0, alpha_i;
+  double k0, alpha_i;  // alpha_i: the first incidence angle, of the detector grid
   HGX_TRY(hgx_hig_beam(h, &k0, &alpha_i, nullptr));
-  const double phi = sc.inplanerot[0] * PI / 180;
+  const double alpha_s = alpha_deg * PI / 180;  // this simulation's incidence angle
+  const double phi = phi_deg * PI / 180;
   if (!c->hig) {
     c->hig = new (std::nothrow) HigWork;
     if (!c->hig) return fail(HGX_ERR_NO_MEMORY, "hgx_hig_compute_gisaxs: out of host memory");
@@ -657,8 +651,13 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     w.grid = nullptr;
     HGX_TRY(hgx_hig_qgrid(c, h, 0.0, 0.0, &w.grid));
     for (int k = 0; k < 8; ++k) w.key[k] = key[k];
+    w.ext_alpha = alpha_i;
   }
   hgx_qgrid g = w.grid;
+  if (w.ext_alpha != alpha_s) {  // layer_qgrid_qz at this angle (vacuum layer: dn2 = 0)
+    HGX_TRY(qgrid_reextend(g, alpha_s, k0, 0.0, 0.0));
+    w.ext_alpha = alpha_s;
+  }
   const long n = (long)g->nqy;
   const long nq = (long)g->nqz;  // 4n
   std::vector<double> ld, lb, lt;
@@ -677,27 +676,40 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
   const int nstruct = (int)in.structures.size();
   HGX_TRY(bI.reserve(sizeof(double) * n * nstruct));
   HGX_TRY(hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(),
-                                 k0, alpha_i, 0, nullptr, (double*)bfc.p, 0));
+                                 k0, alpha_s, 0, nullptr, (double*)bfc.p, 0));
   HGX_CUDA(cudaMemsetAsync(bI.p, 0, sizeof(double) * n * nstruct, st));
 
-  // custom shapes: triangle tuples read once, kept on the device
-  std::map<std::string, std::pair<DevBuf, int>> meshes;
+  // custom shapes: triangle tuples on the device, kept by the context across calls and read
+  // again only when the file changes (the reference reads them on every form-factor call)
+  std::map<std::string, const MeshTuples*> meshes;  // shape key -> tuples
   const std::string dir = in.path.rfind('/') == std::string::npos ? "" : in.path.substr(0, in.path.rfind('/') + 1);
   for (const auto& kv : in.shapes) {
     const hig::Shape& sh = kv.second;
     if (sh.name != "custom") continue;
     std::string path = sh.name_str;
     if (!file_exists(path) && !path.empty() && path[0] != '/' && file_exists(dir + path)) path = dir + path;
-    int ntri = 0;
-    HGX_TRY(hgx_read_shapes_file(c, path.c_str(), nullptr, 0, &ntri));
-    if (ntri < 1) return refuse("shape file '" + path + "' has no triangles");
-    std::vector<double> sd(8 * (size_t)ntri);
-    HGX_TRY(hgx_read_shapes_file(c, path.c_str(), sd.data(), ntri, &ntri));
-    auto& m = meshes[kv.first];
-    HGX_TRY(m.first.reserve(sizeof(double) * sd.size()));
-    HGX_CUDA(cudaMemcpyAsync(m.first.p, sd.data(), sizeof(double) * sd.size(), cudaMemcpyHostToDevice, st));
-    m.second = ntri;
-    HGX_CUDA(cudaStreamSynchronize(st));
+    long long size = -1, mtime = -1;
+    struct stat sb;
+    if (stat(path.c_str(), &sb) == 0) {
+      size = (long long)sb.st_size;
+      mtime = (long long)sb.st_mtim.tv_sec * 1000000000LL + sb.st_mtim.tv_nsec;
+    }
+    MeshTuples& m = w.meshes[path];
+    if (size < 0 || m.ntri < 1 || m.size != size || m.mtime_ns != mtime) {
+      m.ntri = 0;
+      int ntri = 0;
+      HGX_TRY(hgx_read_shapes_file(c, path.c_str(), nullptr, 0, &ntri));
+      if (ntri < 1) return refuse("shape file '" + path + "' has no triangles");
+      std::vector<double> sd(8 * (size_t)ntri);
+      HGX_TRY(hgx_read_shapes_file(c, path.c_str(), sd.data(), ntri, &ntri));
+      HGX_TRY(m.tri.reserve(sizeof(double) * sd.size()));
+      HGX_CUDA(cudaMemcpyAsync(m.tri.p, sd.data(), sizeof(double) * sd.size(), cudaMemcpyHostToDevice, st));
+      HGX_CUDA(cudaStreamSynchronize(st));
+      m.ntri = ntri;
+      m.size = size;
+      m.mtime_ns = mtime;
+    }
+    meshes[kv.first] = &m;
   }
 
   const Rot rot_phi = Rot::axis(2, phi);  // rot_ = RotMatrix_t(2, phi)
@@ -762,8 +774,8 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
           return refuse("shape '" + sh.key + "': '" + sh.name + "' has no analytic form factor here");
         for (const hig::vec3& loc : ekv.second) {
           if (sh.name == "custom") {
-            const auto& m = meshes.at(skey);
-            HGX_TRY(hgx_ff_triangles_q(c, g, (const double*)m.first.p, m.second, srot.m, precision,
+            const MeshTuples& m = *meshes.at(skey);
+            HGX_TRY(hgx_ff_triangles_q(c, g, (const double*)m.tri.p, m.ntri, srot.m, precision,
                                        beff.p, HGX_C128));
           } else {
             const double tv[3] = {loc[0], loc[1], loc[2]};
@@ -802,6 +814,62 @@ int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
     HGX_CUDA(cudaMemcpyAsync(image, w.img.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   }
   return hgx_synchronize(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_image_size: null handle");
+  if (nrow) *nrow = h->in.compute.resolution[1];
+  if (ncol) *ncol = h->in.compute.resolution[0];
+  return HGX_OK;
+}
+
+int hgx_hig_compute_gisaxs(hgx_ctx c, hgx_hig h, int precision, double* image) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: null argument");
+  const hig::Scattering& sc = h->in.scattering;
+  if (scan_count(sc.alphai[0], sc.alphai[1], sc.alphai[2], true) > 1 ||
+      scan_count(sc.inplanerot[0], sc.inplanerot[1], sc.inplanerot[2], false) > 1 ||
+      scan_count(sc.tilt[0], sc.tilt[1], sc.tilt[2], false) > 1)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: more than one alpha_i, phi or tilt (the "
+                                     "reference's compute_gisaxs refuses scans; hgx_hig_compute_scan_point "
+                                     "runs them)");
+  return compute_at(c, h, precision, sc.alphai[0], sc.inplanerot[0], image);
+}
+
+int hgx_hig_scan_size(hgx_hig h, int* nalphai, int* nphi, int* ntilt) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_scan_size: null handle");
+  const hig::Scattering& sc = h->in.scattering;
+  if (nalphai) *nalphai = std::max(0, scan_count(sc.alphai[0], sc.alphai[1], sc.alphai[2], true));
+  if (nphi) *nphi = std::max(0, scan_count(sc.inplanerot[0], sc.inplanerot[1], sc.inplanerot[2], false));
+  if (ntilt) *ntilt = std::max(0, scan_count(sc.tilt[0], sc.tilt[1], sc.tilt[2], false));
+  return HGX_OK;
+}
+
+int hgx_hig_scan_point(hgx_hig h, int p, double* alphai_deg, double* phi_deg, double* tilt_deg) {
+  if (!h) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_scan_point: null handle");
+  int na = 0, np = 0, nt = 0;
+  HGX_TRY(hgx_hig_scan_size(h, &na, &np, &nt));
+  if (p < 0 || (long)p >= (long)na * np * nt) return fail(HGX_ERR_INVALID_ARG, "hgx_hig_scan_point: index out of range");
+  const int i = p / (np * nt), j = (p / nt) % np, k = p % nt;
+  // the values as run_all_gisaxs's loops accumulate them (x += step, from the minimum)
+  const hig::Scattering& sc = h->in.scattering;
+  double a = sc.alphai[0], f = sc.inplanerot[0], t = sc.tilt[0];
+  for (int q = 0; q < i; ++q) a += sc.alphai[2];
+  for (int q = 0; q < j; ++q) f += sc.inplanerot[2];
+  for (int q = 0; q < k; ++q) t += sc.tilt[2];
+  if (alphai_deg) *alphai_deg = a;
+  if (phi_deg) *phi_deg = f;
+  if (tilt_deg) *tilt_deg = t;
+  return HGX_OK;
+}
+
+int hgx_hig_compute_scan_point(hgx_ctx c, hgx_hig h, int precision, int p, double* image) {
+  double a = 0.0, f = 0.0;
+  HGX_TRY(hgx_hig_scan_point(h, p, &a, &f, nullptr));
+  return compute_at(c, h, precision, a, f, image);
 }
 
 }  // extern "C"

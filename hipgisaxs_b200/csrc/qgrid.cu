@@ -5,7 +5,10 @@
 // q-space rows and then reversed so that row 0 is the top of the detector; 2theta per
 // column computed with cos(alpha_f) of the FIRST (unreversed) row for every row, as the
 // reference does; flattened qx, qy, qz per pixel; the 4 DWBA blocks
-// [kzf - kzi, -kzf - kzi, kzf + kzi, -kzf + kzi].
+// [kzf - kzi, -kzf - kzi, kzf + kzi, -kzf + kzi].  Built without fused multiply-adds (the
+// build passes -fmad=false for this file): 2theta = acos(t) with t just below 1 near qy = 0
+// turns a one-ulp change of t into up to ~1e-9 relative in qy, so t is rounded as the
+// reference rounds it.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -50,6 +53,22 @@ __device__ __forceinline__ double2 csqrt_d(double re, double im) {
   return make_double2(fabs(im) / (2.0 * t), copysign(t, im));
 }
 
+// the four DWBA blocks of pixel p (create_qz_extended, src/model/qgrid.cpp:102-127)
+__device__ __forceinline__ void qz_extend_point(double qzp, double k0, double sin_ai, double dn2_re,
+                                                double dn2_im, long p, long n, double2* __restrict__ qz_ext) {
+  double kzi0 = -1 * k0 * sin_ai;
+  double2 r = csqrt_d(sin_ai * sin_ai - dn2_re, -dn2_im);
+  double2 kzi = make_double2(-k0 * r.x, -k0 * r.y);
+  double kzf0 = qzp + kzi0;
+  double2 s = csqrt_d(kzf0 * kzf0 - k0 * k0 * dn2_re, -(k0 * k0 * dn2_im));
+  double sg = kzf0 < 0 ? -1.0 : 1.0;
+  double2 kzf = make_double2(sg * s.x, sg * s.y);
+  qz_ext[p] = make_double2(kzf.x - kzi.x, kzf.y - kzi.y);
+  qz_ext[n + p] = make_double2(-kzf.x - kzi.x, -kzf.y - kzi.y);
+  qz_ext[2 * n + p] = make_double2(kzf.x + kzi.x, kzf.y + kzi.y);
+  qz_ext[3 * n + p] = make_double2(-kzf.x + kzi.x, -kzf.y + kzi.y);
+}
+
 __global__ void qgrid_pixels_kernel(QgridArgs a, const double* __restrict__ alpha,
                                     const double* __restrict__ theta, double* __restrict__ qx,
                                     double* __restrict__ qy, double* __restrict__ qz,
@@ -64,18 +83,26 @@ __global__ void qgrid_pixels_kernel(QgridArgs a, const double* __restrict__ alph
   qy[p] = a.k0 * (cos(alf) * sin(tth));
   double qzp = a.k0 * (sin(alf) + sin_ai);
   qz[p] = qzp;
-  // create_qz_extended
-  double kzi0 = -1 * a.k0 * sin_ai;
-  double2 r = csqrt_d(sin_ai * sin_ai - a.dn2_re, -a.dn2_im);
-  double2 kzi = make_double2(-a.k0 * r.x, -a.k0 * r.y);
-  double kzf0 = qzp + kzi0;
-  double2 s = csqrt_d(kzf0 * kzf0 - a.k0 * a.k0 * a.dn2_re, -(a.k0 * a.k0 * a.dn2_im));
-  double sg = kzf0 < 0 ? -1.0 : 1.0;
-  double2 kzf = make_double2(sg * s.x, sg * s.y);
-  qz_ext[p] = make_double2(kzf.x - kzi.x, kzf.y - kzi.y);
-  qz_ext[n + p] = make_double2(-kzf.x - kzi.x, -kzf.y - kzi.y);
-  qz_ext[2 * n + p] = make_double2(kzf.x + kzi.x, kzf.y + kzi.y);
-  qz_ext[3 * n + p] = make_double2(-kzf.x + kzi.x, -kzf.y + kzi.y);
+  qz_extend_point(qzp, a.k0, sin_ai, a.dn2_re, a.dn2_im, p, n, qz_ext);
+}
+
+// create_qz_extended alone, for another incidence angle over the same detector grid (the
+// reference keeps the grid of its first alpha_i and extends qz for each angle of a scan)
+__global__ void qgrid_reextend_kernel(const double* __restrict__ qz, long n, double k0, double alpha_i,
+                                      double dn2_re, double dn2_im, double2* __restrict__ qz_ext) {
+  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  qz_extend_point(qz[p], k0, sin(alpha_i), dn2_re, dn2_im, p, n, qz_ext);
+}
+
+int qgrid_reextend(hgx_qgrid g, double alpha_i, double k0, double dn2_re, double dn2_im) {
+  if (!g || !g->qz_det) return fail(HGX_ERR_INVALID_ARG, "qgrid_reextend: not a grid made by hgx_qgrid_create");
+  const long n = (long)g->nqy;
+  cudaStream_t st = g->ctx->stream;
+  qgrid_reextend_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g->qz_det, n, k0, alpha_i, dn2_re, dn2_im,
+                                                                     g->qz);
+  HGX_CUDA(cudaGetLastError());
+  return qgrid_finalize(g);
 }
 
 }  // namespace hgx

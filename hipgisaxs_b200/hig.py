@@ -147,6 +147,46 @@ class HiGInput:
         check(lib().hgx_hig_compute_gisaxs(ctx.handle, self._h, PRECISION[precision], C.c_void_p(ptr)))
         return out
 
+    # angle scans (HipGISAXS::run_all_gisaxs)
+    def scan_size(self):
+        """(n_alphai, n_phi, n_tilt) of the scattering block's scans."""
+        a, p, t = C.c_int(), C.c_int(), C.c_int()
+        check(lib().hgx_hig_scan_size(self._h, C.byref(a), C.byref(p), C.byref(t)))
+        return a.value, p.value, t.value
+
+    def scan_points(self):
+        """[(alpha_i, phi, tilt)] in degrees, in the reference's loop order."""
+        na, nph, nt = self.scan_size()
+        out = []
+        for i in range(na * nph * nt):
+            a, p, t = C.c_double(), C.c_double(), C.c_double()
+            check(lib().hgx_hig_scan_point(self._h, i, C.byref(a), C.byref(p), C.byref(t)))
+            out.append((a.value, p.value, t.value))
+        return out
+
+    def compute_scan_point(self, ctx: Context, p: int, precision: str = "f64", out=None):
+        """The image of scan point p (hgx_hig_compute_scan_point)."""
+        nrow, ncol = self.image_size()
+        if out is None:
+            out = np.zeros((nrow, ncol))
+        ptr = out.data_ptr() if _is_tensor(out) else out.ctypes.data
+        check(lib().hgx_hig_compute_scan_point(ctx.handle, self._h, PRECISION[precision], int(p),
+                                               C.c_void_p(ptr)))
+        return out
+
+    def run_all_gisaxs(self, ctx: Context, precision: str = "f64"):
+        """Every scan point's image and, per alpha_i with more than one phi or tilt, their sum
+        (the reference's "averaged" output): (images [(alpha_i, phi, tilt, image)],
+        sums {alpha_i: image})."""
+        na, nph, nt = self.scan_size()
+        images, sums = [], {}
+        for i, (a, p, t) in enumerate(self.scan_points()):
+            img = self.compute_scan_point(ctx, i, precision)
+            images.append((a, p, t, img))
+            if nph > 1 or nt > 1:
+                sums[a] = img.copy() if a not in sums else sums[a] + img
+        return images, sums
+
     # fitting (HiGInput::update_params, HipGISAXSObjectiveFunction)
     def fit_keys(self):
         """The fit parameters' keys in the order of an x vector (fit_param_keys)."""
@@ -167,6 +207,12 @@ class HiGInput:
         check(lib().hgx_hig_fit_reference(self._h, 0, p, 4096, m, 4096, C.byref(npar), C.byref(nperp)))
         return {"path": p.value.decode(), "mask": m.value.decode(), "npar": npar.value,
                 "nperp": nperp.value}
+
+    def override_qregion(self, ny: int, nz: int, i: int = 0):
+        """HipGISAXS::override_qregion: the simulation re-gridded to an ny x nz reference image
+        over the referencedata block's fit region."""
+        check(lib().hgx_hig_override_qregion(self._h, int(ny), int(nz), int(i)))
+        self._reload()
 
     def fit_algorithms(self):
         """The analysis algorithms in file order: [{"name", "metric", "tolerance",

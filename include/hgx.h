@@ -421,6 +421,22 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * scalings and ranged repetitions (the reference's seeded Mersenne Twister).  Other
  * descriptions return HGX_ERR_INVALID_ARG naming the feature. */
 int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
+/* Angle scans, as HipGISAXS::run_all_gisaxs walks them (src/sim/hipgisaxs_main.cpp:283-613):
+ * the numbers of incidence angles, in-plane rotations and tilts (alphai, inplanerot, tilt
+ * blocks: (max - min) / step + 1 truncated, 1 for a zero step; alphai's max raised to its min),
+ * and scan point p = (i * nphi + j) * ntilt + k with its angles in degrees accumulated from the
+ * minimum as the reference's loops accumulate them.  hgx_hig_compute_scan_point is
+ * hgx_hig_compute_gisaxs at point p: the detector grid of the first alpha_i (HipGISAXS::init),
+ * qz_extended and the Fresnel coefficients at the point's alpha_i, the structures rotated by
+ * its phi (run_gisaxs does not use the tilt).  The reference's per-alpha_i "averaged" output
+ * is the plain sum of the point images over phi and tilt, in point order. */
+/* The computation block's pathprefix ("." by default) and runname as written ("" when not
+ * given); the reference writes a run's files under pathprefix/runname_<YYYYmmdd_HHMMSS>
+ * (run_<...> without a runname; ComputeParams, src/model/compute_params.cpp:24-78). */
+int hgx_hig_output_names(hgx_hig h, char* pathprefix, size_t prefix_cap, char* runname, size_t run_cap);
+int hgx_hig_scan_size(hgx_hig h, int* nalphai, int* nphi, int* ntilt);
+int hgx_hig_scan_point(hgx_hig h, int p, double* alphai_deg, double* phi_deg, double* tilt_deg);
+int hgx_hig_compute_scan_point(hgx_ctx ctx, hgx_hig h, int precision, int p, double* image);
 
 /* The fitting block of a HiG description: parameters in key order (the order of
  * HiGInput::fit_param_keys, which the reference's fitters use for their x vectors). */
@@ -444,6 +460,12 @@ int hgx_hig_fit_update(hgx_hig h, const double* x, int nx);
  * not given).  Any output may be NULL. */
 int hgx_hig_fit_reference(hgx_hig h, int i, char* path, size_t path_cap, char* mask, size_t mask_cap,
                           int* npar, int* nperp);
+/* HipGISAXS::override_qregion (src/sim/hipgisaxs_main.cpp:236-277): the simulation re-gridded
+ * to a reference image of ny x nz pixels over the referencedata block's fit region (regmin,
+ * regmax; 0 when not given, as in the reference), i.e. the computation block's resolution and
+ * q-space region replaced (QGrid::update, src/model/qgrid.cpp:133-197).  Only a qspace output
+ * region (the reference has not implemented the others).  Host only. */
+int hgx_hig_override_qregion(hgx_hig h, int ny, int nz, int i);
 /* The fitting block's analysis algorithms in file order (HiGInput::analysis_algo,
  * analysis_distance_metric, analysis_tolerance, analysis_regularization,
  * include/config/hig_input.hpp:338-345): the name ("pso", "lmvm", "pounders", "bruteforce",

@@ -288,6 +288,13 @@ class HipGISAXSG {
   bool gaussian_smearing(real_t*& data, real_t sigma);               // in place
   bool normalize(real_t*& data, unsigned int size);                  // in place
   bool save_gisaxs(real_t* final_data, std::string filename);        // the .out text
+  // the main simulation program's run (HipGISAXS::run_all_gisaxs): every alpha_i x phi x tilt
+  // of the scattering block, each image written as output_dir()/gisaxs_ai=<a>_rot=<phi>_tilt=<t>.out
+  // and, per alpha_i with more than one phi or tilt, their sum as gisaxs_ai=<a>_averaged.out;
+  // output_dir() = pathprefix/runname_<timestamp>, created here (the .tif images of the
+  // reference's image writer are not written)
+  bool run_all_gisaxs(int x_min = 0, int x_max = 0, int x_step = 0);
+  const std::string& output_dir() const;
   unsigned int nrow() const;
   unsigned int ncol() const;
   real_t k0() const;
@@ -315,8 +322,8 @@ class HiGObjectiveFunctionG {
   HiGObjectiveFunctionG& operator=(const HiGObjectiveFunctionG&) = delete;
 
   bool ok() const;
-  // the fitting block's reference data and mask (i = 0); false when the image's size differs
-  // from the detector's (the reference then re-grids its simulation, which is not done here)
+  // the fitting block's reference data and mask (i = 0); an image whose size differs from the
+  // detector's re-grids the simulation to it over the block's fit region (override_qregion)
   bool set_reference_data(int i);
   bool set_reference_data(const real_vec_t& ref, const std::vector<unsigned int>& mask);
   bool simulate_and_set_ref(const real_vec_t& x);    // the simulation at x as the reference

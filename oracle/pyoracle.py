@@ -112,6 +112,17 @@ class Grid:
         else:
             self.activate()
 
+    def reextend(self, alpha_i_deg):
+        """create_qz_extended for another incidence angle over this detector grid (the
+        reference's scans keep the grid of the first angle); later calls that take the grid's
+        alpha_i (propagation_coeffs) use the new one."""
+        assert self.backend == "port"
+        self.alpha_i = alpha_i_deg * 3.141592653589793 / 180
+        rc = lib("port").orc_qz_extended(C.c_int(self.n), _p(self.qz), C.c_double(self.k0),
+                                         C.c_double(self.alpha_i), C.c_double(self.dn2[0]),
+                                         C.c_double(self.dn2[1]), _p(self.qz_ext.view(np.float64)))
+        assert rc == 0, rc
+
     def activate(self):
         """Make this grid the reference's QGrid singleton (ref backend only)."""
         if self.backend != "ref":
@@ -598,13 +609,17 @@ def scale_plan(s, ngr, gw=None):
     return plan
 
 
-def compute_gisaxs(hig, hig_dir=".", rand=None):
+def compute_gisaxs(hig, hig_dir=".", rand=None, alpha_i=None, phi=None):
     """HipGISAXS::compute_gisaxs / run_gisaxs (src/sim/hipgisaxs_main.cpp:630-1440) for the
     configurations hgx_hig_compute_gisaxs supports, composed from this oracle's pinned pieces
     (QGrid, MultiLayer::propagation_coeffs, the analytic and numeric form factors, the
     structure factors, the DWBA combination and the structure sum).  `hig`: the reader's
     JSON model (dict).  Orientations drawn by "range"/"random" call `rand` (default: the C
-    library's rand()) in the reference's order.  Returns the nrow x ncol image (FP64)."""
+    library's rand()) in the reference's order.  alpha_i, phi: a scan point's angles in
+    degrees (run_all_gisaxs, :283-613; default: the first of each): the detector grid stays
+    the first alpha_i's (HipGISAXS::init), qz_extended and the Fresnel coefficients take this
+    alpha_i (layer_qgrid_qz, propagation_coeffs, :779-785), the structures this phi.  Returns
+    the nrow x ncol image (FP64)."""
     rand = rand or _libc_rand()
     sc, cp = hig["scattering"], hig["computation"]
     value, unit = sc["photon_value"], sc["photon_unit"]
@@ -612,11 +627,13 @@ def compute_gisaxs(hig, hig_dir=".", rand=None):
     ncol, nrow = int(cp["resolution"][0]), int(cp["resolution"][1])
     (ymin, zmin), (ymax, zmax) = cp["minpoint"], cp["maxpoint"]
     G = Grid(ncol, nrow, ymin, zmin, ymax, zmax, sc["alphai"][0], kev, (0.0, 0.0))
+    if alpha_i is not None and alpha_i * 3.141592653589793 / 180 != G.alpha_i:
+        G.reextend(alpha_i)
     layers = [(l["refindex"][0], l["refindex"][1], l["thickness"], l["order"])
               for _, l in sorted(hig["layers"].items(), key=lambda kv: int(kv[0]))]
     fc = propagation_coeffs(G, layers, 0)  # particle layer order 0 (:779-785)
     pi = 3.141592653589793
-    rot_phi = rot_axis(2, sc["inplanerot"][0] * pi / 180)
+    rot_phi = rot_axis(2, (sc["inplanerot"][0] if phi is None else phi) * pi / 180)
     meshes = {}
     for key, sh in hig["shapes"].items():
         if sh["name"] == "custom":

@@ -14,6 +14,7 @@
 //   dist2.bin     the same with the sqrt_c_l2_residual metric (one value per pixel)
 //   dist3.bin     sqrt_unit_l2 after simulate_and_set_ref(5, 25, 12), at (5, 25, 12)
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <map>
 #include <stdexcept>
@@ -30,8 +31,38 @@ static bool save(const std::string& path, const double* v, size_t n) {
   return ok;
 }
 
+// argv[2] == "regrid": only the objective, whose reference image differs in size from the
+// detector; writes regrid.txt (n_par n_ver after set_reference_data) and dist_regrid.bin at
+// x = (4.2, 21, 3).
+static int regrid(const char* hig_file) {
+  hig::HiGObjectiveFunctionG obj(hig_file);
+  if (!obj.ok()) return 20;
+  const unsigned np0 = obj.n_par(), nv0 = obj.n_ver();
+  if (!obj.set_reference_data(0)) return 21;
+  hig::real_vec_t d = obj({4.2, 21.0, 3.0});
+  if (d.empty() || !save("dist_regrid.bin", d.data(), d.size())) return 22;
+  std::ofstream f("regrid.txt");
+  f << np0 << " " << nv0 << " " << obj.n_par() << " " << obj.n_ver() << " " << obj.simulator().ncol() << " "
+    << obj.simulator().nrow() << "\n";
+  return 0;
+}
+
+// argv[2] == "scan": HipGISAXSG::run_all_gisaxs of the file, the C library's rand() seeded with 1
+// after the device context exists; writes scan.txt with the output directory
+static int scan(const char* hig_file) {
+  hig::HipGISAXSG sim(0);
+  if (!sim.construct_input(hig_file) || !sim.init()) return 30;
+  srand(1);
+  if (!sim.run_all_gisaxs()) return 31;
+  std::ofstream f("scan.txt");
+  f << sim.output_dir() << "\n";
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 2) return 2;
+  if (argc > 2 && std::string(argv[2]) == "regrid") return regrid(argv[1]);
+  if (argc > 2 && std::string(argv[2]) == "scan") return scan(argv[1]);
   hig::HipGISAXSG sim(0);
   if (!sim.construct_input(argv[1]) || !sim.init()) return 3;
   const size_t n = (size_t)sim.nrow() * sim.ncol();

@@ -67,6 +67,40 @@ def test_compute_gisaxs_f32c_mesh(ctx, po):
 
 
 @pytest.mark.gpu
+def test_compute_gisaxs_mesh_kept_until_file_changes(ctx, po, tmp_path):
+    """The custom shape's triangles stay on the device between calls and are read again when
+    the shape file changes: each image equals the oracle's for the file as it is then."""
+    import shutil
+    import time
+    shutil.copy(os.path.join(HIG, "sim_two_structures.hig"), tmp_path / "m.hig")
+    obj = tmp_path / "octahedron.obj"
+    shutil.copy(os.path.join(HIG, "octahedron.obj"), obj)
+    d = read_hig(str(tmp_path / "m.hig"))
+
+    def both():
+        _srand(5)
+        img = d.compute_gisaxs(ctx)
+        _srand(5)
+        ref = po.compute_gisaxs(d.data, str(tmp_path))
+        assert np.abs(img - ref).max() / np.abs(ref).max() < 1e-11
+        return img
+
+    a = both()
+    np.testing.assert_array_equal(both(), a)  # the kept triangles
+    lines = []
+    for ln in obj.read_text().splitlines():
+        if ln.startswith("v "):
+            x, y, z = (float(t) * 1.3 for t in ln.split()[1:4])
+            ln = f"v {x!r} {y!r} {z!r}"
+        lines.append(ln)
+    obj.write_text("\n".join(lines) + "\n")
+    st = os.stat(obj)
+    os.utime(obj, ns=(st.st_atime_ns, st.st_mtime_ns + 5_000_000_000))
+    b = both()
+    assert np.abs(b - a).max() > 1e-3 * np.abs(a).max()
+
+
+@pytest.mark.gpu
 def test_compute_gisaxs_device_output(ctx, po):
     torch = pytest.importorskip("torch")
     d = read_hig(os.path.join(HIG, "paracrystal.hig"))
@@ -147,3 +181,40 @@ def test_objective_matches_oracle(ctx, po, metric):
     want = np.where(np.isfinite(want), want + reg / want.size, 1e8)
     assert got.shape == want.shape
     np.testing.assert_allclose(got, want, rtol=1e-10, atol=0)
+
+
+@pytest.mark.gpu
+def test_scan_points_match_oracle(ctx, po):
+    """run_all_gisaxs's scan on the device, point by point, against the oracle's composition
+    at each point's alpha_i and phi (grid of the first alpha_i, qz_extended and Fresnel
+    coefficients at the point's); the rand()-drawn orientations continue across points on
+    both sides.  The per-alpha_i sums over phi and tilt are the reference's "averaged" output."""
+    d = read_hig(os.path.join(HIG, "sim_scan.hig"))
+    pts = d.scan_points()
+    _srand(21)
+    images, sums = d.run_all_gisaxs(ctx)
+    _srand(21)
+    refs = [po.compute_gisaxs(d.data, HIG, alpha_i=a, phi=p) for a, p, _ in pts]
+    assert len(images) == len(refs) == 18
+    for (a, p, t, img), ref in zip(images, refs):
+        assert np.abs(img - ref).max() / np.abs(ref).max() < 1e-11, (a, p, t)
+    assert sorted(sums) == sorted({a for a, _, _ in pts})
+    for a in sums:
+        want = sum(ref for (pa, _, _), ref in zip(pts, refs) if pa == a)
+        assert np.abs(sums[a] - want).max() / np.abs(want).max() < 1e-11
+    # a different incidence angle changes the image; the first point equals compute_gisaxs of
+    # the description without scans
+    assert np.abs(images[0][3] - images[6][3]).max() > 1e-6 * np.abs(images[0][3]).max()
+    text = open(os.path.join(HIG, "sim_scan.hig")).read()
+    one = text.replace("alphai = { min = 0.12, max = 0.2, step = 0.04 }, inplanerot = { min = 0, max = 30, "
+                       "step = 15 }, tilt = { min = 0, max = 1, step = 1 }", "alphai = { min = 0.12 }")
+    assert one != text
+    import tempfile
+    with tempfile.TemporaryDirectory() as tdir:
+        p1 = os.path.join(tdir, "one.hig")
+        with open(p1, "w") as f:
+            f.write(one)
+        e = read_hig(p1)
+        _srand(21)
+        first = e.compute_gisaxs(ctx)
+    np.testing.assert_array_equal(first, images[0][3])

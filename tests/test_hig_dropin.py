@@ -129,3 +129,99 @@ def test_hig_driver_matches_oracle_and_api(ctx, po, tmp_path):
     np.testing.assert_allclose(load("dist0.bin"), want, rtol=1e-10)
     # a reference simulated at the truth: zero distance there
     assert abs(load("dist3.bin")[0]) < 1e-20
+
+
+_REGION = ('referencedata = { path = "ref.out", fitregion = { type = "qspace", '
+           'regmin = [ -0.8 0.05 ], regmax = [ 0.6 0.9 ] },')
+
+
+def _regrid_hig():
+    src = open(os.path.join(HIG, "fit_objective.hig")).read()
+    return src.replace('referencedata = { path = "ref.out",', _REGION)
+
+
+def test_override_qregion(tmp_path):
+    (tmp_path / "r.hig").write_text(_regrid_hig())
+    d = read_hig(str(tmp_path / "r.hig"))
+    assert d.image_size() == (28, 40)
+    d.override_qregion(30, 20)
+    assert d.image_size() == (20, 30)
+    assert d.param_resolution() == [30, 20]
+    assert d.param_output_minpoint() == (-0.8, 0.05) and d.param_output_maxpoint() == (0.6, 0.9)
+    # no fit region: the reference's zeros
+    e = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    e.override_qregion(10, 12)
+    assert e.param_output_minpoint() == (0.0, 0.0) and e.param_output_maxpoint() == (0.0, 0.0)
+    # refused: no referencedata block, an empty size, a pixel-space output region
+    with pytest.raises(hg.HgxError):
+        read_hig(os.path.join(HIG, "paracrystal.hig")).override_qregion(10, 10)
+    with pytest.raises(hg.HgxError):
+        d.override_qregion(0, 10)
+    (tmp_path / "p.hig").write_text(_regrid_hig().replace('type = "qspace", minpoint', 'type = "pixels", minpoint'))
+    p = read_hig(str(tmp_path / "p.hig"))
+    assert p.param_output_type() == "pixels"
+    with pytest.raises(hg.HgxError):
+        p.override_qregion(10, 10)
+
+
+@pytest.mark.gpu
+def test_objective_regrids_to_reference(ctx, po, tmp_path):
+    """A reference image of another size: the C++ objective re-grids the simulation over the
+    fit region (override_qregion) and its values equal the Python API's after the same
+    override, and the oracle's composition on the re-gridded description."""
+    exe = _build(tmp_path)
+    hig = tmp_path / "fit.hig"
+    hig.write_text(_regrid_hig())
+    d = read_hig(str(hig))
+    d.override_qregion(30, 20)
+    d.fit_update([5.0, 25.0, 12.0])
+    ref_img = po.compute_gisaxs(d.data, HIG)
+    assert ref_img.shape == (20, 30)
+    with open(tmp_path / "ref.out", "w") as f:
+        for row in ref_img:
+            f.write(" ".join(repr(float(v)) for v in row) + "\n")
+    r = subprocess.run([exe, str(hig), "regrid"], capture_output=True, text=True, timeout=300,
+                       cwd=str(tmp_path))
+    assert r.returncode == 0, (r.returncode, r.stdout + r.stderr)
+    assert (tmp_path / "regrid.txt").read_text().split() == ["40", "28", "30", "20", "30", "20"]
+    got = np.fromfile(tmp_path / "dist_regrid.bin")
+    x = [4.2, 21.0, 3.0]
+    e = read_hig(str(hig))
+    e.override_qregion(30, 20)
+    np.testing.assert_array_equal(got, e.objective(ctx, x, ref_img, None, "sqrt_unit_l2", 0.0))
+    e.fit_update(x)
+    img = po.compute_gisaxs(e.data, HIG)
+    sim = e.compute_gisaxs(ctx)
+    assert np.abs(sim - img).max() / np.abs(img).max() < 1e-11
+    want = po.fit_distance("sqrt_unit_l2", ref_img.ravel(), img.ravel(), None)
+    np.testing.assert_allclose(got, want, rtol=1e-10)
+
+
+@pytest.mark.gpu
+def test_run_all_gisaxs_writes_the_reference_files(ctx, po, tmp_path):
+    """HipGISAXSG::run_all_gisaxs on a scan: one .out file per (alpha_i, phi, tilt) named as the
+    reference names them, and the per-alpha_i sums, under runname_<timestamp>; their values are
+    the Python API's images (which the GPU scan test holds against the oracle) at the .out
+    text's 6 significant digits."""
+    import ctypes
+    import glob
+    exe = _build(tmp_path)
+    hig = os.path.join(HIG, "sim_scan.hig")
+    r = subprocess.run([exe, hig, "scan"], capture_output=True, text=True, timeout=600, cwd=str(tmp_path))
+    assert r.returncode == 0, (r.returncode, r.stdout + r.stderr)
+    outdir = (tmp_path / "scan.txt").read_text().strip()
+    assert os.path.basename(outdir).startswith("simscan_") and len(os.path.basename(outdir)) == len("simscan_") + 15
+    files = sorted(os.path.basename(f) for f in glob.glob(os.path.join(tmp_path, outdir, "*.out")))
+    d = read_hig(hig)
+    ctypes.CDLL(None).srand(1)  # as the driver seeds it
+    images, sums = d.run_all_gisaxs(ctx)
+
+    def fmt(v):
+        return "%g" % v
+
+    want = {f"gisaxs_ai={fmt(a)}_rot={fmt(p)}_tilt={fmt(t)}.out": img for a, p, t, img in images}
+    want.update({f"gisaxs_ai={fmt(a)}_averaged.out": img for a, img in sums.items()})
+    assert files == sorted(want)
+    for name, img in want.items():
+        got = np.loadtxt(os.path.join(tmp_path, outdir, name))
+        np.testing.assert_allclose(got, img, rtol=1e-5, atol=0)

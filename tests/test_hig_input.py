@@ -278,3 +278,37 @@ def test_fit_update_live_against_reference():
     d.fit_update(vals)
     diff = model_diff(d.data, gen.ref_updated(path, keys, vals))
     assert not diff, "\n".join(diff)
+
+
+def test_scan_points_follow_the_reference_loops(tmp_path):
+    """run_all_gisaxs's scan counts ((max - min) / step + 1 truncated; 1 for a zero step;
+    alphai's max raised to its min) and its angles accumulated from the minimum, alpha_i
+    outermost and tilt innermost."""
+    d = read_hig(os.path.join(HIG, "sim_scan.hig"))
+    assert d.scan_size() == (3, 3, 2)
+    want, a = [], 0.12
+    for _ in range(3):
+        p = 0.0
+        for _ in range(3):
+            t = 0.0
+            for _ in range(2):
+                want.append((a, p, t))
+                t += 1.0
+            p += 15.0
+        a += 0.04
+    assert d.scan_points() == want
+    text = open(os.path.join(HIG, "sim_scan.hig")).read()
+    for old, new, size in [
+        ("alphai = { min = 0.12, max = 0.2, step = 0.04 }", "alphai = { min = 0.12, max = 0.05, step = 0.04 }", (1, 3, 2)),
+        ("inplanerot = { min = 0, max = 30, step = 15 }", "inplanerot = { min = 30, max = 0, step = 15 }", (3, 0, 2)),
+        ("tilt = { min = 0, max = 1, step = 1 }", "tilt = { min = 0, max = 1, step = 0 }", (3, 3, 1)),
+    ]:
+        p = tmp_path / "s.hig"
+        p.write_text(text.replace(old, new))
+        e = read_hig(str(p))
+        assert e.scan_size() == size
+        assert len(e.scan_points()) == size[0] * size[1] * size[2]
+    from hipgisaxs_b200._capi import check, lib
+    for p in (-1, 18):
+        with pytest.raises(HgxError):
+            check(lib().hgx_hig_scan_point(d.handle, p, None, None, None))
