@@ -245,4 +245,53 @@ __device__ __forceinline__ zd sf_lattice_eval(const SfLat& a, const zd* m) {
   return t3 * sa * sb * sc;
 }
 
+// sf_lattice_eval for a quad of lanes that hold the four DWBA blocks of one q-point, when the
+// a- and b-direction factors do not depend on the block: m[0] and m[1] free of qz (the
+// rotation's first two rows have no z entry) and a.la[2] == 0 (the b factor squares lb[2]
+// instead of using qz, as the reference does).  Even lanes evaluate the a factor, odd lanes
+// the b factor, on one code path: 1 - cpow(e, N) and 1 - cexp(i q.b N) are both
+// 1 - exp(A) (cos B, sin B), with (A, B) = N log e (cpow_std's polar form; a positive real e
+// takes its real pow) or i q.b N.  The lane pair then swaps factors, and every lane forms
+// t3 * sa * sb * sc in the reference's order, so each value is the one sf_lattice_eval
+// gives.  All 32 lanes of the warp must call it together.
+__device__ __forceinline__ zd sf_lattice_eval_paired(const SfLat& a, const zd* m, bool odd) {
+  const double eps = DBL_EPSILON;
+  const zd one(1.0, 0.0);
+  const double N = odd ? a.rep[1] : a.rep[0];
+  const zd iq = odd ? times_i(m[0] * a.lb[0] + m[1] * a.lb[1] + a.lb[2] * a.lb[2])
+                    : times_i(m[0] * a.la[0] + m[1] * a.la[1] + m[2] * a.la[2]);
+  const zd e = cexp_call(iq);
+  zd X;
+  if (!odd && e.y == 0.0 && e.x > 0.0) {
+    X = one - zd(pow(e.x, N), 0.0);
+  } else {
+    zd arg;
+    if (odd) {
+      arg = iq * N;
+    } else {
+      const zd t = clog_(e);
+      arg = zd(N * t.x, N * t.y);
+    }
+    const double r = exp(arg.x);
+    double s, c;
+    sincos(arg.y, &s, &c);
+    X = one - zd(r * c, r * s);
+  }
+  const zd Y = one - e;
+  zd f = (fabs(Y.y) > eps || fabs(Y.x) > eps) ? X / Y : zd(N, 0.0);
+  f = cpow_call(e, (1.0 - N) / 2.0) * f;
+  const zd g(__shfl_xor_sync(0xffffffffu, f.x, 1), __shfl_xor_sync(0xffffffffu, f.y, 1));
+  const zd sa = odd ? g : f, sb = odd ? f : g;
+
+  zd e_iqc = cexp_call(times_i(m[0] * a.lc[0] + m[1] * a.lc[1] + m[2] * a.lc[2]));
+  zd Xc = one - cpow_call(e_iqc, a.rep[2]);
+  zd Yc = one - e_iqc;
+  zd sc = (fabs(Yc.y) > eps || fabs(Yc.x) > eps) ? Xc / Yc : zd(a.rep[2], 0.0);
+  sc = cpow_call(e_iqc, (1.0 - a.rep[2]) / 2.0) * sc;
+
+  zd t3 = m[0] * a.center[0] + m[1] * a.center[1] + m[2] * a.center[2];
+  t3 = cexp_call(zd(-t3.y, t3.x));
+  return t3 * sa * sb * sc;
+}
+
 }  // namespace hgx

@@ -154,7 +154,11 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
           L.rep[d] = sp[si].rep[d];
           L.center[d] = gp[9 + d];
         }
-        sfv = sf_lattice_eval(L, mr);
+        // the grain's rotation keeps qz out of m[0], m[1] (uniform across the warp: one grain)
+        if (gp[2] == 0.0 && gp[5] == 0.0 && L.la[2] == 0.0)
+          sfv = sf_lattice_eval_paired(L, mr, (k & 1) != 0);
+        else
+          sfv = sf_lattice_eval(L, mr);
       }
       const zd term = fc * sfv * ff;
       zd sum(0, 0);
