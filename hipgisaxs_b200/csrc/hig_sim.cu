@@ -750,6 +750,13 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
       ++si;
       continue;
     }
+    // the paracrystal and Percus-Yevick structure factors do not depend on the grain
+    if (s.type == "paracrystal") {
+      HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1], s.pc_dist[0],
+                                 s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
+    } else if (s.type == "percusyevick") {
+      HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
+    }
     for (int gi = 0; gi < ngr; ++gi) {
       const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
                       Rot::axis(ax1, nn[gi]);
@@ -776,12 +783,15 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
         const int code = shape_code(sh.name);
         if (sh.name != "custom" && code < 0)
           return refuse("shape '" + sh.key + "': '" + sh.name + "' has no analytic form factor here");
+        // a custom shape ignores its location: its form factor at this rotation is computed once
+        // and added once per location, as the reference adds it
+        if (sh.name == "custom" && !ekv.second.empty()) {
+          const MeshTuples& m = *meshes.at(skey);
+          HGX_TRY(hgx_ff_triangles_q(c, g, (const double*)m.tri.p, m.ntri, srot.m, precision, beff.p,
+                                     HGX_C128));
+        }
         for (const hig::vec3& loc : ekv.second) {
-          if (sh.name == "custom") {
-            const MeshTuples& m = *meshes.at(skey);
-            HGX_TRY(hgx_ff_triangles_q(c, g, (const double*)m.tri.p, m.ntri, srot.m, precision,
-                                       beff.p, HGX_C128));
-          } else {
+          if (sh.name != "custom") {
             const double tv[3] = {loc[0], loc[1], loc[2]};
             HGX_TRY(hgx_ff_analytic_params(c, g, code, (int)(prm.size() / 7), prm.data(), 0.0, 0.0, tv,
                                            srot.m, beff.p, HGX_C128));
@@ -793,11 +803,8 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
       // the grain's structure factors and intensity terms, one per scaling/repetition sample
       for (int k = 0; k < nscale; ++k) {
         const ScaleEntry& e = plan[(size_t)gi * nscale + k];
-        if (s.type == "paracrystal") {
-          HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1],
-                                     s.pc_dist[0], s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, bsf.p, HGX_C128));
-        } else if (s.type == "percusyevick") {
-          HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
+        if (s.type == "paracrystal" || s.type == "percusyevick") {
+          // grain-independent: computed once per structure, before the grain loop
         } else {
           const double abc9[9] = {e.la[0], e.la[1], e.la[2], e.lb[0], e.lb[1], e.lb[2], e.lc[0], e.lc[1], e.lc[2]};
           const double one[3] = {1.0, 1.0, 1.0};

@@ -30,7 +30,7 @@ def test_hig_qgrid_matches_oracle(ctx, po, name):
 
 SIM = ["sim_cylinders_hcp.hig", "sim_two_structures.hig", "paracrystal.hig", "percus_yevick.hig",
        "include_main.hig", "sim_scaling.hig", "sim_scaling_mixed.hig", "sim_repetition.hig",
-       "sim_orientations.hig", "sim_shapes.hig"]
+       "sim_orientations.hig", "sim_shapes.hig", "sim_mesh_paracrystal.hig"]
 
 
 def _srand(seed):
