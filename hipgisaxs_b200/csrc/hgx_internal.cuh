@@ -70,7 +70,7 @@ struct HigWork {
   hgx_qgrid grid = nullptr;
   double key[8] = {0};
   double ext_alpha = 0.0;  // the incidence angle the grid's qz blocks were extended for
-  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj;
+  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj, saxs_qz;
   std::map<std::string, MeshTuples> meshes;  // by resolved path
 };
 }  // namespace hgx

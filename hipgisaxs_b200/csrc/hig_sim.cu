@@ -27,8 +27,15 @@
 // Refused with HGX_ERR_INVALID_ARG, naming the feature: clock-seeded random grain positions,
 // "bragg" orientations (the reference's search reads q-grid extents it never sets and fails),
 // structure correlations other than none (the reference indexes its single grain image as if
-// it held one per grain), sliced layers (nslices > 1), SAXS, and angle scans (more than one
-// alpha_i, phi or tilt: compute_gisaxs itself refuses those).
+// it held one per grain), sliced layers (nslices > 1), experiments other than gisaxs and saxs,
+// and angle scans in hgx_hig_compute_gisaxs (more than one alpha_i, phi or tilt:
+// compute_gisaxs itself refuses those; hgx_hig_compute_scan_point runs them).
+//
+// SAXS (expt = "saxs") follows run_gisaxs's other branch: the form factor as in GISAXS (its
+// first block), the lattice structure factor at the detector's real qz, no Fresnel
+// coefficients, and the intensity assigned rather than added, so a structure's image is its
+// last grain's last scaling sample; only that one is computed (the orientations of all grains
+// are still drawn, so rand() advances as in the reference).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdlib.h>
@@ -65,6 +72,28 @@ __global__ void add_scaled_kernel(long n, double dre, double dim, const double2*
   f.x = __dadd_rn(f.x, re);
   f.y = __dadd_rn(f.y, im);
   ff[i] = f;
+}
+
+// The SAXS intensity of one grain and scaling sample (run_gisaxs, :1099-1103): the form
+// factor's first block (the reference sizes it for the extended qz in either experiment),
+// the structure factor at the detector's real qz; the reference assigns (=) where GISAXS
+// accumulates, so each sample replaces the structure's image.  Unfused products and sums, as
+// the reference's complex arithmetic rounds them.
+__global__ void saxs_intensity_kernel(long n, double w, const double2* __restrict__ sf,
+                                      const double2* __restrict__ ff, double* __restrict__ out) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 a = sf[i], b = ff[i];
+  const double ar = __dmul_rn(w, a.x), ai = __dmul_rn(w, a.y);
+  const double tr = __dsub_rn(__dmul_rn(ar, b.x), __dmul_rn(ai, b.y));
+  const double ti = __dadd_rn(__dmul_rn(ar, b.y), __dmul_rn(ai, b.x));
+  out[i] = __dadd_rn(__dmul_rn(tr, tr), __dmul_rn(ti, ti));
+}
+
+// qz of the detector as complex values (imaginary part 0), for SAXS structure factors
+__global__ void real_to_complex_kernel(long n, const double* __restrict__ x, double2* __restrict__ z) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = make_double2(x[i], 0.0);
 }
 
 // The fused grain loop (structures whose unit cell holds analytic shapes only): a quad of
@@ -619,7 +648,8 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
   auto refuse = [](const std::string& why) {
     return fail(HGX_ERR_INVALID_ARG, "hgx_hig_compute_gisaxs: " + why);
   };
-  if (sc.expt != "gisaxs") return refuse("experiment '" + sc.expt + "': only gisaxs (DWBA) is supported");
+  if (sc.expt != "gisaxs" && sc.expt != "saxs")  // StructureFactor refuses the others (sf.cpp:100-102)
+    return refuse("experiment '" + sc.expt + "': only gisaxs and saxs are defined");
   if (cp.nslices > 1) return refuse("sliced layers (nslices > 1) are not supported");
   if (cp.structcorrelation != "null" && cp.structcorrelation != "nGnE")
     return refuse("structure correlation '" + cp.structcorrelation + "' is not supported");
@@ -682,6 +712,20 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
   HGX_TRY(hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(),
                                  k0, alpha_s, 0, nullptr, (double*)bfc.p, 0));
   HGX_CUDA(cudaMemsetAsync(bI.p, 0, sizeof(double) * n * nstruct, st));
+  // SAXS: the lattice structure factor takes the detector's real qz (sf.cpp:199-200)
+  const bool saxs = sc.expt == "saxs";
+  struct GridGuard {
+    hgx_qgrid g = nullptr;
+    ~GridGuard() {
+      if (g) hgx_qgrid_destroy(g);
+    }
+  } gs;
+  if (saxs) {
+    HGX_TRY(w.saxs_qz.reserve(sizeof(double2) * n));
+    real_to_complex_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, g->qz_det, (double2*)w.saxs_qz.p);
+    HGX_CUDA(cudaGetLastError());
+    HGX_TRY(hgx_qgrid_from_arrays(c, (int)n, g->qx, g->qy, (int)n, (const double*)w.saxs_qz.p, g->ncol, &gs.g));
+  }
 
   // custom shapes: triangle tuples on the device, kept by the context across calls and read
   // again only when the file changes (the reference reads them on every form-factor call)
@@ -744,7 +788,7 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
       else if (shape_code(shp->second.name) < 0)
         return refuse("shape '" + shp->second.key + "': '" + shp->second.name + "' has no analytic form factor here");
     }
-    if (all_analytic) {
+    if (all_analytic && !saxs) {
       HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, plan, nscale,
                               (const double2*)bfc.p, Is));
       ++si;
@@ -757,7 +801,7 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     } else if (s.type == "percusyevick") {
       HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, bsf.p, HGX_C128));
     }
-    for (int gi = 0; gi < ngr; ++gi) {
+    for (int gi = saxs ? std::max(ngr - 1, 0) : 0; gi < ngr; ++gi) {  // SAXS: the last grain's image stands
       const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
                       Rot::axis(ax1, nn[gi]);
       const double ddv[3] = {dd[gi], dd[gi + ngr], dd[gi + 2 * ngr]};
@@ -801,16 +845,23 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
         }
       }
       // the grain's structure factors and intensity terms, one per scaling/repetition sample
-      for (int k = 0; k < nscale; ++k) {
+      for (int k = saxs ? std::max(nscale - 1, 0) : 0; k < nscale; ++k) {  // SAXS: the last sample stands
         const ScaleEntry& e = plan[(size_t)gi * nscale + k];
         if (s.type == "paracrystal" || s.type == "percusyevick") {
-          // grain-independent: computed once per structure, before the grain loop
+          // grain-independent: computed once per structure, before the grain loop (in SAXS the
+          // reference reads its first N values, the ones computed here for the first block)
         } else {
           const double abc9[9] = {e.la[0], e.la[1], e.la[2], e.lb[0], e.lb[1], e.lb[2], e.lc[0], e.lc[1], e.lc[2]};
           const double one[3] = {1.0, 1.0, 1.0};
-          HGX_TRY(hgx_sf_lattice(c, g, abc9, e.rep, one, center, rot.m, bsf.p, HGX_C128));
+          HGX_TRY(hgx_sf_lattice(c, saxs ? gs.g : g, abc9, e.rep, one, center, rot.m, bsf.p, HGX_C128));
         }
-        HGX_TRY(hgx_dwba_combine(c, n, (const double*)bfc.p, (const double*)bsf.p, bff.p, HGX_C128, e.w, Is));
+        if (saxs) {
+          saxs_intensity_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, e.w, (const double2*)bsf.p,
+                                                                          (const double2*)bff.p, Is);
+          HGX_CUDA(cudaGetLastError());
+        } else {
+          HGX_TRY(hgx_dwba_combine(c, n, (const double*)bfc.p, (const double*)bsf.p, bff.p, HGX_C128, e.w, Is));
+        }
       }
     }
     ++si;

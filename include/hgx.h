@@ -415,7 +415,9 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * structure factor (lattice, paracrystal or Percus-Yevick) and the DWBA intensity with the
  * layer stack's Fresnel coefficients; the structures summed with their iratios.  image:
  * nrow x ncol doubles (host or device).  precision: HGX_F64, or HGX_F32C for the mesh form
- * factors.  Supported: GISAXS, one alpha_i/phi/tilt, nslices <= 1, no structure correlation,
+ * factors.  Supported: GISAXS and SAXS (expt "saxs": run_gisaxs's Born branch, :1099-1103, whose
+ * assignment leaves each structure the image of its last grain's last scaling sample), one
+ * alpha_i/phi/tilt, nslices <= 1, no structure correlation,
  * regular grain grids; "single", "range", "random" (drawn with the C library's rand() in the
  * reference's order), "gaussian", "normal" and "cauchy" orientations; gaussian/cauchy grain
  * scalings and ranged repetitions (the reference's seeded Mersenne Twister).  Other

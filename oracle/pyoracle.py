@@ -622,6 +622,7 @@ def compute_gisaxs(hig, hig_dir=".", rand=None, alpha_i=None, phi=None):
     the nrow x ncol image (FP64)."""
     rand = rand or _libc_rand()
     sc, cp = hig["scattering"], hig["computation"]
+    saxs = sc["expt"] == "saxs"
     value, unit = sc["photon_value"], sc["photon_unit"]
     kev = value / 1000 if unit == "ev" else value  # HipGISAXS::init, :146-160
     ncol, nrow = int(cp["resolution"][0]), int(cp["resolution"][1])
@@ -737,9 +738,16 @@ def compute_gisaxs(hig, hig_dir=".", rand=None, alpha_i=None, phi=None):
                 elif s["type"] == "percusyevick":
                     py = s["percusyevick"]
                     sf = sf_percus_yevick(G, py["diameter"], py["volfraction"], py["dims"])
+                elif saxs:  # the detector's real qz (sf.cpp:199-200)
+                    sf = sf_lattice_arrays(abc, rp, (1.0, 1.0, 1.0), center, rot, G.qx, G.qy,
+                                           G.qz.astype(np.complex128))
                 else:
                     sf = sf_lattice(G, abc, rp, (1.0, 1.0, 1.0), center, rot)
-                I = dwba_combine(fc, sf, ff, w, I)
+                if saxs:  # run_gisaxs :1099-1103: assigned, not added; the first N values
+                    t = (w * sf[:G.n]) * ff[:G.n]
+                    I = t.real * t.real + t.imag * t.imag
+                else:
+                    I = dwba_combine(fc, sf, ff, w, I)
         intens.append(I)
     ratios = [s["iratio"] for s in hig["structures"].values()]
     img = structure_sum(np.array(intens), ratios)

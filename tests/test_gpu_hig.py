@@ -30,7 +30,8 @@ def test_hig_qgrid_matches_oracle(ctx, po, name):
 
 SIM = ["sim_cylinders_hcp.hig", "sim_two_structures.hig", "paracrystal.hig", "percus_yevick.hig",
        "include_main.hig", "sim_scaling.hig", "sim_scaling_mixed.hig", "sim_repetition.hig",
-       "sim_orientations.hig", "sim_shapes.hig", "sim_mesh_paracrystal.hig"]
+       "sim_orientations.hig", "sim_shapes.hig", "sim_mesh_paracrystal.hig", "sim_saxs.hig",
+       "sim_saxs_py.hig"]
 
 
 def _srand(seed):
@@ -115,6 +116,7 @@ def test_compute_gisaxs_device_output(ctx, po):
 @pytest.mark.gpu
 @pytest.mark.parametrize("edit,words", [
     (("resolution = [ 48 32 ]", "resolution = [ 48 32 ], nslices = 3"), "nslices"),
+    (("scattering = {", 'scattering = { expt = "waxs",'), "experiment"),
     (('stat = "range"', 'stat = "bragg"'), "bragg orientations"),
     (("spacing = [ 150 150 0 ],", 'spacing = [ 150 150 0 ], distribution = "random",'), "distribution"),
     (("alphai = { min = 0.175 }", "alphai = { min = 0.1, max = 0.2, step = 0.05 }"), "alpha_i"),
