@@ -27,7 +27,7 @@
 // Refused with HGX_ERR_INVALID_ARG, naming the feature: clock-seeded random grain positions,
 // "bragg" orientations (the reference's search reads q-grid extents it never sets and fails),
 // structure correlations other than none (the reference indexes its single grain image as if
-// it held one per grain), sliced layers (nslices > 1), experiments other than gisaxs and saxs,
+// it held one per grain), experiments other than gisaxs and saxs,
 // and angle scans in hgx_hig_compute_gisaxs (more than one alpha_i, phi or tilt:
 // compute_gisaxs itself refuses those; hgx_hig_compute_scan_point runs them).
 //
@@ -35,7 +35,8 @@
 // first block), the lattice structure factor at the detector's real qz, no Fresnel
 // coefficients, and the intensity assigned rather than added, so a structure's image is its
 // last grain's last scaling sample; only that one is computed (the orientations of all grains
-// are still drawn, so rand() advances as in the reference).
+// are still drawn, so rand() advances as in the reference).  Sliced layers (nslices > 1) give
+// the reference's empty image: its slicing branch only prints a message.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdlib.h>
@@ -650,7 +651,9 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
   };
   if (sc.expt != "gisaxs" && sc.expt != "saxs")  // StructureFactor refuses the others (sf.cpp:100-102)
     return refuse("experiment '" + sc.expt + "': only gisaxs and saxs are defined");
-  if (cp.nslices > 1) return refuse("sliced layers (nslices > 1) are not supported");
+  // sliced layers: the reference only prints that slicing is not implemented and adds nothing
+  // (:1106-1115), so every structure's image stays zero; the orientations are still drawn
+  const bool sliced = cp.nslices > 1;
   if (cp.structcorrelation != "null" && cp.structcorrelation != "nGnE")
     return refuse("structure correlation '" + cp.structcorrelation + "' is not supported");
   if (in.structures.empty()) return refuse("the description has no structure");
@@ -787,6 +790,10 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
       if (shp->second.name == "custom") all_analytic = false;
       else if (shape_code(shp->second.name) < 0)
         return refuse("shape '" + shp->second.key + "': '" + shp->second.name + "' has no analytic form factor here");
+    }
+    if (sliced) {
+      ++si;
+      continue;
     }
     if (all_analytic && !saxs) {
       HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, plan, nscale,

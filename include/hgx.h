@@ -417,11 +417,12 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * nrow x ncol doubles (host or device).  precision: HGX_F64, or HGX_F32C for the mesh form
  * factors.  Supported: GISAXS and SAXS (expt "saxs": run_gisaxs's Born branch, :1099-1103, whose
  * assignment leaves each structure the image of its last grain's last scaling sample), one
- * alpha_i/phi/tilt, nslices <= 1, no structure correlation,
+ * alpha_i/phi/tilt, no structure correlation,
  * regular grain grids; "single", "range", "random" (drawn with the C library's rand() in the
  * reference's order), "gaussian", "normal" and "cauchy" orientations; gaussian/cauchy grain
  * scalings and ranged repetitions (the reference's seeded Mersenne Twister).  Other
- * descriptions return HGX_ERR_INVALID_ARG naming the feature. */
+ * descriptions return HGX_ERR_INVALID_ARG naming the feature.  nslices > 1 gives the
+ * reference's zero image (its slicing branch only prints that it is not implemented). */
 int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
 /* Angle scans, as HipGISAXS::run_all_gisaxs walks them (src/sim/hipgisaxs_main.cpp:283-613):
  * the numbers of incidence angles, in-plane rotations and tilts (alphai, inplanerot, tilt

@@ -115,7 +115,6 @@ def test_compute_gisaxs_device_output(ctx, po):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("edit,words", [
-    (("resolution = [ 48 32 ]", "resolution = [ 48 32 ], nslices = 3"), "nslices"),
     (("scattering = {", 'scattering = { expt = "waxs",'), "experiment"),
     (('stat = "range"', 'stat = "bragg"'), "bragg orientations"),
     (("spacing = [ 150 150 0 ],", 'spacing = [ 150 150 0 ], distribution = "random",'), "distribution"),
@@ -220,3 +219,24 @@ def test_scan_points_match_oracle(ctx, po):
         _srand(21)
         first = e.compute_gisaxs(ctx)
     np.testing.assert_array_equal(first, images[0][3])
+
+
+@pytest.mark.gpu
+def test_sliced_layers_give_the_reference_empty_image(ctx, tmp_path):
+    """nslices > 1: run_gisaxs's slicing branch only prints that it is not implemented and adds
+    nothing (src/sim/hipgisaxs_main.cpp:1106-1115), so the image is zero; the orientations are
+    still drawn, so rand() is left where the reference leaves it."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    text = open(os.path.join(HIG, "sim_cylinders_hcp.hig")).read()
+    p = tmp_path / "sliced.hig"
+    p.write_text(text.replace("resolution = [ 48 32 ]", "resolution = [ 48 32 ], nslices = 3", 1))
+    d = read_hig(str(p))
+    libc.srand(4)
+    img = d.compute_gisaxs(ctx)
+    after = libc.rand()
+    assert img.shape == d.image_size() and not img.any()
+    # the same description unsliced draws the same orientations
+    libc.srand(4)
+    full = read_hig(os.path.join(HIG, "sim_cylinders_hcp.hig")).compute_gisaxs(ctx)
+    assert libc.rand() == after and full.max() > 0
