@@ -136,8 +136,11 @@ struct FusedArgs {
 
 // Four threads per pixel, one per DWBA block k: each evaluates fc_k sf_k ff_k and the quad
 // adds the four terms in the order k = 0..3 (shuffles), as the step-by-step combination does.
-// SHAPE: the one analytic shape of every element (0: any).
-template <int SHAPE>
+// SHAPE: the one analytic shape of every element (0: any).  PAIRED: every grain of the launch
+// keeps qz out of the rotated qx, qy and every lattice a vector has no z component, so the
+// lattice factor takes sf_lattice_eval_paired (the same values; each variant carries one of
+// the two structure-factor bodies, which keeps the kernel's code smaller).
+template <int SHAPE, int PAIRED>
 __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 : 5) grain_dwba_kernel(FusedArgs a) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long i = t >> 2;
@@ -184,8 +187,7 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
           L.rep[d] = sp[si].rep[d];
           L.center[d] = gp[9 + d];
         }
-        // the grain's rotation keeps qz out of m[0], m[1] (uniform across the warp: one grain)
-        if (gp[2] == 0.0 && gp[5] == 0.0 && L.la[2] == 0.0)
+        if (PAIRED)
           sfv = sf_lattice_eval_paired(L, mr, (k & 1) != 0);
         else
           sfv = sf_lattice_eval(L, mr);
@@ -203,6 +205,20 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
 }
 
 constexpr int FUSED_GRAINS_PER_LAUNCH = 64;  // keeps each launch to tens of milliseconds
+
+template <int PAIRED>
+void launch_grain_kernel(int shape, unsigned blocks, cudaStream_t st, const FusedArgs& a) {
+  switch (shape) {
+    case SH_CYLINDER: grain_dwba_kernel<SH_CYLINDER, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_SPHERE: grain_dwba_kernel<SH_SPHERE, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_BOX: grain_dwba_kernel<SH_BOX, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_CUBE: grain_dwba_kernel<SH_CUBE, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_PRISM3: grain_dwba_kernel<SH_PRISM3, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_PRISM6: grain_dwba_kernel<SH_PRISM6, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    case SH_PYRAMID: grain_dwba_kernel<SH_PYRAMID, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+    default: grain_dwba_kernel<0, PAIRED><<<blocks, 128, 0, st>>>(a); break;
+  }
+}
 
 // RotMatrix_t(axis, angle) and its product (include/numerics/matrix.hpp:43-117)
 struct Rot {
@@ -614,16 +630,17 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
   for (int g0 = 0; g0 < ngr; g0 += FUSED_GRAINS_PER_LAUNCH) {
     a.g0 = g0;
     a.g1 = g0 + FUSED_GRAINS_PER_LAUNCH < ngr ? g0 + FUSED_GRAINS_PER_LAUNCH : ngr;
-    switch (one) {
-      case SH_CYLINDER: grain_dwba_kernel<SH_CYLINDER><<<blocks, 128, 0, st>>>(a); break;
-      case SH_SPHERE: grain_dwba_kernel<SH_SPHERE><<<blocks, 128, 0, st>>>(a); break;
-      case SH_BOX: grain_dwba_kernel<SH_BOX><<<blocks, 128, 0, st>>>(a); break;
-      case SH_CUBE: grain_dwba_kernel<SH_CUBE><<<blocks, 128, 0, st>>>(a); break;
-      case SH_PRISM3: grain_dwba_kernel<SH_PRISM3><<<blocks, 128, 0, st>>>(a); break;
-      case SH_PRISM6: grain_dwba_kernel<SH_PRISM6><<<blocks, 128, 0, st>>>(a); break;
-      case SH_PYRAMID: grain_dwba_kernel<SH_PYRAMID><<<blocks, 128, 0, st>>>(a); break;
-      default: grain_dwba_kernel<0><<<blocks, 128, 0, st>>>(a); break;
+    // the paired lattice factor when it holds for every grain and sample of the launch
+    bool paired = a.sfbuf == nullptr;
+    for (int gi = a.g0; gi < a.g1 && paired; ++gi) {
+      if (gt[12 * (size_t)gi + 2] != 0.0 || gt[12 * (size_t)gi + 5] != 0.0) paired = false;
+      for (int k = 0; k < nscale && paired; ++k)
+        if (plan[(size_t)gi * nscale + k].la[2] != 0.0) paired = false;
     }
+    if (paired)
+      launch_grain_kernel<1>(one, blocks, st, a);
+    else
+      launch_grain_kernel<0>(one, blocks, st, a);
     HGX_CUDA(cudaGetLastError());
   }
   // the tables stay in the context's buffers; the next structure rewrites them in stream order
