@@ -139,7 +139,10 @@ class HiGInput:
         """HipGISAXS::compute_gisaxs on the device (hgx_hig_compute_gisaxs): the nrow x ncol
         intensity image of every structure's grains, summed with the iratios.  `out`: a
         float64 numpy array or CUDA tensor of nrow*ncol values (allocated when None).
-        precision "f32c" computes mesh form factors in compensated FP32."""
+        precision "f32c" computes mesh form factors in compensated FP32.  expt "saxs" takes the
+        reference's Born branch (each structure keeps its last grain's last scaling sample, as
+        the reference's assignment leaves it); nslices > 1 gives the reference's zero image;
+        a description with angle scans is refused (compute_scan_point runs them)."""
         nrow, ncol = self.image_size()
         if out is None:
             out = np.zeros((nrow, ncol))
