@@ -53,6 +53,13 @@ __device__ __forceinline__ zd trans_phase(const zd* m, const double* tv) {
   zd t = m[0] * tv[0] + m[1] * tv[1] + m[2] * tv[2];
   return cexp_(zd(-t.y, t.x));
 }
+// v * trans_phase(m, tv); at the origin the phase is exactly (1, +-0), whose product leaves a
+// finite v as it is (up to the sign of a zero), so it is not evaluated there; a non-finite v
+// still takes the product (inf * 0 makes the NaN the reference's product makes)
+__device__ __forceinline__ zd with_phase(zd v, const zd* m, const double* tv) {
+  if (tv[0] == 0.0 && tv[1] == 0.0 && tv[2] == 0.0 && isfinite(v.x) && isfinite(v.y)) return v;
+  return v * trans_phase(m, tv);
+}
 
 // ff_ana_sphere.cpp:33-45
 static __device__ zd ff_sphere_one(zd qx, zd qy, zd qz, double radius) {
@@ -110,13 +117,13 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
         double h = Z.v[i];
         gh += (sinc_free((m[2] * 0.5) * h) * h) * cexp_(((zd(0, 0.5)) * m[2]) * h);
       }
-      out = fr * gh * trans_phase(m, tv);
+      out = with_phase(fr * gh, m, tv);
       break;
     }
     case SH_SPHERE: {  // ff_ana_sphere.cpp:95-107
       zd acc(0, 0);
       for (int i = 0; i < X.n; ++i) acc += ff_sphere_one(m[0], m[1], m[2], X.v[i]) * X.w[i];
-      out = acc * trans_phase(m, tv);
+      out = with_phase(acc, m, tv);
       break;
     }
     case SH_BOX: {  // ff_ana_box.cpp:35-42,96-125
@@ -126,7 +133,7 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
       for (int i = 0; i < Z.n; ++i)
         sz += (cexp_((zd(0, 0.5) * m[2]) * Z.v[i]) * sinc_free((m[2] * 0.5) * Z.v[i])) *
               (Z.v[i] * Z.w[i]);
-      out = sx * sy * sz * trans_phase(m, tv);
+      out = with_phase(sx * sy * sz, m, tv);
       break;
     }
     case SH_CUBE: {  // ff_ana_cube.cpp:35-42,87-107
@@ -137,7 +144,7 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
         zd s = sinc_free((m[0] * 0.5) * L) * sinc_free((m[1] * 0.5) * L) * sinc_free((m[2] * 0.5) * L);
         acc += ((e * (L * L * L)) * s) * X.w[i];
       }
-      out = acc * trans_phase(m, tv);
+      out = with_phase(acc, m, tv);
       break;
     }
     case SH_PRISM3: {  // ff_ana_prism.cpp:82-108 (unweighted)
@@ -155,7 +162,7 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
         sl += (t9 / t1) * (t4 - t5 - t6);
       }
       for (int i = 0; i < Z.n; ++i) sh += fq_inv(t2, Z.v[i]);
-      out = sl * sh * trans_phase(m, tv);
+      out = with_phase(sl * sh, m, tv);
       break;
     }
     case SH_PRISM6: {  // ff_ana_prism6.cpp:80-98 (unweighted)
@@ -172,7 +179,7 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
         sl += t2 + t3 - t4;
       }
       for (int i = 0; i < Z.n; ++i) sh += fq_inv(m[2] + qm, Z.v[i]);
-      out = t1 * sl * sh * trans_phase(m, tv);
+      out = with_phase(t1 * sl * sh, m, tv);
       break;
     }
     case SH_PYRAMID: {  // ff_ana_pyramid.cpp:118-139
