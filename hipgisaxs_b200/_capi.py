@@ -81,6 +81,7 @@ SIGNATURES = {
     "hgx_mesh_chi2_grad": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
                                 _vp, _vp, _vp]),
     "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
+    "hgx_ff_triangles_noalloc_status": (_i, [_vp, _vp]),
     "hgx_hig_read": (_i, [C.c_char_p, C.POINTER(_vp)]),
     "hgx_hig_json": (_i, [_vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hgx_hig_destroy": (_i, [_vp]),

@@ -725,9 +725,12 @@ int hgx_cyl_batch_eval(hgx_cyl_batch_s* b, const double* models, double* out) {
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
     b->ctx->stream = saved;
     cudaStreamDestroy(cap);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
-    if (s != HGX_OK) return s;
-    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    if (e != cudaSuccess || s != HGX_OK || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);  // a graph ended from a failed capture is not kept
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+      if (s != HGX_OK) return s;
+      return cuda_fail(e2, "cudaStreamEndCapture");
+    }
     b->graph = graph;
     HGX_CUDA(cudaGraphInstantiate(&b->exec, graph, 0));
   }

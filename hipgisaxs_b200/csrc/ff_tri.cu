@@ -963,18 +963,19 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
 
 // ------------------------------------------------------ allocation-free entry ----
 // hgx_ff_triangles_noalloc: the FP32C per-q-point form factor for callers that must not
-// allocate device memory — code running while a CUDA graph is being captured, code that
-// runs inside another framework's memory pool or under a fixed memory budget, and
-// real-time loops where cudaMalloc/cudaFree would synchronise the device.  Its scratch (the
-// FP32 triangle tiles and an error word) is a file-scope static device array of fixed size,
-// reserved when the library's device code is loaded on a GPU and held until exit.
+// allocate device memory — a plug-in that lives inside another framework's memory pool and
+// is handed only device pointers, a service held to a fixed device-memory budget, or a
+// real-time loop in which a cudaMalloc/cudaFree would synchronise the whole device.  Its
+// scratch (the FP32 triangle tiles and an error word) is a file-scope static device array of
+// fixed size, reserved when the library's device code is loaded on a GPU and held until exit.
 //
 // In host code the array name below is only a host-side stand-in, not a device address:
 // the device address is obtained once per device with cudaGetSymbolAddress (set-up done by
-// the first call on each device, with that device current) and passed to the kernels.
-// Every call shares the array: the triangle tiles are fully rewritten by each call and the
-// error word is cleared at its start; calls that overlap on the GPU (different streams,
-// no ordering) race on the array and must be ordered by the caller.
+// the first call on each device, with that device current; make that first call before any
+// stream capture) and passed to the kernels.  Every call shares the array: the triangle
+// tiles are fully rewritten by each call and the error word is cleared at its start; calls
+// that overlap on the GPU (different streams, no ordering) race on the array and must be
+// ordered by the caller.  hgx_ff_triangles_noalloc_status reads the error word back.
 constexpr int NOALLOC_MAX_TRIANGLES = 65536;
 constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 512 tiles, 1.5 MiB
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -1043,5 +1044,29 @@ extern "C" int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int n
   if (ff_type == HGX_C64) ff_tri_points_kernel<128, float2><<<grid, 128, 0, st>>>(a);
   else ff_tri_points_kernel<128, double2><<<grid, 128, 0, st>>>(a);
   HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+// The device error word of the allocation-free entry: waits for `stream`, copies the word
+// into *bits (host memory) and returns HGX_ERR_DEVICE when a kernel of the last call on this
+// device recorded an error (a bounded wait that gave up leaves part of ff unwritten).
+// Allocates nothing.
+extern "C" int hgx_ff_triangles_noalloc_status(void* stream, unsigned* bits) {
+  if (!bits) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc_status: bits is NULL");
+  *bits = 0;
+  int dev = 0;
+  HGX_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_noalloc_status: device index too large");
+  NoallocSlot slot;
+  HGX_TRY(noalloc_setup(dev, &slot));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  unsigned word = 0;
+  HGX_CUDA(cudaMemcpyAsync(&word, slot.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  *bits = word;
+  if (word)
+    return fail(HGX_ERR_DEVICE, "hgx_ff_triangles_noalloc: a kernel recorded device error bits " +
+                                    std::to_string(word) + " (1 = a bounded wait gave up)");
   return HGX_OK;
 }

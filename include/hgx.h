@@ -370,21 +370,27 @@ int hgx_mesh_chi2_grad(hgx_ctx ctx, hgx_qgrid g, int nv, const double* verts, in
                        const unsigned* mask, double scale, double* chi2, double* grad_verts,
                        double* intensity);
 
-/* The FP32C numeric form factor for callers that cannot allocate device memory: code
- * running inside CUDA graph capture, inside another framework's memory pool or under a
- * fixed memory budget, where a cudaMalloc would fail, break the capture or synchronise the
- * device.  No counterpart in the reference.  Allocates nothing: its scratch is a fixed
- * static device array (1.5 MiB per GPU, held until exit), so ntri <= 65536 (larger
- * requests return HGX_ERR_INVALID_ARG).  All array arguments are device memory (same
- * layouts as hgx_ff_triangles; q-point i uses qx/qy[i % nqy]); rot9 is 9 host doubles or
- * NULL for the identity; ff is nqz complex of type ff_type.  Asynchronous on `stream`
- * (a cudaStream_t; NULL = legacy default stream).  The first call on each device looks up
- * the scratch address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  Calls share the scratch: calls that can overlap on the
- * GPU (unordered streams) race and must be ordered by the caller. */
+/* The FP32C numeric form factor for callers that cannot allocate device memory: a plug-in
+ * that runs inside another framework's memory pool and is handed only device pointers, a
+ * service held to a fixed device-memory budget, or a real-time loop in which a cudaMalloc
+ * would synchronise the device.  No counterpart in the reference.  Allocates nothing: its
+ * scratch is a fixed static device array (1.5 MiB per GPU, held until exit), so
+ * ntri <= 65536 (larger requests return HGX_ERR_INVALID_ARG).  All array arguments are
+ * device memory (same layouts as hgx_ff_triangles; q-point i uses qx/qy[i % nqy]); rot9 is
+ * 9 host doubles or NULL for the identity; ff is nqz complex of type ff_type.  Asynchronous
+ * on `stream` (a cudaStream_t; NULL = legacy default stream).  The first call on each
+ * device looks up the scratch address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  Calls share the scratch, which keeps the
+ * last call's contents: calls that can overlap on the GPU (unordered streams) race and must
+ * be ordered by the caller. */
 int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int nqy, const double* qx,
                              const double* qy, int nqz, const double* qz, const double* rot9,
                              void* ff, int ff_type, void* stream);
+/* Device errors of hgx_ff_triangles_noalloc (no counterpart in the reference): waits for
+ * `stream`, writes the error bits its kernels recorded since the start of the last call on
+ * this device into *bits (host memory; 1 = a bounded wait gave up and part of ff is
+ * unwritten) and returns HGX_ERR_DEVICE when they are nonzero.  Allocates nothing. */
+int hgx_ff_triangles_noalloc_status(void* stream, unsigned* bits);
 
 /* -------------------------------------------------------------- HiG input files ---- */
 /* A simulation description read from a HiG file: HiGInput::construct_input_config

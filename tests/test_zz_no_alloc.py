@@ -1,12 +1,14 @@
 """The allocation-free entry point, hgx_ff_triangles_noalloc.
 
-It exists for callers that cannot allocate device memory: code running while a CUDA graph
-is being captured, code living inside another framework's memory pool or under a fixed
-memory budget, where cudaMalloc would fail, break the capture or synchronise the device.
+It exists for callers that cannot allocate device memory: a plug-in living inside another
+framework's memory pool that is handed only device pointers, a service held to a fixed
+device-memory budget, or a real-time loop in which cudaMalloc would synchronise the device.
 It keeps its scratch in a fixed static device array instead.  Here it is called through the
 C ABI and checked against the allocating entry point (hgx_ff_triangles) on two calls in a
 row with different meshes (so stale scratch from the first call cannot leak into the
-second), within the FP32C tolerance used by the other tests (norm-wise 1e-5).
+second), within the FP32C tolerance used by the other tests (norm-wise 1e-5); after each
+call its device error word must read 0, and the device's free memory must not change across
+the second call.
 """
 import numpy as np
 import pytest
@@ -34,6 +36,13 @@ def _noalloc(sd_d, qx_d, qy_d, qz_d, rot, out_d, stream):
         qz_d.numel(), qz_d.data_ptr(), r.ctypes.data, out_d.data_ptr(), _capi.C128, stream)
 
 
+def _status(stream):
+    import ctypes
+    bits = ctypes.c_uint(0xFFFFFFFF)
+    rc = _capi.lib().hgx_ff_triangles_noalloc_status(stream, ctypes.byref(bits))
+    return rc, bits.value
+
+
 def test_noalloc_matches_allocating_entry_on_two_calls(ctx, po):
     torch = pytest.importorskip("torch")
     dev = torch.device("cuda:0")
@@ -45,11 +54,17 @@ def test_noalloc_matches_allocating_entry_on_two_calls(ctx, po):
     qy_d = torch.tensor(G.qy, device=dev)
     qz_d = torch.tensor(G.qz_ext, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    for sd, R in ((_tri_cloud(rng, 300), R1), (_tri_cloud(rng, 70), R2)):
+    for call, (sd, R) in enumerate(((_tri_cloud(rng, 300), R1), (_tri_cloud(rng, 70), R2))):
         ref = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, R, "f32c")
         out = torch.full((4 * G.n,), complex(np.nan, np.nan), dtype=torch.complex128, device=dev)
-        _capi.check(_noalloc(torch.tensor(sd, device=dev), qx_d, qy_d, qz_d, R, out, stream))
+        sd_d = torch.tensor(sd, device=dev)
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(dev)[0]
+        _capi.check(_noalloc(sd_d, qx_d, qy_d, qz_d, R, out, stream))
+        assert _status(stream) == (0, 0)
+        torch.cuda.synchronize()
+        if call == 1:  # the first call may load the library's device code; the second must not allocate
+            assert torch.cuda.mem_get_info(dev)[0] == free0
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert po.rel_err(got, ref) < TOL32
