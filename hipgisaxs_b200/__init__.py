@@ -9,7 +9,7 @@ in csrc/hig_dropin.cpp.
 """
 from ._capi import HgxError, lib  # noqa: F401
 from .core import (Context, QGrid, ff_exact_triangles, ff_triangles,  # noqa: F401
-                   ff_triangles_arrays, ff_tune, measure_peaks)
+                   ff_triangles_arrays, ff_tune, measure_peak_fp64, measure_peaks)
 
 __all__ = ["Context", "QGrid", "ff_triangles", "ff_triangles_arrays", "ff_exact_triangles",
            "ff_tune", "HgxError", "lib"]

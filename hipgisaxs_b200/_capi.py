@@ -80,6 +80,8 @@ SIGNATURES = {
     "hgx_mesh_to_shape_def": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "hgx_mesh_chi2_grad": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
                                 _vp, _vp, _vp]),
+    "hgx_mesh_chi2_grad_ex": (_i, [_vp, _vp, _i, _vp, _i, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _d,
+                                _vp, _vp, _vp, _i]),
     "hgx_ff_triangles_noalloc": (_i, [_vp, _i, _i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
     "hgx_ff_triangles_noalloc_status": (_i, [_vp, _vp]),
     "hgx_hig_read": (_i, [C.c_char_p, C.POINTER(_vp)]),
@@ -106,6 +108,7 @@ SIGNATURES = {
     "hgx_read_mask": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long)]),
     "hgx_hig_objective": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, C.POINTER(C.c_long)]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
+    "hgx_measure_peak_fp64": (_i, [_vp, C.POINTER(_d)]),
 }
 
 _lib = None

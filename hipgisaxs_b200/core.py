@@ -206,6 +206,13 @@ def measure_peaks(ctx: Context, sustained_ms: int = 0):
     return f.value, s.value
 
 
+def measure_peak_fp64(ctx: Context):
+    """FP64 FMA TFLOP/s measured by the library's DFMA probe."""
+    f = C.c_double()
+    check(lib().hgx_measure_peak_fp64(ctx.handle, C.byref(f)))
+    return f.value
+
+
 def ff_triangles_arrays(ctx: Context, shape_def, qx, qy, qz, rot=None, precision="f64",
                         out=None):
     """The reference-shaped call (hgx_ff_triangles): explicit arrays, complex128 result

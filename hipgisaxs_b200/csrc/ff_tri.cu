@@ -2,7 +2,19 @@
 // q' = R q — the reference's "approx triangle" formula (src/ff/cpu/ff_tri_cpu.cpp:233-240,
 // src/ff/gpu/ff_tri_gpu.cu:371-384).
 //
-// Three kernels:
+// Triangle tiles (FP32 kernels).  The triangles are put in Morton order of their centroids
+// (a stable radix sort of 30-bit keys) and cut into tiles of 128, so that each tile covers a
+// compact patch of the mesh.  Each tile carries an FP64 anchor c0 (the mean of its rotated
+// centroids); the FP32 tile data hold only the offsets c' - c0.  Then
+//   e^{i q.c'} = e^{i q.c0} e^{i q.(c' - c0)},
+// where the anchor phase q.c0 is formed and range-reduced in FP64 once per (q-point, tile)
+// and applied as one complex rotation of the tile's partial sums, and the FP32 phase per
+// (q-point, triangle) only spans the tile's extent.  A mesh far from the origin therefore
+// loses no phase accuracy, and when the tile's in-plane phases stay within a few turns (the
+// CTA's largest |q_par| times the tile's largest offset) the row kernel feeds them to the SFU
+// without a per-term reduction.
+//
+// Kernels:
 //  * ff_tri_f64_kernel     — the plain FP64 form: one thread per q-point, triangles staged
 //                            through shared memory, reference arithmetic.  Parity reference
 //                            on the device and the denominator of the FP32 speed-up.
@@ -11,19 +23,20 @@
 //                            triangles (q'.c = q.(R^T c)), the phase splits into an in-plane
 //                            part e^{i(qx c'x + qy c'y)} evaluated per (pixel, triangle) and a
 //                            row part e^{i qz_k c'z} evaluated once per (row, triangle) and
-//                            block k.  With the four real DWBA blocks (qz_3 = -qz_0,
+//                            block k in FP64.  With the four real DWBA blocks (qz_3 = -qz_0,
 //                            qz_1 = -qz_2) one in-plane sincos serves all four blocks.
 //                            Triangle tiles arrive in shared memory by TMA bulk copies,
-//                            double-buffered on mbarriers.  Phases are carried in turns and
-//                            reduced exactly (r = t - rint t) before the SFU sincos.  Sums are
-//                            blocked per tile and folded with TwoSum (compensated).
+//                            double-buffered on mbarriers.  Sums are blocked per tile, rotated
+//                            by the tile's anchor phasor and folded with TwoSum (compensated).
+//  * ff_tri_rows_x2_kernel — the same with packed FP32x2 arithmetic (two pixels per lane pair).
 //  * ff_tri_points_kernel  — FP32 for arbitrary q-point sets (one thread per q-point), the
-//                            same phase/accumulation scheme without the row factorisation.
+//                            same tiles and anchors without the row factorisation.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
 #include <algorithm>
+#include <cub/device/device_radix_sort.cuh>
 #include <mutex>
 
 #include "hgx_internal.cuh"
@@ -32,41 +45,193 @@
 namespace hgx {
 
 constexpr int TILE = 128;                   // triangles per shared-memory tile
-constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (cx,cy,nx,ny) + float2 B[TILE] (cz,nz)
+constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (dx,dy,nx,ny) + float2 B[TILE] (dz,nz)
 constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
+constexpr int TILE_X2_FLOATS = TILE * 10;   // float4 A2[2*TILE] ((dx,dx,dy,dy),(nx,nx,ny,ny)) + float2 B[TILE]
+constexpr uint32_t TILE_X2_BYTES = TILE_X2_FLOATS * 4;
 constexpr double TWO_PI = 6.283185307179586476925286766559;
 constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
+constexpr float TWO_PI_F = 6.28318530717958648f;
+constexpr float INV_TWO_PI_F = 0.159154943091895336f;
+// In-plane phases of a tile with |q_par| * (largest offset) above 4 pi radians get the
+// explicit reduction to [-1/2, 1/2] turn before the SFU; below it they go straight in.
+constexpr float WIDE_PHASE2 = 157.91367f;   // (4 pi)^2
 
 struct Rot9 {
   double r[9];
 };
 
 // ------------------------------------------------------------- triangle prep ----
-// shape_def (T x 8 FP64) -> FP32 tiles.  n' = R^T n and c' = R^T c in FP64; the area is
-// folded into the normal (n~ = s n') and the centroid is carried in turns (c~ = c'/2pi).
-// Padding triangles are zero (they contribute nothing).
-__global__ void tri_prep_kernel(const double* __restrict__ sd, int ntri, int ntiles, Rot9 R,
-                                float* __restrict__ tiles) {
+// Morton order: bounding box of the centroids (per-block partials, then one block), 30-bit
+// keys, stable radix sort (cub), then one CTA per tile writes the tile and its anchor.
+constexpr int BBOX_THREADS = 256;
+constexpr int BBOX_MAX_BLOCKS = 256;
+
+__device__ __forceinline__ void bbox_block_reduce(double* lo, double* hi, double (*s)[6]) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = fmin(lo[k], __shfl_down_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmax(hi[k], __shfl_down_sync(0xffffffffu, hi[k], o));
+    }
+  if (l == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      s[w][k] = lo[k];
+      s[w][3 + k] = hi[k];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int v = 1; v < BBOX_THREADS / 32; ++v)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = fmin(lo[k], s[v][k]);
+        hi[k] = fmax(hi[k], s[v][3 + k]);
+      }
+}
+
+__global__ void __launch_bounds__(BBOX_THREADS) tri_bbox_kernel(const double* __restrict__ sd, int ntri,
+                                                                double* __restrict__ part) {
+  __shared__ double s[BBOX_THREADS / 32][6];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int t = blockIdx.x * BBOX_THREADS + threadIdx.x; t < ntri; t += gridDim.x * BBOX_THREADS)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double c = sd[8L * t + 4 + k];
+      lo[k] = fmin(lo[k], c);
+      hi[k] = fmax(hi[k], c);
+    }
+  bbox_block_reduce(lo, hi, s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      part[6 * blockIdx.x + k] = lo[k];
+      part[6 * blockIdx.x + 3 + k] = hi[k];
+    }
+}
+
+__global__ void __launch_bounds__(BBOX_THREADS) tri_bbox_final_kernel(double* __restrict__ part,
+                                                                      int nparts) {
+  __shared__ double s[BBOX_THREADS / 32][6];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int b = threadIdx.x; b < nparts; b += BBOX_THREADS)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = fmin(lo[k], part[6 * b + k]);
+      hi[k] = fmax(hi[k], part[6 * b + 3 + k]);
+    }
+  bbox_block_reduce(lo, hi, s);
+  __syncthreads();  // every thread has read the partials before block 0's slot is overwritten
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      part[k] = lo[k];
+      part[3 + k] = hi[k];
+    }
+}
+
+// 10 bits of v spread to every third bit.
+__device__ __forceinline__ unsigned spread3(unsigned v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+
+__global__ void tri_key_kernel(const double* __restrict__ sd, int ntri, const double* __restrict__ bbox,
+                               unsigned* __restrict__ keys, int* __restrict__ idx) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntiles * TILE) return;
-  int tile = t / TILE, j = t - tile * TILE;
-  float4* A = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_FLOATS);
-  float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_FLOATS + 4 * TILE);
-  if (t < ntri) {
+  if (t >= ntri) return;
+  unsigned q[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double lo = bbox[k], ext = bbox[3 + k] - lo;
+    double u = ext > 0.0 ? (sd[8L * t + 4 + k] - lo) / ext : 0.0;
+    int b = (int)(u * 1024.0);
+    q[k] = (unsigned)min(1023, max(0, b));
+  }
+  keys[t] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+  idx[t] = t;
+}
+
+// One CTA (128 threads) per tile.  order: the triangle of each sorted slot (NULL: slot i holds
+// triangle i).  Writes the tile (n~ = s R^T n, offsets d = R^T c - c0; in nm for the scalar
+// layout, in turns for the packed layout), its anchor (c0x/2pi, c0y/2pi, c0z, max |d_par|)
+// and, when perm is not NULL, the triangle index of each slot (-1 for padding).  The anchor's
+// sums run in a fixed order (deterministic).  Padding slots are zero (they contribute nothing).
+template <bool X2>
+__global__ void __launch_bounds__(TILE) tri_tile_kernel(const double* __restrict__ sd, int ntri, Rot9 R,
+                                                        const int* __restrict__ order,
+                                                        float* __restrict__ tiles,
+                                                        double4* __restrict__ anchors,
+                                                        int* __restrict__ perm) {
+  __shared__ double s_red[TILE / 32][4];
+  __shared__ double s_c0[3];
+  __shared__ double s_rmax[TILE / 32];
+  const int tile = blockIdx.x, j = threadIdx.x;
+  const long pos = (long)tile * TILE + j;
+  const int t = pos < ntri ? (order ? order[pos] : (int)pos) : -1;
+  if (perm) perm[pos] = t;
+  double s = 0.0, np[3] = {0.0, 0.0, 0.0}, cp[3] = {0.0, 0.0, 0.0};
+  if (t >= 0) {
     const double* p = sd + 8L * t;
-    double s = p[0];
+    s = p[0];
     double n[3] = {p[1], p[2], p[3]}, c[3] = {p[4], p[5], p[6]};
-    double np[3], cp[3];
+#pragma unroll
     for (int l = 0; l < 3; ++l) {
       np[l] = R.r[0 * 3 + l] * n[0] + R.r[1 * 3 + l] * n[1] + R.r[2 * 3 + l] * n[2];
       cp[l] = R.r[0 * 3 + l] * c[0] + R.r[1 * 3 + l] * c[1] + R.r[2 * 3 + l] * c[2];
     }
-    A[j] = make_float4((float)(cp[0] * INV_TWO_PI), (float)(cp[1] * INV_TWO_PI),
-                       (float)(s * np[0]), (float)(s * np[1]));
-    B[j] = make_float2((float)(cp[2] * INV_TWO_PI), (float)(s * np[2]));
+  }
+  double v[4] = {cp[0], cp[1], cp[2], t >= 0 ? 1.0 : 0.0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if ((j & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s_red[j >> 5][k] = v[k];
+  __syncthreads();
+  if (j == 0) {
+    double sum[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < TILE / 32; ++w)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sum[k] += s_red[w][k];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s_c0[k] = sum[k] / sum[3];  // every tile holds >= 1 triangle
+  }
+  __syncthreads();
+  double d[3] = {0.0, 0.0, 0.0};
+  if (t >= 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) d[k] = cp[k] - s_c0[k];
+  double r = sqrt(d[0] * d[0] + d[1] * d[1]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+  if ((j & 31) == 0) s_rmax[j >> 5] = r;
+  __syncthreads();
+  if (j == 0) {
+    double rm = s_rmax[0];
+    for (int w = 1; w < TILE / 32; ++w) rm = fmax(rm, s_rmax[w]);
+    anchors[tile] = make_double4(s_c0[0] * INV_TWO_PI, s_c0[1] * INV_TWO_PI, s_c0[2], rm);
+  }
+  const double u = X2 ? INV_TWO_PI : 1.0;
+  const float dx = (float)(d[0] * u), dy = (float)(d[1] * u), dz = (float)(d[2] * u);
+  const float nx = (float)(s * np[0]), ny = (float)(s * np[1]), nz = (float)(s * np[2]);
+  if (X2) {
+    float4* A2 = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_X2_FLOATS);
+    float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_X2_FLOATS + 8 * TILE);
+    A2[2 * j] = make_float4(dx, dx, dy, dy);
+    A2[2 * j + 1] = make_float4(nx, nx, ny, ny);
+    B[j] = make_float2(dz, nz);
   } else {
-    A[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-    B[j] = make_float2(0.f, 0.f);
+    float4* A = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_FLOATS);
+    float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_FLOATS + 4 * TILE);
+    A[j] = make_float4(dx, dy, nx, ny);
+    B[j] = make_float2(dz, nz);
   }
 }
 
@@ -103,9 +268,32 @@ __device__ __forceinline__ void store_ff<double2>(double2* out, long idx, double
   out[idx] = make_double2(re, im);
 }
 
+// The anchor phasor e^{2 pi i u} of an FP64 phase u in turns, reduced exactly in FP64.
+__device__ __forceinline__ float2 anchor_phasor(double u) {
+  u -= rint(u);
+  float s, c;
+  sincospif((float)(2.0 * u), &s, &c);
+  return make_float2(c, s);
+}
+
+// (re, im) <- (re, im) * (c + i s)
+__device__ __forceinline__ void rotate_pair(float& re, float& im, float2 a) {
+  const float r = re * a.x - im * a.y;
+  im = re * a.y + im * a.x;
+  re = r;
+}
+
+// Rounds x to the nearest integer (ties to even) with two FP32 adds — valid for
+// |x| < 2^22 — so the reduction stays on the FMA pipe instead of the conversion unit.
+__device__ __forceinline__ float round_nearest(float x) {
+  const float magic = 12582912.0f;  // 1.5 * 2^23
+  return (x + magic) - magic;
+}
+
 // ------------------------------------------------------------- row kernel ----
 struct RowArgs {
   const float* tiles;
+  const double4* anchors;
   int ntiles;
   const double* qx;
   const double* qy;
@@ -116,10 +304,10 @@ struct RowArgs {
   unsigned* err;
 };
 
-// Row factor of one (row, triangle) for a real block pair (qz, -qz):
-// Z = e^{i 2pi qz cz~} = (x, y), D = qz n~z; returns (x, y, D*y, D*x).
-__device__ __forceinline__ float4 paired_factor(double q, float cz, float nz) {
-  double u = q * (double)cz;
+// Row factor of one (row, triangle) for a real block pair (qz, -qz), cz in turns (FP64):
+// Z = e^{i 2pi qz cz} = (x, y), D = qz n~z; returns (x, y, D*y, D*x).
+__device__ __forceinline__ float4 paired_factor(double q, double cz, float nz) {
+  double u = q * cz;
   u -= rint(u);
   float s, c;
   sincospif((float)(2.0 * u), &s, &c);
@@ -127,11 +315,12 @@ __device__ __forceinline__ float4 paired_factor(double q, float cz, float nz) {
   return make_float4(c, s, D * s, D * c);
 }
 
-// Row factor for a general complex block: Z = e^{i 2pi qz cz~}, D = qz n~z; returns (Z, D Z).
-__device__ __forceinline__ float4 complex_factor(double2 q, float cz, float nz) {
-  double u = q.x * (double)cz;
+// Row factor for a general complex block, cz in turns: Z = e^{i 2pi qz cz}, D = qz n~z;
+// returns (Z, D Z).
+__device__ __forceinline__ float4 complex_factor(double2 q, double cz, float nz) {
+  double u = q.x * cz;
   u -= rint(u);
-  double amp = exp(-TWO_PI * q.y * (double)cz);
+  double amp = exp(-TWO_PI * q.y * cz);
   double s, c;
   sincospi(2.0 * u, &s, &c);
   double zr = amp * c, zi = amp * s;
@@ -139,11 +328,61 @@ __device__ __forceinline__ float4 complex_factor(double2 q, float cz, float nz) 
   return make_float4((float)zr, (float)zi, (float)(dr * zr - di * zi), (float)(dr * zi + di * zr));
 }
 
-// Rounds x to the nearest integer (ties to even) with two FP32 adds — valid for
-// |x| < 2^22 — so the reduction stays on the FMA pipe instead of the conversion unit.
-__device__ __forceinline__ float round_nearest(float x) {
-  const float magic = 12582912.0f;  // 1.5 * 2^23
-  return (x + magic) - magic;
+// One tile's partial sums of the row kernel (see ff_tri_rows_kernel).  WIDE: the in-plane
+// phases get the explicit reduction to [-1/2, 1/2] turn before the SFU.
+template <int P, int NK, bool PAIRED, bool WIDE>
+__device__ __forceinline__ void row_tile_sums(const float4* __restrict__ A, const float4* __restrict__ RF,
+                                              const float (&qxf)[P], const float (&qyf)[P],
+                                              float (&acc)[P][PAIRED ? 8 : 2 * NK]) {
+  constexpr int NF = PAIRED ? 2 : NK;
+#pragma unroll 2
+  for (int j = 0; j < TILE; ++j) {
+    const float4 t = A[j];
+    float4 f[NF];
+#pragma unroll
+    for (int n = 0; n < NF; ++n) f[n] = RF[j * NF + n];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      float tp = fmaf(qxf[i], t.x, qyf[i] * t.y);  // in-plane phase offset, radians
+      if (WIDE) {
+        float tt = tp * INV_TWO_PI_F;
+        tp = (tt - round_nearest(tt)) * TWO_PI_F;  // reduced to [-pi, pi]
+      }
+      float sn, cs;
+      __sincosf(tp, &sn, &cs);
+      float aq = fmaf(qxf[i], t.z, qyf[i] * t.w);  // in-plane part of q.n~
+      float ur = aq * cs, ui = aq * sn;            // U = aq * E
+      if (PAIRED) {
+#pragma unroll
+        for (int pr = 0; pr < 2; ++pr) {
+          const float4 g = f[pr];  // (x, y, beta, gamma)
+          float* q = acc[i] + 4 * pr;
+          q[0] = fmaf(g.x, ur, q[0]);
+          q[0] = fmaf(-g.z, sn, q[0]);  // P.re += x Ur - beta s
+          q[1] = fmaf(g.x, ui, q[1]);
+          q[1] = fmaf(g.z, cs, q[1]);   // P.im += x Ui + beta c
+          q[2] = fmaf(-g.y, ui, q[2]);
+          q[2] = fmaf(g.w, cs, q[2]);   // M.re += -y Ui + gamma c
+          q[3] = fmaf(g.y, ur, q[3]);
+          q[3] = fmaf(g.w, sn, q[3]);   // M.im += y Ur + gamma s
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+          const float4 g = f[k];  // (Zr, Zi, DZr, DZi)
+          float* q = acc[i] + 2 * k;
+          q[0] = fmaf(ur, g.x, q[0]);
+          q[0] = fmaf(-ui, g.y, q[0]);
+          q[0] = fmaf(g.z, cs, q[0]);
+          q[0] = fmaf(-g.w, sn, q[0]);
+          q[1] = fmaf(ur, g.y, q[1]);
+          q[1] = fmaf(ui, g.x, q[1]);
+          q[1] = fmaf(g.z, sn, q[1]);
+          q[1] = fmaf(g.w, cs, q[1]);
+        }
+      }
+    }
+  }
 }
 
 template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
@@ -152,6 +391,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
   constexpr int NACC = PAIRED ? 8 : 2 * NK;  // float accumulators per pixel
   __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
   __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ unsigned s_q2max;
   // dynamic: row factors (rows_per_cta x TILE x NF float4), then the compensation terms of
   // the running sums (P x NACC x BLOCK floats, thread-minor so accesses are conflict-free)
   extern __shared__ __align__(16) float4 s_dyn[];
@@ -167,6 +407,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
 
   float qxf[P], qyf[P];
   float acc[P][NACC], sum[P][NACC];
+  float q2l = 0.f;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
     int col = colbase + i * tpr;
@@ -174,6 +415,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
     long p = (long)row * a.ncol + col;
     qxf[i] = v ? (float)a.qx[p] : 0.f;
     qyf[i] = v ? (float)a.qy[p] : 0.f;
+    q2l = fmaxf(q2l, fmaf(qxf[i], qxf[i], qyf[i] * qyf[i]));
 #pragma unroll
     for (int n = 0; n < NACC; ++n) {
       acc[i][n] = sum[i][n] = 0.f;
@@ -182,6 +424,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
   }
 
   if (threadIdx.x == 0) {
+    s_q2max = 0u;
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
@@ -193,26 +436,32 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
       bulk_g2s(s_tile[s], a.tiles + (size_t)s * TILE_FLOATS, TILE_BYTES, &s_bar[s]);
     }
   }
+  atomicMax(&s_q2max, __float_as_uint(q2l));  // non-negative floats order as their bits
+  __syncthreads();
+  const float q2max = __uint_as_float(s_q2max);  // the CTA's largest |q_par|^2
 
   for (int s = 0; s < a.ntiles; ++s) {
     const int b = s & 1;
+    const double4 anc = a.anchors[s];
     const bool ok = mbar_wait(&s_bar[b], (s >> 1) & 1);
     const float4* A = reinterpret_cast<const float4*>(s_tile[b]);
     const float2* B = reinterpret_cast<const float2*>(s_tile[b] + 4 * TILE);
     if (ok) {
-      // one float4 row factor per item: (row, triangle, pair or block)
+      // one float4 row factor per item: (row, triangle, pair or block); z phases in FP64
+      const double cz0 = anc.z * INV_TWO_PI;
       for (int it = threadIdx.x; it < R * TILE * NF; it += BLOCK) {
         const int f = it % NF;
         const int rj = it / NF;
         const int r = rj / TILE, j = rj - r * TILE;
         const int grow = blockIdx.y * R + r;
         const float2 bz = B[j];
+        const double cz = cz0 + (double)bz.x * INV_TWO_PI;
         float4 v;
         if (PAIRED) {
-          v = grow < a.nrow ? paired_factor(a.rowqz[(long)grow * 4 + 2 * f].x, bz.x, bz.y)
+          v = grow < a.nrow ? paired_factor(a.rowqz[(long)grow * 4 + 2 * f].x, cz, bz.y)
                             : make_float4(1.f, 0.f, 0.f, 0.f);
         } else {
-          v = grow < a.nrow ? complex_factor(a.rowqz[(long)grow * NK + f], bz.x, bz.y)
+          v = grow < a.nrow ? complex_factor(a.rowqz[(long)grow * NK + f], cz, bz.y)
                             : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         s_rf[it] = v;  // == ((r * TILE + j) * NF + f)
@@ -231,54 +480,20 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
     }
 
     const float4* RF = s_rf + (size_t)lr * TILE * NF;
-#pragma unroll 2
-    for (int j = 0; j < TILE; ++j) {
-      const float4 t = A[j];
-      float4 f[NF];
+    if ((float)(anc.w * anc.w) * q2max > WIDE_PHASE2)  // uniform over the CTA
+      row_tile_sums<P, NK, PAIRED, true>(A, RF, qxf, qyf, acc);
+    else
+      row_tile_sums<P, NK, PAIRED, false>(A, RF, qxf, qyf, acc);
+    // rotate the tile's partial sums by the anchor phasor e^{i(qx c0x + qy c0y)} (FP64
+    // phase), then fold them into the running sums (TwoSum; error terms in smem)
 #pragma unroll
-      for (int n = 0; n < NF; ++n) f[n] = RF[j * NF + n];
+    for (int i = 0; i < P; ++i) {
+      const int col = colbase + i * tpr;
+      const bool v = row < a.nrow && col < a.ncol;
+      const long p = (long)row * a.ncol + col;
+      const float2 e = anchor_phasor(v ? fma(a.qx[p], anc.x, a.qy[p] * anc.y) : 0.0);
 #pragma unroll
-      for (int i = 0; i < P; ++i) {
-        float tp = fmaf(qxf[i], t.x, qyf[i] * t.y);  // in-plane phase, turns
-        float rr = tp - round_nearest(tp);           // exact reduction to [-1/2, 1/2]
-        float sn, cs;
-        __sincosf(rr * 6.28318530717958648f, &sn, &cs);
-        float aq = fmaf(qxf[i], t.z, qyf[i] * t.w);  // in-plane part of q.n~
-        float ur = aq * cs, ui = aq * sn;            // U = aq * E
-        if (PAIRED) {
-#pragma unroll
-          for (int pr = 0; pr < 2; ++pr) {
-            const float4 g = f[pr];  // (x, y, beta, gamma)
-            float* q = acc[i] + 4 * pr;
-            q[0] = fmaf(g.x, ur, q[0]);
-            q[0] = fmaf(-g.z, sn, q[0]);  // P.re += x Ur - beta s
-            q[1] = fmaf(g.x, ui, q[1]);
-            q[1] = fmaf(g.z, cs, q[1]);   // P.im += x Ui + beta c
-            q[2] = fmaf(-g.y, ui, q[2]);
-            q[2] = fmaf(g.w, cs, q[2]);   // M.re += -y Ui + gamma c
-            q[3] = fmaf(g.y, ur, q[3]);
-            q[3] = fmaf(g.w, sn, q[3]);   // M.im += y Ur + gamma s
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < NK; ++k) {
-            const float4 g = f[k];  // (Zr, Zi, DZr, DZi)
-            float* q = acc[i] + 2 * k;
-            q[0] = fmaf(ur, g.x, q[0]);
-            q[0] = fmaf(-ui, g.y, q[0]);
-            q[0] = fmaf(g.z, cs, q[0]);
-            q[0] = fmaf(-g.w, sn, q[0]);
-            q[1] = fmaf(ur, g.y, q[1]);
-            q[1] = fmaf(ui, g.x, q[1]);
-            q[1] = fmaf(g.z, sn, q[1]);
-            q[1] = fmaf(g.w, cs, q[1]);
-          }
-        }
-      }
-    }
-    // fold the tile's partial sums into the running sums (TwoSum; error terms in smem)
-#pragma unroll
-    for (int i = 0; i < P; ++i)
+      for (int n = 0; n < NACC; n += 2) rotate_pair(acc[i][n], acc[i][n + 1], e);
 #pragma unroll
       for (int n = 0; n < NACC; ++n) {
         float* cp = s_cmp + (i * NACC + n) * BLOCK + threadIdx.x;
@@ -286,6 +501,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
         two_sum_fold(sum[i][n], acc[i][n], c);
         *cp = c;
       }
+    }
     __syncthreads();  // every thread is done with tile buffer b and the row factors
     if (threadIdx.x == 0 && s + 2 < a.ntiles) {
       fence_proxy_async_smem();
@@ -331,39 +547,8 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
 // __fadd2_rn, __fmul2_rn): each thread carries its pixels in pairs, so one instruction
 // advances two pixels.  Operands shared by both pixels of a pair (triangle data, row
 // factors) are stored duplicated, (v, v), so they load as packed operands; the signs of
-// the two negative terms are folded into a negated sine instead of negated operands.
-constexpr int TILE_X2_FLOATS = TILE * 10;  // float4 A2[2*TILE] ((cx,cx,cy,cy),(nx,nx,ny,ny)) + float2 B[TILE]
-constexpr uint32_t TILE_X2_BYTES = TILE_X2_FLOATS * 4;
-
-__global__ void tri_prep_x2_kernel(const double* __restrict__ sd, int ntri, int ntiles, Rot9 R,
-                                   float* __restrict__ tiles) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntiles * TILE) return;
-  int tile = t / TILE, j = t - tile * TILE;
-  float4* A = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_X2_FLOATS);
-  float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_X2_FLOATS + 8 * TILE);
-  float cx = 0.f, cy = 0.f, cz = 0.f, nx = 0.f, ny = 0.f, nz = 0.f;
-  if (t < ntri) {
-    const double* p = sd + 8L * t;
-    double s = p[0];
-    double n[3] = {p[1], p[2], p[3]}, c[3] = {p[4], p[5], p[6]};
-    double np[3], cp[3];
-    for (int l = 0; l < 3; ++l) {
-      np[l] = R.r[0 * 3 + l] * n[0] + R.r[1 * 3 + l] * n[1] + R.r[2 * 3 + l] * n[2];
-      cp[l] = R.r[0 * 3 + l] * c[0] + R.r[1 * 3 + l] * c[1] + R.r[2 * 3 + l] * c[2];
-    }
-    cx = (float)(cp[0] * INV_TWO_PI);
-    cy = (float)(cp[1] * INV_TWO_PI);
-    cz = (float)(cp[2] * INV_TWO_PI);
-    nx = (float)(s * np[0]);
-    ny = (float)(s * np[1]);
-    nz = (float)(s * np[2]);
-  }
-  A[2 * j] = make_float4(cx, cx, cy, cy);
-  A[2 * j + 1] = make_float4(nx, nx, ny, ny);
-  B[j] = make_float2(cz, nz);
-}
-
+// the two negative terms are folded into a negated sine instead of negated operands.  Its
+// tiles carry the offsets in turns and every phase is reduced explicitly.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int BLOCK, int PP, typename OUT>
@@ -424,18 +609,20 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_x2_kernel(RowArgs a) {
   const float M = 12582912.0f;  // 1.5 * 2^23: (t + M) - M rounds t to an integer
   for (int s = 0; s < a.ntiles; ++s) {
     const int b = s & 1;
+    const double4 anc = a.anchors[s];
     const bool ok = mbar_wait(&s_bar[b], (s >> 1) & 1);
     const float4* A2 = reinterpret_cast<const float4*>(s_tile[b]);
     const float2* B = reinterpret_cast<const float2*>(s_tile[b] + 8 * TILE);
     if (ok) {
       // two duplicated float4 per (row, triangle, block pair): (x,x,y,y), (beta,beta,gamma,gamma)
+      const double cz0 = anc.z * INV_TWO_PI;
       for (int it = threadIdx.x; it < R * TILE * 2; it += BLOCK) {
         const int f = it & 1;
         const int rj = it >> 1;
         const int r = rj / TILE, j = rj - r * TILE;
         const int grow = blockIdx.y * R + r;
         const float2 bz = B[j];
-        float4 v = grow < a.nrow ? paired_factor(a.rowqz[(long)grow * 4 + 2 * f].x, bz.x, bz.y)
+        float4 v = grow < a.nrow ? paired_factor(a.rowqz[(long)grow * 4 + 2 * f].x, cz0 + (double)bz.x, bz.y)
                                  : make_float4(1.f, 0.f, 0.f, 0.f);
         float4* dst = s_rf + (size_t)(r * TILE + j) * 4 + 2 * f;
         dst[0] = make_float4(v.x, v.x, v.y, v.y);
@@ -464,7 +651,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_x2_kernel(RowArgs a) {
         float2 tp = __ffma2_rn(qx2[pp], f2(c4.x, c4.y), __fmul2_rn(qy2[pp], f2(c4.z, c4.w)));
         float2 k = __fadd2_rn(__fadd2_rn(tp, f2(M, M)), f2(-M, -M));
         float2 rr = __ffma2_rn(k, f2(-1.f, -1.f), tp);  // exact reduction to [-1/2, 1/2]
-        float2 ang = __fmul2_rn(rr, f2(6.28318530717958648f, 6.28318530717958648f));
+        float2 ang = __fmul2_rn(rr, f2(TWO_PI_F, TWO_PI_F));
         float s0, c0, s1, c1;
         __sincosf(ang.x, &s0, &c0);
         __sincosf(ang.y, &s1, &c1);
@@ -484,6 +671,21 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_x2_kernel(RowArgs a) {
         }
       }
     }
+#pragma unroll
+    for (int pp = 0; pp < PP; ++pp)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int col = colbase + (2 * pp + c) * tpr;
+        const bool v = row < a.nrow && col < a.ncol;
+        const long p = (long)row * a.ncol + col;
+        const float2 e = anchor_phasor(v ? fma(a.qx[p], anc.x, a.qy[p] * anc.y) : 0.0);
+#pragma unroll
+        for (int n = 0; n < NACC; n += 2) {
+          float& re = c ? acc[pp][n].y : acc[pp][n].x;
+          float& im = c ? acc[pp][n + 1].y : acc[pp][n + 1].x;
+          rotate_pair(re, im, e);
+        }
+      }
 #pragma unroll
     for (int pp = 0; pp < PP; ++pp)
 #pragma unroll
@@ -534,6 +736,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_rows_x2_kernel(RowArgs a) {
 // ----------------------------------------------------------- points kernel ----
 struct PointArgs {
   const float* tiles;
+  const double4* anchors;
   int ntiles;
   const double* qx;
   const double* qy;
@@ -551,15 +754,19 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
   const long iz = (long)blockIdx.x * BLOCK + threadIdx.x;
   const bool valid = iz < a.nqz;
   float qxf = 0.f, qyf = 0.f, qzr = 0.f, qzi = 0.f;
+  double qxd = 0.0, qyd = 0.0, qzd = 0.0, qzid = 0.0;
   if (valid) {
     long iy = iz % a.nqy;
-    qxf = (float)a.qx[iy];
-    qyf = (float)a.qy[iy];
+    qxd = a.qx[iy];
+    qyd = a.qy[iy];
     double2 q = a.qz[iz];
+    qzd = q.x;
+    qzid = q.y;
+    qxf = (float)qxd;
+    qyf = (float)qyd;
     qzr = (float)q.x;
     qzi = (float)q.y;
   }
-  const float kexp = (float)(-TWO_PI) * qzi;
   float acc[2] = {0.f, 0.f}, sum[2] = {0.f, 0.f}, cmp[2] = {0.f, 0.f};
 
   if (threadIdx.x == 0) {
@@ -576,6 +783,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
   }
   for (int s = 0; s < a.ntiles; ++s) {
     const int b = s & 1;
+    const double4 anc = a.anchors[s];
     const bool ok = mbar_wait(&s_bar[b], (s >> 1) & 1);
     if (__syncthreads_or(!ok)) {
       if (threadIdx.x == 0) {
@@ -592,12 +800,12 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
     for (int j = 0; j < TILE; ++j) {
       const float4 t = A[j];
       const float2 z = B[j];
-      float tp = fmaf(qzr, z.x, fmaf(qxf, t.x, qyf * t.y));
-      float rr = tp - rintf(tp);
+      float tt = fmaf(qzr, z.x, fmaf(qxf, t.x, qyf * t.y)) * INV_TWO_PI_F;  // turns
+      float rr = tt - rintf(tt);
       float sn, cs;
-      __sincosf(rr * 6.28318530717958648f, &sn, &cs);
+      __sincosf(rr * TWO_PI_F, &sn, &cs);
       if (qzi != 0.f) {
-        float amp = __expf(kexp * z.x);
+        float amp = __expf(-qzi * z.x);
         sn *= amp;
         cs *= amp;
       }
@@ -608,6 +816,14 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
       acc[1] = fmaf(ar, sn, acc[1]);
       acc[1] = fmaf(ai, cs, acc[1]);
     }
+    // the anchor e^{i q.c0} (FP64 phase, amplitude e^{-Im(qz) c0z}) on the tile's sums
+    float2 e = anchor_phasor(fma(qxd, anc.x, fma(qyd, anc.y, qzd * anc.z * INV_TWO_PI)));
+    if (qzid != 0.0) {
+      const float amp0 = (float)exp(-qzid * anc.z);
+      e.x *= amp0;
+      e.y *= amp0;
+    }
+    rotate_pair(acc[0], acc[1], e);
     two_sum_fold(sum[0], acc[0], cmp[0]);
     two_sum_fold(sum[1], acc[1], cmp[1]);
     __syncthreads();
@@ -752,6 +968,84 @@ static RowShape row_shape(int nrow, int ncol, int sm_count, int want_p) {
   return best;
 }
 
+// Scratch of the FP32 tile preparation, carved from the context's scratch buffer.
+struct TilePrep {
+  float* tiles = nullptr;
+  double4* anchors = nullptr;
+  int* perm = nullptr;
+  unsigned* keys[2] = {nullptr, nullptr};
+  int* idx[2] = {nullptr, nullptr};
+  double* bbox = nullptr;
+  void* sort_tmp = nullptr;
+  size_t sort_bytes = 0;
+};
+
+static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Prepares the tiles of ntri triangles (layout: scalar or packed) in Morton order, with
+// their anchors and slot -> triangle map, on the context's stream; records them in c->tiles.
+static int prepare_tiles(hgx_ctx c, const double* sd, int ntri, const Rot9& R, bool x2,
+                         TilePrep* out) {
+  cudaStream_t st = c->stream;
+  const int ntiles = (ntri + TILE - 1) / TILE;
+  const size_t tile_bytes = (size_t)ntiles * (x2 ? TILE_X2_BYTES : TILE_BYTES);
+  const int nparts = std::min(BBOX_MAX_BLOCKS, (ntri + BBOX_THREADS - 1) / BBOX_THREADS);
+  const bool sort = ntiles > 1;
+  size_t sort_bytes = 0;
+  if (sort) {
+    HGX_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const unsigned*)nullptr,
+                                             (unsigned*)nullptr, (const int*)nullptr, (int*)nullptr,
+                                             ntri, 0, 30, st));
+  }
+  size_t off[9];
+  size_t total = 0;
+  const size_t sizes[9] = {tile_bytes,
+                           sizeof(double4) * (size_t)ntiles,
+                           sizeof(int) * (size_t)ntiles * TILE,
+                           sort ? sizeof(unsigned) * (size_t)ntri : 0,
+                           sort ? sizeof(unsigned) * (size_t)ntri : 0,
+                           sort ? sizeof(int) * (size_t)ntri : 0,
+                           sort ? sizeof(int) * (size_t)ntri : 0,
+                           sort ? sizeof(double) * 6 * (size_t)nparts : 0,
+                           sort_bytes};
+  for (int i = 0; i < 9; ++i) {
+    off[i] = total;
+    total += align256(sizes[i]);
+  }
+  HGX_TRY(c->scratch.reserve(total));
+  char* base = reinterpret_cast<char*>(c->scratch.p);
+  TilePrep t;
+  t.tiles = reinterpret_cast<float*>(base + off[0]);
+  t.anchors = reinterpret_cast<double4*>(base + off[1]);
+  t.perm = reinterpret_cast<int*>(base + off[2]);
+  const int* order = nullptr;
+  if (sort) {
+    t.keys[0] = reinterpret_cast<unsigned*>(base + off[3]);
+    t.keys[1] = reinterpret_cast<unsigned*>(base + off[4]);
+    t.idx[0] = reinterpret_cast<int*>(base + off[5]);
+    t.idx[1] = reinterpret_cast<int*>(base + off[6]);
+    t.bbox = reinterpret_cast<double*>(base + off[7]);
+    t.sort_tmp = base + off[8];
+    t.sort_bytes = sort_bytes;
+    tri_bbox_kernel<<<nparts, BBOX_THREADS, 0, st>>>(sd, ntri, t.bbox);
+    tri_bbox_final_kernel<<<1, BBOX_THREADS, 0, st>>>(t.bbox, nparts);
+    tri_key_kernel<<<(ntri + 255) / 256, 256, 0, st>>>(sd, ntri, t.bbox, t.keys[0], t.idx[0]);
+    HGX_CUDA(cudaGetLastError());
+    size_t tb = sort_bytes;
+    HGX_CUDA(cub::DeviceRadixSort::SortPairs(t.sort_tmp, tb, t.keys[0], t.keys[1], t.idx[0],
+                                             t.idx[1], ntri, 0, 30, st));
+    order = t.idx[1];
+  }
+  if (x2)
+    tri_tile_kernel<true><<<ntiles, TILE, 0, st>>>(sd, ntri, R, order, t.tiles, t.anchors, t.perm);
+  else
+    tri_tile_kernel<false><<<ntiles, TILE, 0, st>>>(sd, ntri, R, order, t.tiles, t.anchors, t.perm);
+  HGX_CUDA(cudaGetLastError());
+  c->tiles = TileView{t.tiles, t.anchors, t.perm, ntiles, ntri};
+  *out = t;
+  return HGX_OK;
+}
+
 int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, const double* rot9,
                         int precision, void* out, int ff_type, int want_p) {
   cudaStream_t st = c->stream;
@@ -768,23 +1062,19 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
   if (want_p == 0) want_p = g->tuned_p;  // the autotuner's choice for this grid, if any
   const int ntiles = (ntri + TILE - 1) / TILE;
   // paired real DWBA blocks, packed FP32x2 kernel on request (want_p = -2, -4, -8 pixels per
-  // thread).  Measured on a 2048 x 2048 detector with 50,000 triangles it runs at the speed of
-  // the scalar kernel (both sit on the FP32 pipe), so automatic (0) picks the scalar one.
+  // thread); automatic (0) picks the scalar one.
   if (g->mode == 1 && want_p < 0) {
     const int P = -want_p;
     if (P != 2 && P != 4 && P != 8)
       return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: packed kernel takes 2, 4 or 8 pixels per thread");
-    HGX_TRY(c->scratch.reserve((size_t)ntiles * TILE_X2_BYTES));
-    float* tiles = reinterpret_cast<float*>(c->scratch.p);
-    int n = ntiles * TILE;
-    tri_prep_x2_kernel<<<(n + 255) / 256, 256, 0, st>>>(sd, ntri, ntiles, R, tiles);
-    HGX_CUDA(cudaGetLastError());
     RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, P);
     if (sh.P < 2) sh = row_shape(g->nrow, g->ncol, 0, 2);  // keep at least one pair
     if (sh.grid.y > 65535u)
       return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: too many detector rows for one launch");
-    RowArgs a{tiles, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R, out,
-              c->d_err};
+    TilePrep t;
+    HGX_TRY(prepare_tiles(c, sd, ntri, R, true, &t));
+    RowArgs a{t.tiles, t.anchors, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R,
+              out, c->d_err};
     switch (sh.P) {
       case 8:
         return c64 ? launch_rows_x2<256, 4, float2>(a, sh.grid, st) : launch_rows_x2<256, 4, double2>(a, sh.grid, st);
@@ -794,16 +1084,11 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
         return c64 ? launch_rows_x2<256, 1, float2>(a, sh.grid, st) : launch_rows_x2<256, 1, double2>(a, sh.grid, st);
     }
   }
-  // FP32 scalar kernels: triangle tiles in scratch
-  HGX_TRY(c->scratch.reserve((size_t)ntiles * TILE_BYTES));
-  float* tiles = reinterpret_cast<float*>(c->scratch.p);
-  {
-    int n = ntiles * TILE;
-    tri_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(sd, ntri, ntiles, R, tiles);
-    HGX_CUDA(cudaGetLastError());
-  }
+  // FP32 scalar kernels
   if (g->mode == 0) {
-    PointArgs a{tiles, ntiles, g->qx, g->qy, g->qz, g->nqy, g->nqz, R, out, c->d_err};
+    TilePrep t;
+    HGX_TRY(prepare_tiles(c, sd, ntri, R, false, &t));
+    PointArgs a{t.tiles, t.anchors, ntiles, g->qx, g->qy, g->qz, g->nqy, g->nqz, R, out, c->d_err};
     dim3 grid((g->nqz + 127) / 128);
     if (c64) ff_tri_points_kernel<128, float2><<<grid, 128, 0, st>>>(a);
     else ff_tri_points_kernel<128, double2><<<grid, 128, 0, st>>>(a);
@@ -813,8 +1098,10 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
   RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, want_p > 0 ? want_p : 4);
   if (sh.grid.y > 65535u)
     return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: too many detector rows for one launch");
-  RowArgs a{tiles, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R, out,
-            c->d_err};
+  TilePrep t;
+  HGX_TRY(prepare_tiles(c, sd, ntri, R, false, &t));
+  RowArgs a{t.tiles, t.anchors, ntiles, g->qx, g->qy, g->rowqz, g->nqy, g->nrow, g->ncol, sh.R, R,
+            out, c->d_err};
   const bool paired = g->mode == 1;
   switch (sh.P) {
     case 4:
@@ -966,26 +1253,29 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
 // allocate device memory — a plug-in that lives inside another framework's memory pool and
 // is handed only device pointers, a service held to a fixed device-memory budget, or a
 // real-time loop in which a cudaMalloc/cudaFree would synchronise the whole device.  Its
-// scratch (the FP32 triangle tiles and an error word) is a file-scope static device array of
-// fixed size, reserved when the library's device code is loaded on a GPU and held until exit.
+// scratch (the FP32 triangle tiles, their anchors and an error word) lives in file-scope
+// static device arrays of fixed size, reserved when the library's device code is loaded on a
+// GPU and held until exit.
 //
-// In host code the array name below is only a host-side stand-in, not a device address:
-// the device address is obtained once per device with cudaGetSymbolAddress (set-up done by
+// In host code the array names below are only host-side stand-ins, not device addresses:
+// the device addresses are obtained once per device with cudaGetSymbolAddress (set-up done by
 // the first call on each device, with that device current; make that first call before any
 // stream capture) and passed to the kernels.  Every call shares the array: the triangle
 // tiles are fully rewritten by each call and the error word is cleared at its start; calls
 // that overlap on the GPU (different streams, no ordering) race on the array and must be
 // ordered by the caller.  hgx_ff_triangles_noalloc_status reads the error word back.
 constexpr int NOALLOC_MAX_TRIANGLES = 65536;
-constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 512 tiles, 1.5 MiB
+constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 512 tiles, 1.5 MiB + 16 KiB anchors
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) float g_noalloc_tiles[NOALLOC_MAX_TILES * TILE_FLOATS];
+static __device__ __align__(256) double4 g_noalloc_anchors[NOALLOC_MAX_TILES];
 static __device__ __align__(256) unsigned g_noalloc_err;
 
 namespace {
 struct NoallocSlot {
   float* tiles = nullptr;
+  double4* anchors = nullptr;
   unsigned* err = nullptr;
 };
 NoallocSlot g_noalloc_slots[NOALLOC_MAX_DEVICES];
@@ -996,12 +1286,16 @@ int noalloc_setup(int dev, NoallocSlot* out) {
   NoallocSlot& s = g_noalloc_slots[dev];
   if (!s.tiles) {
     void* t = nullptr;
+    void* an = nullptr;
     void* e = nullptr;
     cudaError_t rc = cudaGetSymbolAddress(&t, g_noalloc_tiles);
     if (rc != cudaSuccess) return cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_tiles)");
+    rc = cudaGetSymbolAddress(&an, g_noalloc_anchors);
+    if (rc != cudaSuccess) return cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_anchors)");
     rc = cudaGetSymbolAddress(&e, g_noalloc_err);
     if (rc != cudaSuccess) return cuda_fail(rc, "cudaGetSymbolAddress(g_noalloc_err)");
     s.tiles = static_cast<float*>(t);
+    s.anchors = static_cast<double4*>(an);
     s.err = static_cast<unsigned*>(e);
   }
   *out = s;
@@ -1033,13 +1327,13 @@ extern "C" int hgx_ff_triangles_noalloc(const double* shape_def, int ntri, int n
   Rot9 R = make_rot(rot9);
   const int ntiles = (ntri + TILE - 1) / TILE;
   HGX_CUDA(cudaMemsetAsync(slot.err, 0, sizeof(unsigned), st));
-  {
-    int n = ntiles * TILE;
-    tri_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(shape_def, ntri, ntiles, R, slot.tiles);
-    HGX_CUDA(cudaGetLastError());
-  }
-  PointArgs a{slot.tiles, ntiles, qx, qy, reinterpret_cast<const double2*>(qz), nqy, nqz, R, ff,
-              slot.err};
+  // tiles in the caller's triangle order (no sort, which would need more scratch), each with
+  // its FP64 anchor
+  tri_tile_kernel<false><<<ntiles, TILE, 0, st>>>(shape_def, ntri, R, nullptr, slot.tiles,
+                                                 slot.anchors, nullptr);
+  HGX_CUDA(cudaGetLastError());
+  PointArgs a{slot.tiles, slot.anchors, ntiles, qx, qy, reinterpret_cast<const double2*>(qz), nqy,
+              nqz, R, ff, slot.err};
   dim3 grid((nqz + 127) / 128);
   if (ff_type == HGX_C64) ff_tri_points_kernel<128, float2><<<grid, 128, 0, st>>>(a);
   else ff_tri_points_kernel<128, double2><<<grid, 128, 0, st>>>(a);

@@ -56,6 +56,16 @@ namespace hgx {
 struct MeshWork {
   DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib, bwpart;
 };
+// The FP32 triangle tiles that the last FP32C form-factor call of a context left in its
+// scratch (ff_tri.cu), read by the mesh adjoint: 128 triangles per tile, per-tile anchors
+// (FP64 tile centre: in-plane in turns, z in nm; largest in-plane offset from it, nm) and the
+// caller's index of the triangle in each tile slot (-1 for padding).
+struct TileView {
+  const float* tiles = nullptr;
+  const double4* anchors = nullptr;
+  const int* perm = nullptr;
+  int ntiles = 0, ntri = 0;
+};
 // A custom shape's triangle tuples on the device, with the file's identity when it was read.
 struct MeshTuples {
   DevBuf tri;  // ntri x 8 doubles (read_shapes_file layout)
@@ -81,6 +91,7 @@ struct hgx_ctx_s {
   cudaStream_t stream = nullptr;
   unsigned* d_err = nullptr;  // device error word (DeviceError bits)
   hgx::DevBuf scratch;        // per-call scratch, grown on demand
+  hgx::TileView tiles;        // triangle tiles of the last FP32C form factor (in scratch)
   hgx::DevBuf staging;        // device copies of host inputs
   int sm_count = 148;
   int max_smem_optin = 227 * 1024;

@@ -79,7 +79,7 @@ __global__ void mesh_to_shape_kernel(const double* __restrict__ v, int nv, const
 // ------------------------------------------------------------ adjoint seeds ----
 // Per pixel: A, I, chi^2 term, and the paired seeds (H0+H3, H0-H3, H2+H1, H2-H1) in FP32.
 struct SeedArgs {
-  const float2* F;         // 4N form factor (FP32C output)
+  const void* F;           // 4N form factor (complex64 for FP32C, complex128 for FP64)
   const double2* rowfc;    // nrow x 4
   const double2* rowqz;    // nrow x 4
   const double* qx;
@@ -90,11 +90,28 @@ struct SeedArgs {
   const double* counts;
   const unsigned* mask;
   double scale;
-  float4* seeds;           // 2 float4 per pixel
+  void* seeds;             // 2 float4 (FP32C) or 2 double4 (FP64) per pixel
   double* intensity;       // may be NULL
   double* partial;         // chi^2 per block
 };
 
+__device__ __forceinline__ zd load_ff(const float2* F, long i) {
+  const float2 f = F[i];
+  return zd((double)f.x, (double)f.y);
+}
+__device__ __forceinline__ zd load_ff(const double2* F, long i) { return zd(F[i]); }
+__device__ __forceinline__ void store_seeds(float4* S, long p, const zd* H) {
+  S[2 * p] = make_float4((float)(H[0].x + H[3].x), (float)(H[0].y + H[3].y),
+                         (float)(H[0].x - H[3].x), (float)(H[0].y - H[3].y));
+  S[2 * p + 1] = make_float4((float)(H[2].x + H[1].x), (float)(H[2].y + H[1].y),
+                             (float)(H[2].x - H[1].x), (float)(H[2].y - H[1].y));
+}
+__device__ __forceinline__ void store_seeds(double4* S, long p, const zd* H) {
+  S[2 * p] = make_double4(H[0].x + H[3].x, H[0].y + H[3].y, H[0].x - H[3].x, H[0].y - H[3].y);
+  S[2 * p + 1] = make_double4(H[2].x + H[1].x, H[2].y + H[1].y, H[2].x - H[1].x, H[2].y - H[1].y);
+}
+
+template <typename FT, typename ST>
 __global__ void __launch_bounds__(256) mesh_seed_kernel(SeedArgs a) {
   __shared__ double red[8];
   long n = (long)a.nrow * a.ncol;
@@ -109,8 +126,7 @@ __global__ void __launch_bounds__(256) mesh_seed_kernel(SeedArgs a) {
     double qx = a.qx[p], qy = a.qy[p];
     for (int k = 0; k < 4; ++k) {
       fcK[k] = zd(a.rowfc[4 * row + k]) * K;
-      float2 f = a.F[(long)k * n + p];
-      A += fcK[k] * zd((double)f.x, (double)f.y);
+      A += fcK[k] * load_ff(static_cast<const FT*>(a.F), (long)k * n + p);
       double qz = a.rowqz[4 * row + k].x, s = 0.0;
       for (int j = 0; j < 3; ++j) {
         double m = a.R[3 * j] * qx + a.R[3 * j + 1] * qy + a.R[3 * j + 2] * qz;
@@ -136,10 +152,7 @@ __global__ void __launch_bounds__(256) mesh_seed_kernel(SeedArgs a) {
       zd h = base * fcK[k];
       H[k] = zd(h.y, -h.x) / q2[k];  // times -i
     }
-    a.seeds[2 * p] = make_float4((float)(H[0].x + H[3].x), (float)(H[0].y + H[3].y),
-                                 (float)(H[0].x - H[3].x), (float)(H[0].y - H[3].y));
-    a.seeds[2 * p + 1] = make_float4((float)(H[2].x + H[1].x), (float)(H[2].y + H[1].y),
-                                     (float)(H[2].x - H[1].x), (float)(H[2].y - H[1].y));
+    store_seeds(static_cast<ST*>(a.seeds), p, H);
   }
   // block sum of chi^2 (fixed order)
 #pragma unroll
@@ -154,13 +167,19 @@ __global__ void __launch_bounds__(256) mesh_seed_kernel(SeedArgs a) {
 }
 
 // ------------------------------------------------------------- backward pass ----
-constexpr int BW_THREADS = 128;
+// One CTA per triangle tile of the forward (128 triangles, 2 per thread) and chunk of rows.
+// The tile's offsets d = c' - c0 carry the FP32 phases; the anchor phasor e^{i q_par.c0}
+// (FP64 phase) is folded into the seeds when a pixel is staged, and the row phasors take the
+// full z centroid c0z + dz in FP64.
+constexpr int BW_THREADS = 64;
 constexpr int BW_TPT = 2;                       // triangles per thread
-constexpr int BW_TRI = BW_THREADS * BW_TPT;     // triangles per CTA
+constexpr int BW_TRI = BW_THREADS * BW_TPT;     // triangles per CTA = one forward tile
 constexpr int BW_COLS = 256;                    // pixels staged per step
 
 struct BwArgs {
-  const float* tiles;        // the FP32 triangle tiles of the forward (rotated, turns)
+  const float* tiles;        // the forward's FP32 tiles (offsets in nm, s n' components)
+  const double4* anchors;    // per tile: c0x/2pi, c0y/2pi, c0z, max in-plane offset
+  const int* perm;           // slot -> triangle (-1: padding)
   int ntri;
   const float4* seeds;
   const double* qx;
@@ -170,25 +189,31 @@ struct BwArgs {
   double* partial;           // [chunk][ntri][6]
 };
 
+__device__ __forceinline__ float4 rotate2(float4 v, float ca, float sa) {
+  return make_float4(v.x * ca - v.y * sa, v.x * sa + v.y * ca, v.z * ca - v.w * sa,
+                     v.z * sa + v.w * ca);
+}
+
 __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
-  __shared__ float4 s_px[BW_COLS * 3];  // (qx, qy, -, -), seeds 0, seeds 1
+  __shared__ float4 s_px[BW_COLS * 3];  // (qx, qy, -, -), seeds 0, seeds 1 (anchor-rotated)
   const int TILE_T = 128;               // the forward's tile layout
+  const int tile = blockIdx.x;
   const int chunk = blockIdx.y;
   const int r0 = chunk * a.rows_per_chunk;
   const int r1 = min(a.nrow, r0 + a.rows_per_chunk);
+  const double4 anc = a.anchors[tile];
+  const double cz0 = anc.z * INV_TWO_PI_M;
   // this thread's triangles
   float cx[BW_TPT], cy[BW_TPT], cz[BW_TPT], nx[BW_TPT], ny[BW_TPT], nz[BW_TPT];
   double acc[BW_TPT][6];
-  bool live[BW_TPT];
+  int orig[BW_TPT];
+  const float* tl = a.tiles + (size_t)tile * TILE_T * 6;
 #pragma unroll
   for (int u = 0; u < BW_TPT; ++u) {
-    int t = blockIdx.x * BW_TRI + u * BW_THREADS + threadIdx.x;
-    live[u] = t < a.ntri;
-    int tt = live[u] ? t : 0;
-    const float* tile = a.tiles + (size_t)(tt / TILE_T) * TILE_T * 6;
-    int j = tt % TILE_T;
-    float4 A = reinterpret_cast<const float4*>(tile)[j];
-    float2 B = reinterpret_cast<const float2*>(tile + 4 * TILE_T)[j];
+    const int j = u * BW_THREADS + threadIdx.x;
+    orig[u] = a.perm[(size_t)tile * TILE_T + j];
+    float4 A = reinterpret_cast<const float4*>(tl)[j];
+    float2 B = reinterpret_cast<const float2*>(tl + 4 * TILE_T)[j];
     cx[u] = A.x; cy[u] = A.y; nx[u] = A.z; ny[u] = A.w; cz[u] = B.x; nz[u] = B.y;
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[u][q] = 0.0;
@@ -199,7 +224,8 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
     float x0[BW_TPT], y0[BW_TPT], x2[BW_TPT], y2[BW_TPT];
 #pragma unroll
     for (int u = 0; u < BW_TPT; ++u) {
-      double w0 = qz0 * (double)cz[u], w2 = qz2 * (double)cz[u];
+      const double czt = cz0 + (double)cz[u] * INV_TWO_PI_M;  // full z centroid, turns
+      double w0 = qz0 * czt, w2 = qz2 * czt;
       w0 -= rint(w0);
       w2 -= rint(w2);
       sincospif((float)(2.0 * w0), &y0[u], &x0[u]);
@@ -215,9 +241,14 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
       __syncthreads();
       for (int i = threadIdx.x; i < nc; i += BW_THREADS) {
         long p = (long)row * a.ncol + c0 + i;
-        s_px[3 * i] = make_float4((float)a.qx[p], (float)a.qy[p], 0.f, 0.f);
-        s_px[3 * i + 1] = a.seeds[2 * p];
-        s_px[3 * i + 2] = a.seeds[2 * p + 1];
+        const double qx = a.qx[p], qy = a.qy[p];
+        double w = fma(qx, anc.x, qy * anc.y);
+        w -= rint(w);
+        float sa, ca;
+        sincospif((float)(2.0 * w), &sa, &ca);
+        s_px[3 * i] = make_float4((float)qx, (float)qy, 0.f, 0.f);
+        s_px[3 * i + 1] = rotate2(a.seeds[2 * p], ca, sa);
+        s_px[3 * i + 2] = rotate2(a.seeds[2 * p + 1], ca, sa);
       }
       __syncthreads();
       for (int i = 0; i < nc; ++i) {
@@ -226,8 +257,8 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
         const float4 s21 = s_px[3 * i + 2];  // (P21, M21)
 #pragma unroll
         for (int u = 0; u < BW_TPT; ++u) {
-          float tp = fmaf(q.x, cx[u], q.y * cy[u]);
-          float rr = tp - ((tp + 12582912.0f) - 12582912.0f);  // exact reduction, |tp| < 2^22
+          float tt = fmaf(q.x, cx[u], q.y * cy[u]) * 0.159154943091895336f;  // turns
+          float rr = tt - ((tt + 12582912.0f) - 12582912.0f);  // exact reduction, |tt| < 2^22
           float sn, cs;
           __sincosf(rr * 6.28318530717958648f, &sn, &cs);
           float aq = fmaf(q.x, nx[u], q.y * ny[u]);
@@ -260,9 +291,105 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
   }
 #pragma unroll
   for (int u = 0; u < BW_TPT; ++u) {
-    int t = blockIdx.x * BW_TRI + u * BW_THREADS + threadIdx.x;
-    if (!live[u]) continue;
-    double* dst = a.partial + ((size_t)chunk * a.ntri + t) * 6;
+    if (orig[u] < 0) continue;
+    double* dst = a.partial + ((size_t)chunk * a.ntri + orig[u]) * 6;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) dst[q] = acc[u][q];
+  }
+}
+
+// The plain FP64 backward pass (the FP64 reference of the FP32 one): triangles read from the
+// FP64 tuples and rotated in the kernel, every phase and sum in FP64, same CTA layout
+// (128 triangles per CTA, 2 per thread) and chunking; partial gradients in the caller's
+// triangle order.
+constexpr int BW64_COLS = 128;
+
+struct Bw64Args {
+  const double* sd;          // ntri x 8 tuples
+  int ntri;
+  Rot9d R;
+  const double4* seeds;      // 2 per pixel: (P03, M03), (P21, M21)
+  const double* qx;
+  const double* qy;
+  const double2* rowqz;
+  int nrow, ncol, rows_per_chunk;
+  double* partial;           // [chunk][ntri][6]
+};
+
+__global__ void __launch_bounds__(BW_THREADS) mesh_backward_f64_kernel(Bw64Args a) {
+  __shared__ double2 s_q[BW64_COLS];
+  __shared__ double4 s_s[BW64_COLS * 2];
+  const int chunk = blockIdx.y;
+  const int r0 = chunk * a.rows_per_chunk;
+  const int r1 = min(a.nrow, r0 + a.rows_per_chunk);
+  double c[BW_TPT][3], nn[BW_TPT][3], acc[BW_TPT][6];
+  int tri[BW_TPT];
+#pragma unroll
+  for (int u = 0; u < BW_TPT; ++u) {
+    const int t = blockIdx.x * BW_TRI + u * BW_THREADS + threadIdx.x;
+    tri[u] = t < a.ntri ? t : -1;
+    const double* p = a.sd + 8L * (t < a.ntri ? t : 0);
+    const double s = t < a.ntri ? p[0] : 0.0;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      nn[u][l] = s * (a.R.r[l] * p[1] + a.R.r[3 + l] * p[2] + a.R.r[6 + l] * p[3]);
+      c[u][l] = a.R.r[l] * p[4] + a.R.r[3 + l] * p[5] + a.R.r[6 + l] * p[6];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) acc[u][q] = 0.0;
+  }
+  for (int row = r0; row < r1; ++row) {
+    const double qz0 = a.rowqz[4L * row].x, qz2 = a.rowqz[4L * row + 2].x;
+    double x0[BW_TPT], y0[BW_TPT], x2[BW_TPT], y2[BW_TPT];
+#pragma unroll
+    for (int u = 0; u < BW_TPT; ++u) {
+      sincos(qz0 * c[u][2], &y0[u], &x0[u]);
+      sincos(qz2 * c[u][2], &y2[u], &x2[u]);
+    }
+    for (int c0 = 0; c0 < a.ncol; c0 += BW64_COLS) {
+      const int nc = min(BW64_COLS, a.ncol - c0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < nc; i += BW_THREADS) {
+        const long p = (long)row * a.ncol + c0 + i;
+        s_q[i] = make_double2(a.qx[p], a.qy[p]);
+        s_s[2 * i] = a.seeds[2 * p];
+        s_s[2 * i + 1] = a.seeds[2 * p + 1];
+      }
+      __syncthreads();
+      for (int i = 0; i < nc; ++i) {
+        const double2 q = s_q[i];
+        const double4 s03 = s_s[2 * i], s21 = s_s[2 * i + 1];
+#pragma unroll
+        for (int u = 0; u < BW_TPT; ++u) {
+          double sn, cs;
+          sincos(q.x * c[u][0] + q.y * c[u][1], &sn, &cs);
+          const double aq = q.x * nn[u][0] + q.y * nn[u][1];
+          const double p03r = s03.x * x0[u] - s03.w * y0[u], p03i = s03.y * x0[u] + s03.z * y0[u];
+          const double b03r = s03.z * x0[u] - s03.y * y0[u], b03i = s03.w * x0[u] + s03.x * y0[u];
+          const double p21r = s21.x * x2[u] - s21.w * y2[u], p21i = s21.y * x2[u] + s21.z * y2[u];
+          const double b21r = s21.z * x2[u] - s21.y * y2[u], b21i = s21.w * x2[u] + s21.x * y2[u];
+          const double psr = p03r + p21r, psi = p03i + p21i;
+          const double pzr = qz0 * b03r + qz2 * b21r, pzi = qz0 * b03i + qz2 * b21i;
+          const double pzzr = qz0 * qz0 * p03r + qz2 * qz2 * p21r;
+          const double pzzi = qz0 * qz0 * p03i + qz2 * qz2 * p21i;
+          const double eR = cs * psr - sn * psi, eI = cs * psi + sn * psr;
+          const double ezR = cs * pzr - sn * pzi, ezI = cs * pzi + sn * pzr;
+          const double ezzI = cs * pzzi + sn * pzzr;
+          acc[u][0] += eR * q.x;
+          acc[u][1] += eR * q.y;
+          acc[u][2] += ezR;
+          const double gxy = aq * eI + nn[u][2] * ezI;
+          acc[u][3] -= gxy * q.x;
+          acc[u][4] -= gxy * q.y;
+          acc[u][5] -= aq * ezI + nn[u][2] * ezzI;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < BW_TPT; ++u) {
+    if (tri[u] < 0) continue;
+    double* dst = a.partial + ((size_t)chunk * a.ntri + tri[u]) * 6;
 #pragma unroll
     for (int q = 0; q < 6; ++q) dst[q] = acc[u][q];
   }
@@ -345,13 +472,16 @@ int hgx_mesh_to_shape_def(hgx_ctx c, int nv, const double* verts, int nf, const 
   return hgx_synchronize(c);
 }
 
-int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int nf,
-                       const int* faces, const double* rot9, const double* rowfc,
-                       double dn2_re, double dn2_im, double weight, const double* counts,
-                       const unsigned* mask, double scale, double* chi2, double* grad_verts,
-                       double* intensity) {
+int hgx_mesh_chi2_grad_ex(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int nf,
+                          const int* faces, const double* rot9, const double* rowfc,
+                          double dn2_re, double dn2_im, double weight, const double* counts,
+                          const unsigned* mask, double scale, double* chi2, double* grad_verts,
+                          double* intensity, int precision) {
   if (!c || !g || !verts || !faces || !rowfc || !chi2 || nv < 3 || nf < 1)
     return fail(HGX_ERR_INVALID_ARG, "hgx_mesh_chi2_grad: null argument or empty mesh");
+  if (precision != HGX_F32C && precision != HGX_F64)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_mesh_chi2_grad: unknown precision");
+  const bool f64 = precision == HGX_F64;
   if (g->mode != 1)
     return fail(HGX_ERR_INVALID_ARG, "hgx_mesh_chi2_grad: needs a DWBA grid with real qz constant "
                                      "along rows (vacuum particle layer)");
@@ -379,17 +509,19 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
   HGX_TRY(sd.reserve(sizeof(double) * 8 * nf));
   mesh_to_shape_kernel<<<(nf + 127) / 128, 128, 0, st>>>((const double*)dv, nv, (const int*)df, nf,
                                                          (double*)sd.p, c->d_err);
-  HGX_TRY(F.reserve(sizeof(float2) * 4 * n));
-  // the scalar row kernel (4 pixels/thread): the backward pass reads its triangle tiles
-  HGX_TRY(ff_triangles_device(c, g, (const double*)sd.p, nf, R, HGX_F32C, F.p, HGX_C64, 4));
+  HGX_TRY(F.reserve((f64 ? sizeof(double2) : sizeof(float2)) * 4 * n));
+  // FP32C: the scalar row kernel (4 pixels/thread), whose triangle tiles the backward pass
+  // reads; FP64: the plain FP64 kernel
+  HGX_TRY(ff_triangles_device(c, g, (const double*)sd.p, nf, R, precision, F.p,
+                              f64 ? HGX_C128 : HGX_C64, 4));
   // 3. intensity, chi^2, seeds
   const int sblocks = (int)((n + 255) / 256);
-  HGX_TRY(seeds.reserve(sizeof(float4) * 2 * n));
+  HGX_TRY(seeds.reserve((f64 ? sizeof(double4) : sizeof(float4)) * 2 * n));
   HGX_TRY(part.reserve(sizeof(double) * (sblocks + 1)));
   void* dI = nullptr;
   if (intensity) HGX_TRY(stage_out(c, intensity, sizeof(double) * n, Ib, &dI));
   SeedArgs sa;
-  sa.F = (const float2*)F.p;
+  sa.F = F.p;
   sa.rowfc = (const double2*)dfc;
   sa.rowqz = g->rowqz;
   sa.qx = g->qx;
@@ -402,36 +534,60 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
   sa.counts = (const double*)dc;
   sa.mask = (const unsigned*)dm;
   sa.scale = scale;
-  sa.seeds = (float4*)seeds.p;
+  sa.seeds = seeds.p;
   sa.intensity = (double*)dI;
   sa.partial = (double*)part.p;
-  mesh_seed_kernel<<<sblocks, 256, 0, st>>>(sa);
+  if (f64) mesh_seed_kernel<double2, double4><<<sblocks, 256, 0, st>>>(sa);
+  else mesh_seed_kernel<float2, float4><<<sblocks, 256, 0, st>>>(sa);
   HGX_CUDA(cudaGetLastError());
   std::vector<double> hpart(sblocks);
   HGX_CUDA(cudaMemcpyAsync(hpart.data(), part.p, sizeof(double) * sblocks, cudaMemcpyDeviceToHost, st));
   if (grad_verts) {
-    // 4. backward over (triangle tiles) x (row chunks)
-    const int ntile = (nf + BW_TRI - 1) / BW_TRI;
-    int chunks = std::max(1, (2 * c->sm_count * 4) / std::max(1, ntile));
+    // 4. backward over (triangle tiles) x (row chunks): the FP32C forward's tiles, or the
+    // FP64 tuples in blocks of 128
+    const TileView tv = c->tiles;
+    if (!f64 && (tv.ntri != nf || !tv.perm))
+      return fail(HGX_ERR_INVALID_ARG, "hgx_mesh_chi2_grad: the forward left no triangle tiles");
+    const int ntile = f64 ? (nf + BW_TRI - 1) / BW_TRI : tv.ntiles;
+    int chunks = std::max(1, (c->sm_count * 16) / std::max(1, ntile));
     chunks = std::min(chunks, g->nrow);
     const int rpc = (g->nrow + chunks - 1) / chunks;
     chunks = (g->nrow + rpc - 1) / rpc;
     HGX_TRY(gtri.reserve(sizeof(double) * 6 * nf));
     DevBuf& bwpart = w.bwpart;
     HGX_TRY(bwpart.reserve(sizeof(double) * 6 * (size_t)nf * chunks));
-    BwArgs ba;
-    ba.tiles = reinterpret_cast<const float*>(c->scratch.p);  // tiles left by the forward
-    ba.ntri = nf;
-    ba.seeds = (const float4*)seeds.p;
-    ba.qx = g->qx;
-    ba.qy = g->qy;
-    ba.rowqz = g->rowqz;
-    ba.nrow = g->nrow;
-    ba.ncol = g->ncol;
-    ba.rows_per_chunk = rpc;
-    ba.partial = (double*)bwpart.p;
     dim3 grid(ntile, chunks);
-    mesh_backward_kernel<<<grid, BW_THREADS, 0, st>>>(ba);
+    if (f64) {
+      Bw64Args ba;
+      ba.sd = (const double*)sd.p;
+      ba.ntri = nf;
+      for (int i2 = 0; i2 < 9; ++i2) ba.R.r[i2] = R[i2];
+      ba.seeds = (const double4*)seeds.p;
+      ba.qx = g->qx;
+      ba.qy = g->qy;
+      ba.rowqz = g->rowqz;
+      ba.nrow = g->nrow;
+      ba.ncol = g->ncol;
+      ba.rows_per_chunk = rpc;
+      ba.partial = (double*)bwpart.p;
+      mesh_backward_f64_kernel<<<grid, BW_THREADS, 0, st>>>(ba);
+    } else {
+      BwArgs ba;
+      ba.tiles = tv.tiles;  // tiles left by the forward
+      ba.anchors = tv.anchors;
+      ba.perm = tv.perm;
+      ba.ntri = nf;
+      ba.seeds = (const float4*)seeds.p;
+      ba.qx = g->qx;
+      ba.qy = g->qy;
+      ba.rowqz = g->rowqz;
+      ba.nrow = g->nrow;
+      ba.ncol = g->ncol;
+      ba.rows_per_chunk = rpc;
+      ba.partial = (double*)bwpart.p;
+      mesh_backward_kernel<<<grid, BW_THREADS, 0, st>>>(ba);
+    }
+    HGX_CUDA(cudaGetLastError());
     Rot9d Rd;
     for (int i = 0; i < 9; ++i) Rd.r[i] = R[i];
     mesh_tri_grad_kernel<<<(nf + 127) / 128, 128, 0, st>>>((const double*)bwpart.p, chunks, nf, Rd,
@@ -471,6 +627,15 @@ int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int 
   for (int b = 0; b < sblocks; ++b) s += hpart[b];
   *chi2 = s;
   return HGX_OK;
+}
+
+int hgx_mesh_chi2_grad(hgx_ctx c, hgx_qgrid g, int nv, const double* verts, int nf,
+                       const int* faces, const double* rot9, const double* rowfc,
+                       double dn2_re, double dn2_im, double weight, const double* counts,
+                       const unsigned* mask, double scale, double* chi2, double* grad_verts,
+                       double* intensity) {
+  return hgx_mesh_chi2_grad_ex(c, g, nv, verts, nf, faces, rot9, rowfc, dn2_re, dn2_im, weight,
+                               counts, mask, scale, chi2, grad_verts, intensity, HGX_F32C);
 }
 
 }  // extern "C"

@@ -1,6 +1,6 @@
-// Throughput probes for the roofline denominators of the FP32/SFU-bound kernels:
-// dependent-free FFMA chains (FP32 pipe) and __sinf/__cosf chains (SFU/MUFU pipe), timed
-// with CUDA events on the context's stream.
+// Throughput probes for the roofline denominators of the FP32/SFU/FP64-bound kernels:
+// independent FFMA chains (FP32 pipe), __sinf chains (SFU/MUFU pipe) and DFMA chains (FP64
+// pipe), timed with CUDA events on the context's stream.
 #include <cuda_runtime.h>
 
 #include "hgx_internal.cuh"
@@ -41,9 +41,57 @@ __global__ void __launch_bounds__(256) sfu_probe_kernel(float* out, int iters) {
   if (s == 12345.678f) out[threadIdx.x] = s;
 }
 
+__global__ void __launch_bounds__(256) dfma_probe_kernel(double* out, int iters, double b, double c) {
+  double a[PROBE_CHAINS];
+#pragma unroll
+  for (int k = 0; k < PROBE_CHAINS; ++k) a[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+#pragma unroll
+      for (int k = 0; k < PROBE_CHAINS; ++k) a[k] = fma(a[k], b, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < PROBE_CHAINS; ++k) s += a[k];
+  if (s == 12345.678) out[threadIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace hgx
 
 using namespace hgx;
+
+extern "C" int hgx_measure_peak_fp64(hgx_ctx c, double* fp64_tflops) {
+  if (!c || !fp64_tflops) return fail(HGX_ERR_INVALID_ARG, "hgx_measure_peak_fp64: null argument");
+  HGX_CUDA(cudaSetDevice(c->device));
+  cudaStream_t st = c->stream;
+  HGX_TRY(c->scratch.reserve(4096));
+  double* out = reinterpret_cast<double*>(c->scratch.p);
+  cudaEvent_t e0, e1;
+  HGX_CUDA(cudaEventCreate(&e0));
+  HGX_CUDA(cudaEventCreate(&e1));
+  const int blocks = c->sm_count * 8, threads = 256, iters = 1024;
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    float ms = 0.f;
+    cudaEventRecord(e0, st);
+    dfma_probe_kernel<<<blocks, threads, 0, st>>>(out, iters, 0.999, 1e-4);
+    cudaEventRecord(e1, st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return cuda_fail(e, "hgx_measure_peak_fp64");
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  HGX_CUDA(cudaGetLastError());
+  *fp64_tflops = (double)blocks * threads * iters * 16.0 * PROBE_CHAINS * 2.0 / (best * 1e-3) / 1e12;
+  return HGX_OK;
+}
 
 extern "C" int hgx_measure_peaks(hgx_ctx c, int sustained_ms, double* fp32_tflops,
                                  double* sfu_gops) {

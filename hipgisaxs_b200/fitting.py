@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 from ._capi import F32C, F64, check, lib
-from .core import Context, QGrid, _in
+from .core import PRECISION, Context, QGrid, _in
 
 MODEL_LEN = 16
 THETA = ("radius", "height", "lattice_a", "phi")
@@ -40,8 +40,10 @@ def mesh_to_shape_def(ctx: Context, verts, faces):
 
 
 def mesh_chi2_grad(ctx: Context, grid: QGrid, verts, faces, rowfc, dn2, counts=None, mask=None,
-                   scale=1.0, weight=1.0, rot=None, want_grad=True, want_intensity=False):
-    """(chi2, grad[nv, 3] or None, intensity[N] or None) for a mesh in DWBA."""
+                   scale=1.0, weight=1.0, rot=None, want_grad=True, want_intensity=False,
+                   precision="f32c"):
+    """(chi2, grad[nv, 3] or None, intensity[N] or None) for a mesh in DWBA; precision "f32c"
+    (FP32C forward and backward) or "f64" (plain FP64 throughout)."""
     v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 3)
     f = np.ascontiguousarray(faces, dtype=np.int32).reshape(-1, 3)
     rf = np.ascontiguousarray(rowfc, dtype=np.complex128)
@@ -51,11 +53,12 @@ def mesh_chi2_grad(ctx: Context, grid: QGrid, verts, faces, rowfc, dn2, counts=N
     chi = C.c_double()
     gv = np.zeros((len(v), 3)) if want_grad else None
     inten = np.zeros(grid.nrow * grid.ncol) if want_intensity else None
-    check(lib().hgx_mesh_chi2_grad(
+    check(lib().hgx_mesh_chi2_grad_ex(
         ctx.handle, grid.handle, len(v), v.ctypes.data, len(f), f.ctypes.data,
         None if r is None else r.ctypes.data, rf.ctypes.data, float(dn2[0]), float(dn2[1]),
         float(weight), pc, pm, float(scale), C.byref(chi),
-        None if gv is None else gv.ctypes.data, None if inten is None else inten.ctypes.data))
+        None if gv is None else gv.ctypes.data, None if inten is None else inten.ctypes.data,
+        PRECISION[precision]))
     return chi.value, gv, inten
 
 

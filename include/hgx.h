@@ -369,12 +369,19 @@ int hgx_mesh_chi2_grad(hgx_ctx ctx, hgx_qgrid g, int nv, const double* verts, in
                        double dn2_re, double dn2_im, double weight, const double* counts,
                        const unsigned* mask, double scale, double* chi2, double* grad_verts,
                        double* intensity);
+/* The same with a precision: HGX_F32C (as above) or HGX_F64 (plain FP64 form factor, seeds
+ * and backward pass, every phase in FP64: the reference of the FP32C gradient). */
+int hgx_mesh_chi2_grad_ex(hgx_ctx ctx, hgx_qgrid g, int nv, const double* verts, int nf,
+                          const int* faces, const double* rot9, const double* rowfc,
+                          double dn2_re, double dn2_im, double weight, const double* counts,
+                          const unsigned* mask, double scale, double* chi2, double* grad_verts,
+                          double* intensity, int precision);
 
 /* The FP32C numeric form factor for callers that cannot allocate device memory: a plug-in
  * that runs inside another framework's memory pool and is handed only device pointers, a
  * service held to a fixed device-memory budget, or a real-time loop in which a cudaMalloc
  * would synchronise the device.  No counterpart in the reference.  Allocates nothing: its
- * scratch is a fixed static device array (1.5 MiB per GPU, held until exit), so
+ * scratch is fixed static device arrays (about 1.5 MiB per GPU, held until exit), so
  * ntri <= 65536 (larger requests return HGX_ERR_INVALID_ARG).  All array arguments are
  * device memory (same layouts as hgx_ff_triangles; q-point i uses qx/qy[i % nqy]); rot9 is
  * 9 host doubles or NULL for the identity; ff is nqz complex of type ff_type.  Asynchronous
@@ -529,6 +536,9 @@ int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const dou
  * sustained_ms > 0 the FP32 pipe is first kept busy for that long so that the clocks
  * settle as they do under a long kernel (the sustained figure); 0 gives the burst figure. */
 int hgx_measure_peaks(hgx_ctx ctx, int sustained_ms, double* fp32_tflops, double* sfu_gops);
+/* FP64 FMA throughput (TFLOP/s, FMA = 2) of a DFMA-chain probe on the context's device: the
+ * roofline denominator of the FP64-bound kernels (no counterpart in the reference). */
+int hgx_measure_peak_fp64(hgx_ctx ctx, double* fp64_tflops);
 
 #ifdef __cplusplus
 }

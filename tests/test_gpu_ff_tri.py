@@ -182,3 +182,73 @@ def test_launch_shape_autotuner(ctx, po, golden_grid):
     gp = hg.QGrid.from_arrays(ctx, rng.uniform(-2, 2, 50), rng.uniform(-2, 2, 50),
                               rng.uniform(0, 3, 150) + 0.01j)
     assert gp.mode == 0 and hg.ff_tune(ctx, gp, sd)[0] == 0
+
+
+# A mesh about 1.3 um from the origin: the phases q.c reach ~2,600 rad on these grids, so an
+# FP32 phase would lose ~1e-4 rad per term; the tiles' FP64 anchors keep the FP32C error at
+# the level of a centred mesh.
+OFFSET = np.array([1000.0, -700.0, 300.0])
+# pointwise bound on q-points with |F|^2 >= 1e-6 of the largest |F|^2 (relative error of F)
+PW_FLOOR = 1e-6
+PW_TOL = 2e-5
+
+
+def pointwise_err(a, ref, floor=PW_FLOOR):
+    a, ref = np.asarray(a).ravel(), np.asarray(ref).ravel()
+    p = np.abs(ref) ** 2
+    m = p >= floor * p.max()
+    return float(np.max(np.abs(a[m] - ref[m]) / np.abs(ref[m])))
+
+
+def _offset_star(offset=OFFSET):
+    V, F = meshes.star_mesh()
+    return meshes.shape_def_from_mesh(V + offset, F)
+
+
+@pytest.mark.parametrize("ppt", [4, -4])
+def test_offset_mesh_rows_kernel_vs_oracle(ctx, po, ppt):
+    sd = _offset_star()
+    R = po.rot_mul(po.rot_axis(2, 0.7), po.rot_axis(0, 0.3))
+    G = po.Grid(48, 40, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0)
+    ref = po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext, R)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    assert g.mode == 1
+    f32 = hg.ff_triangles(ctx, g, sd, R, "f32c", pixels_per_thread=ppt)
+    assert po.rel_err(f32, ref) < TOL32
+    assert pointwise_err(f32, ref) < PW_TOL
+    f64 = hg.ff_triangles(ctx, g, sd, R, "f64")
+    assert po.rel_err(f64, ref) < 1e-11
+
+
+def test_offset_mesh_points_kernel_vs_oracle(ctx, po):
+    rng = np.random.default_rng(21)
+    n = 1500
+    qx, qy = rng.uniform(-2, 2, n), rng.uniform(-2, 2, n)
+    qz = rng.uniform(0, 3, 2 * n) + 1j * rng.uniform(0, 1e-3, 2 * n)
+    sd = _offset_star()
+    R = po.rot_mul(po.rot_axis(1, -0.4), po.rot_axis(2, 1.1))
+    g = hg.QGrid.from_arrays(ctx, qx, qy, qz)
+    assert g.mode == 0
+    ref = po.ff_approx_triangle(sd, qx, qy, qz, R)
+    f32 = hg.ff_triangles(ctx, g, sd, R, "f32c")
+    assert po.rel_err(f32, ref) < TOL32
+    assert pointwise_err(f32, ref) < PW_TOL
+
+
+def test_translation_is_a_phase_at_full_size(ctx, po):
+    """Size-independent property on a 256 x 256 DWBA grid with all 50,000 triangles: moving
+    the mesh by t multiplies F by e^{i (Rq).t} (phase formed in FP64 on the host)."""
+    V, F = meshes.star_mesh()
+    sd0 = meshes.shape_def_from_mesh(V, F)
+    sd1 = meshes.shape_def_from_mesh(V + OFFSET, F)
+    R = po.rot_mul(po.rot_axis(2, 0.7), po.rot_axis(0, 0.3))
+    G = po.Grid(256, 256, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    f0 = hg.ff_triangles(ctx, g, sd0, R, "f64").reshape(4, -1)
+    f1 = hg.ff_triangles(ctx, g, sd1, R, "f32c").reshape(4, -1)
+    qz = G.qz_ext.reshape(4, -1).real
+    q = np.stack([np.broadcast_to(G.qx, qz.shape), np.broadcast_to(G.qy, qz.shape), qz], -1)
+    ph = np.exp(1j * ((q @ np.asarray(R).T) @ OFFSET))
+    expect = ph * f0
+    assert po.rel_err(f1, expect) < TOL32
+    assert pointwise_err(f1, expect) < PW_TOL
