@@ -225,12 +225,17 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
     b32.tune([p0], reps=2)
     c32, g32 = b32.eval([p0])
     c64, g64 = b64.eval([p0])
-    for _ in range(3):
-        b32.eval([p0])
-    t = time.perf_counter()
-    for _ in range(steps):
-        b32.eval([p0])
-    dt32 = (time.perf_counter() - t) / steps
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        t = time.perf_counter()
+        for _ in range(n):
+            fn()
+        return (time.perf_counter() - t) / n
+
+    dt32 = timed(lambda: b32.eval([p0]), steps)
+    dt64 = timed(lambda: b64.eval([p0]), steps)  # the same fused forward + adjoint in FP64
     # plain FP64 form, central differences: 9 forwards + chi^2 on the device
     d_counts = torch.tensor(counts, device=dev)
     d_I = torch.empty(n * n, dtype=torch.float64, device=dev)
@@ -260,6 +265,9 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
         "plain_fp64_fd": {"value": 1.0 / dtfd, "ms_per_eval": 1e3 * dtfd,
                           "method": "plain FP64 forward x 9 (central differences, h 1e-4 rel)"},
         "speedup_vs_plain_fp64": dtfd / dt32,
+        "fp64_adjoint": {"value": 1.0 / dt64, "ms_per_eval": 1e3 * dt64,
+                         "method": "the same fused forward + adjoint with FP64 per-pixel sums"},
+        "speedup_vs_fp64_adjoint": dt64 / dt32,
         "rel_err_chi2_vs_fp64": abs(c32[0] - c64[0]) / abs(c64[0]),
         "rel_err_grad_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
         "fd_vs_adjoint_rel": float(np.linalg.norm(gfd - g64[0]) / np.linalg.norm(g64[0])),
@@ -286,12 +294,8 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
     tbest, _, ttimes = bb32.tune(models, reps=2)
     cc32, gg32 = bb32.eval(models)
     cc64, gg64 = bb64.eval(models)
-    for _ in range(3):
-        bb32.eval(models)
-    t = time.perf_counter()
-    for _ in range(steps):
-        bb32.eval(models)
-    dtb = (time.perf_counter() - t) / steps
+    dtb = timed(lambda: bb32.eval(models), steps)
+    dtb64 = timed(lambda: bb64.eval(models), steps)
     # 256 sequential plain launches: the plain FP64 central-difference evaluation of a
     # subsample of candidates, scaled by pixel count
     sub = 8
@@ -330,6 +334,9 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
         "sequential_plain_fp64_fd": {"value": nc / dts, "s_per_batch": dts,
                                      "sample": f"{sub} candidates timed, scaled by pixels"},
         "speedup_vs_sequential_plain": dts / dtb,
+        "fp64_adjoint": {"value": nc / dtb64, "ms_per_batch": 1e3 * dtb64,
+                         "method": "the same graph-captured batch with FP64 per-pixel sums"},
+        "speedup_vs_fp64_adjoint": dtb64 / dtb,
         "max_rel_err_chi2_vs_fp64": rel_c, "max_rel_err_grad_vs_fp64": rel_g}
     bb32.close()
     bb64.close()
@@ -479,8 +486,20 @@ def mesh_grad_bench(ctx, grid, steps=2):
         t = time.perf_counter()
         fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale, want_grad=False)
         dtf = min(dtf, time.perf_counter() - t)
+    # the plain FP64 forward + adjoint once on the same inputs (its own warm-up call first)
+    fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale, want_grad=False,
+                           precision="f64")
+    t = time.perf_counter()
+    chi64, gv64, _ = fitting.mesh_chi2_grad(ctx, grid, V, F, rowfc, dn2, counts, None, scale,
+                                            precision="f64")
+    dt64 = time.perf_counter() - t
     nparam = 3 * len(V)
     return {"metric": "chi2+grad evals/s", "value": 1.0 / dt, "s_per_eval": dt,
+            "fp64_adjoint": {"s_per_eval": dt64, "method": "plain FP64 form factor, seeds and "
+                             "backward pass on the same inputs (one timed call)"},
+            "speedup_vs_fp64_adjoint": dt64 / dt,
+            "rel_err_chi2_vs_fp64": abs(chi - chi64) / abs(chi64),
+            "rel_err_grad_vs_fp64": float(np.linalg.norm(gv - gv64) / np.linalg.norm(gv64)),
             "forward_only_s": dtf, "vertices": len(V), "triangles": len(F),
             "gradient_components": nparam,
             "central_differences_estimate_s": (1 + 2 * nparam) * dtf,
@@ -633,16 +652,18 @@ def main():
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
+        reps64 = 2
         a0.record(stream)
-        hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
+        for _ in range(reps64):
+            hg.ff_triangles(ctx, grid, sd_dev, None, "f64", out=out64, out_type="c128")
         a1.record(stream)
         torch.cuda.synchronize()
-        ms64 = a0.elapsed_time(a1)
+        ms64 = a0.elapsed_time(a1) / reps64
         # accuracy of the timed FP32 output against the FP64 kernel (norm-wise)
         d = (out.to(torch.complex128) - out64)
         relerr = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(out64))
         v64 = evals / (ms64 * 1e-3)
-        f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64,
+        f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64, "launches_timed": reps64,
                "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr}
         del out64
 
