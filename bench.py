@@ -97,6 +97,11 @@ def parse():
     ap.add_argument("--no-fitting", action="store_true")
     ap.add_argument("--no-exact", action="store_true")
     ap.add_argument("--no-hig", action="store_true")
+    ap.add_argument("--grid", type=int, default=0,
+                    help="detector rows = columns of the form-factor workload (default 2048; "
+                         "smaller grids are for profiling captures, not bench lines)")
+    ap.add_argument("--ppt", type=int, default=0,
+                    help="row-kernel pixels per thread (0: the library's autotuner chooses)")
     return ap.parse_args()
 
 
@@ -551,7 +556,10 @@ def run_reference(args, rank):
 
 
 def main():
+    global NCOL, NROW
     args = parse()
+    if args.grid:
+        NCOL = NROW = args.grid
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -585,10 +593,14 @@ def main():
 
     # launch shape chosen by the library's autotuner on this grid (outside the timed region;
     # 8,192 triangles rank the candidates, whose cost is linear in the triangle count)
-    tuned_p, _, tune_times = hg.ff_tune(ctx, grid, sd_dev[:8192], None, "c64", reps=2)
+    if args.ppt:
+        tuned_p, tune_times = args.ppt, {}
+    else:
+        tuned_p, _, tune_times = hg.ff_tune(ctx, grid, sd_dev[:8192], None, "c64", reps=2)
 
     def step():
-        hg.ff_triangles(ctx, grid, sd_dev, None, "f32c", out=out, out_type="c64")
+        hg.ff_triangles(ctx, grid, sd_dev, None, "f32c", out=out, out_type="c64",
+                        pixels_per_thread=tuned_p)
 
     def barrier():
         if dist is not None:
