@@ -1,0 +1,158 @@
+// FP32-compensated bodies of the fused grain kernel (hig_sim.cu) for a real rotated q (grids
+// whose DWBA qz blocks are real: a vacuum particle layer): the cylinder, sphere and box form
+// factors and the lattice structure factor of the reference's formulas, with every phase
+// formed and range-reduced in FP64 and only the transcendental of the reduced argument (and
+// the sums) in FP32.  Grids with complex qz keep the FP64 bodies of ana_sf.cuh.
+//
+// Lattice structure factor (src/sf/sf.cpp:164-246): for a real angle theta the reference's
+// principal-branch expression
+//   pow(e, (1 - N)/2) (1 - pow(e, N)) / (1 - e),  e = e^{i theta}
+// equals sin(N theta_r / 2) / sin(theta_r / 2) with theta_r the principal angle of e in
+// (-pi, pi]; on the b axis the numerator takes exp(i N theta) with the unreduced theta,
+// which for a non-integer N adds the phase e^{i pi k (N - 1)}, theta = theta_r + 2 pi k.
+// N is returned where the reference's guard |1 - e| <= eps takes N.
+#pragma once
+
+#include "ana_sf.cuh"
+
+namespace hgx {
+
+constexpr double INV_2PI_A = 0.15915494309189533576888376337251;
+
+struct cf {
+  float x, y;
+};
+__device__ __forceinline__ cf cmul(cf a, cf b) { return cf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+__device__ __forceinline__ cf cscale(cf a, float s) { return cf{a.x * s, a.y * s}; }
+__device__ __forceinline__ cf cadd(cf a, cf b) { return cf{a.x + b.x, a.y + b.y}; }
+
+// e^{2 pi i u} of a phase in turns (FP64), reduced exactly before the FP32 sincospi
+__device__ __forceinline__ cf expi_turns(double u) {
+  u -= rint(u);
+  float s, c;
+  sincospif((float)(2.0 * u), &s, &c);
+  return cf{c, s};
+}
+// e^{i ph}, ph in radians (FP64)
+__device__ __forceinline__ cf expi_f(double ph) { return expi_turns(ph * INV_2PI_A); }
+
+// sin(x)/x (hig::sinc) given sin x from expi_f; the Taylor form near 0
+__device__ __forceinline__ float sinc_from(double x, float sinx) {
+  if (fabs(x) > 1e-2) return sinx / (float)x;
+  const float x2 = (float)(x * x);
+  return 1.f - x2 * (1.f / 6.f - x2 * (1.f / 120.f));
+}
+
+// with_phase of ana_sf.cuh: v e^{i m.tv}, not evaluated at the origin
+__device__ __forceinline__ cf with_phase_f(cf v, const double* m, const double* tv) {
+  if (tv[0] == 0.0 && tv[1] == 0.0 && tv[2] == 0.0) return v;
+  return cmul(v, expi_f(m[0] * tv[0] + m[1] * tv[1] + m[2] * tv[2]));
+}
+
+// (sin x - x cos x) / x^3 of the sphere, by its series below x = 0.5 (where the difference
+// cancels in FP32)
+__device__ __forceinline__ float sphere_kernel_f(double x) {
+  if (x < 0.5) {
+    const float x2 = (float)(x * x);
+    return 1.f / 3.f - x2 * (1.f / 30.f - x2 * (1.f / 840.f - x2 * (1.f / 45360.f - x2 * (1.f / 3991680.f))));
+  }
+  const cf e = expi_f(x);
+  return (e.y - (float)x * e.x) / (float)(x * x * x);
+}
+
+// The analytic form factor of shape `a` (SHAPE: cylinder, sphere or box) at the real rotated
+// q (m) translated by tv: ff_analytic_eval of ana_sf.cuh in FP32C.
+template <int SHAPE>
+__device__ __forceinline__ cf ff_analytic_f32c(const AnaShape& a, const double* m, const double* tv) {
+  const Dist& X = a.d[0];
+  const Dist& Y = a.d[1];
+  const Dist& Z = a.d[2];
+  cf out{0.f, 0.f};
+  if (SHAPE == SH_CYLINDER) {  // ff_ana_cylinder.cpp:34-42,100-117 (unweighted)
+    const double qpar = sqrt(m[0] * m[0] + m[1] * m[1]);
+    float fr = 0.f;
+    for (int i = 0; i < X.n; ++i) {
+      const double r = X.v[i], x = qpar * r;
+      if (x * x > CUTINY_REF) fr += (float)(2. * PI_REF * r * r) * (j1f((float)x) / (float)x);
+    }
+    cf gh{0.f, 0.f};
+    for (int i = 0; i < Z.n; ++i) {
+      const double h = Z.v[i], x = m[2] * 0.5 * h;
+      const cf e = expi_f(x);
+      gh = cadd(gh, cscale(e, sinc_from(x, e.y) * (float)h));
+    }
+    out = with_phase_f(cscale(gh, fr), m, tv);
+  } else if (SHAPE == SH_SPHERE) {  // ff_ana_sphere.cpp:33-45,95-107 (weighted)
+    const double q = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    cf acc{0.f, 0.f};
+    if (q >= 2.2250738585072014e-308)
+      for (int i = 0; i < X.n; ++i) {
+        const double R = X.v[i];
+        const float c0 = sphere_kernel_f(q * R) * (float)(4. * PI_REF * R * R * R * X.w[i]);
+        acc = cadd(acc, cscale(expi_f(m[2] * R), c0));
+      }
+    out = with_phase_f(acc, m, tv);
+  } else if (SHAPE == SH_BOX) {  // ff_ana_box.cpp:35-42,96-125 (weighted)
+    float sx = 0.f, sy = 0.f;
+    cf sz{0.f, 0.f};
+    for (int i = 0; i < X.n; ++i) {
+      const double x = m[0] * 0.5 * X.v[i];
+      sx += sinc_from(x, expi_f(x).y) * (float)(X.v[i] * X.w[i]);
+    }
+    for (int i = 0; i < Y.n; ++i) {
+      const double x = m[1] * 0.5 * Y.v[i];
+      sy += sinc_from(x, expi_f(x).y) * (float)(Y.v[i] * Y.w[i]);
+    }
+    for (int i = 0; i < Z.n; ++i) {
+      const double x = m[2] * 0.5 * Z.v[i];
+      const cf e = expi_f(x);
+      sz = cadd(sz, cscale(e, sinc_from(x, e.y) * (float)(Z.v[i] * Z.w[i])));
+    }
+    out = with_phase_f(cscale(sz, sx * sy), m, tv);
+  }
+  return out;
+}
+
+__device__ __forceinline__ bool odd_integer(double k) { return fmod(k, 2.0) != 0.0; }
+
+// sin(N theta_r / 2) / sin(theta_r / 2) on the principal angle theta_r of e^{i theta}
+__device__ __forceinline__ float dirichlet_principal(double theta, double N) {
+  if (N == 1.0) return 1.f;
+  double t = theta * INV_2PI_A;
+  t -= rint(t);
+  if (t == 0.0) return (float)N;
+  double v = N * t;
+  const double k = rint(v);
+  v -= k;
+  const float num = odd_integer(k) ? -sinpif((float)v) : sinpif((float)v);
+  return num / sinpif((float)t);
+}
+
+// the b-axis factor: e^{i pi k (N - 1)} sin(N theta / 2) / sin(theta / 2)
+__device__ __forceinline__ cf dirichlet_b(double theta, double N) {
+  if (N == rint(N)) return cf{dirichlet_principal(theta, N), 0.f};
+  const double u = theta * INV_2PI_A;
+  const double k = rint(u), t = u - k;
+  if (t == 0.0) return cf{(float)N, 0.f};
+  double v = N * u;
+  const double kv = rint(v);
+  v -= kv;
+  const float num = odd_integer(kv) ? -sinpif((float)v) : sinpif((float)v);
+  const float den = odd_integer(k) ? -sinpif((float)t) : sinpif((float)t);
+  return cscale(expi_turns(k * (N - 1.0) * 0.5), num / den);
+}
+
+// sf_lattice_eval of ana_sf.cuh for a real rotated q, FP32C.  The b angle keeps the
+// reference's lb[2] * lb[2] term (src/sf/sf.cpp:212).
+__device__ __forceinline__ cf sf_lattice_f32c(const SfLat& L, const double* m) {
+  const double ta = m[0] * L.la[0] + m[1] * L.la[1] + m[2] * L.la[2];
+  const double tb = m[0] * L.lb[0] + m[1] * L.lb[1] + L.lb[2] * L.lb[2];
+  const double tc = m[0] * L.lc[0] + m[1] * L.lc[1] + m[2] * L.lc[2];
+  const float sa = dirichlet_principal(ta, L.rep[0]);
+  const cf sb = dirichlet_b(tb, L.rep[1]);
+  const float sc = dirichlet_principal(tc, L.rep[2]);
+  const cf t3 = expi_f(m[0] * L.center[0] + m[1] * L.center[1] + m[2] * L.center[2]);
+  return cmul(t3, cscale(sb, sa * sc));
+}
+
+}  // namespace hgx

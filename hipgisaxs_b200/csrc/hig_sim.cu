@@ -51,6 +51,7 @@
 #include <vector>
 
 #include "ana_sf.cuh"
+#include "ana_sf_f32.cuh"
 #include "hgx_internal.cuh"
 #include "hig_config.hpp"
 
@@ -202,6 +203,81 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
     }
   }
   if (live && k == 0) a.out[i] = acc;
+}
+
+// The fused grain loop in FP32C for grids with real qz and unit cells of one shape among
+// cylinder, sphere and box: the same quad layout and order of sums as grain_dwba_kernel, the
+// form and structure factors from ana_sf_f32.cuh (FP64 phases, FP32 transcendentals and
+// sums), the DWBA terms in FP32 and the intensity accumulated in FP64.
+template <int SHAPE>
+__global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = t >> 2;
+  const int k = (int)(t & 3);
+  const bool live = i < a.n;  // every lane takes part in the shuffles
+  const long ii = live ? i : 0;
+  const double qx = a.qx[ii], qy = a.qy[ii];
+  const double qz = a.qz[k * a.n + ii].x;
+  const double2 fcd = a.fc[k * a.n + ii];
+  const cf fc{(float)fcd.x, (float)fcd.y};
+  const int base = (threadIdx.x & 31) & ~3;
+  double acc = (live && k == 0) ? a.out[i] : 0.0;
+  for (int g = a.g0; g < a.g1; ++g) {
+    const double* gp = a.grains + 12 * (long)g;
+    cf ff{0.f, 0.f};
+    for (int e = 0; e < a.nelem; ++e) {
+      const double* er = a.elem_rot + 9 * ((long)g * a.nelem + e);
+      double m[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) m[j] = er[3 * j] * qx + er[3 * j + 1] * qy + er[3 * j + 2] * qz;
+      const cf eff = ff_analytic_f32c<SHAPE>(a.shapes[e], m, a.elems[e].loc);
+      ff = cadd(ff, cmul(cf{(float)a.elems[e].dre, (float)a.elems[e].dim}, eff));
+    }
+    double mr[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) mr[j] = gp[3 * j] * qx + gp[3 * j + 1] * qy + gp[3 * j + 2] * qz;
+    const ScaleEntry* sp = a.scales + (long)g * a.nscale;
+    for (int si = 0; si < a.nscale; ++si) {
+      cf sfv;
+      if (a.sfbuf) {
+        const double2 v = a.sfbuf[k * a.n + ii];
+        sfv = cf{(float)v.x, (float)v.y};
+      } else {
+        SfLat L;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          L.la[d] = sp[si].la[d];
+          L.lb[d] = sp[si].lb[d];
+          L.lc[d] = sp[si].lc[d];
+          L.rep[d] = sp[si].rep[d];
+          L.center[d] = gp[9 + d];
+        }
+        sfv = sf_lattice_f32c(L, mr);
+      }
+      const cf term = cmul(cmul(fc, sfv), ff);
+      cf sum{0.f, 0.f};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        sum = cadd(sum, cf{__shfl_sync(0xffffffffu, term.x, base + j),
+                           __shfl_sync(0xffffffffu, term.y, base + j)});
+      const float w = (float)sp[si].w;
+      acc += (double)(w * w * (sum.x * sum.x + sum.y * sum.y));
+    }
+  }
+  if (live && k == 0) a.out[i] = acc;
+}
+
+// true when the FP32C grain kernel has a body for this shape
+static bool grain_f32c_shape(int shape) {
+  return shape == SH_CYLINDER || shape == SH_SPHERE || shape == SH_BOX;
+}
+
+static void launch_grain_f32c(int shape, unsigned blocks, cudaStream_t st, const FusedArgs& a) {
+  switch (shape) {
+    case SH_CYLINDER: grain_dwba_f32c_kernel<SH_CYLINDER><<<blocks, 128, 0, st>>>(a); break;
+    case SH_SPHERE: grain_dwba_f32c_kernel<SH_SPHERE><<<blocks, 128, 0, st>>>(a); break;
+    default: grain_dwba_f32c_kernel<SH_BOX><<<blocks, 128, 0, st>>>(a); break;
+  }
 }
 
 constexpr int FUSED_GRAINS_PER_LAUNCH = 64;  // keeps each launch to tens of milliseconds
@@ -544,7 +620,7 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
                            const hig::Input& in, const Rot& rot_phi, const std::vector<double>& dd,
                            const std::vector<double>& nn, int ngr, int ax1, int ax2, int ax3,
                            const std::vector<ScaleEntry>& plan, int nscale, const double2* fc,
-                           double* Is) {
+                           double* Is, int precision) {
   cudaStream_t st = c->stream;
   std::vector<AnaShape> shapes;
   std::vector<FusedElem> elems;
@@ -627,9 +703,16 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
   int one = nelem > 0 ? shapes[0].shape : 0;  // the shape every element shares, if any
   for (int e = 1; e < nelem; ++e)
     if (shapes[e].shape != one) one = 0;
+  // FP32C: grids with real qz blocks (paired rows) and one shape with an FP32C body
+  const bool f32c = precision == HGX_F32C && g->mode == 1 && grain_f32c_shape(one);
   for (int g0 = 0; g0 < ngr; g0 += FUSED_GRAINS_PER_LAUNCH) {
     a.g0 = g0;
     a.g1 = g0 + FUSED_GRAINS_PER_LAUNCH < ngr ? g0 + FUSED_GRAINS_PER_LAUNCH : ngr;
+    if (f32c) {
+      launch_grain_f32c(one, blocks, st, a);
+      HGX_CUDA(cudaGetLastError());
+      continue;
+    }
     // the paired lattice factor when it holds for every grain and sample of the launch
     bool paired = a.sfbuf == nullptr;
     for (int gi = a.g0; gi < a.g1 && paired; ++gi) {
@@ -814,7 +897,7 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     }
     if (all_analytic && !saxs) {
       HGX_TRY(fused_structure(c, g, w, s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, plan, nscale,
-                              (const double2*)bfc.p, Is));
+                              (const double2*)bfc.p, Is, precision));
       ++si;
       continue;
     }

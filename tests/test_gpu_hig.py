@@ -240,3 +240,28 @@ def test_sliced_layers_give_the_reference_empty_image(ctx, tmp_path):
     libc.srand(4)
     full = read_hig(os.path.join(HIG, "sim_cylinders_hcp.hig")).compute_gisaxs(ctx)
     assert libc.rand() == after and full.max() > 0
+
+
+# Descriptions whose unit cells hold one cylinder, sphere or box shape on a DWBA grid with
+# real qz: the fused grain kernel's FP32C bodies (FP64 phases, FP32 transcendentals and sums).
+F32C_SIM = ["sim_cylinders_hcp.hig", "paracrystal.hig", "percus_yevick.hig", "sim_scaling.hig",
+            "sim_repetition.hig", "sim_orientations.hig"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", F32C_SIM)
+def test_compute_gisaxs_f32c_analytic(ctx, po, name):
+    """The FP32C grain kernel against the oracle's FP64 composition: norm-wise relative error
+    of the image below 1e-5 and every pixel within 1e-5 of the image's largest value; the
+    image differs from the FP64 kernel's (the FP32C bodies ran)."""
+    d = read_hig(os.path.join(HIG, name))
+    _srand(5)
+    img = d.compute_gisaxs(ctx, precision="f32c")
+    _srand(5)
+    img64 = d.compute_gisaxs(ctx, precision="f64")
+    _srand(5)
+    ref = po.compute_gisaxs(d.data, HIG)
+    assert np.all(np.isfinite(img))
+    assert po.rel_err(img, ref) < 1e-5
+    assert np.abs(img - ref).max() / np.abs(ref).max() < 1e-5
+    assert not np.array_equal(img, img64)
