@@ -97,6 +97,7 @@ def parse():
     ap.add_argument("--no-fitting", action="store_true")
     ap.add_argument("--no-exact", action="store_true")
     ap.add_argument("--no-hig", action="store_true")
+    ap.add_argument("--no-config1", action="store_true")
     ap.add_argument("--grid", type=int, default=0,
                     help="detector rows = columns of the form-factor workload (default 2048; "
                          "smaller grids are for profiling captures, not bench lines)")
@@ -463,6 +464,79 @@ def hig_bench(ctx, steps=3, ng=25):
     return res
 
 
+# Config 1: cylinders (R 5 nm, H 10 nm, 5 % Gaussian size spread sampled at 11 values over
+# +-3 sigma, summed unweighted as the reference does) on a 2-D hexagonal lattice a = 20 nm with
+# 20 x 20 repetitions, one grain, over a Si-like substrate (delta 4.88e-6, beta 7.37e-8, also
+# the particles' index), 10 keV, alpha_i 0.20 deg, 1024 x 1024 detector over qy in [-2, 2],
+# qz in [0, 3] nm^-1, DWBA.
+CONFIG1_HIG = """hipGisaxsInput = {
+	shape = { key = "cyl", name = "cylinder", refindex = { delta = 4.88E-06, beta = 7.37E-08 },
+		param = { type = "radius", stat = "gaussian", min = 4.25, max = 5.75, p1 = 5, p2 = 0.25, nvalues = 11 },
+		param = { type = "height", stat = "gaussian", min = 8.5, max = 11.5, p1 = 10, p2 = 0.5, nvalues = 11 } },
+	unitcell = { key = "u1", element = { shape:key = "cyl", locations = [[0 0 0]] } },
+	layer = { key = "substr", order = -1, refindex = { delta = 4.88E-06, beta = 7.37E-08 } },
+	structure = { key = "st1",
+		grain = { unitcell:key = "u1", lattice = { type = "hex" }, repetition = [20 20 1], scaling = 20 },
+		ensemble = { maxgrains = [1 1 1] } },
+	instrumentation = { scattering = { alphai = { min = 0.2 }, photon = { value = 10000, unit = "ev" } },
+		detector = { pixelsize = 0.172, sdd = 4000, directbeam = [ 0 0 ] } },
+	computation = { runname = "config1", outputregion = { type = "qspace", minpoint = [ -2 0 ], maxpoint = [ 2 3 ] },
+		resolution = [ NRES NRES ] }
+}
+"""
+
+
+def config1_bench(ctx, steps=3, n=1024, cpu=True):
+    """Config 1 through HipGISAXS::compute_gisaxs (hgx_hig_compute_gisaxs, host image out, the
+    call synchronous; best of `steps` by the host clock), FP32C and FP64 on the same
+    description; beside them the reference's own CPU functions at full size (oracle/_ref:
+    AnalyticFormFactor cylinder, StructureFactor, MultiLayer::propagation_coeffs, all host
+    threads) with the restated DWBA combination, which is also the accuracy reference."""
+    import tempfile
+    from hipgisaxs_b200.hig import read_hig
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    res = {"metric": "pixel-evals/s", "workload": "cylinders R 5 H 10 (5% spread, 11 samples), "
+           "hex lattice a 20 nm x 20 x 20, Si-like substrate, 10 keV, alpha_i 0.20 deg, "
+           f"{n}x{n} DWBA", "pixels": n * n}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "config1.hig")
+        with open(path, "w") as f:
+            f.write(CONFIG1_HIG.replace("NRES", str(n)))
+        d = read_hig(path)
+        imgs = {}
+        for prec in ("f32c", "f64"):
+            imgs[prec] = d.compute_gisaxs(ctx, precision=prec)
+            best = float("inf")
+            for _ in range(steps):
+                t = time.perf_counter()
+                d.compute_gisaxs(ctx, precision=prec)
+                best = min(best, time.perf_counter() - t)
+            res[prec] = {"ms": 1e3 * best, "value": n * n / best}
+        d.close()
+    i32, i64 = imgs["f32c"].ravel(), imgs["f64"].ravel()
+    res["value"] = res["f32c"]["value"]
+    res["fp32c_speedup_vs_fp64"] = res["f64"]["ms"] / res["f32c"]["ms"]
+    res["rel_err_fp32c_vs_fp64"] = po.rel_err(i32, i64)
+    res["max_rel_err_fp32c_vs_fp64"] = float(np.abs(i32 - i64).max() / np.abs(i64).max())
+    if cpu and po.available("ref"):
+        threads = po.set_threads(os.cpu_count() or 1, "ref")
+        G = po.Grid(n, n, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0, backend="ref")
+        t = time.perf_counter()
+        ff = po.ff_analytic(G, "cylinder", po.cylinder_params(5.0, 10.0, 0.05, 11))
+        a, b, c, _ = po.lattice_vectors("hex")
+        sf = po.sf_lattice(G, (a, b, c), (20, 20, 1), (20.0, 20.0, 20.0))
+        fc = po.propagation_coeffs(G, [(4.88e-6, 7.37e-8, 0.0, -1)], 0)
+        ref = po.dwba_combine(fc, sf, complex(-2 * 4.88e-6, -2 * 7.37e-8) * ff, 1.0)
+        dt = time.perf_counter() - t
+        res["cpu_reference"] = {"value": n * n / dt, "ms": 1e3 * dt, "cores": threads,
+                                "kind": "reference", "sample": f"the full {n}x{n} image"}
+        res["speedup_vs_cpu_reference"] = res["value"] / res["cpu_reference"]["value"]
+        res["rel_err_fp32c_vs_reference"] = po.rel_err(i32, ref)
+        res["rel_err_fp64_vs_reference"] = po.rel_err(i64, ref)
+    return res
+
+
 def mesh_grad_bench(ctx, grid, steps=2):
     """Config 3, mesh part: chi^2 and the gradient with respect to all 25,002 x 3 vertex
     coordinates of the 50,000-triangle star mesh on the 2048 x 2048 DWBA detector (forward
@@ -692,6 +766,10 @@ def main():
     if not args.no_hig and rank == 0 and world == 1:
         hig = hig_bench(ctx)
 
+    cfg1 = None
+    if not args.no_config1 and rank == 0 and world == 1:
+        cfg1 = config1_bench(ctx, cpu=not args.no_cpu_baseline)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         g = grid.read(qz_det=False, alpha=False)
@@ -727,7 +805,7 @@ def main():
                                  "frac": sfu_rate / peak_sfu},
                          "hbm_view": hbm_view(ms_step)},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
-            "exact_triangle": exact, "hig_simulation": hig,
+            "exact_triangle": exact, "hig_simulation": hig, "config1_dwba_1024sq": cfg1,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

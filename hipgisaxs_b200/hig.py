@@ -139,7 +139,9 @@ class HiGInput:
         """HipGISAXS::compute_gisaxs on the device (hgx_hig_compute_gisaxs): the nrow x ncol
         intensity image of every structure's grains, summed with the iratios.  `out`: a
         float64 numpy array or CUDA tensor of nrow*ncol values (allocated when None).
-        precision "f32c" computes mesh form factors in compensated FP32.  expt "saxs" takes the
+        precision "f32c" computes mesh form factors in compensated FP32, and on grids with
+        real qz the fused grain kernel's cylinder, sphere and box cells and lattice structure
+        factors in FP32C (FP64 phases, FP32 transcendentals and sums).  expt "saxs" takes the
         reference's Born branch (each structure keeps its last grain's last scaling sample, as
         the reference's assignment leaves it); nslices > 1 gives the reference's zero image;
         a description with angle scans is refused (compute_scan_point runs them)."""

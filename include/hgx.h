@@ -428,7 +428,9 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * structure factor (lattice, paracrystal or Percus-Yevick) and the DWBA intensity with the
  * layer stack's Fresnel coefficients; the structures summed with their iratios.  image:
  * nrow x ncol doubles (host or device).  precision: HGX_F64, or HGX_F32C for the mesh form
- * factors.  Supported: GISAXS and SAXS (expt "saxs": run_gisaxs's Born branch, :1099-1103, whose
+ * factors and, on grids with real qz blocks, the fused grain kernel's cylinder, sphere and box
+ * unit cells with their lattice structure factors (FP64 phase reduction, FP32 transcendentals
+ * and sums, FP64 intensity; other cells stay FP64).  Supported: GISAXS and SAXS (expt "saxs": run_gisaxs's Born branch, :1099-1103, whose
  * assignment leaves each structure the image of its last grain's last scaling sample), one
  * alpha_i/phi/tilt, no structure correlation,
  * regular grain grids; "single", "range", "random" (drawn with the C library's rand() in the
