@@ -107,6 +107,7 @@ SIGNATURES = {
     "hgx_read_image": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long), C.POINTER(_i), C.POINTER(_i)]),
     "hgx_read_mask": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long)]),
     "hgx_hig_objective": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, C.POINTER(C.c_long)]),
+    "hgx_hig_objective_grad": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, _vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
     "hgx_measure_peak_fp64": (_i, [_vp, C.POINTER(_d)]),
 }

@@ -152,7 +152,114 @@ __global__ void __launch_bounds__(FD_THREADS) fit_terms_kernel(int metric, long 
   }
 }
 
+// d(distance)/d(data) of the scalar measures.  With t = T(data) (square or cube root),
+// r = T(ref), masks m in {0, 1}:
+//   unit L2:  sum m (t/N - r/R)^2, N = |t|_m:   (2m/N) ((t/N - r/R) - (t/N) K),
+//             K = sum m (t/N - r/R) (t/N)
+//   c L2:     sum m (r - c t)^2, c = <t, r>_m / |t|_m^2 (the least-squares scale, so its own
+//             change drops out):   -2 m c (r - c t)
+//   unit L1:  sum m |t/N - r/R|, N = sum m |t|:   (m/N) (sgn(t/N - r/R) - K),
+//             K = sum m sgn(t/N - r/R) (t/N)
+// each times T'(data); 0 where data <= 0 (the root's derivative is unbounded there).
+__global__ void __launch_bounds__(FD_THREADS) fit_kterm_kernel(int metric, long n, const double* __restrict__ ref,
+                                                               const double* __restrict__ dat,
+                                                               const unsigned* __restrict__ mask, Norms nm,
+                                                               double* __restrict__ part) {
+  double acc = 0.0;
+  for (long i = (long)blockIdx.x * FD_THREADS + threadIdx.x; i < n; i += (long)FD_BLOCKS * FD_THREADS) {
+    const double m = mask ? (double)mask[i] : 1.0;
+    const double nd = transform(metric, dat[i]) / nm.dat_norm, nr = transform(metric, ref[i]) / nm.ref_norm;
+    double k = is_l1(metric) ? m * ((nd > nr) - (nd < nr)) * nd : m * (nd - nr) * nd;
+    acc += isfinite(k) ? k : 0.0;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(FD_THREADS) fit_lambda_kernel(int metric, long n, const double* __restrict__ ref,
+                                                                const double* __restrict__ dat,
+                                                                const unsigned* __restrict__ mask, Norms nm,
+                                                                const double* __restrict__ K,
+                                                                double* __restrict__ lambda) {
+  for (long i = (long)blockIdx.x * FD_THREADS + threadIdx.x; i < n; i += (long)FD_BLOCKS * FD_THREADS) {
+    const double m = mask ? (double)mask[i] : 1.0;
+    const double d = dat[i];
+    const double td = transform(metric, d), tr = transform(metric, ref[i]);
+    double g;
+    if (metric == M_SQRT_C_L2 || metric == M_CBRT_C_L2) {
+      g = -2.0 * m * nm.c * (tr - nm.c * td);
+    } else {
+      const double nd = td / nm.dat_norm, nr = tr / nm.ref_norm;
+      if (is_l1(metric)) g = m / nm.dat_norm * ((double)((nd > nr) - (nd < nr)) - K[0]);
+      else g = 2.0 * m / nm.dat_norm * ((nd - nr) - nd * K[0]);
+    }
+    const double dT = is_cbrt(metric) ? 1.0 / (3.0 * td * td) : 0.5 / td;
+    const double v = g * dT;
+    lambda[i] = (d > 0.0 && isfinite(v)) ? v : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(FD_THREADS) dot_partial_kernel(long n, const double* __restrict__ a,
+                                                                 const double* __restrict__ b,
+                                                                 double* __restrict__ part) {
+  double acc = 0.0;
+  for (long i = (long)blockIdx.x * FD_THREADS + threadIdx.x; i < n; i += (long)FD_BLOCKS * FD_THREADS)
+    acc += a[i] * b[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
 }  // namespace
+
+// The norms of pass 1 (host copies), shared by the distance and its gradient.
+static int fit_norms(hgx_ctx c, int metric, long n, const double* dr, const double* dd, const unsigned* dm,
+                     Norms* nm) {
+  cudaStream_t st = c->stream;
+  HGX_TRY(c->scratch.reserve(sizeof(double) * (3 * FD_BLOCKS + 4)));
+  double* part = reinterpret_cast<double*>(c->scratch.p);
+  double* sums = part + 3 * FD_BLOCKS;
+  fit_norms_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(metric, n, dr, dd, dm, part);
+  for (int k = 0; k < 3; ++k) fit_sums_kernel<<<1, FD_THREADS, 0, st>>>(part, FD_BLOCKS, 3, k, sums);
+  HGX_CUDA(cudaGetLastError());
+  double h[3];
+  HGX_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  const bool l1 = metric == M_SQRT_UNIT_L1 || metric == M_CBRT_UNIT_L1;
+  nm->ref_norm = l1 ? h[0] : sqrt(h[0]);
+  nm->dat_norm = l1 ? h[1] : sqrt(h[1]);
+  nm->c = h[2] / (nm->dat_norm * nm->dat_norm);
+  return HGX_OK;
+}
+
+// d(distance)/d(data) of a scalar measure (not the residual-vector forms), device arrays.
+int fit_distance_gradient(hgx_ctx c, int metric, long n, const double* ref, const double* data,
+                          const unsigned* mask, double* lambda) {
+  if (metric < 0 || metric > M_CBRT_UNIT_L1 || metric == M_SQRT_UNIT_L2_RES || metric == M_SQRT_C_L2_RES)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective_grad: the gradient is defined for the scalar "
+                                     "distance measures (not the residual vectors)");
+  Norms nm;
+  HGX_TRY(fit_norms(c, metric, n, ref, data, mask, &nm));
+  cudaStream_t st = c->stream;
+  double* part = reinterpret_cast<double*>(c->scratch.p);
+  double* sums = part + 3 * FD_BLOCKS;
+  fit_kterm_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(metric, n, ref, data, mask, nm, part);
+  fit_sums_kernel<<<1, FD_THREADS, 0, st>>>(part, FD_BLOCKS, 1, 0, sums + 3);
+  fit_lambda_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(metric, n, ref, data, mask, nm, sums + 3, lambda);
+  HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+int device_dot(hgx_ctx c, long n, const double* a, const double* b, double* out) {
+  cudaStream_t st = c->stream;
+  HGX_TRY(c->scratch.reserve(sizeof(double) * (FD_BLOCKS + 4)));
+  double* part = reinterpret_cast<double*>(c->scratch.p);
+  dot_partial_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(n, a, b, part);
+  fit_sums_kernel<<<1, FD_THREADS, 0, st>>>(part, FD_BLOCKS, 1, 0, part + FD_BLOCKS);
+  HGX_CUDA(cudaGetLastError());
+  HGX_CUDA(cudaMemcpyAsync(out, part + FD_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  return HGX_OK;
+}
 
 }  // namespace hgx
 

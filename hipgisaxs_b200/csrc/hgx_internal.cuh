@@ -81,8 +81,17 @@ struct HigWork {
   double key[8] = {0};
   double ext_alpha = 0.0;  // the incidence angle the grid's qz blocks were extended for
   DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj, saxs_qz;
+  // the objective's gradient: the tables' changes, d(distance)/d(image), d(image)/dx
+  DevBuf tshapes, telems, tgt, ter, tsc, lam, dimg;
   std::map<std::string, MeshTuples> meshes;  // by resolved path
 };
+// d(image)/dx of hgx_hig_compute_gisaxs for one fit variable, added into dI (hig_sim.cu).
+int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, double step, double* dI);
+// d(distance)/d(data) of a scalar fitting distance (fit_distance.cu), and a deterministic dot
+// product of two device vectors (FP64, result on the host).
+int fit_distance_gradient(hgx_ctx c, int metric, long n, const double* ref, const double* data,
+                          const unsigned* mask, double* lambda);
+int device_dot(hgx_ctx c, long n, const double* a, const double* b, double* out);
 }  // namespace hgx
 
 // -------------------------------------------------------------- the context ----

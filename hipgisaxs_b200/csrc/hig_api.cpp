@@ -3,6 +3,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
+#include <cmath>
 #include <iterator>
 #include <new>
 #include <string>
@@ -229,6 +231,52 @@ int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const dou
   for (long k = 0; k < nd; ++k) dist[k] = isfinite(dist[k]) ? dist[k] + reg_dist : 1e8;
   if (ndist) *ndist = nd;
   return HGX_OK;
+}
+
+// The objective of hgx_hig_objective for a scalar distance measure and its gradient with
+// respect to the fit parameters.  The reference's LMVM fitter takes this gradient by central
+// differences, two simulations per parameter (src/analyzer/hipgisaxs_fit_lmvm.cpp:190-223, the
+// objective dist[0], src/analyzer/objective_func.cpp:107-115).  Here: one simulation, then
+// lambda = d(distance)/d(image) on the device, then per parameter the tangent of the image
+// (hig_image_tangent) contracted with lambda, plus the regularisation's reg_alpha (x - mean).
+int hgx_hig_objective_grad(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
+                           const unsigned* mask, int metric, double reg_alpha, double* dist, double* grad) {
+  if (!ctx || !h || !x || !ref || !dist || !grad)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective_grad: null argument");
+  if (metric == 4 || metric == 5)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective_grad: the gradient is defined for the scalar "
+                                     "distance measures (not the residual vectors)");
+  if (nx != (int)h->in.fit_params.size())
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective_grad: x must hold one value per fit parameter");
+  long nd = 0;
+  HGX_TRY(hgx_hig_objective(ctx, h, x, nx, ref, mask, metric, reg_alpha, dist, &nd));
+  int nrow = 0, ncol = 0;
+  HGX_TRY(hgx_hig_image_size(h, &nrow, &ncol));
+  const long n = (long)nrow * ncol;
+  HigWork& w = *ctx->hig;
+  DevBuf bref, bmask;
+  const void *dref = nullptr, *dmask = nullptr;
+  HGX_TRY(stage_in(ctx, ref, sizeof(double) * n, bref, &dref));
+  if (mask) HGX_TRY(stage_in(ctx, mask, sizeof(unsigned) * n, bmask, &dmask));
+  HGX_TRY(w.lam.reserve(sizeof(double) * n));
+  HGX_TRY(w.dimg.reserve(sizeof(double) * n));
+  HGX_TRY(fit_distance_gradient(ctx, metric, n, (const double*)dref, (const double*)w.obj.p,
+                                (const unsigned*)dmask, (double*)w.lam.p));
+  const bool finite = dist[0] != 1e8;  // a non-finite distance is replaced by 1e8: no slope
+  int i = 0;
+  for (const auto& kv : h->in.fit_params) {
+    const double mean = (kv.second.range[1] - kv.second.range[0]) / 2.0 + kv.second.range[0];
+    const double step = 1e-6 * std::max(1.0, std::fabs(x[i]));
+    double g = 0.0;
+    if (finite) {
+      HGX_CUDA(cudaMemsetAsync(w.dimg.p, 0, sizeof(double) * n, ctx->stream));
+      HGX_TRY(hig_image_tangent(ctx, h, kv.second.variable, x[i], step, (double*)w.dimg.p));
+      HGX_TRY(device_dot(ctx, n, (const double*)w.lam.p, (const double*)w.dimg.p, &g));
+      g += reg_alpha * (x[i] - mean);
+    }
+    grad[i++] = g;
+  }
+  return hgx_synchronize(ctx);
 }
 
 }  // extern "C"

@@ -925,6 +925,25 @@ real_vec_t HiGObjectiveFunctionG::operator()(const real_vec_t& x) {
   return real_vec_t(dist.begin(), dist.begin() + nd);
 }
 
+bool HiGObjectiveFunctionG::value_and_gradient(const real_vec_t& x, real_t& f, real_vec_t& g) {
+  Impl& m = *impl_;
+  HipGISAXSG::Impl& s = *m.sim.impl_;
+  if (!m.good || m.ref.empty() || m.metric < 0) {
+    s.refuse("value_and_gradient(): the objective has no reference data or distance metric");
+    return false;
+  }
+  std::vector<double> xd(x.begin(), x.end()), gd(x.size());
+  double dist = 0.0;
+  if (!s.check(hgx_hig_objective_grad(s.ctx, s.h, xd.data(), (int)xd.size(), m.ref.data(),
+                                      m.mask.empty() ? nullptr : m.mask.data(), m.metric, m.alpha, &dist,
+                                      gd.data()),
+               "value_and_gradient()"))
+    return false;
+  f = dist;
+  g.assign(gd.begin(), gd.end());
+  return true;
+}
+
 int HiGObjectiveFunctionG::num_fit_params() const { return (int)impl_->sim.impl_->params().size(); }
 
 std::vector<std::string> HiGObjectiveFunctionG::fit_param_keys() const { return impl_->sim.fit_param_keys(); }

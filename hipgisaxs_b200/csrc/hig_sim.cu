@@ -52,6 +52,7 @@
 
 #include "ana_sf.cuh"
 #include "ana_sf_f32.cuh"
+#include "ana_sf_tangent.cuh"
 #include "hgx_internal.cuh"
 #include "hig_config.hpp"
 
@@ -277,6 +278,122 @@ static void launch_grain_f32c(int shape, unsigned blocks, cudaStream_t st, const
     case SH_CYLINDER: grain_dwba_f32c_kernel<SH_CYLINDER><<<blocks, 128, 0, st>>>(a); break;
     case SH_SPHERE: grain_dwba_f32c_kernel<SH_SPHERE><<<blocks, 128, 0, st>>>(a); break;
     default: grain_dwba_f32c_kernel<SH_BOX><<<blocks, 128, 0, st>>>(a); break;
+  }
+}
+
+// The tangent of the fused grain loop (FP64, real qz): for one direction of the fit
+// parameters, the change of every pixel's intensity.  Per grain and sample the quad forms the
+// amplitude A = w sum_k fc_k sf_k ff_k with the forward's device functions and its change dA
+// from the hand-written tangents (ana_sf_tangent.cuh) of the tables' changes (shape samples
+// and weights, locations, grain and element rotations, grain centres, lattice vectors, sample
+// weights); dI = 2 Re(conj(A) dA), accumulated over the grains into dI (scaled by `scale`,
+// the structure's share of the image).  The Fresnel coefficients, dn2 and grain-independent
+// structure factors do not change.
+struct TangentArgs {
+  FusedArgs a;                // the tables at the current parameters (a.out unused)
+  const AnaShape* dshapes;    // their changes, same layout
+  const FusedElem* delems;
+  const double* dgrains;
+  const double* delem_rot;
+  const ScaleEntry* dscales;
+  double scale;
+  double* dI;                 // N, accumulated
+};
+
+template <int SHAPE>
+__global__ void __launch_bounds__(128) grain_tangent_kernel(TangentArgs ta) {
+  const FusedArgs& a = ta.a;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = t >> 2;
+  const int k = (int)(t & 3);
+  const bool live = i < a.n;  // every lane takes part in the shuffles
+  const long ii = live ? i : 0;
+  const double q[3] = {a.qx[ii], a.qy[ii], a.qz[k * a.n + ii].x};
+  const zd qzc(q[2], 0.0);
+  const zd fc(a.fc[k * a.n + ii]);
+  const int base = (threadIdx.x & 31) & ~3;
+  double acc = 0.0;
+  for (int g = a.g0; g < a.g1; ++g) {
+    const double* gp = a.grains + 12 * (long)g;
+    const double* dgp = ta.dgrains + 12 * (long)g;
+    zd ff(0, 0), dff(0, 0);
+    for (int e = 0; e < a.nelem; ++e) {
+      const double* er = a.elem_rot + 9 * ((long)g * a.nelem + e);
+      const double* der = ta.delem_rot + 9 * ((long)g * a.nelem + e);
+      double m[3], dm[3];
+      zd mz[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        m[j] = er[3 * j] * q[0] + er[3 * j + 1] * q[1] + er[3 * j + 2] * q[2];
+        dm[j] = der[3 * j] * q[0] + der[3 * j + 1] * q[1] + der[3 * j + 2] * q[2];
+      }
+      Rot9d Re;
+#pragma unroll
+      for (int r = 0; r < 9; ++r) Re.r[r] = er[r];
+      rotate_q(Re, q[0], q[1], qzc, mz);
+      const zd F = ff_analytic_eval<SHAPE>(a.shapes[e], mz, a.elems[e].loc);
+      const zd dF = ff_analytic_tangent<SHAPE>(a.shapes[e], ta.dshapes[e], m, dm, a.elems[e].loc,
+                                               ta.delems[e].loc);
+      const zd dn2(a.elems[e].dre, a.elems[e].dim);
+      ff += dn2 * F;
+      dff += dn2 * dF;
+    }
+    double mr[3], dmr[3];
+    zd mrz[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      mr[j] = gp[3 * j] * q[0] + gp[3 * j + 1] * q[1] + gp[3 * j + 2] * q[2];
+      dmr[j] = dgp[3 * j] * q[0] + dgp[3 * j + 1] * q[1] + dgp[3 * j + 2] * q[2];
+    }
+    Rot9d R;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) R.r[r] = gp[r];
+    rotate_q(R, q[0], q[1], qzc, mrz);
+    const ScaleEntry* sp = a.scales + (long)g * a.nscale;
+    const ScaleEntry* dsp = ta.dscales + (long)g * a.nscale;
+    for (int si = 0; si < a.nscale; ++si) {
+      zd sfv, dsf(0, 0);
+      if (a.sfbuf) {
+        sfv = zd(a.sfbuf[k * a.n + ii]);
+      } else {
+        SfLat L, dL;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          L.la[d] = sp[si].la[d];
+          L.lb[d] = sp[si].lb[d];
+          L.lc[d] = sp[si].lc[d];
+          L.rep[d] = sp[si].rep[d];
+          L.center[d] = gp[9 + d];
+          dL.la[d] = dsp[si].la[d];
+          dL.lb[d] = dsp[si].lb[d];
+          dL.lc[d] = dsp[si].lc[d];
+          dL.rep[d] = 0.0;
+          dL.center[d] = dgp[9 + d];
+        }
+        sfv = sf_lattice_eval(L, mrz);
+        dsf = sf_lattice_tangent(L, dL, mr, dmr);
+      }
+      const zd term = fc * sfv * ff;
+      const zd dterm = fc * (dsf * ff + sfv * dff);
+      zd A(0, 0), dA(0, 0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        A += zd(__shfl_sync(0xffffffffu, term.x, base + j), __shfl_sync(0xffffffffu, term.y, base + j));
+        dA += zd(__shfl_sync(0xffffffffu, dterm.x, base + j), __shfl_sync(0xffffffffu, dterm.y, base + j));
+      }
+      const double w = sp[si].w, dw = dsp[si].w;
+      // d |w A|^2 = 2 w dw |A|^2 + 2 w^2 Re(conj(A) dA)
+      acc += 2.0 * w * dw * (A.x * A.x + A.y * A.y) + 2.0 * w * w * (A.x * dA.x + A.y * dA.y);
+    }
+  }
+  if (live && k == 0) ta.dI[i] += ta.scale * acc;
+}
+
+static void launch_grain_tangent(int shape, unsigned blocks, cudaStream_t st, const TangentArgs& t) {
+  switch (shape) {
+    case SH_CYLINDER: grain_tangent_kernel<SH_CYLINDER><<<blocks, 128, 0, st>>>(t); break;
+    case SH_SPHERE: grain_tangent_kernel<SH_SPHERE><<<blocks, 128, 0, st>>>(t); break;
+    default: grain_tangent_kernel<SH_BOX><<<blocks, 128, 0, st>>>(t); break;
   }
 }
 
@@ -616,14 +733,22 @@ static int orientations(const hig::Structure& s, int ngr, std::vector<double>& n
 // structure factor once when it does not depend on the grain, then the grain kernel in
 // launches of FUSED_GRAINS_PER_LAUNCH grains (the grains in order, so the sums run as in the
 // step-by-step path).
-static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Structure& s, const hig::Unitcell& uc,
-                           const hig::Input& in, const Rot& rot_phi, const std::vector<double>& dd,
-                           const std::vector<double>& nn, int ngr, int ax1, int ax2, int ax3,
-                           const std::vector<ScaleEntry>& plan, int nscale, const double2* fc,
-                           double* Is, int precision) {
-  cudaStream_t st = c->stream;
+// The fused grain kernel's tables of one structure: every element-location's analytic shape,
+// location and dn2 (unit-cell elements in shape-key order, locations in file order), and per
+// grain its rotation and centre (12 doubles) and every element's rotation (9 doubles).
+struct FusedTables {
   std::vector<AnaShape> shapes;
   std::vector<FusedElem> elems;
+  std::vector<double> gt, er;
+};
+
+static int fused_tables(const hig::Structure& s, const hig::Unitcell& uc, const hig::Input& in,
+                        const Rot& rot_phi, const std::vector<double>& dd, const std::vector<double>& nn,
+                        int ngr, int ax1, int ax2, int ax3, FusedTables& T) {
+  std::vector<AnaShape>& shapes = T.shapes;
+  std::vector<FusedElem>& elems = T.elems;
+  shapes.clear();
+  elems.clear();
   std::vector<const hig::Shape*> owner;
   for (const auto& ekv : uc.elements) {  // in shape-key order, locations in file order
     const hig::Shape& sh = in.shapes.at(ekv.first);
@@ -647,7 +772,10 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
     }
   }
   const int nelem = (int)elems.size();
-  std::vector<double> gt(12 * (size_t)ngr), er(9 * (size_t)ngr * (nelem > 0 ? nelem : 1));
+  std::vector<double>& gt = T.gt;
+  std::vector<double>& er = T.er;
+  gt.assign(12 * (size_t)ngr, 0.0);
+  er.assign(9 * (size_t)ngr * (nelem > 0 ? nelem : 1), 0.0);
   for (int gi = 0; gi < ngr; ++gi) {
     const Rot rot = ((rot_phi * Rot::axis(ax3, nn[2 * ngr + gi])) * Rot::axis(ax2, nn[ngr + gi])) *
                     Rot::axis(ax1, nn[gi]);
@@ -663,6 +791,22 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
       for (int r = 0; r < 9; ++r) er[9 * ((size_t)gi * nelem + e) + r] = srot.m[r];
     }
   }
+  return HGX_OK;
+}
+
+static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Structure& s, const hig::Unitcell& uc,
+                           const hig::Input& in, const Rot& rot_phi, const std::vector<double>& dd,
+                           const std::vector<double>& nn, int ngr, int ax1, int ax2, int ax3,
+                           const std::vector<ScaleEntry>& plan, int nscale, const double2* fc,
+                           double* Is, int precision) {
+  cudaStream_t st = c->stream;
+  FusedTables T;
+  HGX_TRY(fused_tables(s, uc, in, rot_phi, dd, nn, ngr, ax1, ax2, ax3, T));
+  const std::vector<AnaShape>& shapes = T.shapes;
+  const std::vector<FusedElem>& elems = T.elems;
+  const std::vector<double>& gt = T.gt;
+  const std::vector<double>& er = T.er;
+  const int nelem = (int)elems.size();
   DevBuf &bshapes = w.shapes, &belems = w.elems, &bgt = w.gt, &ber = w.er, &bsf = w.sf, &bsc = w.sc;
   if (nelem > 0) {
     HGX_TRY(bshapes.reserve(sizeof(AnaShape) * nelem));
@@ -1042,3 +1186,219 @@ int hgx_hig_compute_scan_point(hgx_ctx c, hgx_hig h, int precision, int p, doubl
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------- tangent of the image ----
+namespace hgx {
+namespace {
+
+// What a fit parameter must leave unchanged for the fused grain loop's tangent to be the
+// image's: the layers and the beam (Fresnel coefficients, grid), the structures' types,
+// iratios, liquid structure-factor parameters, grain counts and repetitions, and the shapes'
+// refractive indices (dn2).
+std::vector<double> fixed_quantities(const hig::Input& in) {
+  std::vector<double> f;
+  for (const auto& kv : in.layers) {
+    const hig::Layer& l = kv.second;
+    f.insert(f.end(), {l.refindex.delta, l.refindex.beta, l.thickness, (double)l.order});
+  }
+  for (const auto& kv : in.shapes)
+    f.insert(f.end(), {kv.second.refindex.delta, kv.second.refindex.beta});
+  for (const auto& kv : in.structures) {
+    const hig::Structure& s = kv.second;
+    f.insert(f.end(), {s.iratio, (double)s.pc_dims, s.pc_dist[0], s.pc_dist[1], s.pc_sdev[0], s.pc_sdev[1],
+                       s.pc_domain, (double)s.py_dims, s.py_diameter, s.py_volfract, s.maxgrains[0],
+                       s.maxgrains[1], s.maxgrains[2], s.repetition[0], s.repetition[1], s.repetition[2]});
+  }
+  const hig::Scattering& sc = in.scattering;
+  f.insert(f.end(), {sc.alphai[0], sc.inplanerot[0], sc.photon_value});
+  const hig::Compute& cp = in.compute;
+  f.insert(f.end(), {cp.minpoint[0], cp.minpoint[1], cp.maxpoint[0], cp.maxpoint[1],
+                     (double)cp.resolution[0], (double)cp.resolution[1]});
+  return f;
+}
+
+// The tables of every structure at one parameter setting.
+struct StructTables {
+  FusedTables f;
+  std::vector<ScaleEntry> plan;
+  int ngr = 0, nscale = 0, shape = 0;
+  bool liquid = false;
+};
+
+int all_tables(const hig::Input& in, std::vector<StructTables>& out, std::string& why) {
+  out.clear();
+  const Rot rot_phi = Rot::axis(2, in.scattering.inplanerot[0] * PI / 180);
+  for (const auto& skv : in.structures) {
+    const hig::Structure& s = skv.second;
+    const hig::Unitcell& uc = in.unitcells.at(s.unitcell_key);
+    StructTables T;
+    std::vector<double> dd, nn, gw;
+    regular_centres(s, dd, T.ngr);
+    HGX_TRY(orientations(s, T.ngr, nn, gw));
+    double r1[3], r2[3], r3[3];
+    rotation_of(s.rot1, r1);
+    rotation_of(s.rot2, r2);
+    rotation_of(s.rot3, r3);
+    if (!scale_plan(s, T.ngr, gw, T.plan, T.nscale, why)) return HGX_ERR_INVALID_ARG;
+    HGX_TRY(fused_tables(s, uc, in, rot_phi, dd, nn, T.ngr, (int)r1[0], (int)r2[0], (int)r3[0], T.f));
+    T.shape = T.f.shapes.empty() ? 0 : T.f.shapes[0].shape;
+    for (const AnaShape& a : T.f.shapes)
+      if (a.shape != T.shape) T.shape = 0;
+    T.liquid = s.type == "paracrystal" || s.type == "percusyevick";
+    out.push_back(std::move(T));
+  }
+  return HGX_OK;
+}
+
+}  // namespace
+
+// dI/dx for the fit variable `var` at its current value x0 in h (FP64): the change of every
+// pixel of hgx_hig_compute_gisaxs's image, added into dI (device, nrow x ncol).  The tables
+// of the fused grain loop (shape samples and weights, locations, rotations, centres, lattice
+// vectors, sample weights) are functions of the description that the host builds; their
+// changes are taken by central differences of that set-up at x0 +- step (algebraic in x, so
+// accurate to ~1e-10), and the kernel carries them through the form and structure factors and
+// the DWBA sum with the hand-written tangents.  Needs a preceding hgx_hig_compute_gisaxs of h
+// (its grid and Fresnel coefficients).  Refused: parameters that change a quantity listed in
+// fixed_quantities or a table's size, grids with complex qz, shapes other than cylinders,
+// spheres and boxes, SAXS, sliced layers, random orientations.
+int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, double step, double* dI) {
+  auto refuse = [&](const std::string& why) {
+    return fail(HGX_ERR_INVALID_ARG, "hgx_hig_objective_grad: parameter '" + var + "': " + why);
+  };
+  const hig::Input& in = h->in;
+  if (in.scattering.expt != "gisaxs") return refuse("gradients are built for GISAXS (DWBA) descriptions");
+  if (in.compute.nslices > 1) return refuse("sliced layers");
+  if (!c->hig || !c->hig->grid) return refuse("no simulation of the description has run on this context");
+  hgx_qgrid g = c->hig->grid;
+  if (g->mode != 1) return refuse("the grid's qz blocks are complex");
+  for (const auto& kv : in.structures) {
+    const hig::Structure& s = kv.second;
+    if (s.orientation_stat == "range" || s.orientation_stat == "random")
+      return refuse("structure '" + s.key + "': orientations drawn at random change between evaluations");
+    if (s.type == "paracrystal" && s.lattice.type == "") return refuse("paracrystal without lattice");
+    const hig::Unitcell& uc = in.unitcells.at(s.unitcell_key);
+    for (const auto& e : uc.elements) {
+      const std::string& nm = in.shapes.at(e.first).name;
+      if (nm != "cylinder" && nm != "sphere" && nm != "box")
+        return refuse("shape '" + e.first + "' (" + nm + "): tangents are built for cylinders, spheres and boxes");
+    }
+  }
+  // the set-up at x0 - step, x0 + step and x0
+  std::string why, err;
+  hig::Input ip = in, im = in;
+  if (!hig::update_param(ip, var, x0 + step, err) || !hig::update_param(im, var, x0 - step, err))
+    return refuse(err);
+  if (fixed_quantities(ip) != fixed_quantities(im))
+    return refuse("it changes a refractive index, a layer, the beam, a liquid structure factor, an iratio, "
+                  "a grain count or a repetition");
+  std::vector<StructTables> T0, Tp, Tm;
+  int st0 = all_tables(in, T0, why);
+  if (st0 != HGX_OK) return why.empty() ? st0 : refuse(why);
+  if (all_tables(ip, Tp, why) != HGX_OK || all_tables(im, Tm, why) != HGX_OK) return refuse(why);
+  const double inv = 1.0 / (2.0 * step);
+  // iratios as the structure sum rescales them
+  double rsum = 0.0;
+  for (const auto& kv : in.structures) rsum += kv.second.iratio;
+  cudaStream_t st = c->stream;
+  HigWork& w = *c->hig;
+  const long n = (long)g->nqy;
+  size_t si = 0;
+  for (const auto& skv : in.structures) {
+    const StructTables &A = T0[si], &P = Tp[si], &M = Tm[si];
+    ++si;
+    if (P.ngr != M.ngr || P.nscale != M.nscale || P.f.shapes.size() != M.f.shapes.size() ||
+        A.ngr != P.ngr || A.nscale != P.nscale || A.f.shapes.size() != P.f.shapes.size())
+      return refuse("it changes the number of grains, samples or elements");
+    if (A.shape == 0) return refuse("a unit cell mixes shapes");
+    // table changes
+    FusedTables D = A.f;
+    for (size_t e = 0; e < D.shapes.size(); ++e) {
+      for (int d = 0; d < 4; ++d) {
+        const Dist &dp = P.f.shapes[e].d[d], &dm = M.f.shapes[e].d[d];
+        if (dp.n != dm.n || dp.n != A.f.shapes[e].d[d].n)
+          return refuse("it changes the number of a shape's samples (the reference's sampling steps)");
+        for (int j = 0; j < dp.n; ++j) {
+          D.shapes[e].d[d].v[j] = (dp.v[j] - dm.v[j]) * inv;
+          D.shapes[e].d[d].w[j] = (dp.w[j] - dm.w[j]) * inv;
+        }
+      }
+      for (int k = 0; k < 3; ++k) D.elems[e].loc[k] = (P.f.elems[e].loc[k] - M.f.elems[e].loc[k]) * inv;
+    }
+    for (size_t j = 0; j < D.gt.size(); ++j) D.gt[j] = (P.f.gt[j] - M.f.gt[j]) * inv;
+    for (size_t j = 0; j < D.er.size(); ++j) D.er[j] = (P.f.er[j] - M.f.er[j]) * inv;
+    std::vector<ScaleEntry> Dp = A.plan;
+    for (size_t j = 0; j < Dp.size(); ++j) {
+      for (int k = 0; k < 3; ++k) {
+        if (P.plan[j].rep[k] != M.plan[j].rep[k]) return refuse("it changes a repetition");
+        Dp[j].la[k] = (P.plan[j].la[k] - M.plan[j].la[k]) * inv;
+        Dp[j].lb[k] = (P.plan[j].lb[k] - M.plan[j].lb[k]) * inv;
+        Dp[j].lc[k] = (P.plan[j].lc[k] - M.plan[j].lc[k]) * inv;
+        if (A.plan[j].rep[k] != rint(A.plan[j].rep[k])) return refuse("a repetition is not an integer");
+      }
+      Dp[j].w = (P.plan[j].w - M.plan[j].w) * inv;
+    }
+    // device tables: values in the forward's buffers, changes in the tangent buffers
+    const int nelem = (int)A.f.elems.size();
+    DevBuf &bs = w.shapes, &be = w.elems, &bg = w.gt, &br = w.er, &bc = w.sc;
+    DevBuf &ds = w.tshapes, &de = w.telems, &dg = w.tgt, &dr = w.ter, &dc = w.tsc;
+    auto up = [&](DevBuf& b, const void* p, size_t bytes) -> int {
+      HGX_TRY(b.reserve(bytes > 0 ? bytes : 16));
+      if (bytes) HGX_CUDA(cudaMemcpyAsync(b.p, p, bytes, cudaMemcpyHostToDevice, st));
+      return HGX_OK;
+    };
+    HGX_TRY(up(bs, A.f.shapes.data(), sizeof(AnaShape) * nelem));
+    HGX_TRY(up(be, A.f.elems.data(), sizeof(FusedElem) * nelem));
+    HGX_TRY(up(bg, A.f.gt.data(), sizeof(double) * A.f.gt.size()));
+    HGX_TRY(up(br, A.f.er.data(), sizeof(double) * A.f.er.size()));
+    HGX_TRY(up(bc, A.plan.data(), sizeof(ScaleEntry) * A.plan.size()));
+    HGX_TRY(up(ds, D.shapes.data(), sizeof(AnaShape) * nelem));
+    HGX_TRY(up(de, D.elems.data(), sizeof(FusedElem) * nelem));
+    HGX_TRY(up(dg, D.gt.data(), sizeof(double) * D.gt.size()));
+    HGX_TRY(up(dr, D.er.data(), sizeof(double) * D.er.size()));
+    HGX_TRY(up(dc, Dp.data(), sizeof(ScaleEntry) * Dp.size()));
+    const hig::Structure& s = skv.second;
+    TangentArgs ta;
+    FusedArgs& a = ta.a;
+    a.shapes = (const AnaShape*)bs.p;
+    a.elems = (const FusedElem*)be.p;
+    a.nelem = nelem;
+    a.grains = (const double*)bg.p;
+    a.elem_rot = (const double*)br.p;
+    a.scales = (const ScaleEntry*)bc.p;
+    a.nscale = A.nscale;
+    a.sfbuf = nullptr;
+    if (s.type == "paracrystal") {
+      HGX_TRY(hgx_sf_paracrystal(c, g, s.pc_dims, lattice_code(s.lattice.type), s.pc_dist[1], s.pc_dist[0],
+                                 s.pc_sdev[1], s.pc_sdev[0], s.pc_domain, w.sf.p, HGX_C128));
+      a.sfbuf = (const double2*)w.sf.p;
+    } else if (s.type == "percusyevick") {
+      HGX_TRY(hgx_sf_percus_yevick(c, g, s.py_diameter, s.py_volfract, s.py_dims, w.sf.p, HGX_C128));
+      a.sfbuf = (const double2*)w.sf.p;
+    }
+    a.qx = g->qx;
+    a.qy = g->qy;
+    a.qz = g->qz;
+    a.fc = (const double2*)w.fc.p;
+    a.n = n;
+    a.out = nullptr;
+    ta.dshapes = (const AnaShape*)ds.p;
+    ta.delems = (const FusedElem*)de.p;
+    ta.dgrains = (const double*)dg.p;
+    ta.delem_rot = (const double*)dr.p;
+    ta.dscales = (const ScaleEntry*)dc.p;
+    ta.scale = rsum != 1.0 ? s.iratio / rsum : s.iratio;
+    ta.dI = dI;
+    const unsigned blocks = (unsigned)((4 * n + 127) / 128);
+    for (int g0 = 0; g0 < A.ngr; g0 += FUSED_GRAINS_PER_LAUNCH) {
+      a.g0 = g0;
+      a.g1 = std::min(A.ngr, g0 + FUSED_GRAINS_PER_LAUNCH);
+      launch_grain_tangent(A.shape, blocks, st, ta);
+      HGX_CUDA(cudaGetLastError());
+    }
+    // the tables are read by the kernels before the next structure's copies (stream order)
+  }
+  return HGX_OK;
+}
+
+}  // namespace hgx

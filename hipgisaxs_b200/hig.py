@@ -260,6 +260,21 @@ class HiGInput:
         self._reload()
         return dist[:nd.value].copy()
 
+    def objective_grad(self, ctx: Context, x, ref, mask=None, metric="sqrt_unit_l2", reg_alpha=0.0):
+        """(distance, gradient) of the objective at x for a scalar distance measure: the
+        gradient by the tangent of the simulation (hgx_hig_objective_grad), one value per fit
+        parameter in fit_keys() order."""
+        xa = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        pr, kr = _in(ref, np.float64)
+        pm, km = (None, None) if mask is None else _in(mask, np.uint32)
+        dist = np.zeros(1)
+        grad = np.zeros(xa.size)
+        check(lib().hgx_hig_objective_grad(ctx.handle, self._h, xa.ctypes.data, int(xa.size), pr, pm,
+                                           METRICS.get(metric, metric), float(reg_alpha),
+                                           dist.ctypes.data, grad.ctypes.data))
+        self._reload()
+        return float(dist[0]), grad
+
     @property
     def handle(self):
         return self._h

@@ -530,6 +530,21 @@ int hgx_fit_distance(hgx_ctx ctx, int metric, long n, const double* ref, const d
  * 1 value, or nrow*ncol for the residual forms; *ndist receives the count. */
 int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
                       const unsigned* mask, int metric, double reg_alpha, double* dist, long* ndist);
+/* hgx_hig_objective for a scalar distance measure (not the residual vectors) and its
+ * gradient with respect to the fit parameters (grad: nx host doubles, key order).  The
+ * reference's LMVM fitter differentiates dist[0] by central differences, two simulations per
+ * parameter (src/analyzer/hipgisaxs_fit_lmvm.cpp:190-223).  Here one FP64 simulation, the
+ * derivative of the distance with respect to the image on the device, and per parameter the
+ * tangent of the image through the fused grain loop's form factors, lattice structure factor
+ * and DWBA sum (hand-written derivatives), contracted with it; the regularisation adds
+ * reg_alpha (x - mean).  Parameters: anything that moves the analytic shapes' samples and
+ * weights (cylinder, sphere, box), element locations, orientations (not "range"/"random"),
+ * grain spacings, lattice vectors or scalings; parameters that change refractive indices,
+ * layers, the beam, liquid structure factors, iratios or a sample count return
+ * HGX_ERR_INVALID_ARG with the reason.  DWBA grids with real qz (vacuum particle layer). */
+int hgx_hig_objective_grad(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
+                           const unsigned* mask, int metric, double reg_alpha, double* dist,
+                           double* grad);
 
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA

@@ -330,6 +330,10 @@ class HiGObjectiveFunctionG {
   bool set_distance_metric(const std::string& name);  // sqrt_unit_l2, sqrt_c_l2, ...
   bool set_regularization(real_t alpha);
   real_vec_t operator()(const real_vec_t& x);        // empty on failure
+  // the scalar objective (operator()'s one distance; not the residual metrics) and its
+  // gradient by the simulation's tangent (hgx_hig_objective_grad), where the reference's LMVM
+  // fitter takes two simulations per parameter; false on failure
+  bool value_and_gradient(const real_vec_t& x, real_t& f, real_vec_t& g);
   int num_fit_params() const;
   std::vector<std::string> fit_param_keys() const;
   std::vector<std::pair<real_t, real_t>> fit_param_limits() const;

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from conftest import ROOT
+import hipgisaxs_b200 as hg
 from hipgisaxs_b200.hig import read_hig
 
 HIG = os.path.join(ROOT, "tests", "golden", "hig")
@@ -265,3 +266,67 @@ def test_compute_gisaxs_f32c_analytic(ctx, po, name):
     assert po.rel_err(img, ref) < 1e-5
     assert np.abs(img - ref).max() / np.abs(ref).max() < 1e-5
     assert not np.array_equal(img, img64)
+
+
+def _oracle_objective(po, d, x, ref_img, mask, metric, alpha):
+    d.fit_update(x)
+    img = po.compute_gisaxs(d.data, HIG)
+    v = po.fit_distance(metric, ref_img, img, mask)[0]
+    means = [(fp["range"][1] + fp["range"][0]) / 2.0 for _, fp in sorted(d.fit_params.items())]
+    return v + (alpha / 2) * sum((xi - m) ** 2 for xi, m in zip(x, means))
+
+
+def _richardson(f, x, j, h):
+    def central(hh):
+        xp, xm = np.array(x, float), np.array(x, float)
+        xp[j] += hh
+        xm[j] -= hh
+        return (f(xp) - f(xm)) / (2 * hh)
+    return (4 * central(h / 2) - central(h)) / 3
+
+
+GRAD_CASES = [("fit_objective.hig", [5.0, 25.0, 12.0], [4.2, 21.0, 0.3]),
+              ("fit_grad_shapes.hig", [4.3, 0.5, 6.5, 1.05, 1.5, 1.0, 75.0],
+               [4.0, 0.4, 6.0, 1.0, 1.0, 3.0, 70.0])]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(GRAD_CASES)))
+@pytest.mark.parametrize("metric", ["sqrt_unit_l2", "sqrt_c_l2", "cbrt_unit_l2", "sqrt_unit_l1"])
+def test_objective_gradient_matches_oracle_differences(ctx, po, case, metric):
+    """d(objective)/dx by the simulation's tangent (hgx_hig_objective_grad) against Richardson
+    central differences of the oracle's objective (FP64), every parameter kind: a cylinder's
+    radius, a sphere distribution's mean and width, a box's size, a lattice vector, a grain
+    translation, an orientation mean (gaussian weights), a grain scaling and spacing, an
+    orientation angle.  Tolerance: 1e-5 of the gradient's norm, component by component."""
+    name, xtrue, x = GRAD_CASES[case]
+    d = read_hig(os.path.join(HIG, name))
+    d.fit_update(xtrue)
+    ref_img = po.compute_gisaxs(d.data, HIG)
+    mask = np.ones(ref_img.size, dtype=np.uint32)
+    mask[::7] = 0
+    alpha = 0.3
+    f, g = d.objective_grad(ctx, x, ref_img, mask, metric, alpha)
+    f0 = d.objective(ctx, x, ref_img, mask, metric, alpha)[0]
+    assert abs(f - f0) <= 1e-14 * abs(f0)
+
+    def fo(xx):
+        return _oracle_objective(po, d, xx, ref_img, mask, metric, alpha)
+
+    assert abs(fo(x) - f) < 1e-10 * abs(f)
+    fd = np.array([_richardson(fo, x, j, 1e-3 * max(1.0, abs(x[j]))) for j in range(len(x))])
+    scale = np.linalg.norm(fd)
+    assert np.all(np.abs(g - fd) <= 1e-5 * scale), (g, fd)
+
+
+@pytest.mark.gpu
+def test_objective_gradient_refuses_what_it_cannot_differentiate(ctx, po):
+    d = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    ref_img = np.ones(d.image_size())
+    x = [4.2, 21.0, 0.3]
+    with pytest.raises(hg.HgxError):  # residual-vector measures have no scalar gradient
+        d.objective_grad(ctx, x, ref_img, None, "sqrt_unit_l2_residual")
+    d2 = read_hig(os.path.join(HIG, "fit_update.hig"))  # random orientations, iratios, layers
+    with pytest.raises(hg.HgxError):
+        d2.objective_grad(ctx, [float(v) for v in range(len(d2.fit_keys()))],
+                          np.ones(d2.image_size()), None, "sqrt_unit_l2")
