@@ -45,7 +45,7 @@
 namespace hgx {
 
 constexpr int TILE = 128;                   // triangles per shared-memory tile
-constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (dx,dy,nx,ny) + float2 B[TILE] (dz,nz)
+constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (dx,nx,dy,ny) + float2 B[TILE] (dz,nz)
 constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
 constexpr int TILE_X2_FLOATS = TILE * 10;   // float4 A2[2*TILE] ((dx,dx,dy,dy),(nx,nx,ny,ny)) + float2 B[TILE]
 constexpr uint32_t TILE_X2_BYTES = TILE_X2_FLOATS * 4;
@@ -158,8 +158,9 @@ __global__ void tri_key_kernel(const double* __restrict__ sd, int ntri, const do
 }
 
 // One CTA (128 threads) per tile.  order: the triangle of each sorted slot (NULL: slot i holds
-// triangle i).  Writes the tile (n~ = s R^T n, offsets d = R^T c - c0; in nm for the scalar
-// layout, in turns for the packed layout), its anchor (c0x/2pi, c0y/2pi, c0z, max |d_par|)
+// triangle i).  Writes the tile (n~ = s R^T n, offsets d = R^T c - c0; the scalar layout
+// float4 (dx, n~x, dy, n~y) + float2 (dz, n~z) in nm, so that (dx, n~x) and (dy, n~y) load as
+// FP32x2 pairs; the packed layout in turns), its anchor (c0x/2pi, c0y/2pi, c0z, max |d_par|)
 // and, when perm is not NULL, the triangle index of each slot (-1 for padding).  The anchor's
 // sums run in a fixed order (deterministic).  Padding slots are zero (they contribute nothing).
 template <bool X2>
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(TILE) tri_tile_kernel(const double* __restrict
   } else {
     float4* A = reinterpret_cast<float4*>(tiles + (size_t)tile * TILE_FLOATS);
     float2* B = reinterpret_cast<float2*>(tiles + (size_t)tile * TILE_FLOATS + 4 * TILE);
-    A[j] = make_float4(dx, dy, nx, ny);
+    A[j] = make_float4(dx, nx, dy, ny);
     B[j] = make_float2(dz, nz);
   }
 }
@@ -343,14 +344,17 @@ __device__ __forceinline__ void row_tile_sums(const float4* __restrict__ A, cons
     for (int n = 0; n < NF; ++n) f[n] = RF[j * NF + n];
 #pragma unroll
     for (int i = 0; i < P; ++i) {
-      float tp = fmaf(qxf[i], t.x, qyf[i] * t.y);  // in-plane phase offset, radians
+      // (q_par.d, q_par.n~) as one FP32x2 multiply and one FP32x2 FMA
+      const float2 pa = __ffma2_rn(make_float2(qxf[i], qxf[i]), make_float2(t.x, t.y),
+                                   __fmul2_rn(make_float2(qyf[i], qyf[i]), make_float2(t.z, t.w)));
+      float tp = pa.x;  // in-plane phase offset, radians
       if (WIDE) {
         float tt = tp * INV_TWO_PI_F;
         tp = (tt - round_nearest(tt)) * TWO_PI_F;  // reduced to [-pi, pi]
       }
       float sn, cs;
       __sincosf(tp, &sn, &cs);
-      float aq = fmaf(qxf[i], t.z, qyf[i] * t.w);  // in-plane part of q.n~
+      const float aq = pa.y;  // in-plane part of q.n~
       float ur = aq * cs, ui = aq * sn;            // U = aq * E
       if (PAIRED) {
 #pragma unroll
@@ -800,7 +804,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
     for (int j = 0; j < TILE; ++j) {
       const float4 t = A[j];
       const float2 z = B[j];
-      float tt = fmaf(qzr, z.x, fmaf(qxf, t.x, qyf * t.y)) * INV_TWO_PI_F;  // turns
+      float tt = fmaf(qzr, z.x, fmaf(qxf, t.x, qyf * t.z)) * INV_TWO_PI_F;  // turns
       float rr = tt - rintf(tt);
       float sn, cs;
       __sincosf(rr * TWO_PI_F, &sn, &cs);
@@ -809,7 +813,7 @@ __global__ void __launch_bounds__(BLOCK) ff_tri_points_kernel(PointArgs a) {
         sn *= amp;
         cs *= amp;
       }
-      float ar = fmaf(qzr, z.y, fmaf(qxf, t.z, qyf * t.w));
+      float ar = fmaf(qzr, z.y, fmaf(qxf, t.y, qyf * t.w));
       float ai = qzi * z.y;
       acc[0] = fmaf(ar, cs, acc[0]);
       acc[0] = fmaf(-ai, sn, acc[0]);

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
     orig[u] = a.perm[(size_t)tile * TILE_T + j];
     float4 A = reinterpret_cast<const float4*>(tl)[j];
     float2 B = reinterpret_cast<const float2*>(tl + 4 * TILE_T)[j];
-    cx[u] = A.x; cy[u] = A.y; nx[u] = A.z; ny[u] = A.w; cz[u] = B.x; nz[u] = B.y;
+    cx[u] = A.x; nx[u] = A.y; cy[u] = A.z; ny[u] = A.w; cz[u] = B.x; nz[u] = B.y;  // (dx, nx, dy, ny)
 #pragma unroll
     for (int q = 0; q < 6; ++q) acc[u][q] = 0.0;
   }
