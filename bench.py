@@ -36,9 +36,10 @@ QMIN_Y, QMIN_Z, QMAX_Y, QMAX_Z = -2.0, 0.0, 2.0, 3.0
 ENERGY_KEV, ALPHA_I_DEG = 10.0, 0.20
 PI_REF = 3.141592653589793
 # FP32 FLOP of the row-factorised kernel per (pixel, triangle) for the 4 paired real
-# DWBA blocks (FMA = 2): in-plane phase 3, reduction 2, angle scale 1, in-plane q.n 3,
-# U = q.n E 2, 16 FFMA accumulations 32  -> 43 FLOP and 2 SFU ops per 4 evaluations.
-FLOP_PER_PIXEL_TRI = 43.0
+# DWBA blocks (FMA = 2): in-plane phase offset q_par.d 3, in-plane q_par.n~ 3, U = (q.n~) E 2,
+# 16 FFMA accumulations 32 -> 40 FLOP and 2 SFU ops (sin, cos) per 4 evaluations.  Not
+# counted: the explicit reduction on wide tiles, the per-tile anchor rotation and TwoSum fold.
+FLOP_PER_PIXEL_TRI = 40.0
 SFU_PER_PIXEL_TRI = 2.0
 # DRAM bytes per launch of the row kernel: ncu dram__bytes_read.sum + dram__bytes_write.sum
 # of one 1536 x 1536 launch (41.1 MB + 24.0 MB, 50,000 triangles) scaled by pixel count to
