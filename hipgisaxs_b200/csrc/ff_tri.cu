@@ -3,7 +3,7 @@
 // src/ff/gpu/ff_tri_gpu.cu:371-384).
 //
 // Triangle tiles (FP32 kernels).  The triangles are put in Morton order of their centroids
-// (a stable radix sort of 30-bit keys) and cut into tiles of 128, so that each tile covers a
+// (a stable radix sort of 30-bit keys) and cut into tiles of 256, so that each tile covers a
 // compact patch of the mesh.  Each tile carries an FP64 anchor c0 (the mean of its rotated
 // centroids); the FP32 tile data hold only the offsets c' - c0.  Then
 //   e^{i q.c'} = e^{i q.c0} e^{i q.(c' - c0)},
@@ -44,7 +44,7 @@
 
 namespace hgx {
 
-constexpr int TILE = 128;                   // triangles per shared-memory tile
+constexpr int TILE = TRI_TILE;              // triangles per shared-memory tile (256)
 constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (dx,nx,dy,ny) + float2 B[TILE] (dz,nz)
 constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
 constexpr int TILE_X2_FLOATS = TILE * 10;   // float4 A2[2*TILE] ((dx,dx,dy,dy),(nx,nx,ny,ny)) + float2 B[TILE]
@@ -53,9 +53,11 @@ constexpr double TWO_PI = 6.283185307179586476925286766559;
 constexpr double INV_TWO_PI = 0.15915494309189533576888376337251;
 constexpr float TWO_PI_F = 6.28318530717958648f;
 constexpr float INV_TWO_PI_F = 0.159154943091895336f;
-// In-plane phases of a tile with |q_par| * (largest offset) above 4 pi radians get the
-// explicit reduction to [-1/2, 1/2] turn before the SFU; below it they go straight in.
-constexpr float WIDE_PHASE2 = 157.91367f;   // (4 pi)^2
+// In-plane phases of a tile with |q_par| * (largest offset) above 8 pi radians get the
+// explicit reduction to [-1/2, 1/2] turn before the SFU; below it they go straight in (the SFU
+// reduces its argument itself; its error grows with |x| by the rounding of x / 2 pi, about
+// 2^-24 |x|, 1.5e-6 rad at 8 pi).
+constexpr float WIDE_PHASE2 = 631.65468f;   // (8 pi)^2
 
 struct Rot9 {
   double r[9];
@@ -1269,7 +1271,7 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
 // that overlap on the GPU (different streams, no ordering) race on the array and must be
 // ordered by the caller.  hgx_ff_triangles_noalloc_status reads the error word back.
 constexpr int NOALLOC_MAX_TRIANGLES = 65536;
-constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 512 tiles, 1.5 MiB + 16 KiB anchors
+constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 256 tiles, 1.5 MiB + 8 KiB anchors
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) float g_noalloc_tiles[NOALLOC_MAX_TILES * TILE_FLOATS];

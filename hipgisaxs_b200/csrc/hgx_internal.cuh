@@ -56,8 +56,11 @@ namespace hgx {
 struct MeshWork {
   DevBuf bv, bf, bfc, bc, bm, sd, F, seeds, part, gtri, vptr, vfac, gvb, Ib, bwpart;
 };
+// Triangles per tile of the FP32C triangle kernels (ff_tri.cu) and of the mesh adjoint's
+// backward pass, which reads the forward's tiles.
+constexpr int TRI_TILE = 256;
 // The FP32 triangle tiles that the last FP32C form-factor call of a context left in its
-// scratch (ff_tri.cu), read by the mesh adjoint: 128 triangles per tile, per-tile anchors
+// scratch (ff_tri.cu), read by the mesh adjoint: TRI_TILE triangles per tile, per-tile anchors
 // (FP64 tile centre: in-plane in turns, z in nm; largest in-plane offset from it, nm) and the
 // caller's index of the triangle in each tile slot (-1 for padding).
 struct TileView {

@@ -167,11 +167,11 @@ __global__ void __launch_bounds__(256) mesh_seed_kernel(SeedArgs a) {
 }
 
 // ------------------------------------------------------------- backward pass ----
-// One CTA per triangle tile of the forward (128 triangles, 2 per thread) and chunk of rows.
+// One CTA per triangle tile of the forward (TRI_TILE triangles, 2 per thread) and chunk of rows.
 // The tile's offsets d = c' - c0 carry the FP32 phases; the anchor phasor e^{i q_par.c0}
 // (FP64 phase) is folded into the seeds when a pixel is staged, and the row phasors take the
 // full z centroid c0z + dz in FP64.
-constexpr int BW_THREADS = 64;
+constexpr int BW_THREADS = TRI_TILE / 2;
 constexpr int BW_TPT = 2;                       // triangles per thread
 constexpr int BW_TRI = BW_THREADS * BW_TPT;     // triangles per CTA = one forward tile
 constexpr int BW_COLS = 256;                    // pixels staged per step
@@ -196,7 +196,7 @@ __device__ __forceinline__ float4 rotate2(float4 v, float ca, float sa) {
 
 __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
   __shared__ float4 s_px[BW_COLS * 3];  // (qx, qy, -, -), seeds 0, seeds 1 (anchor-rotated)
-  const int TILE_T = 128;               // the forward's tile layout
+  const int TILE_T = TRI_TILE;          // the forward's tile layout
   const int tile = blockIdx.x;
   const int chunk = blockIdx.y;
   const int r0 = chunk * a.rows_per_chunk;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
 
 // The plain FP64 backward pass (the FP64 reference of the FP32 one): triangles read from the
 // FP64 tuples and rotated in the kernel, every phase and sum in FP64, same CTA layout
-// (128 triangles per CTA, 2 per thread) and chunking; partial gradients in the caller's
+// (TRI_TILE triangles per CTA, 2 per thread) and chunking; partial gradients in the caller's
 // triangle order.
 constexpr int BW64_COLS = 128;
 
