@@ -3,7 +3,7 @@
 // src/ff/gpu/ff_tri_gpu.cu:371-384).
 //
 // Triangle tiles (FP32 kernels).  The triangles are put in Morton order of their centroids
-// (a stable radix sort of 30-bit keys) and cut into tiles of 256, so that each tile covers a
+// (a stable radix sort of 30-bit keys) and cut into tiles of 512, so that each tile covers a
 // compact patch of the mesh.  Each tile carries an FP64 anchor c0 (the mean of its rotated
 // centroids); the FP32 tile data hold only the offsets c' - c0.  Then
 //   e^{i q.c'} = e^{i q.c0} e^{i q.(c' - c0)},
@@ -44,7 +44,7 @@
 
 namespace hgx {
 
-constexpr int TILE = TRI_TILE;              // triangles per shared-memory tile (256)
+constexpr int TILE = TRI_TILE;              // triangles per shared-memory tile (512)
 constexpr int TILE_FLOATS = TILE * 6;       // float4 A[TILE] (dx,nx,dy,ny) + float2 B[TILE] (dz,nz)
 constexpr uint32_t TILE_BYTES = TILE_FLOATS * 4;
 constexpr int TILE_X2_FLOATS = TILE * 10;   // float4 A2[2*TILE] ((dx,dx,dy,dy),(nx,nx,ny,ny)) + float2 B[TILE]
@@ -275,7 +275,7 @@ __device__ __forceinline__ void store_ff<double2>(double2* out, long idx, double
 __device__ __forceinline__ float2 anchor_phasor(double u) {
   u -= rint(u);
   float s, c;
-  sincospif((float)(2.0 * u), &s, &c);
+  __sincosf((float)(TWO_PI * u), &s, &c);  // |argument| <= pi
   return make_float2(c, s);
 }
 
@@ -392,7 +392,7 @@ __device__ __forceinline__ void row_tile_sums(const float4* __restrict__ A, cons
 }
 
 template <int BLOCK, int P, int NK, bool PAIRED, typename OUT>
-__global__ void __launch_bounds__(BLOCK) ff_tri_rows_kernel(RowArgs a) {
+__global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
   constexpr int NF = PAIRED ? 2 : NK;        // float4 row factors per (row, triangle)
   constexpr int NACC = PAIRED ? 8 : 2 * NK;  // float accumulators per pixel
   __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
@@ -954,17 +954,20 @@ static int dispatch_rows(const RowArgs& a, dim3 grid, int nk, bool paired, cudaS
 }
 
 // Launch shape for the row kernel: P pixels per thread, threads per row a power of two
-// (>= 32) covering the row when it is short, several rows per CTA in that case.
+// (>= 64) covering the row when it is short, up to 4 rows per CTA in that case (the row
+// factors of R rows x 512 triangles must fit the CTA's shared memory: at most 227 KB with the
+// static tiles, the row factors and the compensation terms; the packed kernel with 8 pixels
+// per thread keeps R <= 2).
 struct RowShape {
   int P, tpr, R;
   dim3 grid;
 };
 
-static RowShape row_shape(int nrow, int ncol, int sm_count, int want_p) {
+static RowShape row_shape(int nrow, int ncol, int sm_count, int want_p, bool packed = false) {
   const int BLOCK = 256;
   RowShape best{};
   for (int P = want_p; P >= 1; P >>= 1) {
-    int tpr = 32;
+    int tpr = (packed && P >= 8) ? 128 : 64;
     while (tpr < BLOCK && tpr * P < ncol) tpr <<= 1;
     int R = BLOCK / tpr;
     dim3 g((ncol + tpr * P - 1) / (tpr * P), (nrow + R - 1) / R);
@@ -1066,6 +1069,10 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
     return HGX_OK;
   }
   if (want_p == 0) want_p = g->tuned_p;  // the autotuner's choice for this grid, if any
+  if (want_p != 0 && want_p != 1 && want_p != 2 && want_p != 4 && want_p != -2 && want_p != -4 &&
+      want_p != -8)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: pixels per thread must be 1, 2 or 4 (scalar) "
+                                     "or -2, -4, -8 (packed)");
   const int ntiles = (ntri + TILE - 1) / TILE;
   // paired real DWBA blocks, packed FP32x2 kernel on request (want_p = -2, -4, -8 pixels per
   // thread); automatic (0) picks the scalar one.
@@ -1073,8 +1080,8 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
     const int P = -want_p;
     if (P != 2 && P != 4 && P != 8)
       return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: packed kernel takes 2, 4 or 8 pixels per thread");
-    RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, P);
-    if (sh.P < 2) sh = row_shape(g->nrow, g->ncol, 0, 2);  // keep at least one pair
+    RowShape sh = row_shape(g->nrow, g->ncol, c->sm_count, P, true);
+    if (sh.P < 2) sh = row_shape(g->nrow, g->ncol, 0, 2, true);  // keep at least one pair
     if (sh.grid.y > 65535u)
       return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: too many detector rows for one launch");
     TilePrep t;
@@ -1271,7 +1278,7 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
 // that overlap on the GPU (different streams, no ordering) race on the array and must be
 // ordered by the caller.  hgx_ff_triangles_noalloc_status reads the error word back.
 constexpr int NOALLOC_MAX_TRIANGLES = 65536;
-constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 256 tiles, 1.5 MiB + 8 KiB anchors
+constexpr int NOALLOC_MAX_TILES = NOALLOC_MAX_TRIANGLES / TILE;  // 128 tiles, 1.5 MiB + 4 KiB anchors
 constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) float g_noalloc_tiles[NOALLOC_MAX_TILES * TILE_FLOATS];

@@ -58,7 +58,7 @@ struct MeshWork {
 };
 // Triangles per tile of the FP32C triangle kernels (ff_tri.cu) and of the mesh adjoint's
 // backward pass, which reads the forward's tiles.
-constexpr int TRI_TILE = 256;
+constexpr int TRI_TILE = 512;
 // The FP32 triangle tiles that the last FP32C form-factor call of a context left in its
 // scratch (ff_tri.cu), read by the mesh adjoint: TRI_TILE triangles per tile, per-tile anchors
 // (FP64 tile centre: in-plane in turns, z in nm; largest in-plane offset from it, nm) and the
