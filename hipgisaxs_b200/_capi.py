@@ -44,9 +44,13 @@ SIGNATURES = {
     "hgx_param_distribution": (_i, [_i, _d, _d, _d, _d, _i, _vp, _vp, _i, C.POINTER(_i)]),
     "hgx_ff_analytic": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp,
                              _vp, _d, _d, _vp, _vp, _vp, _i]),
+    "hgx_ff_analytic_ex": (_i, [_vp, _vp, _i, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp,
+                             _vp, _d, _d, _vp, _vp, _vp, _i, _i]),
     "hgx_ff_analytic_params": (_i, [_vp, _vp, _i, _i, _vp, _d, _d, _vp, _vp, _vp, _i]),
+    "hgx_ff_analytic_params_ex": (_i, [_vp, _vp, _i, _i, _vp, _d, _d, _vp, _vp, _vp, _i, _i]),
     "hgx_lattice_vectors": (_i, [_i, C.c_char_p, _vp, _vp]),
     "hgx_sf_lattice": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i]),
+    "hgx_sf_lattice_ex": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i]),
     "hgx_sf_paracrystal": (_i, [_vp, _vp, _i, _i, _d, _d, _d, _d, _d, _vp, _i]),
     "hgx_sf_percus_yevick": (_i, [_vp, _vp, _d, _d, _i, _vp, _i]),
     "hgx_propagation_coeffs": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _i]),

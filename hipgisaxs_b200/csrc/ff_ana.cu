@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "ana_sf.cuh"
+#include "ana_sf_f32.cuh"
 #include "cplx.cuh"
 #include "hgx_internal.cuh"
 
@@ -52,6 +53,22 @@ __global__ void __launch_bounds__(128) ff_analytic_kernel(const AnaArgs* __restr
   zd m[3];
   rotate_q(a.R, a.qx[iy], a.qy[iy], zd(a.qz[iz]), m);
   put<OUT>(a.out, iz, ff_analytic_eval(a.s, m, a.tv));
+}
+
+// FP32C for a grid with real qz: the rotated q is real, the body is ana_sf_f32.cuh's (FP64
+// phase reduction, FP32 transcendentals and sums).  SHAPE: cylinder, sphere or box.
+template <int SHAPE, typename OUT>
+__global__ void __launch_bounds__(128) ff_analytic_f32c_kernel(const AnaArgs* __restrict__ ap) {
+  const AnaArgs& a = *ap;
+  long iz = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (iz >= a.nqz) return;
+  long iy = iz % a.nqy;
+  const double qx = a.qx[iy], qy = a.qy[iy], qz = a.qz[iz].x;
+  double m[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) m[j] = a.R.r[3 * j] * qx + a.R.r[3 * j + 1] * qy + a.R.r[3 * j + 2] * qz;
+  const cf v = ff_analytic_f32c<SHAPE>(a.s, m, a.tv);
+  put<OUT>(a.out, iz, zd((double)v.x, (double)v.y));
 }
 
 // ------------------------------------------------------------------- host side ----
@@ -188,7 +205,8 @@ int ana_shape_from_params(int shape, int nparam, const double* params, double ta
   return check_dims(out);
 }
 
-int ff_analytic_launch(hgx_ctx c, hgx_qgrid g, const AnaArgs& host_args, void* out, int ff_type) {
+int ff_analytic_launch(hgx_ctx c, hgx_qgrid g, const AnaArgs& host_args, void* out, int ff_type,
+                       int precision) {
   // the argument block (about 4 KB) goes to device scratch so the kernel can index it freely
   AnaArgs a = host_args;
   a.qx = g->qx;
@@ -202,6 +220,22 @@ int ff_analytic_launch(hgx_ctx c, hgx_qgrid g, const AnaArgs& host_args, void* o
   AnaArgs* d_args = reinterpret_cast<AnaArgs*>(c->scratch.p);
   HGX_CUDA(cudaMemcpyAsync(d_args, &a, sizeof(AnaArgs), cudaMemcpyHostToDevice, c->stream));
   dim3 grid((g->nqz + 127) / 128);
+  const int sh = a.s.shape;
+  if (precision == HGX_F32C && g->mode == 1 && (sh == SH_CYLINDER || sh == SH_SPHERE || sh == SH_BOX)) {
+    cudaStream_t st = c->stream;
+    if (sh == SH_CYLINDER) {
+      if (a.out_c64) ff_analytic_f32c_kernel<SH_CYLINDER, float2><<<grid, 128, 0, st>>>(d_args);
+      else ff_analytic_f32c_kernel<SH_CYLINDER, double2><<<grid, 128, 0, st>>>(d_args);
+    } else if (sh == SH_SPHERE) {
+      if (a.out_c64) ff_analytic_f32c_kernel<SH_SPHERE, float2><<<grid, 128, 0, st>>>(d_args);
+      else ff_analytic_f32c_kernel<SH_SPHERE, double2><<<grid, 128, 0, st>>>(d_args);
+    } else {
+      if (a.out_c64) ff_analytic_f32c_kernel<SH_BOX, float2><<<grid, 128, 0, st>>>(d_args);
+      else ff_analytic_f32c_kernel<SH_BOX, double2><<<grid, 128, 0, st>>>(d_args);
+    }
+    HGX_CUDA(cudaGetLastError());
+    return HGX_OK;
+  }
   if (a.out_c64) ff_analytic_kernel<float2><<<grid, 128, 0, c->stream>>>(d_args);
   else ff_analytic_kernel<double2><<<grid, 128, 0, c->stream>>>(d_args);
   HGX_CUDA(cudaGetLastError());
@@ -229,11 +263,13 @@ int hgx_param_distribution(int stat, double pmin, double pmax, double mean, doub
   return HGX_OK;
 }
 
-int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
-                    const double* w1, int n2, const double* v2, const double* w2, int n3,
-                    const double* v3, const double* w3, int n4, const double* v4,
-                    const double* w4, double tau, double eta, const double* transvec,
-                    const double* rot9, void* ff, int ff_type) {
+int hgx_ff_analytic_ex(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
+                       const double* w1, int n2, const double* v2, const double* w2, int n3,
+                       const double* v3, const double* w3, int n4, const double* v4,
+                       const double* w4, double tau, double eta, const double* transvec,
+                       const double* rot9, void* ff, int ff_type, int precision) {
+  if (precision != HGX_F64 && precision != HGX_F32C)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: unknown precision");
   if (!c || !g || !ff) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: null argument");
   if (g->ctx != c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_analytic: grid of another context");
   if (ff_type != HGX_C128 && ff_type != HGX_C64)
@@ -259,7 +295,7 @@ int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
     HGX_TRY(tmp.reserve(esz * (size_t)g->nqz));
     dout = tmp.p;
   }
-  HGX_TRY(ff_analytic_launch(c, g, a, dout, ff_type));
+  HGX_TRY(ff_analytic_launch(c, g, a, dout, ff_type, precision));
   if (host_out) {
     HGX_CUDA(cudaMemcpyAsync(ff, dout, esz * (size_t)g->nqz, cudaMemcpyDeviceToHost, c->stream));
     return hgx_synchronize(c);
@@ -267,13 +303,22 @@ int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
   return HGX_OK;
 }
 
+int hgx_ff_analytic(hgx_ctx c, hgx_qgrid g, int shape, int n1, const double* v1,
+                    const double* w1, int n2, const double* v2, const double* w2, int n3,
+                    const double* v3, const double* w3, int n4, const double* v4,
+                    const double* w4, double tau, double eta, const double* transvec,
+                    const double* rot9, void* ff, int ff_type) {
+  return hgx_ff_analytic_ex(c, g, shape, n1, v1, w1, n2, v2, w2, n3, v3, w3, n4, v4, w4, tau, eta,
+                            transvec, rot9, ff, ff_type, HGX_F64);
+}
+
 // The reference's parameter routing (the compute_* switch statements of
 // src/ff/ff_ana_*.cpp) plus param_distribution, then hgx_ff_analytic.
 // params: 7 doubles per parameter (ShapeParamType, StatisticType, min, max, mean,
 // deviation, nvalues).
-int hgx_ff_analytic_params(hgx_ctx c, hgx_qgrid g, int shape, int nparam, const double* params,
-                           double tau, double eta, const double* transvec, const double* rot9,
-                           void* ff, int ff_type) {
+int hgx_ff_analytic_params_ex(hgx_ctx c, hgx_qgrid g, int shape, int nparam, const double* params,
+                              double tau, double eta, const double* transvec, const double* rot9,
+                              void* ff, int ff_type, int precision) {
   AnaShape s;
   HGX_TRY(ana_shape_from_params(shape, nparam, params, tau, eta, s));
   std::vector<double> v[4], w[4];
@@ -282,10 +327,17 @@ int hgx_ff_analytic_params(hgx_ctx c, hgx_qgrid g, int shape, int nparam, const 
     w[k].assign(s.d[k].w, s.d[k].w + s.d[k].n);
   }
   auto ptr = [](std::vector<double>& x) { return x.empty() ? nullptr : x.data(); };
-  return hgx_ff_analytic(c, g, shape, (int)v[0].size(), ptr(v[0]), ptr(w[0]), (int)v[1].size(),
-                         ptr(v[1]), ptr(w[1]), (int)v[2].size(), ptr(v[2]), ptr(w[2]),
-                         (int)v[3].size(), ptr(v[3]), ptr(w[3]), tau, eta, transvec, rot9, ff,
-                         ff_type);
+  return hgx_ff_analytic_ex(c, g, shape, (int)v[0].size(), ptr(v[0]), ptr(w[0]), (int)v[1].size(),
+                            ptr(v[1]), ptr(w[1]), (int)v[2].size(), ptr(v[2]), ptr(w[2]),
+                            (int)v[3].size(), ptr(v[3]), ptr(w[3]), tau, eta, transvec, rot9, ff,
+                            ff_type, precision);
+}
+
+int hgx_ff_analytic_params(hgx_ctx c, hgx_qgrid g, int shape, int nparam, const double* params,
+                           double tau, double eta, const double* transvec, const double* rot9,
+                           void* ff, int ff_type) {
+  return hgx_ff_analytic_params_ex(c, g, shape, nparam, params, tau, eta, transvec, rot9, ff, ff_type,
+                                   HGX_F64);
 }
 
 }  // extern "C"

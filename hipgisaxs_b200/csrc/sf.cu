@@ -15,6 +15,7 @@
 #include <string>
 
 #include "ana_sf.cuh"
+#include "ana_sf_f32.cuh"
 #include "cplx.cuh"
 #include "hgx_internal.cuh"
 
@@ -42,6 +43,23 @@ __global__ void __launch_bounds__(128) sf_lattice_kernel(SfArgs a) {
     reinterpret_cast<double2*>(a.out)[i] = v.d2();
   else
     reinterpret_cast<float2*>(a.out)[i] = make_float2((float)v.x, (float)v.y);
+}
+
+// FP32C for a grid with real qz (ana_sf_f32.cuh: FP64 phase reduction, FP32 sines).
+template <typename OUT>
+__global__ void __launch_bounds__(128) sf_lattice_f32c_kernel(SfArgs a) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nqz) return;
+  long j = i % a.nqy;
+  const double qx = a.qx[j], qy = a.qy[j], qz = a.qz[i].x;
+  double m[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) m[k] = a.R.r[3 * k] * qx + a.R.r[3 * k + 1] * qy + a.R.r[3 * k + 2] * qz;
+  const cf v = sf_lattice_f32c(a.L, m);
+  if (sizeof(OUT) == sizeof(double2))
+    reinterpret_cast<double2*>(a.out)[i] = make_double2((double)v.x, (double)v.y);
+  else
+    reinterpret_cast<float2*>(a.out)[i] = make_float2(v.x, v.y);
 }
 
 }  // namespace hgx
@@ -106,9 +124,11 @@ int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3) {
   return HGX_OK;
 }
 
-int hgx_sf_lattice(hgx_ctx c, hgx_qgrid g, const double* abc9, const double* repet,
-                   const double* scaling, const double* center, const double* rot9, void* sf,
-                   int sf_type) {
+int hgx_sf_lattice_ex(hgx_ctx c, hgx_qgrid g, const double* abc9, const double* repet,
+                      const double* scaling, const double* center, const double* rot9, void* sf,
+                      int sf_type, int precision) {
+  if (precision != HGX_F64 && precision != HGX_F32C)
+    return fail(HGX_ERR_INVALID_ARG, "hgx_sf_lattice: unknown precision");
   if (!c || !g || !abc9 || !repet || !scaling || !sf)
     return fail(HGX_ERR_INVALID_ARG, "hgx_sf_lattice: null argument");
   if (g->ctx != c) return fail(HGX_ERR_INVALID_ARG, "hgx_sf_lattice: grid of another context");
@@ -136,10 +156,24 @@ int hgx_sf_lattice(hgx_ctx c, hgx_qgrid g, const double* abc9, const double* rep
   HGX_TRY(stage_out(c, sf, bytes, tmp, &dout));
   a.out = dout;
   dim3 grid((g->nqz + 127) / 128);
-  if (sf_type == HGX_C64) sf_lattice_kernel<float2><<<grid, 128, 0, c->stream>>>(a);
-  else sf_lattice_kernel<double2><<<grid, 128, 0, c->stream>>>(a);
+  bool integral = true;  // FP32C takes the closed form for integer repetitions
+  for (int i = 0; i < 3; ++i) integral = integral && a.L.rep[i] == rint(a.L.rep[i]);
+  if (precision == HGX_F32C && g->mode == 1 && integral) {
+    if (sf_type == HGX_C64) sf_lattice_f32c_kernel<float2><<<grid, 128, 0, c->stream>>>(a);
+    else sf_lattice_f32c_kernel<double2><<<grid, 128, 0, c->stream>>>(a);
+  } else if (sf_type == HGX_C64) {
+    sf_lattice_kernel<float2><<<grid, 128, 0, c->stream>>>(a);
+  } else {
+    sf_lattice_kernel<double2><<<grid, 128, 0, c->stream>>>(a);
+  }
   HGX_CUDA(cudaGetLastError());
   return finish_out(c, sf, bytes, dout);
+}
+
+int hgx_sf_lattice(hgx_ctx c, hgx_qgrid g, const double* abc9, const double* repet,
+                   const double* scaling, const double* center, const double* rot9, void* sf,
+                   int sf_type) {
+  return hgx_sf_lattice_ex(c, g, abc9, repet, scaling, center, rot9, sf, sf_type, HGX_F64);
 }
 
 }  // extern "C"

@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 from ._capi import C64, C128, check, lib
-from .core import CTYPE, Context, QGrid, _in, _is_tensor
+from .core import CTYPE, PRECISION, Context, QGrid, _in, _is_tensor
 
 SHAPE = {"box": 2, "cube": 3, "cylinder": 4, "sphere": 5, "prism3": 8, "prism6": 9,
          "pyramid": 14}
@@ -41,8 +41,9 @@ def param_distribution(stat, pmin, pmax, mean, dev, nvalues):
 
 
 def ff_analytic(ctx: Context, grid: QGrid, shape, dims, tau=0.0, eta=0.0, transvec=(0, 0, 0),
-                rot=None, out=None, out_type="c128"):
-    """dims: up to four (values, weights-or-None) pairs in the order of hgx_ff_analytic."""
+                rot=None, out=None, out_type="c128", precision="f64"):
+    """dims: up to four (values, weights-or-None) pairs in the order of hgx_ff_analytic;
+    precision "f32c" on real-qz grids for cylinders, spheres and boxes."""
     args = []
     keep = []
     for i in range(4):
@@ -56,9 +57,9 @@ def ff_analytic(ctx: Context, grid: QGrid, shape, dims, tau=0.0, eta=0.0, transv
     tv = np.ascontiguousarray(transvec, dtype=np.float64)
     r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64).reshape(9)
     out = _out(out, grid.nqz, out_type)
-    check(lib().hgx_ff_analytic(ctx.handle, grid.handle, SHAPE[shape], *args, float(tau),
-                                float(eta), tv.ctypes.data, None if r is None else r.ctypes.data,
-                                _ptr(out), CTYPE[out_type]))
+    check(lib().hgx_ff_analytic_ex(ctx.handle, grid.handle, SHAPE[shape], *args, float(tau),
+                                   float(eta), tv.ctypes.data, None if r is None else r.ctypes.data,
+                                   _ptr(out), CTYPE[out_type], PRECISION[precision]))
     return out
 
 
@@ -70,17 +71,17 @@ def param_rows(params):
 
 
 def ff_analytic_params(ctx: Context, grid: QGrid, shape, params, tau=0.0, eta=0.0,
-                       transvec=(0, 0, 0), rot=None, out=None, out_type="c128"):
+                       transvec=(0, 0, 0), rot=None, out=None, out_type="c128", precision="f64"):
     """params: dicts {type, stat, min, max, mean, deviation, nvalues} (HiG shape parameters)."""
     P = params if isinstance(params, np.ndarray) else param_rows(params)
     P = np.ascontiguousarray(P, dtype=np.float64)
     tv = np.ascontiguousarray(transvec, dtype=np.float64)
     r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64).reshape(9)
     out = _out(out, grid.nqz, out_type)
-    check(lib().hgx_ff_analytic_params(ctx.handle, grid.handle, SHAPE[shape], len(P),
-                                       P.ctypes.data, float(tau), float(eta), tv.ctypes.data,
-                                       None if r is None else r.ctypes.data, _ptr(out),
-                                       CTYPE[out_type]))
+    check(lib().hgx_ff_analytic_params_ex(ctx.handle, grid.handle, SHAPE[shape], len(P),
+                                          P.ctypes.data, float(tau), float(eta), tv.ctypes.data,
+                                          None if r is None else r.ctypes.data, _ptr(out),
+                                          CTYPE[out_type], PRECISION[precision]))
     return out
 
 
@@ -92,16 +93,16 @@ def lattice_vectors(kind, hkl="100"):
 
 
 def sf_lattice(ctx: Context, grid: QGrid, abc, repet, scaling, center=(0, 0, 0), rot=None,
-               out=None, out_type="c128"):
+               out=None, out_type="c128", precision="f64"):
     abc9 = np.ascontiguousarray(np.asarray(abc, dtype=np.float64).reshape(9))
     rp = np.ascontiguousarray(repet, dtype=np.float64)
     sc = np.ascontiguousarray(scaling, dtype=np.float64)
     ce = np.ascontiguousarray(center, dtype=np.float64)
     r = None if rot is None else np.ascontiguousarray(rot, dtype=np.float64).reshape(9)
     out = _out(out, grid.nqz, out_type)
-    check(lib().hgx_sf_lattice(ctx.handle, grid.handle, abc9.ctypes.data, rp.ctypes.data,
-                               sc.ctypes.data, ce.ctypes.data, None if r is None else r.ctypes.data,
-                               _ptr(out), CTYPE[out_type]))
+    check(lib().hgx_sf_lattice_ex(ctx.handle, grid.handle, abc9.ctypes.data, rp.ctypes.data,
+                                  sc.ctypes.data, ce.ctypes.data, None if r is None else r.ctypes.data,
+                                  _ptr(out), CTYPE[out_type], PRECISION[precision]))
     return out
 
 

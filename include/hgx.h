@@ -153,12 +153,25 @@ int hgx_ff_analytic(hgx_ctx ctx, hgx_qgrid g, int shape, int n1, const double* v
                     const double* v3, const double* w3, int n4, const double* v4,
                     const double* w4, double tau, double eta, const double* transvec,
                     const double* rot9, void* ff, int ff_type);
+/* The same with a precision (no counterpart in the reference, which computes in its build's one
+ * precision): HGX_F64 as above, or HGX_F32C on grids with real qz for cylinders, spheres and
+ * boxes (phases formed and reduced in FP64, FP32 transcendentals and sums); other shapes and
+ * complex-qz grids are evaluated in FP64. */
+int hgx_ff_analytic_ex(hgx_ctx ctx, hgx_qgrid g, int shape, int n1, const double* v1,
+                       const double* w1, int n2, const double* v2, const double* w2, int n3,
+                       const double* v3, const double* w3, int n4, const double* v4,
+                       const double* w4, double tau, double eta, const double* transvec,
+                       const double* rot9, void* ff, int ff_type, int precision);
 /* AnalyticFormFactor::compute (src/ff/ff_ana.cpp:61-161) from HiG-style shape parameters:
  * 7 doubles per parameter (ShapeParamType, StatisticType, min, max, mean, deviation,
  * nvalues), routed to dimensions and sampled as the reference's compute_* functions do. */
 int hgx_ff_analytic_params(hgx_ctx ctx, hgx_qgrid g, int shape, int nparam,
                            const double* params, double tau, double eta,
                            const double* transvec, const double* rot9, void* ff, int ff_type);
+/* hgx_ff_analytic_params with a precision, as hgx_ff_analytic_ex. */
+int hgx_ff_analytic_params_ex(hgx_ctx ctx, hgx_qgrid g, int shape, int nparam, const double* params,
+                              double tau, double eta, const double* transvec, const double* rot9,
+                              void* ff, int ff_type, int precision);
 
 /* ---------------------------------------------------------- structure factor ---- */
 /* Lattice::construct_vectors (src/model/structure.cpp:86-182): unscaled a, b, c (9) and
@@ -170,6 +183,12 @@ int hgx_lattice_vectors(int type, const char* hkl, double* abc9, double* t3);
 int hgx_sf_lattice(hgx_ctx ctx, hgx_qgrid g, const double* abc9, const double* repet,
                    const double* scaling, const double* center, const double* rot9, void* sf,
                    int sf_type);
+/* The same with a precision: HGX_F32C on grids with real qz and integer repetitions takes the
+ * closed form sin(N theta_r / 2) / sin(theta_r / 2) that the reference's principal-branch
+ * powers reduce to for a real angle (FP64 angles and reductions, FP32 sines); otherwise FP64. */
+int hgx_sf_lattice_ex(hgx_ctx ctx, hgx_qgrid g, const double* abc9, const double* repet,
+                      const double* scaling, const double* center, const double* rot9, void* sf,
+                      int sf_type, int precision);
 
 /* Paracrystal structure factors: StructureFactor::paracrystal1d / paracrystal2d_cubic /
  * paracrystal2d_hex (src/sf/liquid.cpp:29-110), selected as compute_structure_factor selects

@@ -124,3 +124,28 @@ def test_distances(ctx, po):
     np.testing.assert_array_equal(model.residual_vector(ctx, ref, data, mask), mask * (ref - data))
     # deterministic: the same value twice, bit for bit
     assert model.chi2(ctx, data, ref, mask, 1.3) == model.chi2(ctx, data, ref, mask, 1.3)
+
+
+@pytest.mark.parametrize("name", [n for n in _names("ffana_") if n.split("_")[1] in
+                                  ("cylinder", "sphere", "box") and n.endswith("g16")])
+def test_analytic_golden_f32c(ctx, po, golden, golden_grid, name):
+    """The FP32C analytic form factor (cylinders, spheres, boxes on a grid with real qz)
+    against the compiled reference's values: norm-wise relative error below 1e-5."""
+    d = golden(name)
+    G, _, g = _grid(ctx, golden_grid, str(d["grid"]))
+    assert g.mode == 1
+    ff = model.ff_analytic_params(ctx, g, name.split("_")[1], d["params"], float(d["tau"]),
+                                  float(d["eta"]), d["transvec"], d["rot"], precision="f32c")
+    assert po.rel_err(ff, d["ff"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", [n for n in _names("sf_") if n.endswith("g16")])
+def test_sf_golden_f32c(ctx, po, golden, golden_grid, name):
+    """The FP32C lattice structure factor (closed form, FP64 angles) against the compiled
+    reference's principal-branch values on a grid with real qz: norm-wise 1e-5."""
+    d = golden(name)
+    G, _, g = _grid(ctx, golden_grid, str(d["grid"]))
+    assert g.mode == 1
+    sf = model.sf_lattice(ctx, g, d["abc"], d["repet"], d["scaling"], d["center"], d["rot"],
+                          precision="f32c")
+    assert po.rel_err(sf, d["sf"]) < 1e-5
