@@ -275,7 +275,7 @@ __device__ __forceinline__ void store_ff<double2>(double2* out, long idx, double
 __device__ __forceinline__ float2 anchor_phasor(double u) {
   u -= rint(u);
   float s, c;
-  __sincosf((float)(TWO_PI * u), &s, &c);  // |argument| <= pi
+  sincospif((float)(2.0 * u), &s, &c);
   return make_float2(c, s);
 }
 

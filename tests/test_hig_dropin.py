@@ -81,7 +81,9 @@ def test_hig_driver_matches_oracle_and_api(ctx, po, tmp_path):
     mask = np.ones(nrow * ncol, dtype=np.uint32)
     mask[::5] = 0
     hig = _write_case(tmp_path, ref_img, mask)
-    r = subprocess.run([exe, hig], capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    # the FP64 kernels (HGX_PRECISION=f64) for parity with the oracle at 1e-11
+    env = dict(os.environ, HGX_PRECISION="f64")
+    r = subprocess.run([exe, hig], capture_output=True, text=True, timeout=300, cwd=str(tmp_path), env=env)
     assert r.returncode == 0, (r.returncode, r.stdout + r.stderr)
 
     def load(name):
@@ -103,6 +105,16 @@ def test_hig_driver_matches_oracle_and_api(ctx, po, tmp_path):
     want0 = po.compute_gisaxs(d0.data, HIG)
     sim0 = load("sim0.bin").reshape(nrow, ncol)
     assert np.abs(sim0 - want0).max() / np.abs(want0).max() < 1e-11
+    # the drop-in's default, FP32C: within 1e-5 of the oracle
+    sub = tmp_path / "f32c"
+    sub.mkdir()
+    hig32 = _write_case(sub, ref_img, mask)
+    env32 = {k: v for k, v in os.environ.items() if k != "HGX_PRECISION"}
+    r = subprocess.run([exe, hig32], capture_output=True, text=True, timeout=300, cwd=str(sub), env=env32)
+    assert r.returncode == 0, (r.returncode, r.stdout + r.stderr)
+    sim0_32 = np.fromfile(sub / "sim0.bin").reshape(nrow, ncol)
+    assert np.abs(sim0_32 - want0).max() / np.abs(want0).max() < 1e-5
+    assert not np.array_equal(sim0_32, sim0)
     sim1 = load("sim1.bin").reshape(nrow, ncol)
     assert np.abs(sim1 - ref_img).max() / np.abs(ref_img).max() < 1e-11
     txt = np.loadtxt(tmp_path / "sim1.out")
