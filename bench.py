@@ -48,6 +48,30 @@ TRAFFIC_BYTES_PER_LAUNCH = 115.8e6
 TRAFFIC_SOURCE = "ncu capture at 1536x1536 (65.1 MB) scaled by pixels to 2048x2048"
 
 
+# Executed FLOP per unit of the other timed kernels, from ncu thread-instruction counts
+# (2 x FMA + MUL + ADD of each precision) of one launch on the bench's own descriptions,
+# recorded in profiles/roofline_other_kernels.md:
+#   mesh_backward_kernel     82.5 FP32 per (pixel, triangle)   (the expression: 80)
+#   ff_exact_kernel          611 FP64 per (q-point, triangle)
+#   grain_dwba_kernel        6418 FP64 per (pixel, grain), hcp cylinders (HIG_ENSEMBLE)
+#   grain_dwba_f32c_kernel   1226 FP32 + 367 FP64 per (pixel, grain), the same description
+MESH_FWD_FLOP_PER_PIXEL_TRI = FLOP_PER_PIXEL_TRI
+MESH_BWD_FLOP_PER_PIXEL_TRI = 80.0
+EXACT_FP64_FLOP_PER_EVAL = 611.0
+GRAIN_FP64_FLOP_PER_PIXEL_GRAIN = 6418.0
+GRAIN_F32C_FP32_FLOP_PER_PIXEL_GRAIN = 1226.0
+GRAIN_F32C_FP64_FLOP_PER_PIXEL_GRAIN = 367.0
+
+
+def roofline_of(bound, flop_per_unit, units, seconds, peak, unit, source):
+    """A roofline sub-object: achieved TFLOP/s = flop_per_unit x units / seconds, its fraction
+    of the measured peak of the bounding pipe (the library's own probes on this GPU)."""
+    ach = flop_per_unit * units / seconds / 1e12
+    return {"bound": bound, "flop_per_unit": flop_per_unit, "unit": unit, "units": units,
+            "achieved": ach, "peak": peak, "units_rate": "TFLOP/s", "frac": ach / peak,
+            "flop_source": source}
+
+
 def hbm_view(ms_step):
     """The row kernel against HBM bandwidth (MEASURED_PEAKS.json): its algorithmic bytes per
     launch are the q-grid read once (qx, qy FP64) and the complex64 output written once; the
@@ -721,6 +745,7 @@ def main():
     ctx.synchronize()
 
     peak_fp32, peak_sfu = hg.measure_peaks(ctx, sustained_ms=2000)
+    peak_fp64 = hg.measure_peak_fp64(ctx)
 
     clk = Clocks(local)
     barrier()
@@ -792,14 +817,31 @@ def main():
     if not args.no_fitting:
         fit = fitting_bench(ctx, torch, dev, stream)
         fit["mesh_vertices_2048sq"] = mesh_grad_bench(ctx, grid)
+        mv = fit["mesh_vertices_2048sq"]
+        mv["roofline"] = roofline_of(
+            "fp32", MESH_FWD_FLOP_PER_PIXEL_TRI + MESH_BWD_FLOP_PER_PIXEL_TRI, float(n) * mv["triangles"],
+            mv["s_per_eval"], peak_fp32, "(pixel, triangle): forward 40 + backward 80",
+            "the expressions as written; ncu counts 82.5 executed in the backward")
 
     exact = None
     if not args.no_exact:
         exact = exact_bench(ctx, torch, stream, sd)
+        exact["roofline"] = roofline_of("fp64", EXACT_FP64_FLOP_PER_EVAL, exact["value"], 1.0, peak_fp64,
+                                        "(q-point, triangle)", "ncu executed FP64 FLOP, 512^2 launch")
 
     hig = None
     if not args.no_hig and rank == 0 and world == 1:
         hig = hig_bench(ctx)
+        pg = float(hig["pixels"]) * hig["grains"]
+        hig["roofline"] = roofline_of("fp64", GRAIN_FP64_FLOP_PER_PIXEL_GRAIN, pg,
+                                      hig["ms_per_simulation"] * 1e-3, peak_fp64, "(pixel, grain)",
+                                      "ncu executed FP64 FLOP of grain_dwba_kernel on this description; "
+                                      "the time is the whole simulation")
+        if "f32c" in hig:
+            hig["f32c"]["roofline"] = roofline_of(
+                "fp32", GRAIN_F32C_FP32_FLOP_PER_PIXEL_GRAIN, pg, hig["f32c"]["ms_per_simulation"] * 1e-3,
+                peak_fp32, "(pixel, grain)", "ncu executed FP32 FLOP of grain_dwba_f32c_kernel (plus 367 "
+                "FP64 per unit); its SFU pipe is the busiest (56% in ncu)")
 
     cfg1 = None
     if not args.no_config1 and rank == 0 and world == 1:
@@ -839,6 +881,8 @@ def main():
                          "sfu": {"achieved_gops": sfu_rate, "peak_gops": peak_sfu,
                                  "frac": sfu_rate / peak_sfu},
                          "hbm_view": hbm_view(ms_step)},
+            "peaks": {"fp32_tflops": peak_fp32, "fp64_tflops": peak_fp64, "sfu_gops": peak_sfu,
+                      "source": "the library's probes on this GPU (FFMA sustained 2 s, DFMA burst, __sinf)"},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
             "exact_triangle": exact, "hig_simulation": hig, "config1_dwba_1024sq": cfg1,
             "gpu_launches": 2 * args.steps, "clocks": clocks,
