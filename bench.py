@@ -42,10 +42,13 @@ PI_REF = 3.141592653589793
 FLOP_PER_PIXEL_TRI = 40.0
 SFU_PER_PIXEL_TRI = 2.0
 # DRAM bytes per launch of the row kernel: ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one 1536 x 1536 launch (41.1 MB + 24.0 MB, 50,000 triangles) scaled by pixel count to
-# 2048 x 2048 (q-grid reads and output writes grow with pixels; the triangle tiles stay in L2)
-TRAFFIC_BYTES_PER_LAUNCH = 115.8e6
-TRAFFIC_SOURCE = "ncu capture at 1536x1536 (65.1 MB) scaled by pixels to 2048x2048"
+# of one 2048 x 2048 launch with 50,000 triangles (75.2 MB + 84.7 MB; profiles/ff_tri_rows_mesh50k.md)
+TRAFFIC_BYTES_PER_LAUNCH = 159.9e6
+TRAFFIC_SOURCE = "ncu capture of a 2048x2048 launch (75.2 MB read + 84.7 MB write)"
+# the library's kernels per form-factor step (bounding box 2, Morton keys, tiles, row kernel);
+# CUB's radix sort of the keys adds 6 launches per step
+HGX_LAUNCHES_PER_STEP = 5
+CUB_LAUNCHES_PER_STEP = 6
 
 
 # Executed FLOP per unit of the other timed kernels, from ncu thread-instruction counts
@@ -885,7 +888,9 @@ def main():
                       "source": "the library's probes on this GPU (FFMA sustained 2 s, DFMA burst, __sinf)"},
             "cpu_baseline": cpu, "e2e": e2e, "fp64_plain": f64, "fitting": fit,
             "exact_triangle": exact, "hig_simulation": hig, "config1_dwba_1024sq": cfg1,
-            "gpu_launches": 2 * args.steps, "clocks": clocks,
+            "gpu_launches": HGX_LAUNCHES_PER_STEP * args.steps,
+            "library_launches": {"cub_radix_sort": CUB_LAUNCHES_PER_STEP * args.steps},
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     grid.close()
