@@ -20,8 +20,11 @@
 //   kernel written without its branch sign, which cancels), Pc = e^{i(cx q'x + cy q'y)}.
 // Derivatives: dFr/dR = sum_i 2 pi r_i J0(q|| r_i) r_i / R; dG/dH = sum_j e^{i qz h_j} h_j / H;
 // dS/dtheta from the closed form (series near t = 0); dtheta/dphi = a (u . dq'/dphi).
-// Per-row factors are FP64; per-pixel Bessel sums in T (FP32 or FP64); lattice phases are
-// reduced in FP64; chi^2 and gradient sums are FP64 and deterministic.
+// |Pc| = 1, so I = |K Q|^2 (Fr Sa Sb)^2 and every derivative of I is real arithmetic on three
+// FP64 row scalars and the pixel's Fr, dFr/dR, Sa, Sb, dSa, dSb.  Row factors are FP64; the
+// pixel pass is FP64 throughout (HGX_F64) or FP32C (lattice turns reduced in FP64, radial sums
+// interpolated from FP64 tables, Dirichlet kernels and derivative products in FP32); chi^2 and
+// gradient sums are FP64 and deterministic.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -71,6 +74,9 @@ struct CylCand {
   double K[2];       // weight * dn2
   double center[3];
   double ua[2], ub[2], uc;  // unscaled lattice vectors (in-plane a, b; c along z)
+  double ka[2], kb[2];      // a ua / 2pi, a ub / 2pi: lattice phases in turns
+  float ser[2][8];          // FP32C Dirichlet series of the a- and b-directions (cyl_dirichlet_series)
+  float fa, fua[2], fub[2], frep[2], fscale;  // FP32 copies for the FP32C pixel pass
   int nr, nh;
   int row0, col0, nrows, ncols;
   long px_off;       // offset of this candidate's pixels in counts / intensity
@@ -83,7 +89,8 @@ struct CylCand {
 };
 
 struct RowTab {
-  double2 Q, QH, Qa;
+  double q2, qh, qa;     // |K Q|^2, |K|^2 Re(conj(Q) dQ/dH), |K|^2 Re(conj(Q) dQ/da)
+  float q2f, qhf, qaf;   // the same rounded to FP32 (the FP32C derivative products)
 };
 
 // S_N(theta) = sin(N pi t)/sin(pi t), t = theta/2pi reduced, and dS/dtheta (FP64).
@@ -114,69 +121,172 @@ __device__ __forceinline__ void dirichlet(double theta, double N, double* S, dou
   *dS = (N * cn * s1 - sn * c1) / (2.0 * s1 * s1);
 }
 
-// ---------------------------------------------------------------- row table ----
-__global__ void cyl_rows_kernel(const CylCand* __restrict__ cands,
-                                const double2* __restrict__ rowqz,
-                                const double2* __restrict__ rowfc, RowTab* __restrict__ tab) {
-  const CylCand& c = cands[blockIdx.y];
-  int lr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (lr >= c.nrows) return;
-  int grow = c.row0 + lr;
-  zd Q(0, 0), QH(0, 0), Qa(0, 0);
-  for (int k = 0; k < 4; ++k) {
-    double qz = rowqz[4L * grow + k].x;
-    zd fc(rowfc[4L * grow + k]);
-    zd G(0, 0), GH(0, 0);
-    for (int j = 0; j < c.nh; ++j) {
-      double h = c.h[j];
-      double x = 0.5 * qz * h;  // sinc(qz h / 2) e^{i qz h / 2} h
-      double sx, cx;
-      sincos(x, &sx, &cx);
-      double sincv = fabs(x) > 1.0e-14 ? sx / x : 1.0 - x * x / 6.0 + x * x * x * x / 120.0;
-      G += zd(cx, sx) * (sincv * h);
-      double s2, c2;
-      sincos(2.0 * x, &s2, &c2);
-      GH += zd(c2, s2) * (h / c.H);
-    }
-    double Sc, dSc;
-    double thc = c.a * c.uc * qz;
-    dirichlet(thc, c.rep[2], &Sc, &dSc);
-    zd Zc = expi(c.center[2] * qz);
-    zd f = fc * Zc;
-    Q += f * (G * Sc);
-    QH += f * (GH * Sc);
-    Qa += f * (G * (dSc * thc / c.a));
+// Round to the nearest integer (ties to even) on the FP64 add pipe, for |x| < 2^51: adding
+// 1.5 * 2^52 leaves no fraction bits, subtracting it again returns the rounded value.
+constexpr double RND52 = 6755399441055744.0;
+__device__ __forceinline__ double round_fp64(double x) { return __dsub_rn(__dadd_rn(x, RND52), RND52); }
+
+// sin(pi x) and cos(pi x) for |x| <= 1 in FP32 on the FMA pipe: x = r + k/2 with k = rint(2x)
+// (rounded by the 1.5 * 2^23 constant, whose low mantissa bits then hold k mod 4) and
+// |r| <= 1/4 exact; Taylor polynomials of sin(pi r)/r (to r^8) and cos(pi r) (to r^10), whose
+// truncation is below 2e-9 at |pi r| = pi/4; then the rotation by k quarter turns.  Absolute
+// error about one FP32 ulp; sin keeps its relative accuracy near 0.
+__device__ __forceinline__ void sincospi_f32(float x, float* s, float* c) {
+  const float M = 12582912.0f;
+  const float b = __fadd_rn(2.0f * x, M);
+  const int q = __float_as_int(b) & 3;
+  const float r = x - 0.5f * __fsub_rn(b, M);
+  const float r2 = r * r;
+  const float ps = fmaf(fmaf(fmaf(fmaf(0.08214588463306427f, r2, -0.5992645025253296f), r2,
+                                  2.550163984298706f), r2, -5.167712688446045f), r2,
+                        3.1415927410125732f);
+  const float pc = fmaf(fmaf(fmaf(fmaf(fmaf(-0.025806890800595284f, r2, 0.23533062636852264f), r2,
+                                       -1.3352627754211426f), r2, 4.058712005615234f), r2,
+                             -4.934802055358887f), r2, 1.0f);
+  const float sv = r * ps;
+  float so = (q & 1) ? pc : sv, co = (q & 1) ? -sv : pc;
+  if (q & 2) {
+    so = -so;
+    co = -co;
   }
-  RowTab t;
-  t.Q = Q.d2();
-  t.QH = QH.d2();
-  t.Qa = Qa.d2();
-  tab[c.rowtab0 + lr] = t;
+  *s = so;
+  *c = co;
+}
+
+// The Dirichlet kernel in FP32 arithmetic at a turn t already reduced to [-1/2, 1/2] in FP64.
+// N t is reduced modulo 2 in FP64 too (sin and cos of pi N t keep their values), so both sines
+// keep FP32 accuracy for any N.  For |theta| N < 1 the closed form's derivative cancels; there
+// the series in y = (theta N)^2 with the candidate's scaled power sums: e[0..3] for S, e[4..7]
+// for dS.
+__device__ __forceinline__ void dirichlet_f32(double t, double N, float Nf, const float* e,
+                                              float* S, float* dS) {
+  if (N == 1.0) {
+    *S = 1.0f;
+    *dS = 0.0f;
+    return;
+  }
+  const float tf = (float)t;
+  const float thN = 6.28318530718f * tf * Nf;
+  if (fabsf(thN) < 1.0f) {
+    const float y = thN * thN;
+    *S = Nf * (1.0f - y * (e[0] - y * (e[1] - y * (e[2] - y * e[3]))));
+    *dS = -thN * Nf * Nf * (e[4] - y * (e[5] - y * (e[6] - y * e[7])));
+    return;
+  }
+  const double u = N * t;
+  float sn, cn, s1, c1;
+  sincospi_f32((float)(u - 2.0 * round_fp64(0.5 * u)), &sn, &cn);
+  sincospi_f32(tf, &s1, &c1);
+  const float inv = __frcp_rn(s1), Sv = sn * inv;
+  *S = Sv;
+  *dS = 0.5f * (Nf * cn - Sv * c1) * inv;
+}
+
+// ---------------------------------------------------------------- row table ----
+// One warp per (candidate, ROI row): lane 8 k + j takes DWBA block k and the height samples
+// j, j + 8, ...; xor shuffles close the height sums inside each group of 8 lanes and then the
+// block sums across the groups (a fixed tree, so every lane holds the same bits).  The row's
+// scalars of the intensity and its H- and a-derivatives: the centre phase has modulus 1 and
+// drops out of |A|^2.
+__device__ __forceinline__ void cyl_rows_body(const CylCand& c, int bx, const double2* __restrict__ rowqz,
+                                              const double2* __restrict__ rowfc, RowTab* __restrict__ tab) {
+  const int lr = (int)((bx * blockDim.x + threadIdx.x) >> 5);
+  if (lr >= c.nrows) return;  // whole warps
+  const int lane = threadIdx.x & 31, k = lane >> 3;
+  const int grow = c.row0 + lr;
+  const double qz = rowqz[4L * grow + k].x;
+  zd G(0, 0), GH(0, 0);
+  for (int j = lane & 7; j < c.nh; j += 8) {
+    double h = c.h[j];
+    double x = 0.5 * qz * h;  // sinc(qz h / 2) e^{i qz h / 2} h
+    double sx, cx;
+    sincos(x, &sx, &cx);
+    double sincv = fabs(x) > 1.0e-14 ? sx / x : 1.0 - x * x / 6.0 + x * x * x * x / 120.0;
+    G += zd(cx, sx) * (sincv * h);
+    double s2, c2;
+    sincos(2.0 * x, &s2, &c2);
+    GH += zd(c2, s2) * (h / c.H);
+  }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    G.x += __shfl_xor_sync(0xffffffffu, G.x, o);
+    G.y += __shfl_xor_sync(0xffffffffu, G.y, o);
+    GH.x += __shfl_xor_sync(0xffffffffu, GH.x, o);
+    GH.y += __shfl_xor_sync(0xffffffffu, GH.y, o);
+  }
+  double Sc, dSc;
+  const double thc = c.a * c.uc * qz;
+  dirichlet(thc, c.rep[2], &Sc, &dSc);
+  const zd f = zd(rowfc[4L * grow + k]) * expi(c.center[2] * qz);
+  zd Q = f * (G * Sc), QH = f * (GH * Sc), Qa = f * (G * (dSc * thc / c.a));
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1) {
+    Q.x += __shfl_xor_sync(0xffffffffu, Q.x, o);
+    Q.y += __shfl_xor_sync(0xffffffffu, Q.y, o);
+    QH.x += __shfl_xor_sync(0xffffffffu, QH.x, o);
+    QH.y += __shfl_xor_sync(0xffffffffu, QH.y, o);
+    Qa.x += __shfl_xor_sync(0xffffffffu, Qa.x, o);
+    Qa.y += __shfl_xor_sync(0xffffffffu, Qa.y, o);
+  }
+  if (lane == 0) {
+    const double K2 = c.K[0] * c.K[0] + c.K[1] * c.K[1];
+    RowTab t;
+    t.q2 = K2 * norm2(Q);
+    t.qh = K2 * (Q.x * QH.x + Q.y * QH.y);
+    t.qa = K2 * (Q.x * Qa.x + Q.y * Qa.y);
+    t.q2f = (float)t.q2;
+    t.qhf = (float)t.qh;
+    t.qaf = (float)t.qa;
+    tab[c.rowtab0 + lr] = t;
+  }
 }
 
 // --------------------------------------------------------- radial-sum tables ----
-// One node per thread: (fr, frR) at q = |j - 1| h, as the pixel pass would sum them, except
-// that the q_par -> 0 guard takes the smooth limit (J1(x)/x -> 1/2, J0 -> 1) so that the
-// interpolation near q = 0 is right; pixels that meet the guard sum directly.
-__global__ void cyl_table_kernel(const CylCand* __restrict__ cands, double h, double2* __restrict__ table) {
-  const CylCand& c = cands[blockIdx.y];
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= CYL_NTAB) return;
+// 8 lanes per node: lane l sums the radius samples l, l + 8, ..., xor shuffles close the sum
+// ((fr, frR) at q = |j - 1| h, as the pixel pass would sum them), except that the q_par -> 0
+// guard takes the smooth limit (J1(x)/x -> 1/2, J0 -> 1) so that the interpolation near q = 0
+// is right; pixels that meet the guard sum directly.  Each FP64 sum is stored as an FP32 pair
+// (hi, lo = sum - hi): the pixel pass interpolates both in FP32, so no rounding of a node,
+// common to every pixel near that q_par, reaches the intensity.
+__device__ __forceinline__ void cyl_table_body(const CylCand& c, int bx, double h, float4* __restrict__ table) {
+  const int j = (int)((bx * blockDim.x + threadIdx.x) >> 3), l = threadIdx.x & 7;
   const double qp = fabs((double)(j - 1) * h);
   double fr = 0.0, frR = 0.0;
-  for (int i = 0; i < c.nr; ++i) {
-    const double r = c.r[i];
-    const double x = qp * r;
-    const double two_pi_r = 2.0 * PI_D * r;
-    if (x * x > 1.0e-13) {
-      fr += two_pi_r * r * j1(x) / x;
-      frR += two_pi_r * r * j0(x);
-    } else {
-      fr += two_pi_r * r * 0.5;
-      frR += two_pi_r * r;
+  if (j < CYL_NTAB)  // lanes past the last node still join the shuffles
+    for (int i = l; i < c.nr; i += 8) {
+      const double r = c.r[i];
+      const double x = qp * r;
+      const double two_pi_r = 2.0 * PI_D * r;
+      if (x * x > 1.0e-13) {
+        fr += two_pi_r * r * j1(x) / x;
+        frR += two_pi_r * r * j0(x);
+      } else {
+        fr += two_pi_r * r * 0.5;
+        frR += two_pi_r * r;
+      }
     }
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    fr += __shfl_xor_sync(0xffffffffu, fr, o);
+    frR += __shfl_xor_sync(0xffffffffu, frR, o);
   }
-  table[(long)blockIdx.y * CYL_NTAB + j] = make_double2(fr, frR / c.R);
+  if (j < CYL_NTAB && l == 0) {
+    const double v = frR / c.R;
+    const float fh = (float)fr, vh = (float)v;
+    table[(long)blockIdx.y * CYL_NTAB + j] = make_float4(fh, (float)(fr - fh), vh, (float)(v - vh));
+  }
+}
+
+// The per-evaluation set-up in one launch: blocks [0, row_blocks) build the row table (a warp
+// per ROI row), the rest (FP32C only) the radial-sum tables; grid y = candidate.
+__global__ void cyl_prep_kernel(const CylCand* __restrict__ cands, int row_blocks,
+                                const double2* __restrict__ rowqz, const double2* __restrict__ rowfc,
+                                RowTab* __restrict__ tab, double h, float4* __restrict__ table) {
+  const CylCand& c = cands[blockIdx.y];
+  if ((int)blockIdx.x < row_blocks)
+    cyl_rows_body(c, blockIdx.x, rowqz, rowfc, tab);
+  else
+    cyl_table_body(c, blockIdx.x - row_blocks, h, table);
 }
 
 // --------------------------------------------------------------- pixel pass ----
@@ -192,21 +302,9 @@ struct CylArgs {
   const unsigned* mask;  // may be NULL
   double* intensity;     // may be NULL
   double* partial;       // 5 doubles per item (chi2, dR, dH, da, dphi)
-  const double2* table;  // FP32C: CYL_NTAB (fr, frR) per candidate
+  const float4* table;   // FP32C: CYL_NTAB (fr hi, lo, frR/R hi, lo) per candidate
   double inv_h;          // 1 / node spacing of the table
-};
-
-template <typename T>
-struct BesselT;
-template <>
-struct BesselT<float> {
-  static __device__ __forceinline__ float J0(float x) { return j0f(x); }
-  static __device__ __forceinline__ float J1(float x) { return j1f(x); }
-};
-template <>
-struct BesselT<double> {
-  static __device__ __forceinline__ double J0(double x) { return j0(x); }
-  static __device__ __forceinline__ double J1(double x) { return j1(x); }
+  const float* wf;       // FP32C: mask / max(counts, 1) per pixel (may be NULL: forward only)
 };
 
 template <int NT>
@@ -235,8 +333,14 @@ __device__ __forceinline__ double block_sum5(double* v, double* sh) {
   return v[0];
 }
 
+// Per pixel: I = q2 (Fr Sa Sb)^2 and its derivatives
+//   dI/dR = 2 q2 Fr dFr/dR (Sa Sb)^2,  dI/dH = 2 qh (Fr Sa Sb)^2,
+//   dI/da = 2 Fr^2 Sa Sb (q2 d(Sa Sb)/da + qa Sa Sb),  dI/dphi = 2 q2 Fr^2 Sa Sb d(Sa Sb)/dphi,
+// then the chi^2 terms w (s I - C)^2, w = mask / max(C, 1), and their derivatives.
+// The FP64 form: every Bessel function and Dirichlet kernel in FP64 per pixel, FP64 sums.
 template <typename T, int NT, int PPT>
 __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
+  static_assert(std::is_same<T, double>::value, "FP32C has its own kernel");
   __shared__ double sh[(NT / 32) * 5];
   for (long it = blockIdx.x; it < a.nitems; it += gridDim.x) {
     const int2 item = a.items[it];
@@ -249,80 +353,42 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
       if (idx >= npx) continue;
       int lr = (int)(idx / c.ncols), lc = (int)(idx - (long)lr * c.ncols);
       long p = (long)(c.row0 + lr) * a.grid_ncol + (c.col0 + lc);
-      double qx = a.qx[p], qy = a.qy[p];
-      double mx = c.cphi * qx - c.sphi * qy, my = c.sphi * qx + c.cphi * qy;
-      double qpar = sqrt(mx * mx + my * my);
-      // radial sums (precision T); FP32C interpolates the candidate's table except where a
-      // radius sample meets the reference's q_par -> 0 guard (then the terms are summed)
-      T fr = 0, frR = 0;
-      double frt = 0.0, frRt = 0.0;  // interpolated (FP64 tables)
-      bool direct = true;
-      if constexpr (std::is_same<T, float>::value) {
-        if (qpar * qpar * c.rmin * c.rmin > 1.0e-13) {
-          direct = false;
-          const double u = qpar * a.inv_h + 1.0;
-          const int i0 = min(max((int)u, 1), CYL_NTAB - 3);
-          const double t = u - i0;
-          const double2* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
-          const double w0 = -t * (t - 1.0) * (t - 2.0) * (1.0 / 6.0);
-          const double w1 = (t + 1.0) * (t - 1.0) * (t - 2.0) * 0.5;
-          const double w2 = -(t + 1.0) * t * (t - 2.0) * 0.5;
-          const double w3 = (t + 1.0) * t * (t - 1.0) * (1.0 / 6.0);
-          const double2 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
-          frt = w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x;
-          frRt = w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y;
-        }
-      }
-      if (direct) {
-        const T qp = (T)qpar;
-        for (int i = 0; i < c.nr; ++i) {
-          T r = (T)c.r[i];
-          T x = qp * r;
-          if ((double)x * (double)x > 1.0e-13) {
-            T two_pi_r = (T)(2.0 * PI_D) * r;
-            fr += two_pi_r * r * BesselT<T>::J1(x) / x;
-            frR += two_pi_r * r * BesselT<T>::J0(x);
-          }
-        }
-        frR /= (T)c.R;
-      }
-      const double FR = direct ? (double)fr : frt, FRR = direct ? (double)frR : frRt;
-      // lattice factors in FP64
-      double tha = c.a * (c.ua[0] * mx + c.ua[1] * my);
-      double thb = c.a * (c.ub[0] * mx + c.ub[1] * my);
+      const double qx = a.qx[p], qy = a.qy[p];
+      const double mx = c.cphi * qx - c.sphi * qy, my = c.sphi * qx + c.cphi * qy;
+      const double qpar = sqrt(mx * mx + my * my);
       double Sa, dSa, Sb, dSb;
-      dirichlet(tha, c.rep[0], &Sa, &dSa);
-      dirichlet(thb, c.rep[1], &Sb, &dSb);
-      double dtha_dphi = c.a * (c.ua[0] * (-my) + c.ua[1] * mx);
-      double dthb_dphi = c.a * (c.ub[0] * (-my) + c.ub[1] * mx);
-      double ph = c.center[0] * mx + c.center[1] * my;
-      double dph = c.center[0] * (-my) + c.center[1] * mx;
-      zd Pc = expi(ph);
-      const RowTab rt = a.tab[c.rowtab0 + lr];
-      // amplitude and its derivatives (FP64 combination of T radial sums)
-      zd KQ = zd(c.K[0], c.K[1]) * zd(rt.Q);
-      double SS = Sa * Sb;
-      zd base = KQ * Pc;  // K Q Pc
-      zd A = base * (FR * SS);
-      zd dA_R = base * (FRR * SS);
-      zd dA_H = (zd(c.K[0], c.K[1]) * zd(rt.QH)) * Pc * (FR * SS);
-      zd dA_a = Pc * zd(c.K[0], c.K[1]) * FR *
-                (zd(rt.Q) * ((dSa * tha / c.a) * Sb + Sa * (dSb * thb / c.a)) + zd(rt.Qa) * SS);
-      zd dA_p = KQ * FR *
-                (Pc * (dSa * dtha_dphi * Sb + Sa * dSb * dthb_dphi) + Pc * zd(0, dph) * SS);
-      double I = A.x * A.x + A.y * A.y;
+      dirichlet(c.a * (c.ua[0] * mx + c.ua[1] * my), c.rep[0], &Sa, &dSa);
+      dirichlet(c.a * (c.ub[0] * mx + c.ub[1] * my), c.rep[1], &Sb, &dSb);
+      double FR = 0.0, FRR = 0.0;
+      for (int i = 0; i < c.nr; ++i) {
+        const double r = c.r[i], x = qpar * r;
+        if (x * x > 1.0e-13) {
+          const double two_pi_r = 2.0 * PI_D * r;
+          FR += two_pi_r * r * j1(x) / x;
+          FRR += two_pi_r * r * j0(x);
+        }
+      }
+      FRR /= c.R;
+      const RowTab& rt = a.tab[c.rowtab0 + lr];
+      const double SS = Sa * Sb, F = FR * SS;
+      const double I = rt.q2 * (F * F);
       if (a.intensity) a.intensity[c.px_off + idx] = I;
       if (a.counts) {
-        double C = a.counts[c.px_off + idx];
-        double m = a.mask ? (double)a.mask[c.px_off + idx] : 1.0;
-        double w = m / (C > 1.0 ? C : 1.0);
-        double res = c.scale * I - C;
-        double g = 2.0 * w * res * c.scale;
+        const double pa = c.ua[0] * mx + c.ua[1] * my, pb = c.ub[0] * mx + c.ub[1] * my;
+        const double ra = c.ua[1] * mx - c.ua[0] * my, rb = c.ub[1] * mx - c.ub[0] * my;
+        const double dSSa = dSa * pa * Sb + Sa * dSb * pb;
+        const double dSSp = c.a * (dSa * ra * Sb + Sa * dSb * rb);
+        const double FRF = FR * F;
+        const double C = a.counts[c.px_off + idx];
+        const double mk = a.mask ? (double)a.mask[c.px_off + idx] : 1.0;
+        const double w = mk / (C > 1.0 ? C : 1.0);
+        const double res = c.scale * I - C;
+        const double g = 2.0 * w * res * c.scale;
         acc[0] += w * res * res;
-        acc[1] += g * 2.0 * (A.x * dA_R.x + A.y * dA_R.y);
-        acc[2] += g * 2.0 * (A.x * dA_H.x + A.y * dA_H.y);
-        acc[3] += g * 2.0 * (A.x * dA_a.x + A.y * dA_a.y);
-        acc[4] += g * 2.0 * (A.x * dA_p.x + A.y * dA_p.y);
+        acc[1] += g * (2.0 * rt.q2 * F * FRR * SS);
+        acc[2] += g * (2.0 * rt.qh * F * F);
+        acc[3] += g * (2.0 * FRF * (rt.q2 * dSSa + rt.qa * SS));
+        acc[4] += g * (2.0 * rt.q2 * FRF * dSSp);
       }
     }
     if (a.counts) {
@@ -331,6 +397,120 @@ __global__ void __launch_bounds__(NT) cyl_pixels_kernel(CylArgs a) {
 #pragma unroll
         for (int q = 0; q < 5; ++q) a.partial[5 * it + q] = acc[q];
     }
+  }
+}
+
+// The FP32C form.  FP64: the rotated q (mx, my), q_par and the table coordinate, the lattice
+// turns and N t (reduced with round_fp64), the residual s I - C and the sums over threads and
+// items.  FP32: the radial sums interpolated from the (hi, lo) tables, the Dirichlet kernels
+// (own sincospi on the FMA pipe) and all derivative products, and each thread's sums over its
+// PPT pixels.  The row scalar q2 multiplies (Fr Sa Sb)^2 in FP64, so no rounding common to
+// many pixels (a row or candidate constant) reaches I: the chi^2 gradient sums residuals of
+// both signs over the detector, and such an error would add up where the residuals cancel.
+// Row and column advance by integer steps (no division per pixel); weights w come from a
+// per-pixel FP32 array made once when the batch is created.
+template <int NT, int PPT>
+__global__ void __launch_bounds__(NT) cyl_pixels_f32c_kernel(CylArgs a) {
+  __shared__ double sh[(NT / 32) * 5];
+  for (long it = blockIdx.x; it < a.nitems; it += gridDim.x) {
+    const int2 item = a.items[it];
+    const CylCand& c = a.cands[item.x];
+    const int ncols = c.ncols;
+    const long npx = (long)c.nrows * ncols;
+    const int first = item.y + threadIdx.x;
+    int lr = first / ncols, lc = first - lr * ncols;
+    const int dq = NT / ncols, dr = NT - dq * ncols;
+    float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < PPT; ++j) {
+      if (j > 0) {
+        lr += dq;
+        lc += dr;
+        if (lc >= ncols) {
+          lc -= ncols;
+          ++lr;
+        }
+      }
+      const long idx = (long)first + (long)j * NT;
+      if (idx >= npx) continue;
+      const long p = (long)(c.row0 + lr) * a.grid_ncol + (c.col0 + lc);
+      const double qx = a.qx[p], qy = a.qy[p];
+      const double mx = c.cphi * qx - c.sphi * qy, my = c.sphi * qx + c.cphi * qy;
+      const double q2d = mx * mx + my * my;
+      float FR = 0.f, FRR = 0.f;
+      if (q2d * c.rmin * c.rmin > 1.0e-13) {
+        // node below u = q_par / h + 1 by the FP64 rounding constant (its low word is the index)
+        const double u = sqrt(q2d) * a.inv_h + 1.0;
+        const double rb = __dadd_rn(__dadd_rn(u, -0.5), RND52);
+        const int k = __double2loint(rb), i0 = min(max(k, 1), CYL_NTAB - 3);
+        float t = (float)(u - __dsub_rn(rb, RND52));
+        if (i0 != k) t += (float)(k - i0);
+        const float w0 = -t * (t - 1.0f) * (t - 2.0f) * (1.0f / 6.0f);
+        const float w1 = (t + 1.0f) * (t - 1.0f) * (t - 2.0f) * 0.5f;
+        const float w2 = -(t + 1.0f) * t * (t - 2.0f) * 0.5f;
+        const float w3 = (t + 1.0f) * t * (t - 1.0f) * (1.0f / 6.0f);
+        const float4* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
+        const float4 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
+        FR = (w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x) + (w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y);
+        FRR = (w0 * f0.z + w1 * f1.z + w2 * f2.z + w3 * f3.z) + (w0 * f0.w + w1 * f1.w + w2 * f2.w + w3 * f3.w);
+      } else {  // the reference's q_par -> 0 guard: sum the terms that pass it
+        const float qp = (float)sqrt(q2d);
+        for (int i = 0; i < c.nr; ++i) {
+          const float r = (float)c.r[i], x = qp * r;
+          if ((double)x * (double)x > 1.0e-13) {
+            const float two_pi_r = (float)(2.0 * PI_D) * r;
+            FR += two_pi_r * r * j1f(x) / x;
+            FRR += two_pi_r * r * j0f(x);
+          }
+        }
+        FRR /= (float)c.R;
+      }
+      double ta = c.ka[0] * mx + c.ka[1] * my, tb = c.kb[0] * mx + c.kb[1] * my;
+      ta -= round_fp64(ta);
+      tb -= round_fp64(tb);
+      float Sa, dSa, Sb, dSb;
+      dirichlet_f32(ta, c.rep[0], c.frep[0], c.ser[0], &Sa, &dSa);
+      dirichlet_f32(tb, c.rep[1], c.frep[1], c.ser[1], &Sb, &dSb);
+      const RowTab& rt = a.tab[c.rowtab0 + lr];
+      const float SS = Sa * Sb, F = FR * SS;
+      const double I = rt.q2 * (double)(F * F);
+      if (a.intensity) a.intensity[c.px_off + idx] = I;
+      if (a.counts) {
+        const float X = (float)mx, Y = (float)my;
+        const float pa = c.fua[0] * X + c.fua[1] * Y, pb = c.fub[0] * X + c.fub[1] * Y;
+        const float ra = c.fua[1] * X - c.fua[0] * Y, rb = c.fub[1] * X - c.fub[0] * Y;
+        const float dSSa = dSa * pa * Sb + Sa * dSb * pb;
+        const float dSSp = c.fa * (dSa * ra * Sb + Sa * dSb * rb);
+        const float FRF = FR * F;
+        const float w = a.wf[c.px_off + idx];
+        const float res = (float)(c.scale * I - a.counts[c.px_off + idx]);
+        const float g = 2.0f * w * res * c.fscale;
+        acc[0] += w * res * res;
+        acc[1] += g * (2.0f * rt.q2f * F * FRR * SS);
+        acc[2] += g * (2.0f * rt.qhf * F * F);
+        acc[3] += g * (2.0f * FRF * (rt.q2f * dSSa + rt.qaf * SS));
+        acc[4] += g * (2.0f * rt.q2f * FRF * dSSp);
+      }
+    }
+    if (a.counts) {
+      double accd[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) accd[q] = (double)acc[q];
+      block_sum5<NT>(accd, sh);
+      if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) a.partial[5 * it + q] = accd[q];
+    }
+  }
+}
+
+// FP32C: the per-pixel weights mask / max(C, 1) as FP32, once per batch.
+__global__ void cyl_weights_kernel(const double* __restrict__ counts, const unsigned* __restrict__ mask,
+                                   long n, float* __restrict__ wf) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double C = counts[i];
+    const double m = mask ? (double)mask[i] : 1.0;
+    wf[i] = (float)(m / (C > 1.0 ? C : 1.0));
   }
 }
 
@@ -359,9 +539,15 @@ static cudaError_t cyl_pixels_at(int shape, unsigned blocks, const CylArgs& a, c
     if (shape == I) {
       constexpr int NT = CYL_SHAPES[I].threads, PPT = CYL_SHAPES[I].ppt;
       static_assert(NT % 32 == 0 && NT <= 1024 && NT * PPT >= CYL_MIN_TILE, "bad tile shape");
-      if (occ)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, cyl_pixels_kernel<T, NT, PPT>, NT, 0);
-      cyl_pixels_kernel<T, NT, PPT><<<blocks, NT, 0, st>>>(a);
+      if constexpr (std::is_same<T, float>::value) {
+        if (occ)
+          return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, cyl_pixels_f32c_kernel<NT, PPT>, NT, 0);
+        cyl_pixels_f32c_kernel<NT, PPT><<<blocks, NT, 0, st>>>(a);
+      } else {
+        if (occ)
+          return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, cyl_pixels_kernel<T, NT, PPT>, NT, 0);
+        cyl_pixels_kernel<T, NT, PPT><<<blocks, NT, 0, st>>>(a);
+      }
       return cudaGetLastError();
     }
     return cyl_pixels_at<T, I + 1>(shape, blocks, a, st, occ);
@@ -432,6 +618,27 @@ __global__ void __launch_bounds__(128) cyl_plain_kernel(const CylCand* __restric
 }
 
 // ------------------------------------------------------------------- host ----
+// Scaled power sums of the FP32C Dirichlet series (dirichlet_f32): with c_j = j - (N-1)/2,
+// s_2k = sum_j c_j^2k (polynomials in N, exact for integer N: N(N^2-1)/12,
+// N(N^2-1)(3N^2-7)/240, N(N^2-1)(3N^4-18N^2+31)/1344, N(N^2-1)(5N^6-55N^4+239N^2-381)/11520),
+//   S  = N (1 - y e0 + y^2 e1 - y^3 e2 + y^4 e3),          e_k = s_2k+2 / ((2k+2)! N^(2k+3)),
+//   dS = -theta N^3 (e4 - y e5 + y^2 e6 - y^3 e7),       e_4+k = s_2k+2 / ((2k+1)! N^(2k+3)),
+// y = (theta N)^2 < 1; the first omitted term is below 3e-10 of N.
+void cyl_dirichlet_series(double N, float* e) {
+  for (int i = 0; i < 8; ++i) e[i] = 0.0f;
+  if (N == 1.0) return;
+  const double n2 = N * N, base = N * (n2 - 1.0);
+  const double s[4] = {base / 12.0, base * (3.0 * n2 - 7.0) / 240.0,
+                       base * (3.0 * n2 * n2 - 18.0 * n2 + 31.0) / 1344.0,
+                       base * (5.0 * n2 * n2 * n2 - 55.0 * n2 * n2 + 239.0 * n2 - 381.0) / 11520.0};
+  const double fs[4] = {2.0, 24.0, 720.0, 40320.0}, fd[4] = {1.0, 6.0, 120.0, 5040.0};
+  double np = N * n2;  // N^(2k+3)
+  for (int k = 0; k < 4; ++k, np *= n2) {
+    e[k] = (float)(s[k] / (fs[k] * np));
+    e[4 + k] = (float)(s[k] / (fd[k] * np));
+  }
+}
+
 int cyl_fill_cand(const double* m, const double* abc9, const int* roi, double scale, CylCand& c) {
   c = CylCand();
   c.R = m[M_R];
@@ -455,6 +662,15 @@ int cyl_fill_cand(const double* m, const double* abc9, const int* roi, double sc
   c.ub[0] = abc9[3];
   c.ub[1] = abc9[4];
   c.uc = abc9[8];
+  c.fa = (float)c.a;
+  for (int i = 0; i < 2; ++i) {
+    c.ka[i] = c.a * c.ua[i] / (2.0 * PI_D);
+    c.kb[i] = c.a * c.ub[i] / (2.0 * PI_D);
+    c.fua[i] = (float)c.ua[i];
+    c.fub[i] = (float)c.ub[i];
+    c.frep[i] = (float)c.rep[i];
+    cyl_dirichlet_series(c.rep[i], c.ser[i]);
+  }
   // size distributions: Gaussian over +-3 sigma sampled as param_distribution does
   double s = m[M_SPREAD];
   int n = (int)m[M_NSAMP];
@@ -486,6 +702,7 @@ int cyl_fill_cand(const double* m, const double* abc9, const int* roi, double sc
   c.nrows = roi[2];
   c.ncols = roi[3];
   c.scale = scale;
+  c.fscale = (float)scale;
   return HGX_OK;
 }
 
@@ -510,6 +727,7 @@ struct hgx_cyl_batch_s {
   int persistent_blocks = 0;
   int shape = 0;  // tile shape of the pixel pass (index into the shape table)
   hgx::DevBuf d_table;  // FP32C radial-sum tables
+  hgx::DevBuf d_wf;     // FP32C per-pixel weights mask / max(counts, 1)
   hgx::DevBuf d_plain;  // the candidate record of hgx_cyl_plain_forward
   double table_h = 1.0;  // their node spacing
 };
@@ -522,9 +740,13 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
                            cudaMemcpyHostToDevice, st));
   int maxrows = 0;
   for (int i = 0; i < b->ncand; ++i) maxrows = std::max(maxrows, b->rois[4 * i + 2]);
-  dim3 rg((maxrows + 127) / 128, b->ncand);
-  cyl_rows_kernel<<<rg, 128, 0, st>>>((const CylCand*)b->d_cands.p, b->grid->rowqz,
-                                      (const double2*)b->d_rowfc.p, (RowTab*)b->d_tab.p);
+  // row table (a warp per row, 4 rows per block) and, in FP32C, the radial-sum tables (16
+  // nodes per block) in one launch
+  const int row_blocks = (maxrows + 3) / 4;
+  const int table_blocks = b->precision == HGX_F32C ? (8 * CYL_NTAB + 127) / 128 : 0;
+  cyl_prep_kernel<<<dim3(row_blocks + table_blocks, b->ncand), 128, 0, st>>>(
+      (const CylCand*)b->d_cands.p, row_blocks, b->grid->rowqz, (const double2*)b->d_rowfc.p,
+      (RowTab*)b->d_tab.p, b->table_h, (float4*)b->d_table.p);
   CylArgs a;
   a.cands = (const CylCand*)b->d_cands.p;
   a.items = (const int2*)b->d_items.p;
@@ -537,11 +759,9 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
   a.mask = with_counts ? (const unsigned*)b->d_mask.p : nullptr;
   a.intensity = with_intensity ? (double*)b->d_inten.p : nullptr;
   a.partial = (double*)b->d_partial.p;
-  a.table = (const double2*)b->d_table.p;
+  a.table = (const float4*)b->d_table.p;
   a.inv_h = 1.0 / b->table_h;
-  if (b->precision == HGX_F32C)
-    cyl_table_kernel<<<dim3((CYL_NTAB + 127) / 128, b->ncand), 128, 0, st>>>(
-        (const CylCand*)b->d_cands.p, b->table_h, (double2*)b->d_table.p);
+  a.wf = with_counts ? (const float*)b->d_wf.p : nullptr;
   long blocks = std::min<long>(b->nitems, (long)b->persistent_blocks);
   cudaError_t e = b->precision == HGX_F64
                       ? cyl_pixels_at<double, 0>(b->shape, (unsigned)blocks, a, st, nullptr)
@@ -696,7 +916,15 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
     double qm = 0.0;
     for (int i = 0; i < g->nqy; ++i) qm = std::max(qm, sqrt(hx[i] * hx[i] + hy[i] * hy[i]));
     b->table_h = (qm > 0.0 ? qm : 1.0) * (1.0 + 1e-9) / CYL_QT;
-    if ((s = b->d_table.reserve(sizeof(double2) * CYL_NTAB * (size_t)ncand))) return bail(s);
+    if ((s = b->d_table.reserve(sizeof(float4) * CYL_NTAB * (size_t)ncand))) return bail(s);
+    if (counts) {
+      if ((s = b->d_wf.reserve(sizeof(float) * px))) return bail(s);
+      cyl_weights_kernel<<<(unsigned)std::min<long>((px + 255) / 256, 4L * c->sm_count * 8), 256, 0, st>>>(
+          (const double*)b->d_counts.p, (const unsigned*)b->d_mask.p, px, (float*)b->d_wf.p);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return bail(cuda_fail(e, "hgx_cyl_batch_create: weights"));
+    }
   }
   if ((s = cyl_apply_shape(b, 0))) return bail(s);
   *out = b;
