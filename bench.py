@@ -58,6 +58,17 @@ CUB_LAUNCHES_PER_STEP = 6
 #   ff_exact_kernel          611 FP64 per (q-point, triangle)
 #   grain_dwba_kernel        6418 FP64 per (pixel, grain), hcp cylinders (HIG_ENSEMBLE)
 #   grain_dwba_f32c_kernel   1226 FP32 + 367 FP64 per (pixel, grain), the same description
+#   cyl_pixels_f32c_kernel   221 FP32 + 60 FP64 per ROI pixel (the 256-candidate batch)
+#   cyl_pixels_kernel<double>  1418 FP64 per ROI pixel (the same batch)
+#   grain_dwba_f32c_kernel   4033 FP32 + 639 FP64 and 743 XU-pipe operations per pixel (config 1)
+#   grain_dwba_kernel        20170 FP64 per pixel (config 1)
+CYL_F32C_FP32_FLOP_PER_PIXEL = 221.0
+CYL_F32C_FP64_FLOP_PER_PIXEL = 60.0
+CYL_F64_FLOP_PER_PIXEL = 1418.0
+CFG1_F32C_FP32_FLOP_PER_PIXEL = 4033.0
+CFG1_F32C_FP64_FLOP_PER_PIXEL = 639.0
+CFG1_F32C_XU_PER_PIXEL = 743.0
+CFG1_F64_FLOP_PER_PIXEL = 20170.0
 MESH_FWD_FLOP_PER_PIXEL_TRI = FLOP_PER_PIXEL_TRI
 MESH_BWD_FLOP_PER_PIXEL_TRI = 80.0
 EXACT_FP64_FLOP_PER_EVAL = 611.0
@@ -300,7 +311,8 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
                           "method": "plain FP64 forward x 9 (central differences, h 1e-4 rel)"},
         "speedup_vs_plain_fp64": dtfd / dt32,
         "fp64_adjoint": {"value": 1.0 / dt64, "ms_per_eval": 1e3 * dt64,
-                         "method": "the same fused forward + adjoint with FP64 per-pixel sums"},
+                         "method": "the same fused forward + adjoint in FP64: every Bessel function "
+                                   "and Dirichlet kernel per pixel (no radial tables)"},
         "speedup_vs_fp64_adjoint": dt64 / dt32,
         "rel_err_chi2_vs_fp64": abs(c32[0] - c64[0]) / abs(c64[0]),
         "rel_err_grad_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
@@ -369,7 +381,8 @@ def fitting_bench(ctx, torch, dev, stream, steps=5):
                                      "sample": f"{sub} candidates timed, scaled by pixels"},
         "speedup_vs_sequential_plain": dts / dtb,
         "fp64_adjoint": {"value": nc / dtb64, "ms_per_batch": 1e3 * dtb64,
-                         "method": "the same graph-captured batch with FP64 per-pixel sums"},
+                         "method": "the same graph-captured batch in FP64: every Bessel function and "
+                                            "Dirichlet kernel per pixel (no radial tables)"},
         "speedup_vs_fp64_adjoint": dtb64 / dtb,
         "max_rel_err_chi2_vs_fp64": rel_c, "max_rel_err_grad_vs_fp64": rel_g}
     bb32.close()
@@ -819,6 +832,14 @@ def main():
     fit = None
     if not args.no_fitting:
         fit = fitting_bench(ctx, torch, dev, stream)
+        bt = fit["batch_256_rois"]
+        bt["roofline"] = roofline_of(
+            "fp32", CYL_F32C_FP32_FLOP_PER_PIXEL, float(bt["pixels"]), bt["ms_per_batch"] * 1e-3, peak_fp32,
+            "ROI pixel", "ncu executed FP32 FLOP of cyl_pixels_f32c_kernel (plus 60 FP64 per pixel); issue-"
+            "bound with no pipe above 31% in ncu; the time is the whole graph (set-up, pixel pass, sums)")
+        bt["fp64_adjoint"]["roofline"] = roofline_of(
+            "fp64", CYL_F64_FLOP_PER_PIXEL, float(bt["pixels"]), bt["fp64_adjoint"]["ms_per_batch"] * 1e-3,
+            peak_fp64, "ROI pixel", "ncu executed FP64 FLOP of cyl_pixels_kernel<double>")
         fit["mesh_vertices_2048sq"] = mesh_grad_bench(ctx, grid)
         mv = fit["mesh_vertices_2048sq"]
         mv["roofline"] = roofline_of(
@@ -849,6 +870,19 @@ def main():
     cfg1 = None
     if not args.no_config1 and rank == 0 and world == 1:
         cfg1 = config1_bench(ctx, cpu=not args.no_cpu_baseline)
+        npx1 = float(cfg1["pixels"])
+        t32, t64 = cfg1["f32c"]["ms"] * 1e-3, cfg1["f64"]["ms"] * 1e-3
+        r32 = roofline_of("fp32", CFG1_F32C_FP32_FLOP_PER_PIXEL, npx1, t32, peak_fp32, "pixel",
+                          "ncu executed FP32 FLOP of grain_dwba_f32c_kernel (plus 639 FP64 per pixel); "
+                          "the time is the whole simulation (set-up, Fresnel coefficients, grain kernel, sums)")
+        xu = CFG1_F32C_XU_PER_PIXEL * npx1 / t32 / 1e9
+        r32["sfu"] = {"ops_per_unit": CFG1_F32C_XU_PER_PIXEL, "achieved_gops": xu, "peak_gops": peak_sfu,
+                      "frac": xu / peak_sfu, "note": "XU-pipe thread operations (transcendentals and "
+                      "conversions); the busiest pipe of the grain kernel (61% in ncu)"}
+        cfg1["f32c"]["roofline"] = r32
+        cfg1["f64"]["roofline"] = roofline_of("fp64", CFG1_F64_FLOP_PER_PIXEL, npx1, t64, peak_fp64, "pixel",
+                                              "ncu executed FP64 FLOP of grain_dwba_kernel; the time is "
+                                              "the whole simulation")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

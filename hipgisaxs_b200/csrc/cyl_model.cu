@@ -434,7 +434,14 @@ __global__ void __launch_bounds__(NT) cyl_pixels_f32c_kernel(CylArgs a) {
       const long idx = (long)first + (long)j * NT;
       if (idx >= npx) continue;
       const long p = (long)(c.row0 + lr) * a.grid_ncol + (c.col0 + lc);
-      const double qx = a.qx[p], qy = a.qy[p];
+      const double qx = __ldg(a.qx + p), qy = __ldg(a.qy + p);
+      // the pixel's counts and weight issued early (read-only loads, independent of the math)
+      double C = 0.0;
+      float w = 0.0f;
+      if (a.counts) {
+        C = __ldg(a.counts + c.px_off + idx);
+        w = __ldg(a.wf + c.px_off + idx);
+      }
       const double mx = c.cphi * qx - c.sphi * qy, my = c.sphi * qx + c.cphi * qy;
       const double q2d = mx * mx + my * my;
       float FR = 0.f, FRR = 0.f;
@@ -450,7 +457,7 @@ __global__ void __launch_bounds__(NT) cyl_pixels_f32c_kernel(CylArgs a) {
         const float w2 = -(t + 1.0f) * t * (t - 2.0f) * 0.5f;
         const float w3 = (t + 1.0f) * t * (t - 1.0f) * (1.0f / 6.0f);
         const float4* tb = a.table + (long)item.x * CYL_NTAB + (i0 - 1);
-        const float4 f0 = tb[0], f1 = tb[1], f2 = tb[2], f3 = tb[3];
+        const float4 f0 = __ldg(tb), f1 = __ldg(tb + 1), f2 = __ldg(tb + 2), f3 = __ldg(tb + 3);
         FR = (w0 * f0.x + w1 * f1.x + w2 * f2.x + w3 * f3.x) + (w0 * f0.y + w1 * f1.y + w2 * f2.y + w3 * f3.y);
         FRR = (w0 * f0.z + w1 * f1.z + w2 * f2.z + w3 * f3.z) + (w0 * f0.w + w1 * f1.w + w2 * f2.w + w3 * f3.w);
       } else {  // the reference's q_par -> 0 guard: sum the terms that pass it
@@ -471,9 +478,9 @@ __global__ void __launch_bounds__(NT) cyl_pixels_f32c_kernel(CylArgs a) {
       float Sa, dSa, Sb, dSb;
       dirichlet_f32(ta, c.rep[0], c.frep[0], c.ser[0], &Sa, &dSa);
       dirichlet_f32(tb, c.rep[1], c.frep[1], c.ser[1], &Sb, &dSb);
-      const RowTab& rt = a.tab[c.rowtab0 + lr];
+      const RowTab* rt = a.tab + c.rowtab0 + lr;
       const float SS = Sa * Sb, F = FR * SS;
-      const double I = rt.q2 * (double)(F * F);
+      const double I = __ldg(&rt->q2) * (double)(F * F);
       if (a.intensity) a.intensity[c.px_off + idx] = I;
       if (a.counts) {
         const float X = (float)mx, Y = (float)my;
@@ -482,14 +489,14 @@ __global__ void __launch_bounds__(NT) cyl_pixels_f32c_kernel(CylArgs a) {
         const float dSSa = dSa * pa * Sb + Sa * dSb * pb;
         const float dSSp = c.fa * (dSa * ra * Sb + Sa * dSb * rb);
         const float FRF = FR * F;
-        const float w = a.wf[c.px_off + idx];
-        const float res = (float)(c.scale * I - a.counts[c.px_off + idx]);
+        const float q2f = __ldg(&rt->q2f), qhf = __ldg(&rt->qhf), qaf = __ldg(&rt->qaf);
+        const float res = (float)(c.scale * I - C);
         const float g = 2.0f * w * res * c.fscale;
         acc[0] += w * res * res;
-        acc[1] += g * (2.0f * rt.q2f * F * FRR * SS);
-        acc[2] += g * (2.0f * rt.qhf * F * F);
-        acc[3] += g * (2.0f * FRF * (rt.q2f * dSSa + rt.qaf * SS));
-        acc[4] += g * (2.0f * rt.q2f * FRF * dSSp);
+        acc[1] += g * (2.0f * q2f * F * FRR * SS);
+        acc[2] += g * (2.0f * qhf * F * F);
+        acc[3] += g * (2.0f * FRF * (q2f * dSSa + qaf * SS));
+        acc[4] += g * (2.0f * q2f * FRF * dSSp);
       }
     }
     if (a.counts) {
