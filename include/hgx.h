@@ -308,9 +308,11 @@ int hgx_save_gisaxs(hgx_ctx ctx, const double* image, int nrow, int ncol, const 
  * abc9: unscaled lattice vectors with a, b in the plane and c along z (hex, cubic).
  * rois: 4 ints per candidate (row0, col0, nrows, ncols); counts: the candidates' ROI images
  * concatenated (row-major), or NULL for forward-only batches; mask: same layout or NULL;
- * scale: the model-to-counts factor of the chi^2.  precision: HGX_F32C (the radial Bessel
- * sums interpolated from per-candidate FP64 tables over q_par, FP64 lattice phases and
- * reductions) or HGX_F64 (every Bessel function evaluated per pixel). */
+ * scale: the model-to-counts factor of the chi^2.  precision: HGX_F32C (per-pixel arithmetic
+ * in FP32: the radial sums interpolated from per-candidate tables over q_par, the lattice
+ * factors from FP64-reduced turns; FP64 q, residuals and reductions; about 1e-7 of the FP64
+ * chi^2, 1e-6 of its gradient) or HGX_F64 (every Bessel function and lattice factor evaluated
+ * per pixel in FP64).  An FP32C batch with counts keeps one FP32 weight per ROI pixel. */
 typedef struct hgx_cyl_batch_s* hgx_cyl_batch;
 int hgx_cyl_batch_create(hgx_ctx ctx, hgx_qgrid g, const double* rowfc, const double* abc9,
                          int ncand, const int* rois, const double* counts,
