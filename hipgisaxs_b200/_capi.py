@@ -112,6 +112,9 @@ SIGNATURES = {
     "hgx_read_mask": (_i, [C.c_char_p, _vp, C.c_long, C.POINTER(C.c_long)]),
     "hgx_hig_objective": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, C.POINTER(C.c_long)]),
     "hgx_hig_objective_grad": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _d, _vp, _vp]),
+    "hgx_hig_population_create": (_i, [_vp, _vp, _i, _vp, _vp, _i, _d, _i, C.POINTER(_vp)]),
+    "hgx_hig_population_eval": (_i, [_vp, _vp, _i, _vp]),
+    "hgx_hig_population_destroy": (_i, [_vp]),
     "hgx_measure_peaks": (_i, [_vp, _i, C.POINTER(_d), C.POINTER(_d)]),
     "hgx_measure_peak_fp64": (_i, [_vp, C.POINTER(_d)]),
 }

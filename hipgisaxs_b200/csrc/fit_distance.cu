@@ -152,6 +152,79 @@ __global__ void __launch_bounds__(FD_THREADS) fit_terms_kernel(int metric, long 
   }
 }
 
+// A population of images (candidate = blockIdx.y, images npop x n): the same passes as one
+// distance, each candidate's partial sums in its own slice, the norms formed on the device
+// from the pass-1 sums exactly as the host forms them for one distance.
+__global__ void __launch_bounds__(FD_THREADS) fit_norms_pop_kernel(int metric, long n, const double* __restrict__ ref,
+                                                                   const double* __restrict__ imgs,
+                                                                   const unsigned* __restrict__ mask,
+                                                                   double* __restrict__ part) {
+  const double* dat = imgs + (long)blockIdx.y * n;
+  double* pp = part + (long)blockIdx.y * 3 * FD_BLOCKS;
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (long i = (long)blockIdx.x * FD_THREADS + threadIdx.x; i < n; i += (long)FD_BLOCKS * FD_THREADS) {
+    const double m = mask ? (double)mask[i] : 1.0;
+    const double tr = transform(metric, ref[i]), td = transform(metric, dat[i]);
+    if (is_l1(metric)) {
+      a += m * fabs(tr);
+      b += m * fabs(td);
+    } else {
+      const double rr = tr * tr, dd = td * td, rd = fabs(td * tr);
+      a += m * (isnan(rr) ? 0 : rr);
+      b += m * (isnan(dd) ? 0 : dd);
+      c += m * (isnan(rd) ? 0 : rd);
+    }
+  }
+  a = block_sum(a);
+  b = block_sum(b);
+  c = block_sum(c);
+  if (threadIdx.x == 0) {
+    pp[3 * blockIdx.x] = a;
+    pp[3 * blockIdx.x + 1] = b;
+    pp[3 * blockIdx.x + 2] = c;
+  }
+}
+
+// one block per candidate: the three pass-1 sums (each in the order of fit_sums_kernel)
+__global__ void __launch_bounds__(FD_THREADS) fit_sums3_pop_kernel(const double* __restrict__ part,
+                                                                   double* __restrict__ sums) {
+  const double* pp = part + (long)blockIdx.x * 3 * FD_BLOCKS;
+  for (int k = 0; k < 3; ++k) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < FD_BLOCKS; i += FD_THREADS) acc += pp[3 * i + k];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) sums[4 * blockIdx.x + k] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(FD_THREADS) fit_terms_pop_kernel(int metric, long n, const double* __restrict__ ref,
+                                                                   const double* __restrict__ imgs,
+                                                                   const unsigned* __restrict__ mask,
+                                                                   const double* __restrict__ sums,
+                                                                   double* __restrict__ part) {
+  const double* h = sums + 4 * (long)blockIdx.y;
+  Norms nm;
+  const bool l1 = is_l1(metric);
+  nm.ref_norm = l1 ? h[0] : sqrt(h[0]);
+  nm.dat_norm = l1 ? h[1] : sqrt(h[1]);
+  nm.c = h[2] / (nm.dat_norm * nm.dat_norm);
+  const double* dat = imgs + (long)blockIdx.y * n;
+  double acc = 0.0;
+  for (long i = (long)blockIdx.x * FD_THREADS + threadIdx.x; i < n; i += (long)FD_BLOCKS * FD_THREADS)
+    acc += fit_term(metric, mask ? (double)mask[i] : 1.0, ref[i], dat[i], nm);
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[(long)blockIdx.y * FD_BLOCKS + blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(FD_THREADS) fit_final_pop_kernel(const double* __restrict__ part,
+                                                                   double* __restrict__ out) {
+  const double* pp = part + (long)blockIdx.x * FD_BLOCKS;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < FD_BLOCKS; i += FD_THREADS) acc += pp[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) out[blockIdx.x] = acc;
+}
+
 // d(distance)/d(data) of the scalar measures.  With t = T(data) (square or cube root),
 // r = T(ref), masks m in {0, 1}:
 //   unit L2:  sum m (t/N - r/R)^2, N = |t|_m:   (2m/N) ((t/N - r/R) - (t/N) K),
@@ -245,6 +318,23 @@ int fit_distance_gradient(hgx_ctx c, int metric, long n, const double* ref, cons
   fit_kterm_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(metric, n, ref, data, mask, nm, part);
   fit_sums_kernel<<<1, FD_THREADS, 0, st>>>(part, FD_BLOCKS, 1, 0, sums + 3);
   fit_lambda_kernel<<<FD_BLOCKS, FD_THREADS, 0, st>>>(metric, n, ref, data, mask, nm, sums + 3, lambda);
+  HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+long fit_population_scratch(int npop) { return (long)npop * (4L * FD_BLOCKS + 4); }
+
+int fit_distance_population(cudaStream_t st, int metric, long n, const double* ref, const double* imgs,
+                            const unsigned* mask, int npop, double* scratch, double* dist) {
+  if (metric < 0 || metric > M_CBRT_UNIT_L1 || metric == M_SQRT_UNIT_L2_RES || metric == M_SQRT_C_L2_RES)
+    return fail(HGX_ERR_INVALID_ARG, "fit_distance_population: a scalar distance measure is needed");
+  double* part3 = scratch;
+  double* part1 = part3 + 3L * FD_BLOCKS * npop;
+  double* sums = part1 + (long)FD_BLOCKS * npop;
+  fit_norms_pop_kernel<<<dim3(FD_BLOCKS, npop), FD_THREADS, 0, st>>>(metric, n, ref, imgs, mask, part3);
+  fit_sums3_pop_kernel<<<npop, FD_THREADS, 0, st>>>(part3, sums);
+  fit_terms_pop_kernel<<<dim3(FD_BLOCKS, npop), FD_THREADS, 0, st>>>(metric, n, ref, imgs, mask, sums, part1);
+  fit_final_pop_kernel<<<npop, FD_THREADS, 0, st>>>(part1, dist);
   HGX_CUDA(cudaGetLastError());
   return HGX_OK;
 }

@@ -95,6 +95,13 @@ int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, d
 int fit_distance_gradient(hgx_ctx c, int metric, long n, const double* ref, const double* data,
                           const unsigned* mask, double* lambda);
 int device_dot(hgx_ctx c, long n, const double* a, const double* b, double* out);
+// The scalar fitting distance of npop images (imgs: npop x n, device) against one reference,
+// enqueued on st without a host round trip: dist (device, npop) holds each candidate's value
+// as hgx_fit_distance computes it for one image (the same sums in the same order).  scratch:
+// fit_population_scratch(npop) doubles.
+long fit_population_scratch(int npop);
+int fit_distance_population(cudaStream_t st, int metric, long n, const double* ref, const double* imgs,
+                            const unsigned* mask, int npop, double* scratch, double* dist);
 }  // namespace hgx
 
 // -------------------------------------------------------------- the context ----

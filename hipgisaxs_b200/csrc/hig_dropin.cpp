@@ -944,6 +944,40 @@ bool HiGObjectiveFunctionG::value_and_gradient(const real_vec_t& x, real_t& f, r
   return true;
 }
 
+bool HiGObjectiveFunctionG::evaluate_population(const std::vector<real_vec_t>& X, real_vec_t& dist) {
+  Impl& m = *impl_;
+  HipGISAXSG::Impl& s = *m.sim.impl_;
+  if (!m.good || m.ref.empty() || m.metric < 0) {
+    s.refuse("evaluate_population(): the objective has no reference data or distance metric");
+    return false;
+  }
+  if (X.empty()) {
+    s.refuse("evaluate_population(): empty population");
+    return false;
+  }
+  const size_t nx = s.params().size();
+  std::vector<double> xs;
+  for (const real_vec_t& x : X) {
+    if (x.size() != nx) {
+      s.refuse("evaluate_population(): each candidate needs one value per fit parameter");
+      return false;
+    }
+    xs.insert(xs.end(), x.begin(), x.end());
+  }
+  hgx_hig_pop pop = nullptr;
+  if (!s.check(hgx_hig_population_create(s.ctx, s.h, (int)X.size(), m.ref.data(),
+                                         m.mask.empty() ? nullptr : m.mask.data(), m.metric, m.alpha,
+                                         HGX_F64, &pop),
+               "evaluate_population()"))
+    return false;
+  std::vector<double> d(X.size());
+  const bool good = s.check(hgx_hig_population_eval(pop, xs.data(), (int)nx, d.data()), "evaluate_population()");
+  hgx_hig_population_destroy(pop);
+  if (!good) return false;
+  dist.assign(d.begin(), d.end());
+  return true;
+}
+
 int HiGObjectiveFunctionG::num_fit_params() const { return (int)impl_->sim.impl_->params().size(); }
 
 std::vector<std::string> HiGObjectiveFunctionG::fit_param_keys() const { return impl_->sim.fit_param_keys(); }

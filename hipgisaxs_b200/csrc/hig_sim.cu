@@ -134,6 +134,9 @@ struct FusedArgs {
   const double2* fc;
   long n;
   double* out;             // N intensities, accumulated
+  // a population launch (grid y = candidate): per-candidate strides of shapes, elems and
+  // scales (records), grains and elem_rot (doubles) and out (doubles); 0 otherwise
+  long ps_shape = 0, ps_elem = 0, ps_grain = 0, ps_er = 0, ps_scale = 0, ps_out = 0;
 };
 
 // Four threads per pixel, one per DWBA block k: each evaluates fc_k sf_k ff_k and the quad
@@ -153,19 +156,26 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
   const zd qz(a.qz[k * a.n + ii]);
   const zd fc(a.fc[k * a.n + ii]);
   const int base = (threadIdx.x & 31) & ~3;
-  double acc = (live && k == 0) ? a.out[i] : 0.0;
+  const long cy = blockIdx.y;  // the candidate of a population launch
+  const AnaShape* shapes = a.shapes + cy * a.ps_shape;
+  const FusedElem* elems = a.elems + cy * a.ps_elem;
+  const double* grains = a.grains + cy * a.ps_grain;
+  const double* elem_rot = a.elem_rot + cy * a.ps_er;
+  const ScaleEntry* scales = a.scales + cy * a.ps_scale;
+  double* out = a.out + cy * a.ps_out;
+  double acc = (live && k == 0) ? out[i] : 0.0;
   for (int g = a.g0; g < a.g1; ++g) {
-    const double* gp = a.grains + 12 * (long)g;
+    const double* gp = grains + 12 * (long)g;
     zd ff(0, 0);
     for (int e = 0; e < a.nelem; ++e) {
-      const double* er = a.elem_rot + 9 * ((long)g * a.nelem + e);
+      const double* er = elem_rot + 9 * ((long)g * a.nelem + e);
       Rot9d Re;
 #pragma unroll
       for (int r = 0; r < 9; ++r) Re.r[r] = er[r];
       zd m[3];
       rotate_q(Re, qx, qy, qz, m);
-      const zd eff = ff_analytic_eval<SHAPE>(a.shapes[e], m, a.elems[e].loc);
-      const double dre = a.elems[e].dre, dim = a.elems[e].dim;
+      const zd eff = ff_analytic_eval<SHAPE>(shapes[e], m, elems[e].loc);
+      const double dre = elems[e].dre, dim = elems[e].dim;
       ff.x = __dadd_rn(ff.x, __dsub_rn(__dmul_rn(dre, eff.x), __dmul_rn(dim, eff.y)));
       ff.y = __dadd_rn(ff.y, __dadd_rn(__dmul_rn(dre, eff.y), __dmul_rn(dim, eff.x)));
     }
@@ -174,7 +184,7 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
     for (int r = 0; r < 9; ++r) R.r[r] = gp[r];
     zd mr[3];
     rotate_q(R, qx, qy, qz, mr);
-    const ScaleEntry* sp = a.scales + (long)g * a.nscale;
+    const ScaleEntry* sp = scales + (long)g * a.nscale;
     for (int si = 0; si < a.nscale; ++si) {
       zd sfv;
       if (a.sfbuf) {
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
       acc += sum.x * sum.x + sum.y * sum.y;
     }
   }
-  if (live && k == 0) a.out[i] = acc;
+  if (live && k == 0) out[i] = acc;
 }
 
 // The fused grain loop in FP32C for grids with real qz and unit cells of one shape among
@@ -222,22 +232,29 @@ __global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
   const double2 fcd = a.fc[k * a.n + ii];
   const cf fc{(float)fcd.x, (float)fcd.y};
   const int base = (threadIdx.x & 31) & ~3;
-  double acc = (live && k == 0) ? a.out[i] : 0.0;
+  const long cy = blockIdx.y;  // the candidate of a population launch
+  const AnaShape* shapes = a.shapes + cy * a.ps_shape;
+  const FusedElem* elems = a.elems + cy * a.ps_elem;
+  const double* grains = a.grains + cy * a.ps_grain;
+  const double* elem_rot = a.elem_rot + cy * a.ps_er;
+  const ScaleEntry* scales = a.scales + cy * a.ps_scale;
+  double* out = a.out + cy * a.ps_out;
+  double acc = (live && k == 0) ? out[i] : 0.0;
   for (int g = a.g0; g < a.g1; ++g) {
-    const double* gp = a.grains + 12 * (long)g;
+    const double* gp = grains + 12 * (long)g;
     cf ff{0.f, 0.f};
     for (int e = 0; e < a.nelem; ++e) {
-      const double* er = a.elem_rot + 9 * ((long)g * a.nelem + e);
+      const double* er = elem_rot + 9 * ((long)g * a.nelem + e);
       double m[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) m[j] = er[3 * j] * qx + er[3 * j + 1] * qy + er[3 * j + 2] * qz;
-      const cf eff = ff_analytic_f32c<SHAPE>(a.shapes[e], m, a.elems[e].loc);
-      ff = cadd(ff, cmul(cf{(float)a.elems[e].dre, (float)a.elems[e].dim}, eff));
+      const cf eff = ff_analytic_f32c<SHAPE>(shapes[e], m, elems[e].loc);
+      ff = cadd(ff, cmul(cf{(float)elems[e].dre, (float)elems[e].dim}, eff));
     }
     double mr[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) mr[j] = gp[3 * j] * qx + gp[3 * j + 1] * qy + gp[3 * j + 2] * qz;
-    const ScaleEntry* sp = a.scales + (long)g * a.nscale;
+    const ScaleEntry* sp = scales + (long)g * a.nscale;
     for (int si = 0; si < a.nscale; ++si) {
       cf sfv;
       if (a.sfbuf) {
@@ -265,7 +282,7 @@ __global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
       acc += (double)(w * w * (sum.x * sum.x + sum.y * sum.y));
     }
   }
-  if (live && k == 0) a.out[i] = acc;
+  if (live && k == 0) out[i] = acc;
 }
 
 // true when the FP32C grain kernel has a body for this shape
@@ -1402,3 +1419,431 @@ int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, d
 }
 
 }  // namespace hgx
+
+// ------------------------------------------------------- a fitting population ----
+// The particle loop of the reference's PSO fitter (src/analyzer/hipgisaxs_fit_pso.cpp:521-545)
+// calls the objective once per particle: per particle the parameters, one simulation, one
+// distance.  A population here evaluates all candidates of a generation together: the host
+// builds each candidate's fused grain tables from a copy of the description with the
+// candidate's parameters, and one CUDA graph (recorded on the first evaluation, replayed after)
+// copies the tables from pinned memory, runs every launch of the fused grain kernel for all
+// candidates at once (grid y = candidate), sums the structures and reduces every candidate's
+// distance, and copies the npop distances back.  The grid, the Fresnel coefficients and any
+// grain-independent (paracrystal, Percus-Yevick) structure factor are made once, at creation:
+// candidates may change only what the fused tables hold (shape samples, locations,
+// orientations, lattice vectors, scalings), as for the objective's gradient.
+namespace hgx {
+namespace {
+
+__global__ void pop_structure_sum_kernel(const double* __restrict__ I, const double* __restrict__ r,
+                                         int ns, long n, double* __restrict__ out) {
+  const long z = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  const double* Ic = I + (long)blockIdx.y * ns * n;
+  double sum = 0.0;
+  // as hgx_structure_sum: separate multiply and add, structures in order
+  for (int s = 0; s < ns; ++s) sum = __dadd_rn(sum, __dmul_rn(Ic[(long)s * n + z], r[s]));
+  out[(long)blockIdx.y * n + z] = sum;
+}
+
+// one structure's per-candidate table sizes and its launch choices
+struct PopStruct {
+  int ngr = 0, nscale = 0, nelem = 0, shape = 0;
+  bool liquid = false, f32c = false;
+  size_t o_shapes = 0, o_elems = 0, o_gt = 0, o_er = 0, o_sc = 0;  // byte offsets in the staging block
+  size_t n_gt = 0, n_er = 0, n_sc = 0;                               // per candidate (doubles, doubles, entries)
+  long sf_off = 0;                                                    // liquid: offset in sf (complex values)
+};
+
+}  // namespace
+}  // namespace hgx
+
+struct hgx_hig_pop_s {
+  hgx_ctx ctx = nullptr;
+  hig::Input in;                  // the description at creation (candidates change copies)
+  std::vector<double> fixed;      // fixed_quantities(in)
+  int npop = 0, nx = 0, metric = 0, precision = HGX_F64;
+  double reg_alpha = 0.0;
+  long n = 0;
+  int nstruct = 0;
+  hgx_qgrid grid = nullptr;
+  std::vector<hgx::PopStruct> st;
+  size_t stage_bytes = 0;         // tables of one candidate, all structures
+  unsigned char* h_stage = nullptr;  // pinned: npop x stage_bytes
+  double* h_dist = nullptr;       // pinned: npop
+  hgx::DevBuf d_stage, fc, sf, I, img, ref, mask, ratios, scratch, dist;
+  std::vector<int> variants;      // the paired / per-block choice of every FP64 launch, as recorded
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace hgx {
+namespace {
+
+int pop_refuse(const std::string& why) { return fail(HGX_ERR_INVALID_ARG, "hgx_hig_population: " + why); }
+
+// the description's fused tables with candidate x applied (a copy of the description)
+int pop_tables(const hgx_hig_pop_s& P, const double* x, std::vector<StructTables>& T) {
+  hig::Input ip = P.in;
+  int i = 0;
+  for (const auto& kv : ip.fit_params) {
+    std::string err;
+    if (!hig::update_param(ip, kv.second.variable, x[i++], err)) return pop_refuse(err);
+  }
+  if (fixed_quantities(ip) != P.fixed)
+    return pop_refuse("a candidate changes a refractive index, a layer, the beam, a liquid structure factor, "
+                      "an iratio, a grain count or a repetition");
+  std::string why;
+  const int s = all_tables(ip, T, why);
+  if (s != HGX_OK) return why.empty() ? s : pop_refuse(why);
+  if ((int)T.size() != P.nstruct) return pop_refuse("a candidate changes the structures");
+  for (int k = 0; k < P.nstruct; ++k) {
+    const PopStruct& ps = P.st[k];
+    const StructTables& t = T[k];
+    if (t.ngr != ps.ngr || t.nscale != ps.nscale || (int)t.f.elems.size() != ps.nelem ||
+        t.f.gt.size() != ps.n_gt || t.f.er.size() != ps.n_er || t.plan.size() != ps.n_sc)
+      return pop_refuse("a candidate changes the number of grains, samples or elements");
+    for (const AnaShape& a : t.f.shapes)
+      if (a.shape != t.f.shapes[0].shape || (ps.shape != 0 && a.shape != ps.shape))
+        return pop_refuse("a candidate changes a shape");
+  }
+  return HGX_OK;
+}
+
+// the paired lattice factor of a launch holds when it holds for every candidate
+bool pop_paired(const std::vector<std::vector<StructTables>>& all, int k, int g0, int g1) {
+  for (const auto& T : all) {
+    const StructTables& t = T[k];
+    if (t.liquid) return false;
+    for (int gi = g0; gi < g1; ++gi) {
+      if (t.f.gt[12 * (size_t)gi + 2] != 0.0 || t.f.gt[12 * (size_t)gi + 5] != 0.0) return false;
+      for (int s = 0; s < t.nscale; ++s)
+        if (t.plan[(size_t)gi * t.nscale + s].la[2] != 0.0) return false;
+    }
+  }
+  return true;
+}
+
+// grains per launch: about FUSED_GRAINS_PER_LAUNCH grain evaluations over all candidates
+int pop_chunk(int npop) { return std::max(1, FUSED_GRAINS_PER_LAUNCH / npop); }
+
+int pop_enqueue(hgx_hig_pop_s& P, cudaStream_t st) {
+  const long n = P.n;
+  HGX_CUDA(cudaMemcpyAsync(P.d_stage.p, P.h_stage, P.stage_bytes * P.npop, cudaMemcpyHostToDevice, st));
+  HGX_CUDA(cudaMemsetAsync(P.I.p, 0, sizeof(double) * n * P.nstruct * P.npop, st));
+  const unsigned char* base = (const unsigned char*)P.d_stage.p;
+  const int chunk = pop_chunk(P.npop);
+  size_t vi = 0;
+  for (int k = 0; k < P.nstruct; ++k) {
+    const PopStruct& ps = P.st[k];
+    FusedArgs a;
+    a.shapes = (const AnaShape*)(base + ps.o_shapes);
+    a.elems = (const FusedElem*)(base + ps.o_elems);
+    a.nelem = ps.nelem;
+    a.grains = (const double*)(base + ps.o_gt);
+    a.elem_rot = (const double*)(base + ps.o_er);
+    a.scales = (const ScaleEntry*)(base + ps.o_sc);
+    a.nscale = ps.nscale;
+    a.sfbuf = ps.liquid ? (const double2*)P.sf.p + ps.sf_off : nullptr;
+    a.qx = P.grid->qx;
+    a.qy = P.grid->qy;
+    a.qz = P.grid->qz;
+    a.fc = (const double2*)P.fc.p;
+    a.n = n;
+    a.out = (double*)P.I.p + (size_t)k * n;
+    // candidate strides: the staging block repeats every stage_bytes, a multiple of each record
+    const long sb = (long)P.stage_bytes;
+    a.ps_shape = sb / (long)sizeof(AnaShape);
+    a.ps_elem = sb / (long)sizeof(FusedElem);
+    a.ps_grain = sb / 8;
+    a.ps_er = sb / 8;
+    a.ps_scale = sb / (long)sizeof(ScaleEntry);
+    a.ps_out = n * P.nstruct;
+    const dim3 grid((unsigned)((4 * n + 127) / 128), (unsigned)P.npop);
+    for (int g0 = 0; g0 < ps.ngr; g0 += chunk) {
+      a.g0 = g0;
+      a.g1 = std::min(ps.ngr, g0 + chunk);
+      if (ps.f32c) {
+        switch (ps.shape) {
+          case SH_CYLINDER: grain_dwba_f32c_kernel<SH_CYLINDER><<<grid, 128, 0, st>>>(a); break;
+          case SH_SPHERE: grain_dwba_f32c_kernel<SH_SPHERE><<<grid, 128, 0, st>>>(a); break;
+          default: grain_dwba_f32c_kernel<SH_BOX><<<grid, 128, 0, st>>>(a); break;
+        }
+      } else {
+        const int paired = P.variants[vi++];
+#define HGX_POP_LAUNCH(S)                                                   \
+  (paired ? (void)(grain_dwba_kernel<S, 1><<<grid, 128, 0, st>>>(a))      \
+          : (void)(grain_dwba_kernel<S, 0><<<grid, 128, 0, st>>>(a)))
+        switch (ps.shape) {
+          case SH_CYLINDER: HGX_POP_LAUNCH(SH_CYLINDER); break;
+          case SH_SPHERE: HGX_POP_LAUNCH(SH_SPHERE); break;
+          case SH_BOX: HGX_POP_LAUNCH(SH_BOX); break;
+          case SH_CUBE: HGX_POP_LAUNCH(SH_CUBE); break;
+          case SH_PRISM3: HGX_POP_LAUNCH(SH_PRISM3); break;
+          case SH_PRISM6: HGX_POP_LAUNCH(SH_PRISM6); break;
+          case SH_PYRAMID: HGX_POP_LAUNCH(SH_PYRAMID); break;
+          default: HGX_POP_LAUNCH(0); break;
+        }
+#undef HGX_POP_LAUNCH
+      }
+      HGX_CUDA(cudaGetLastError());
+    }
+  }
+  pop_structure_sum_kernel<<<dim3((unsigned)((n + 255) / 256), (unsigned)P.npop), 256, 0, st>>>(
+      (const double*)P.I.p, (const double*)P.ratios.p, P.nstruct, n, (double*)P.img.p);
+  HGX_CUDA(cudaGetLastError());
+  HGX_TRY(fit_distance_population(st, P.metric, n, (const double*)P.ref.p, (const double*)P.img.p,
+                                  (const unsigned*)P.mask.p, P.npop, (double*)P.scratch.p, (double*)P.dist.p));
+  HGX_CUDA(cudaMemcpyAsync(P.h_dist, P.dist.p, sizeof(double) * P.npop, cudaMemcpyDeviceToHost, st));
+  return HGX_OK;
+}
+
+}  // namespace
+}  // namespace hgx
+
+extern "C" {
+
+int hgx_hig_population_destroy(hgx_hig_pop p) {
+  if (!p) return HGX_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->grid) hgx_qgrid_destroy(p->grid);
+  if (p->h_stage) cudaFreeHost(p->h_stage);
+  if (p->h_dist) cudaFreeHost(p->h_dist);
+  delete p;
+  return HGX_OK;
+}
+
+int hgx_hig_population_create(hgx_ctx c, hgx_hig h, int npop, const double* ref, const unsigned* mask,
+                              int metric, double reg_alpha, int precision, hgx_hig_pop* out) {
+  if (!c || !h || !ref || !out || npop < 1) return pop_refuse("null argument or empty population");
+  *out = nullptr;
+  if (metric < 0 || metric > 7 || metric == 4 || metric == 5)
+    return pop_refuse("a scalar distance measure is needed (not the residual vectors)");
+  if (precision != HGX_F64 && precision != HGX_F32C) return pop_refuse("unknown precision");
+  if (npop > 65535) return pop_refuse("at most 65,535 candidates");
+  const hig::Input& in = h->in;
+  const hig::Compute& cp = in.compute;
+  if (in.scattering.expt != "gisaxs") return pop_refuse("populations are built for GISAXS (DWBA) descriptions");
+  if (cp.nslices > 1) return pop_refuse("sliced layers");
+  if (cp.structcorrelation != "null" && cp.structcorrelation != "nGnE")
+    return pop_refuse("structure correlation '" + cp.structcorrelation + "' is not supported");
+  if (in.structures.empty()) return pop_refuse("the description has no structure");
+  for (const auto& kv : in.structures) {
+    const hig::Structure& s = kv.second;
+    if (s.distribution != "regular") return pop_refuse("structure '" + s.key + "': ensemble distribution '" + s.distribution + "'");
+    if (!in.unitcells.count(s.unitcell_key)) return pop_refuse("structure '" + s.key + "': unknown unit cell");
+    if (s.maxgrains[0] < 1 || s.maxgrains[1] < 1 || s.maxgrains[2] < 1) return pop_refuse("maxgrains must be >= 1");
+    if (s.orientation_stat == "range" || s.orientation_stat == "random")
+      return pop_refuse("structure '" + s.key + "': orientations drawn at random change between candidates");
+    if (s.type == "paracrystal" && s.lattice.type == "") return pop_refuse("paracrystal without lattice");
+    for (const auto& e : in.unitcells.at(s.unitcell_key).elements) {
+      auto shp = in.shapes.find(e.first);
+      if (shp == in.shapes.end()) return pop_refuse("unknown shape '" + e.first + "'");
+      if (shp->second.name == "custom" || shape_code(shp->second.name) < 0)
+        return pop_refuse("shape '" + e.first + "' (" + shp->second.name + "): the fused grain loop takes analytic shapes");
+    }
+  }
+  HGX_CUDA(cudaSetDevice(c->device));
+  auto p = new (std::nothrow) hgx_hig_pop_s;
+  if (!p) return fail(HGX_ERR_NO_MEMORY, "hgx_hig_population_create: host allocation");
+  auto bail = [&](int s) {
+    hgx_hig_population_destroy(p);
+    return s;
+  };
+  p->ctx = c;
+  p->in = in;
+  p->fixed = fixed_quantities(in);
+  p->npop = npop;
+  p->nx = (int)in.fit_params.size();
+  p->metric = metric;
+  p->precision = precision;
+  p->reg_alpha = reg_alpha;
+  cudaStream_t st = c->stream;
+  // grid and Fresnel coefficients as hgx_hig_compute_gisaxs makes them
+  double k0, alpha_i;
+  int s = hgx_hig_beam(h, &k0, &alpha_i, nullptr);
+  if (s) return bail(s);
+  const double alpha_s = in.scattering.alphai[0] * PI / 180;
+  if ((s = hgx_hig_qgrid(c, h, 0.0, 0.0, &p->grid))) return bail(s);
+  if (alpha_s != alpha_i && (s = qgrid_reextend(p->grid, alpha_s, k0, 0.0, 0.0))) return bail(s);
+  hgx_qgrid g = p->grid;
+  p->n = (long)g->nqy;
+  const long n = p->n, nq = (long)g->nqz;
+  std::vector<double> ld, lb, lt;
+  std::vector<int> lo;
+  for (const auto& kv : in.layers) {
+    ld.push_back(kv.second.refindex.delta);
+    lb.push_back(kv.second.refindex.beta);
+    lt.push_back(kv.second.thickness);
+    lo.push_back(kv.second.order);
+  }
+  if ((s = p->fc.reserve(sizeof(double2) * nq))) return bail(s);
+  if ((s = hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(), k0, alpha_s, 0,
+                                  nullptr, (double*)p->fc.p, 0)))
+    return bail(s);
+  // the table layout (from the description's own parameters) and the grain-independent factors
+  std::vector<StructTables> T0;
+  std::string why;
+  s = all_tables(in, T0, why);
+  if (s) return bail(why.empty() ? s : pop_refuse(why));
+  p->nstruct = (int)T0.size();
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~(size_t)255;
+    return o;
+  };
+  int nliquid = 0;
+  for (const StructTables& t : T0) {
+    PopStruct ps;
+    ps.ngr = t.ngr;
+    ps.nscale = t.nscale;
+    ps.nelem = (int)t.f.elems.size();
+    ps.shape = t.shape;
+    ps.liquid = t.liquid;
+    ps.f32c = precision == HGX_F32C && g->mode == 1 && grain_f32c_shape(t.shape);
+    ps.n_gt = t.f.gt.size();
+    ps.n_er = t.f.er.size();
+    ps.n_sc = t.plan.size();
+    ps.o_shapes = take(sizeof(AnaShape) * ps.nelem);
+    ps.o_elems = take(sizeof(FusedElem) * ps.nelem);
+    ps.o_gt = take(sizeof(double) * ps.n_gt);
+    ps.o_er = take(sizeof(double) * ps.n_er);
+    ps.o_sc = take(sizeof(ScaleEntry) * ps.n_sc);
+    if (ps.liquid) ps.sf_off = (long)nliquid++ * nq;
+    p->st.push_back(ps);
+  }
+  // one candidate's block, a multiple of 256 bytes and of every record size (the kernels step
+  // from candidate to candidate by whole records)
+  size_t unit = 256;
+  for (size_t r : {sizeof(AnaShape), sizeof(FusedElem), sizeof(ScaleEntry), sizeof(double)}) {
+    size_t a = unit, b = r;
+    while (b) {
+      const size_t t = a % b;
+      a = b;
+      b = t;
+    }
+    unit = unit / a * r;  // lcm
+  }
+  p->stage_bytes = (off + unit - 1) / unit * unit;
+  if (cudaMallocHost(&p->h_stage, p->stage_bytes * npop) != cudaSuccess ||
+      cudaMallocHost(&p->h_dist, sizeof(double) * npop) != cudaSuccess)
+    return bail(fail(HGX_ERR_NO_MEMORY, "hgx_hig_population_create: pinned host memory"));
+  if ((s = p->d_stage.reserve(p->stage_bytes * npop)) || (s = p->I.reserve(sizeof(double) * n * p->nstruct * npop)) ||
+      (s = p->img.reserve(sizeof(double) * n * npop)) || (s = p->ref.reserve(sizeof(double) * n)) ||
+      (s = p->ratios.reserve(sizeof(double) * p->nstruct)) ||
+      (s = p->scratch.reserve(sizeof(double) * fit_population_scratch(npop))) ||
+      (s = p->dist.reserve(sizeof(double) * npop)))
+    return bail(s);
+  if (nliquid > 0 && (s = p->sf.reserve(sizeof(double2) * nq * nliquid))) return bail(s);
+  int li = 0;
+  for (const auto& kv : in.structures) {
+    const hig::Structure& S = kv.second;
+    if (S.type == "paracrystal")
+      s = hgx_sf_paracrystal(c, g, S.pc_dims, lattice_code(S.lattice.type), S.pc_dist[1], S.pc_dist[0], S.pc_sdev[1],
+                             S.pc_sdev[0], S.pc_domain, (double2*)p->sf.p + (long)li++ * nq, HGX_C128);
+    else if (S.type == "percusyevick")
+      s = hgx_sf_percus_yevick(c, g, S.py_diameter, S.py_volfract, S.py_dims, (double2*)p->sf.p + (long)li++ * nq,
+                               HGX_C128);
+    if (s) return bail(s);
+  }
+  std::vector<double> r;
+  double rsum = 0.0;
+  for (const auto& kv : in.structures) {
+    r.push_back(kv.second.iratio);
+    rsum += kv.second.iratio;
+  }
+  if (rsum != 1.0)
+    for (double& v : r) v /= rsum;
+  cudaError_t e = cudaMemcpyAsync(p->ratios.p, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(p->ref.p, ref, sizeof(double) * n, is_device_ptr(ref) ? cudaMemcpyDeviceToDevice
+                                                                            : cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && mask) {
+    if ((s = p->mask.reserve(sizeof(unsigned) * n))) return bail(s);
+    e = cudaMemcpyAsync(p->mask.p, mask, sizeof(unsigned) * n, is_device_ptr(mask) ? cudaMemcpyDeviceToDevice
+                                                                                  : cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "hgx_hig_population_create: copies"));
+  *out = p;
+  return HGX_OK;
+}
+
+int hgx_hig_population_eval(hgx_hig_pop p, const double* X, int nx, double* dist) {
+  if (!p || !X || !dist) return pop_refuse("null argument");
+  if (nx != p->nx) return pop_refuse("X must hold one value per fit parameter and candidate");
+  if (is_device_ptr(dist) || is_device_ptr(X)) return pop_refuse("X and dist are host arrays");
+  HGX_CUDA(cudaSetDevice(p->ctx->device));
+  cudaStream_t st = p->ctx->stream;
+  HGX_CUDA(cudaStreamSynchronize(st));  // the pinned staging block is about to change
+  std::vector<std::vector<StructTables>> all((size_t)p->npop);
+  for (int i = 0; i < p->npop; ++i) {
+    HGX_TRY(pop_tables(*p, X + (size_t)i * nx, all[i]));
+    unsigned char* blk = p->h_stage + (size_t)i * p->stage_bytes;
+    for (int k = 0; k < p->nstruct; ++k) {
+      const PopStruct& ps = p->st[k];
+      const StructTables& t = all[i][k];
+      memcpy(blk + ps.o_shapes, t.f.shapes.data(), sizeof(AnaShape) * ps.nelem);
+      memcpy(blk + ps.o_elems, t.f.elems.data(), sizeof(FusedElem) * ps.nelem);
+      memcpy(blk + ps.o_gt, t.f.gt.data(), sizeof(double) * ps.n_gt);
+      memcpy(blk + ps.o_er, t.f.er.data(), sizeof(double) * ps.n_er);
+      memcpy(blk + ps.o_sc, t.plan.data(), sizeof(ScaleEntry) * ps.n_sc);
+    }
+  }
+  // the paired / per-block choice of every FP64 launch for this generation
+  std::vector<int> v;
+  const int chunk = pop_chunk(p->npop);
+  for (int k = 0; k < p->nstruct; ++k) {
+    const PopStruct& ps = p->st[k];
+    if (ps.f32c) continue;
+    for (int g0 = 0; g0 < ps.ngr; g0 += chunk) v.push_back(pop_paired(all, k, g0, std::min(ps.ngr, g0 + chunk)));
+  }
+  if (p->exec && v != p->variants) {  // another kernel variant: record the graph again
+    cudaGraphExecDestroy(p->exec);
+    cudaGraphDestroy(p->graph);
+    p->exec = nullptr;
+    p->graph = nullptr;
+  }
+  p->variants = v;
+  if (!p->exec) {
+    cudaStream_t cap = nullptr;
+    HGX_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int s = HGX_OK;
+    if (e == cudaSuccess) s = pop_enqueue(*p, cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+    cudaStreamDestroy(cap);
+    if (e != cudaSuccess || s != HGX_OK || e2 != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+      if (s != HGX_OK) return s;
+      return cuda_fail(e2, "cudaStreamEndCapture");
+    }
+    p->graph = graph;
+    HGX_CUDA(cudaGraphInstantiate(&p->exec, graph, 0));
+  }
+  HGX_CUDA(cudaGraphLaunch(p->exec, st));
+  HGX_CUDA(cudaStreamSynchronize(st));
+  HGX_TRY(hgx_synchronize(p->ctx));
+  // the regularisation of HipGISAXSObjectiveFunction::operator() (objective_func_hipgisaxs.cpp:300-320)
+  for (int i = 0; i < p->npop; ++i) {
+    double pmean = 0.0;
+    int j = 0;
+    for (const auto& kv : p->in.fit_params) {
+      const double mean = (kv.second.range[1] - kv.second.range[0]) / 2.0 + kv.second.range[0];
+      double t = X[(size_t)i * nx + j++] - mean;
+      t *= t;
+      pmean += t;
+    }
+    const double reg = (p->reg_alpha / 2) * pmean;
+    dist[i] = isfinite(p->h_dist[i]) ? p->h_dist[i] + reg : 1e8;
+  }
+  return HGX_OK;
+}
+
+}  // extern "C"

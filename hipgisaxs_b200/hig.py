@@ -275,6 +275,12 @@ class HiGInput:
         self._reload()
         return float(dist[0]), grad
 
+    def population(self, ctx: Context, npop: int, ref, mask=None, metric="sqrt_unit_l2", reg_alpha=0.0,
+                   precision: str = "f64"):
+        """A fitting population of this description (hgx_hig_population_*): evaluates npop
+        parameter vectors per call, each distance the one objective() returns for it."""
+        return HiGPopulation(ctx, self, npop, ref, mask, metric, reg_alpha, precision)
+
     @property
     def handle(self):
         return self._h
@@ -326,3 +332,38 @@ def read_mask(path: str):
     check(lib().hgx_read_mask(os.fsencode(path), m.ctypes.data, cnt.value, C.byref(cnt)))
     return m
 
+
+class HiGPopulation:
+    """hgx_hig_population: the particle loop of the reference's PSO fitter
+    (src/analyzer/hipgisaxs_fit_pso.cpp:521-545) for npop candidates per evaluation, on a copy
+    of the description taken at creation."""
+
+    def __init__(self, ctx: Context, d: HiGInput, npop: int, ref, mask=None, metric="sqrt_unit_l2",
+                 reg_alpha=0.0, precision: str = "f64"):
+        pr, kr = _in(ref, np.float64)
+        pm, km = (None, None) if mask is None else _in(mask, np.uint32)
+        h = C.c_void_p()
+        check(lib().hgx_hig_population_create(ctx.handle, d.handle, int(npop), pr, pm,
+                                              METRICS.get(metric, metric), float(reg_alpha),
+                                              PRECISION[precision], C.byref(h)))
+        self._h = h
+        self.npop = int(npop)
+        self.nx = len(d.fit_keys())
+
+    def eval(self, X) -> np.ndarray:
+        """Distances of the npop rows of X (npop x nx, fit_keys() order per row)."""
+        Xa = np.ascontiguousarray(X, dtype=np.float64).reshape(self.npop, self.nx)
+        dist = np.zeros(self.npop)
+        check(lib().hgx_hig_population_eval(self._h, Xa.ctypes.data, int(self.nx), dist.ctypes.data))
+        return dist
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().hgx_hig_population_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

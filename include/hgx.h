@@ -566,6 +566,30 @@ int hgx_hig_objective(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const dou
 int hgx_hig_objective_grad(hgx_ctx ctx, hgx_hig h, const double* x, int nx, const double* ref,
                            const unsigned* mask, int metric, double reg_alpha, double* dist,
                            double* grad);
+/* A fitting population of a HiG description: the particle loop of the reference's PSO fitter
+ * (src/analyzer/hipgisaxs_fit_pso.cpp:521-545), which calls the objective
+ * (HipGISAXSObjectiveFunction::operator(), src/analyzer/objective_func_hipgisaxs.cpp:263-320)
+ * once per particle, for npop candidates at a time.  _create copies the description (later
+ * changes to h do not reach the population), builds the grid, the Fresnel coefficients and any
+ * paracrystal or Percus-Yevick structure factor once, and keeps ref (nrow x ncol) and mask.
+ * _eval: X = npop x nx parameter vectors (host, key order per row), dist = npop host doubles,
+ * each the value hgx_hig_objective returns for that row (the same simulation arithmetic and
+ * distance sums at HGX_F64; HGX_F32C runs the fused grain kernel's FP32C bodies where
+ * hgx_hig_compute_gisaxs would).  One evaluation: the host builds every candidate's grain
+ * tables; a CUDA graph, recorded on the first evaluation and replayed after, copies them from
+ * pinned memory, runs each fused grain launch for all candidates together, sums the
+ * structures, reduces all distances and copies them back.  Candidates may move what those
+ * tables hold (shape samples and weights, locations, orientations other than "range"/"random",
+ * spacings, lattice vectors, scalings); a candidate that changes a refractive index, a layer,
+ * the beam, a liquid structure factor, an iratio, a grain, sample or element count returns
+ * HGX_ERR_INVALID_ARG with the reason.  GISAXS descriptions of analytic shapes; scalar
+ * distance measures only. */
+typedef struct hgx_hig_pop_s* hgx_hig_pop;
+int hgx_hig_population_create(hgx_ctx ctx, hgx_hig h, int npop, const double* ref,
+                              const unsigned* mask, int metric, double reg_alpha, int precision,
+                              hgx_hig_pop* out);
+int hgx_hig_population_eval(hgx_hig_pop pop, const double* X, int nx, double* dist);
+int hgx_hig_population_destroy(hgx_hig_pop pop);
 
 /* ------------------------------------------------------------- measurement ---- */
 /* Throughput probes for roofline denominators (no reference counterpart): FP32 FFMA

@@ -334,6 +334,11 @@ class HiGObjectiveFunctionG {
   // gradient by the simulation's tangent (hgx_hig_objective_grad), where the reference's LMVM
   // fitter takes two simulations per parameter; false on failure
   bool value_and_gradient(const real_vec_t& x, real_t& f, real_vec_t& g);
+  // the scalar objective of every candidate of a population (the particle loop of the
+  // reference's PSO fitter, src/analyzer/hipgisaxs_fit_pso.cpp:521-545) in one batched
+  // evaluation (hgx_hig_population_*; a caller that evaluates many generations keeps a
+  // population handle of the C ABI, whose graph is then replayed); false on failure
+  bool evaluate_population(const std::vector<real_vec_t>& X, real_vec_t& dist);
   int num_fit_params() const;
   std::vector<std::string> fit_param_keys() const;
   std::vector<std::pair<real_t, real_t>> fit_param_limits() const;

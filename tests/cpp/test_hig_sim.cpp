@@ -13,6 +13,7 @@
 //   dist1.bin     the same with regularization 0.5
 //   dist2.bin     the same with the sqrt_c_l2_residual metric (one value per pixel)
 //   dist3.bin     sqrt_unit_l2 after simulate_and_set_ref(5, 25, 12), at (5, 25, 12)
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -110,6 +111,15 @@ int main(int argc, char** argv) {
   obj.set_regularization(0.5);
   d = obj(x);
   if (d.empty() || !save("dist1.bin", d.data(), d.size())) return 12;
+  {  // a population of two candidates: each the operator() value of its row
+    const std::vector<hig::real_vec_t> X = {x, {4.0, 20.0, 2.5}};
+    hig::real_vec_t pd;
+    if (!obj.evaluate_population(X, pd) || pd.size() != 2) return 18;
+    const hig::real_vec_t d1 = obj(X[1]);
+    if (d1.empty() || std::fabs(pd[0] - d[0]) > 1e-12 * std::fabs(d[0]) ||
+        std::fabs(pd[1] - d1[0]) > 1e-12 * std::fabs(d1[0]))
+      return 19;
+  }
   if (!obj.set_distance_metric("sqrt_c_l2_residual")) return 13;
   d = obj(x);
   if (d.size() != n || !save("dist2.bin", d.data(), d.size())) return 14;

@@ -323,6 +323,51 @@ def test_objective_gradient_matches_oracle_differences(ctx, po, case, metric):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", range(len(GRAD_CASES)))
+def test_population_matches_objective_calls(ctx, po, case):
+    """hgx_hig_population: every candidate's distance equals hgx_hig_objective's for its
+    parameter vector (the same simulation arithmetic and distance sums, one call per particle
+    as the reference's PSO loop makes them), on the first evaluation (graph recorded) and on a
+    second generation (replayed); the FP32C population within 1e-5 of it."""
+    name, xtrue, x0 = GRAD_CASES[case]
+    d = read_hig(os.path.join(HIG, name))
+    d.fit_update(xtrue)
+    ref_img = po.compute_gisaxs(d.data, HIG)
+    mask = np.ones(ref_img.size, dtype=np.uint32)
+    mask[::5] = 0
+    rng = np.random.default_rng(7 + case)
+    npop = 6
+    pop = d.population(ctx, npop, ref_img, mask, "sqrt_c_l2", 0.2)
+    pop32 = d.population(ctx, npop, ref_img, mask, "sqrt_c_l2", 0.2, "f32c")
+    for gen in range(2):
+        X = np.array(x0) * (1 + rng.uniform(-0.03, 0.03, (npop, len(x0))))
+        got, got32 = pop.eval(X), pop32.eval(X)
+        for i in range(npop):
+            want = d.objective(ctx, X[i], ref_img, mask, "sqrt_c_l2", 0.2)[0]
+            assert abs(got[i] - want) <= 1e-12 * abs(want), (gen, i, got[i], want)
+            assert abs(got32[i] - want) <= 1e-5 * abs(want), (gen, i, got32[i], want)
+    pop.close()
+    pop32.close()
+
+
+@pytest.mark.gpu
+def test_population_refusals(ctx):
+    d = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    ref_img = np.ones(d.image_size())
+    with pytest.raises(hg.HgxError):  # the residual vectors are not one value per candidate
+        d.population(ctx, 4, ref_img, None, "sqrt_unit_l2_residual")
+    d2 = read_hig(os.path.join(HIG, "fit_update.hig"))  # random orientations
+    with pytest.raises(hg.HgxError):
+        d2.population(ctx, 4, np.ones(d2.image_size()))
+    pop = d.population(ctx, 2, ref_img)
+    with pytest.raises(hg.HgxError):  # one row per candidate, one value per fit parameter
+        lib_x = np.ones((2, len(d.fit_keys()) + 1))
+        hg._capi.check(hg.lib().hgx_hig_population_eval(pop._h, lib_x.ctypes.data, lib_x.shape[1],
+                                                        np.zeros(2).ctypes.data))
+    pop.close()
+
+
+@pytest.mark.gpu
 def test_objective_gradient_refuses_what_it_cannot_differentiate(ctx, po):
     d = read_hig(os.path.join(HIG, "fit_objective.hig"))
     ref_img = np.ones(d.image_size())
