@@ -543,6 +543,65 @@ CONFIG1_HIG = """hipGisaxsInput = {
 """
 
 
+# The population leg: config 1's description at 512 x 512 with a fitting block over the
+# lattice constant (the grain scaling).  (The cylinder's size distribution is summed unweighted,
+# as the reference sums it, so moving a Gaussian mean would not change the image.)
+POP_FIT = """	fitting = {
+		fitparam = { key = "a_lat", variable = "structure['st1']:grain:scaling", range = { min = 19, max = 21 }, init = 20 },
+		algorithm = { algoname = "pso", distancemetric = "sqrt_unit_l2" }
+	}
+}
+"""
+
+
+def population_bench(ctx, npop=64, n=512, steps=3):
+    """A PSO generation of npop candidates of config 1's description through
+    hgx_hig_population_eval (one recorded graph), FP64 and FP32C, against the reference's way:
+    one objective call (one simulation and one distance) per particle (hgx_hig_objective)."""
+    import tempfile
+    from hipgisaxs_b200.hig import read_hig
+    text = CONFIG1_HIG.replace("NRES", str(n)).rstrip().rstrip("}").rstrip() + ",\n" + POP_FIT
+    rng = np.random.default_rng(20240605)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "pop.hig")
+        with open(path, "w") as f:
+            f.write(text)
+        d = read_hig(path)
+        d.fit_update([20.3])
+        ref = d.compute_gisaxs(ctx).ravel()
+        X = rng.uniform(19.2, 20.8, (npop, 1))
+        res = {"metric": "objective evals/s", "candidates": npop, "pixels": n * n,
+               "workload": f"config 1 description at {n}x{n}, fit parameter: the lattice constant",
+               "distance": "sqrt_unit_l2"}
+        for prec in ("f64", "f32c"):
+            pop = d.population(ctx, npop, ref, None, "sqrt_unit_l2", 0.0, prec)
+            v = pop.eval(X)  # records the graph
+            best = float("inf")
+            for _ in range(steps):
+                t = time.perf_counter()
+                v = pop.eval(X)
+                best = min(best, time.perf_counter() - t)
+            pop.close()
+            res[prec] = {"ms_per_generation": 1e3 * best, "value": npop / best}
+            res[prec + "_dist"] = v
+        d.objective(ctx, X[0], ref)
+        t = time.perf_counter()
+        seq = np.array([d.objective(ctx, x, ref)[0] for x in X])
+        dts = time.perf_counter() - t
+        res["sequential_objective_calls"] = {"ms_per_generation": 1e3 * dts, "value": npop / dts,
+                                             "method": "hgx_hig_objective once per candidate (FP64), "
+                                                       "as the reference's PSO loop calls its objective"}
+        res["speedup_vs_sequential"] = dts / (res["f64"]["ms_per_generation"] * 1e-3)
+        res["fp32c_speedup_vs_fp64"] = res["f64"]["ms_per_generation"] / res["f32c"]["ms_per_generation"]
+        d64 = res.pop("f64_dist")
+        d32 = res.pop("f32c_dist")
+        res["max_rel_diff_vs_sequential"] = float(np.max(np.abs(d64 - seq) / np.abs(seq)))
+        res["max_rel_err_fp32c_vs_fp64"] = float(np.max(np.abs(d32 - d64) / np.abs(d64)))
+        res["value"] = res["f64"]["value"]
+        d.close()
+    return res
+
+
 def config1_bench(ctx, steps=3, n=1024, cpu=True):
     """Config 1 through HipGISAXS::compute_gisaxs (hgx_hig_compute_gisaxs, host image out, the
     call synchronous; best of `steps` by the host clock), FP32C and FP64 on the same
@@ -870,6 +929,7 @@ def main():
     cfg1 = None
     if not args.no_config1 and rank == 0 and world == 1:
         cfg1 = config1_bench(ctx, cpu=not args.no_cpu_baseline)
+        cfg1["population_512sq"] = population_bench(ctx)
         npx1 = float(cfg1["pixels"])
         t32, t64 = cfg1["f32c"]["ms"] * 1e-3, cfg1["f64"]["ms"] * 1e-3
         r32 = roofline_of("fp32", CFG1_F32C_FP32_FLOP_PER_PIXEL, npx1, t32, peak_fp32, "pixel",
