@@ -83,10 +83,18 @@ struct HigWork {
   hgx_qgrid grid = nullptr;
   double key[8] = {0};
   double ext_alpha = 0.0;  // the incidence angle the grid's qz blocks were extended for
-  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj, saxs_qz;
+  long grid_gen = 0;       // counts the grids made, so that cached results can name theirs
+  std::vector<double> fc_key;  // what the Fresnel coefficients in fc were made for
+  // pinned staging of the host tables of one simulation: bump-allocated, reset at its start
+  unsigned char* h_arena = nullptr;
+  size_t arena_cap = 0, arena_off = 0;
+  DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj, saxs_qz, ratios;
   // the objective's gradient: the tables' changes, d(distance)/d(image), d(image)/dx
   DevBuf tshapes, telems, tgt, ter, tsc, lam, dimg;
   std::map<std::string, MeshTuples> meshes;  // by resolved path
+  ~HigWork() {
+    if (h_arena) cudaFreeHost(h_arena);
+  }
 };
 // d(image)/dx of hgx_hig_compute_gisaxs for one fit variable, added into dI (hig_sim.cu).
 int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, double step, double* dI);

@@ -94,6 +94,42 @@ __global__ void saxs_intensity_kernel(long n, double w, const double2* __restric
 }
 
 // qz of the detector as complex values (imaginary part 0), for SAXS structure factors
+// img[z] = sum_s I_s[z] r_s per image (grid y = image of a population, 0 otherwise), as
+// hgx_structure_sum forms it: separate multiply and add, structures in order
+// (src/sim/hipgisaxs_main.cpp:1352-1362)
+__global__ void image_structure_sum_kernel(const double* __restrict__ I, const double* __restrict__ r,
+                                           int ns, long n, double* __restrict__ out) {
+  const long z = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  const double* Ic = I + (long)blockIdx.y * ns * n;
+  double sum = 0.0;
+  for (int s = 0; s < ns; ++s) sum = __dadd_rn(sum, __dmul_rn(Ic[(long)s * n + z], r[s]));
+  out[(long)blockIdx.y * n + z] = sum;
+}
+
+// Copies host data to dev through the context's pinned arena: one asynchronous copy from
+// pinned memory (a copy from pageable memory waits for the host).  The arena is reset at the
+// start of each simulation and grows only after the stream has finished reading it.
+int arena_copy(HigWork& w, cudaStream_t st, void* dev, const void* src, size_t bytes) {
+  if (!bytes) return HGX_OK;
+  const size_t step = (bytes + 255) & ~(size_t)255;
+  if (w.arena_off + step > w.arena_cap) {
+    HGX_CUDA(cudaStreamSynchronize(st));  // copies in flight still read the old arena
+    if (w.h_arena) cudaFreeHost(w.h_arena);
+    w.h_arena = nullptr;
+    w.arena_cap = 0;
+    w.arena_off = 0;
+    const size_t cap = std::max<size_t>(2 * step, (size_t)1 << 20);
+    HGX_CUDA(cudaMallocHost(&w.h_arena, cap));
+    w.arena_cap = cap;
+  }
+  unsigned char* dst = w.h_arena + w.arena_off;
+  memcpy(dst, src, bytes);
+  w.arena_off += step;
+  HGX_CUDA(cudaMemcpyAsync(dev, dst, bytes, cudaMemcpyHostToDevice, st));
+  return HGX_OK;
+}
+
 __global__ void real_to_complex_kernel(long n, const double* __restrict__ x, double2* __restrict__ z) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) z[i] = make_double2(x[i], 0.0);
@@ -828,15 +864,15 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
   if (nelem > 0) {
     HGX_TRY(bshapes.reserve(sizeof(AnaShape) * nelem));
     HGX_TRY(belems.reserve(sizeof(FusedElem) * nelem));
-    HGX_CUDA(cudaMemcpyAsync(bshapes.p, shapes.data(), sizeof(AnaShape) * nelem, cudaMemcpyHostToDevice, st));
-    HGX_CUDA(cudaMemcpyAsync(belems.p, elems.data(), sizeof(FusedElem) * nelem, cudaMemcpyHostToDevice, st));
+    HGX_TRY(arena_copy(w, st, bshapes.p, shapes.data(), sizeof(AnaShape) * nelem));
+    HGX_TRY(arena_copy(w, st, belems.p, elems.data(), sizeof(FusedElem) * nelem));
   }
   HGX_TRY(bgt.reserve(sizeof(double) * gt.size()));
   HGX_TRY(ber.reserve(sizeof(double) * er.size()));
-  HGX_CUDA(cudaMemcpyAsync(bgt.p, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice, st));
-  HGX_CUDA(cudaMemcpyAsync(ber.p, er.data(), sizeof(double) * er.size(), cudaMemcpyHostToDevice, st));
+  HGX_TRY(arena_copy(w, st, bgt.p, gt.data(), sizeof(double) * gt.size()));
+  HGX_TRY(arena_copy(w, st, ber.p, er.data(), sizeof(double) * er.size()));
   HGX_TRY(bsc.reserve(sizeof(ScaleEntry) * plan.size()));
-  HGX_CUDA(cudaMemcpyAsync(bsc.p, plan.data(), sizeof(ScaleEntry) * plan.size(), cudaMemcpyHostToDevice, st));
+  HGX_TRY(arena_copy(w, st, bsc.p, plan.data(), sizeof(ScaleEntry) * plan.size()));
   FusedArgs a;
   a.shapes = (const AnaShape*)bshapes.p;
   a.elems = (const FusedElem*)belems.p;
@@ -940,6 +976,10 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     if (!c->hig) return fail(HGX_ERR_NO_MEMORY, "hgx_hig_compute_gisaxs: out of host memory");
   }
   HigWork& w = *c->hig;
+  if (w.arena_off) {  // a simulation that ended early may still have copies in flight
+    HGX_CUDA(cudaStreamSynchronize(st));
+    w.arena_off = 0;
+  }
   const double key[8] = {(double)cp.resolution[0], (double)cp.resolution[1], cp.minpoint[0], cp.minpoint[1],
                          cp.maxpoint[0], cp.maxpoint[1], alpha_i, k0};
   bool same = w.grid != nullptr;
@@ -950,6 +990,7 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     HGX_TRY(hgx_hig_qgrid(c, h, 0.0, 0.0, &w.grid));
     for (int k = 0; k < 8; ++k) w.key[k] = key[k];
     w.ext_alpha = alpha_i;
+    ++w.grid_gen;
   }
   hgx_qgrid g = w.grid;
   if (w.ext_alpha != alpha_s) {  // layer_qgrid_qz at this angle (vacuum layer: dn2 = 0)
@@ -967,14 +1008,23 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     lo.push_back(kv.second.order);
   }
   DevBuf &bfc = w.fc, &bff = w.ff, &beff = w.eff, &bsf = w.sf, &bI = w.I;
+  const bool fc_grows = bfc.bytes < sizeof(double2) * nq;
   HGX_TRY(bfc.reserve(sizeof(double2) * nq));
   HGX_TRY(bff.reserve(sizeof(double2) * nq));
   HGX_TRY(beff.reserve(sizeof(double2) * nq));
   HGX_TRY(bsf.reserve(sizeof(double2) * nq));
   const int nstruct = (int)in.structures.size();
   HGX_TRY(bI.reserve(sizeof(double) * n * nstruct));
-  HGX_TRY(hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(),
-                                 k0, alpha_s, 0, nullptr, (double*)bfc.p, 0));
+  // the Fresnel coefficients depend on the grid, the beam and the layers only: kept between
+  // simulations of the same set-up (a fit moves none of them)
+  std::vector<double> fkey = {(double)w.grid_gen, k0, alpha_s};
+  for (size_t i = 0; i < ld.size(); ++i) fkey.insert(fkey.end(), {ld[i], lb[i], lt[i], (double)lo[i]});
+  if (fc_grows || fkey != w.fc_key) {
+    w.fc_key.clear();
+    HGX_TRY(hgx_propagation_coeffs(c, g, (int)ld.size(), ld.data(), lb.data(), lt.data(), lo.data(),
+                                   k0, alpha_s, 0, nullptr, (double*)bfc.p, 0));
+    w.fc_key = fkey;
+  }
   HGX_CUDA(cudaMemsetAsync(bI.p, 0, sizeof(double) * n * nstruct, st));
   // SAXS: the lattice structure factor takes the detector's real qz (sf.cpp:199-200)
   const bool saxs = sc.expt == "saxs";
@@ -1134,16 +1184,27 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     }
     ++si;
   }
+  // the structure sum (hgx_structure_sum's rescaling of the iratios and order of sums)
   std::vector<double> ratios;
-  for (const auto& kv : in.structures) ratios.push_back(kv.second.iratio);
-  if (is_device_ptr(image)) {
-    HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), image));
-  } else {
-    HGX_TRY(w.img.reserve(sizeof(double) * n));
-    HGX_TRY(hgx_structure_sum(c, nstruct, n, (const double*)bI.p, ratios.data(), (double*)w.img.p));
-    HGX_CUDA(cudaMemcpyAsync(image, w.img.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  double rsum = 0.0;
+  for (const auto& kv : in.structures) {
+    ratios.push_back(kv.second.iratio);
+    rsum += kv.second.iratio;
   }
-  return hgx_synchronize(c);
+  if (rsum != 1.0)
+    for (double& v : ratios) v /= rsum;
+  HGX_TRY(w.ratios.reserve(sizeof(double) * nstruct));
+  HGX_TRY(arena_copy(w, st, w.ratios.p, ratios.data(), sizeof(double) * nstruct));
+  const bool dev_out = is_device_ptr(image);
+  if (!dev_out) HGX_TRY(w.img.reserve(sizeof(double) * n));
+  double* dimg = dev_out ? image : (double*)w.img.p;
+  image_structure_sum_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>((const double*)bI.p, (const double*)w.ratios.p,
+                                                                        nstruct, n, dimg);
+  HGX_CUDA(cudaGetLastError());
+  if (!dev_out) HGX_CUDA(cudaMemcpyAsync(image, dimg, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  const int s_end = hgx_synchronize(c);
+  w.arena_off = 0;
+  return s_end;
 }
 
 }  // namespace
@@ -1435,17 +1496,6 @@ int hig_image_tangent(hgx_ctx c, hgx_hig h, const std::string& var, double x0, d
 namespace hgx {
 namespace {
 
-__global__ void pop_structure_sum_kernel(const double* __restrict__ I, const double* __restrict__ r,
-                                         int ns, long n, double* __restrict__ out) {
-  const long z = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= n) return;
-  const double* Ic = I + (long)blockIdx.y * ns * n;
-  double sum = 0.0;
-  // as hgx_structure_sum: separate multiply and add, structures in order
-  for (int s = 0; s < ns; ++s) sum = __dadd_rn(sum, __dmul_rn(Ic[(long)s * n + z], r[s]));
-  out[(long)blockIdx.y * n + z] = sum;
-}
-
 // one structure's per-candidate table sizes and its launch choices
 struct PopStruct {
   int ngr = 0, nscale = 0, nelem = 0, shape = 0;
@@ -1589,7 +1639,7 @@ int pop_enqueue(hgx_hig_pop_s& P, cudaStream_t st) {
       HGX_CUDA(cudaGetLastError());
     }
   }
-  pop_structure_sum_kernel<<<dim3((unsigned)((n + 255) / 256), (unsigned)P.npop), 256, 0, st>>>(
+  image_structure_sum_kernel<<<dim3((unsigned)((n + 255) / 256), (unsigned)P.npop), 256, 0, st>>>(
       (const double*)P.I.p, (const double*)P.ratios.p, P.nstruct, n, (double*)P.img.p);
   HGX_CUDA(cudaGetLastError());
   HGX_TRY(fit_distance_population(st, P.metric, n, (const double*)P.ref.p, (const double*)P.img.p,
