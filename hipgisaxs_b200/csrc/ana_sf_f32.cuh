@@ -14,6 +14,7 @@
 #pragma once
 
 #include "ana_sf.cuh"
+#include "turns.cuh"
 
 namespace hgx {
 
@@ -26,11 +27,12 @@ __device__ __forceinline__ cf cmul(cf a, cf b) { return cf{a.x * b.x - a.y * b.y
 __device__ __forceinline__ cf cscale(cf a, float s) { return cf{a.x * s, a.y * s}; }
 __device__ __forceinline__ cf cadd(cf a, cf b) { return cf{a.x + b.x, a.y + b.y}; }
 
-// e^{2 pi i u} of a phase in turns (FP64), reduced exactly before the FP32 sincospi
+// e^{2 pi i u} of a phase in turns (FP64), reduced exactly (FP64 add pipe) before the FP32
+// sincospi (FMA pipe)
 __device__ __forceinline__ cf expi_turns(double u) {
-  u -= rint(u);
+  u -= round_fp64(u);
   float s, c;
-  sincospif((float)(2.0 * u), &s, &c);
+  sincospi_f32((float)(2.0 * u), &s, &c);
   return cf{c, s};
 }
 // e^{i ph}, ph in radians (FP64)
@@ -113,32 +115,39 @@ __device__ __forceinline__ cf ff_analytic_f32c(const AnaShape& a, const double* 
   return out;
 }
 
-__device__ __forceinline__ bool odd_integer(double k) { return fmod(k, 2.0) != 0.0; }
+// an integer-valued k (|k| < 2^51) is odd
+__device__ __forceinline__ bool odd_integer(double k) { return 0.5 * k != round_fp64(0.5 * k); }
+
+__device__ __forceinline__ float sinpi_f32(float x) {  // |x| <= 1
+  float s, c;
+  sincospi_f32(x, &s, &c);
+  return s;
+}
 
 // sin(N theta_r / 2) / sin(theta_r / 2) on the principal angle theta_r of e^{i theta}
 __device__ __forceinline__ float dirichlet_principal(double theta, double N) {
   if (N == 1.0) return 1.f;
   double t = theta * INV_2PI_A;
-  t -= rint(t);
+  t -= round_fp64(t);
   if (t == 0.0) return (float)N;
   double v = N * t;
-  const double k = rint(v);
+  const double k = round_fp64(v);
   v -= k;
-  const float num = odd_integer(k) ? -sinpif((float)v) : sinpif((float)v);
-  return num / sinpif((float)t);
+  const float num = odd_integer(k) ? -sinpi_f32((float)v) : sinpi_f32((float)v);
+  return num / sinpi_f32((float)t);
 }
 
 // the b-axis factor: e^{i pi k (N - 1)} sin(N theta / 2) / sin(theta / 2)
 __device__ __forceinline__ cf dirichlet_b(double theta, double N) {
-  if (N == rint(N)) return cf{dirichlet_principal(theta, N), 0.f};
+  if (N == round_fp64(N)) return cf{dirichlet_principal(theta, N), 0.f};
   const double u = theta * INV_2PI_A;
-  const double k = rint(u), t = u - k;
+  const double k = round_fp64(u), t = u - k;
   if (t == 0.0) return cf{(float)N, 0.f};
   double v = N * u;
-  const double kv = rint(v);
+  const double kv = round_fp64(v);
   v -= kv;
-  const float num = odd_integer(kv) ? -sinpif((float)v) : sinpif((float)v);
-  const float den = odd_integer(k) ? -sinpif((float)t) : sinpif((float)t);
+  const float num = odd_integer(kv) ? -sinpi_f32((float)v) : sinpi_f32((float)v);
+  const float den = odd_integer(k) ? -sinpi_f32((float)t) : sinpi_f32((float)t);
   return cscale(expi_turns(k * (N - 1.0) * 0.5), num / den);
 }
 
