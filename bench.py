@@ -889,7 +889,7 @@ def main():
         del out64
 
     fit = None
-    if not args.no_fitting:
+    if not args.no_fitting and world == 1:  # the single-GPU legs stay out of scaling runs
         fit = fitting_bench(ctx, torch, dev, stream)
         bt = fit["batch_256_rois"]
         bt["roofline"] = roofline_of(
@@ -907,7 +907,7 @@ def main():
             "the expressions as written; ncu counts 82.5 executed in the backward")
 
     exact = None
-    if not args.no_exact:
+    if not args.no_exact and world == 1:
         exact = exact_bench(ctx, torch, stream, sd)
         exact["roofline"] = roofline_of("fp64", EXACT_FP64_FLOP_PER_EVAL, exact["value"], 1.0, peak_fp64,
                                         "(q-point, triangle)", "ncu executed FP64 FLOP, 512^2 launch")
