@@ -175,6 +175,9 @@ constexpr int BW_THREADS = TRI_TILE / 2;
 constexpr int BW_TPT = 2;                       // triangles per thread
 constexpr int BW_TRI = BW_THREADS * BW_TPT;     // triangles per CTA = one forward tile
 constexpr int BW_COLS = 256;                    // pixels staged per step
+// In-plane phases of a staged chunk with |q_par| x (tile's largest offset) up to 8 pi go to the
+// SFU without the explicit reduction, as in the forward row kernel (ff_tri.cu)
+constexpr float BW_WIDE_PHASE2 = 631.65468f;     // (8 pi)^2
 
 struct BwArgs {
   const float* tiles;        // the forward's FP32 tiles (offsets in nm, s n' components)
@@ -221,16 +224,24 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
   for (int row = r0; row < r1; ++row) {
     const double qz0 = a.rowqz[4L * row].x, qz2 = a.rowqz[4L * row + 2].x;
     const float fq0 = (float)qz0, fq2 = (float)qz2;
-    float x0[BW_TPT], y0[BW_TPT], x2[BW_TPT], y2[BW_TPT];
+    // row phasors Z_0 = (x0, y0), Z_2 = (x2, y2) of each triangle, paired across the two block
+    // pairs for the FP32x2 operations below: X = (x0, x2), Y = (y0, y2), Yn = -Y
+    float2 X[BW_TPT], Y[BW_TPT], Yn[BW_TPT];
 #pragma unroll
     for (int u = 0; u < BW_TPT; ++u) {
       const double czt = cz0 + (double)cz[u] * INV_TWO_PI_M;  // full z centroid, turns
       double w0 = qz0 * czt, w2 = qz2 * czt;
       w0 -= rint(w0);
       w2 -= rint(w2);
-      sincospif((float)(2.0 * w0), &y0[u], &x0[u]);
-      sincospif((float)(2.0 * w2), &y2[u], &x2[u]);
+      float x0, y0, x2, y2;
+      sincospif((float)(2.0 * w0), &y0, &x0);
+      sincospif((float)(2.0 * w2), &y2, &x2);
+      X[u] = make_float2(x0, x2);
+      Y[u] = make_float2(y0, y2);
+      Yn[u] = make_float2(-y0, -y2);
     }
+    const float fq00 = fq0 * fq0, fq22 = fq2 * fq2;
+    const float rmax2 = (float)(anc.w * anc.w);
     for (int c0 = 0; c0 < a.ncol; c0 += BW_COLS) {
       float part[BW_TPT][6];  // FP32 sums over one chunk of pixels, folded into FP64 below
 #pragma unroll
@@ -239,6 +250,7 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
         for (int q = 0; q < 6; ++q) part[u][q] = 0.f;
       const int nc = min(BW_COLS, a.ncol - c0);
       __syncthreads();
+      int wide = 0;  // some staged pixel has |q_par| x (tile's largest offset) above 8 pi
       for (int i = threadIdx.x; i < nc; i += BW_THREADS) {
         long p = (long)row * a.ncol + c0 + i;
         const double qx = a.qx[p], qy = a.qy[p];
@@ -246,38 +258,48 @@ __global__ void __launch_bounds__(BW_THREADS) mesh_backward_kernel(BwArgs a) {
         w -= rint(w);
         float sa, ca;
         sincospif((float)(2.0 * w), &sa, &ca);
-        s_px[3 * i] = make_float4((float)qx, (float)qy, 0.f, 0.f);
-        s_px[3 * i + 1] = rotate2(a.seeds[2 * p], ca, sa);
-        s_px[3 * i + 2] = rotate2(a.seeds[2 * p + 1], ca, sa);
+        const float fx = (float)qx, fy = (float)qy;
+        wide |= (fx * fx + fy * fy) * rmax2 > BW_WIDE_PHASE2;
+        s_px[3 * i] = make_float4(fx, fy, 0.f, 0.f);
+        // the seeds (P03, M03) and (P21, M21) interleaved, so that each FP32x2 operand below is
+        // an aligned register pair of one shared-memory load: (P03r, P21r, P03i, P21i) and
+        // (M03r, M21r, M03i, M21i)
+        const float4 s03 = rotate2(a.seeds[2 * p], ca, sa), s21 = rotate2(a.seeds[2 * p + 1], ca, sa);
+        s_px[3 * i + 1] = make_float4(s03.x, s21.x, s03.y, s21.y);
+        s_px[3 * i + 2] = make_float4(s03.z, s21.z, s03.w, s21.w);
       }
-      __syncthreads();
+      wide = __syncthreads_or(wide);
       for (int i = 0; i < nc; ++i) {
         const float4 q = s_px[3 * i];
-        const float4 s03 = s_px[3 * i + 1];  // (P03, M03)
-        const float4 s21 = s_px[3 * i + 2];  // (P21, M21)
+        const float4 A = s_px[3 * i + 1], B = s_px[3 * i + 2];
+        const float2 sx = make_float2(A.x, A.y), sy = make_float2(A.z, A.w);
+        const float2 sz = make_float2(B.x, B.y), sw = make_float2(B.z, B.w);
 #pragma unroll
         for (int u = 0; u < BW_TPT; ++u) {
-          float tt = fmaf(q.x, cx[u], q.y * cy[u]) * 0.159154943091895336f;  // turns
-          float rr = tt - ((tt + 12582912.0f) - 12582912.0f);  // exact reduction, |tt| < 2^22
+          float tp = fmaf(q.x, cx[u], q.y * cy[u]);  // in-plane phase offset, radians
+          if (wide) {  // reduced to [-pi, pi] before the SFU
+            const float tt = tp * 0.159154943091895336f;
+            tp = (tt - ((tt + 12582912.0f) - 12582912.0f)) * 6.28318530717958648f;
+          }
           float sn, cs;
-          __sincosf(rr * 6.28318530717958648f, &sn, &cs);
-          float aq = fmaf(q.x, nx[u], q.y * ny[u]);
-          // Psi_03 = P03 x0 + i M03 y0 ; B03 = M03 x0 + i P03 y0 (likewise 21)
-          float p03r = s03.x * x0[u] - s03.w * y0[u], p03i = s03.y * x0[u] + s03.z * y0[u];
-          float b03r = s03.z * x0[u] - s03.y * y0[u], b03i = s03.w * x0[u] + s03.x * y0[u];
-          float p21r = s21.x * x2[u] - s21.w * y2[u], p21i = s21.y * x2[u] + s21.z * y2[u];
-          float b21r = s21.z * x2[u] - s21.y * y2[u], b21i = s21.w * x2[u] + s21.x * y2[u];
-          float psr = p03r + p21r, psi = p03i + p21i;
-          float pzr = fq0 * b03r + fq2 * b21r, pzi = fq0 * b03i + fq2 * b21i;
-          float pzzr = fq0 * fq0 * p03r + fq2 * fq2 * p21r, pzzi = fq0 * fq0 * p03i + fq2 * fq2 * p21i;
+          __sincosf(tp, &sn, &cs);
+          const float aq = fmaf(q.x, nx[u], q.y * ny[u]);
+          // Psi_03 = P03 x0 + i M03 y0, B03 = M03 x0 + i P03 y0 (likewise 21), as pairs (03, 21)
+          const float2 pr = __ffma2_rn(sw, Yn[u], __fmul2_rn(sx, X[u]));  // Re Psi
+          const float2 pim = __ffma2_rn(sz, Y[u], __fmul2_rn(sy, X[u]));  // Im Psi
+          const float2 br = __ffma2_rn(sy, Yn[u], __fmul2_rn(sz, X[u]));  // Re B
+          const float2 bim = __ffma2_rn(sx, Y[u], __fmul2_rn(sw, X[u]));  // Im B
+          const float psr = pr.x + pr.y, psi = pim.x + pim.y;
+          const float pzr = fq0 * br.x + fq2 * br.y, pzi = fq0 * bim.x + fq2 * bim.y;
+          const float pzzr = fq00 * pr.x + fq22 * pr.y, pzzi = fq00 * pim.x + fq22 * pim.y;
           // E * Psi etc.
-          float eR = cs * psr - sn * psi, eI = cs * psi + sn * psr;
-          float ezR = cs * pzr - sn * pzi, ezI = cs * pzi + sn * pzr;
-          float ezzI = cs * pzzi + sn * pzzr;
+          const float eR = cs * psr - sn * psi, eI = cs * psi + sn * psr;
+          const float ezR = cs * pzr - sn * pzi, ezI = cs * pzi + sn * pzr;
+          const float ezzI = cs * pzzi + sn * pzzr;
           part[u][0] = fmaf(eR, q.x, part[u][0]);
           part[u][1] = fmaf(eR, q.y, part[u][1]);
           part[u][2] += ezR;
-          float gxy = fmaf(aq, eI, nz[u] * ezI);
+          const float gxy = fmaf(aq, eI, nz[u] * ezI);
           part[u][3] = fmaf(-gxy, q.x, part[u][3]);
           part[u][4] = fmaf(-gxy, q.y, part[u][4]);
           part[u][5] -= fmaf(aq, ezI, nz[u] * ezzI);
