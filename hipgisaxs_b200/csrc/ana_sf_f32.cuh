@@ -116,6 +116,62 @@ __device__ __forceinline__ cf ff_analytic_f32c(const AnaShape& a, const double* 
 }
 
 // an integer-valued k (|k| < 2^51) is odd
+// The quad of four lanes (one per DWBA block) of the fused grain kernel: the sum of v over the
+// quad, the same bits in every lane (an xor butterfly of commutative adds).
+__device__ __forceinline__ float quad_sum(float v) {
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  return v;
+}
+
+// ff_analytic_f32c for a quad whose rotated in-plane q (m[0], m[1]) is the same in its four
+// lanes (the element's rotation keeps qz out of them): what depends on the in-plane q only - the
+// cylinder's radial sum, the box's x and y sums - is split among the lanes (lane k takes the
+// samples k, k + 4, ...) and summed by quad_sum; the qz parts stay per lane.  Every lane of the
+// warp calls it (shuffles); the sphere, whose |q| involves qz, keeps ff_analytic_f32c.
+template <int SHAPE>
+__device__ __forceinline__ cf ff_analytic_f32c_quad(const AnaShape& a, const double* m, const double* tv, int k) {
+  const Dist& X = a.d[0];
+  const Dist& Y = a.d[1];
+  const Dist& Z = a.d[2];
+  if (SHAPE == SH_CYLINDER) {
+    const double qpar = sqrt(m[0] * m[0] + m[1] * m[1]);
+    float fr = 0.f;
+    for (int i = k; i < X.n; i += 4) {
+      const double r = X.v[i], x = qpar * r;
+      if (x * x > CUTINY_REF) fr += (float)(2. * PI_REF * r * r) * (j1f((float)x) / (float)x);
+    }
+    fr = quad_sum(fr);
+    cf gh{0.f, 0.f};
+    for (int i = 0; i < Z.n; ++i) {
+      const double h = Z.v[i], x = m[2] * 0.5 * h;
+      const cf e = expi_f(x);
+      gh = cadd(gh, cscale(e, sinc_from(x, e.y) * (float)h));
+    }
+    return with_phase_f(cscale(gh, fr), m, tv);
+  } else if (SHAPE == SH_BOX) {
+    float sx = 0.f, sy = 0.f;
+    for (int i = k; i < X.n; i += 4) {
+      const double x = m[0] * 0.5 * X.v[i];
+      sx += sinc_from(x, expi_f(x).y) * (float)(X.v[i] * X.w[i]);
+    }
+    for (int i = k; i < Y.n; i += 4) {
+      const double x = m[1] * 0.5 * Y.v[i];
+      sy += sinc_from(x, expi_f(x).y) * (float)(Y.v[i] * Y.w[i]);
+    }
+    sx = quad_sum(sx);
+    sy = quad_sum(sy);
+    cf sz{0.f, 0.f};
+    for (int i = 0; i < Z.n; ++i) {
+      const double x = m[2] * 0.5 * Z.v[i];
+      const cf e = expi_f(x);
+      sz = cadd(sz, cscale(e, sinc_from(x, e.y) * (float)(Z.v[i] * Z.w[i])));
+    }
+    return with_phase_f(cscale(sz, sx * sy), m, tv);
+  }
+  return ff_analytic_f32c<SHAPE>(a, m, tv);
+}
+
 __device__ __forceinline__ bool odd_integer(double k) { return 0.5 * k != round_fp64(0.5 * k); }
 
 __device__ __forceinline__ float sinpi_f32(float x) {  // |x| <= 1

@@ -749,6 +749,9 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
                                                       (double*)b->d_out.p);
     HGX_CUDA(cudaMemcpyAsync(b->h_out, b->d_out.p, sizeof(double) * 5 * b->ncand,
                              cudaMemcpyDeviceToHost, st));
+    // the context's device error word beside the results (read after the one synchronisation)
+    HGX_CUDA(cudaMemcpyAsync(b->h_out + 5 * b->ncand, b->ctx->d_err, sizeof(unsigned),
+                             cudaMemcpyDeviceToHost, st));
   }
   HGX_CUDA(cudaGetLastError());
   return HGX_OK;
@@ -845,7 +848,7 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
     return s;
   };
   if (cudaMallocHost(&b->h_cands, sizeof(CylCand) * ncand) != cudaSuccess ||
-      cudaMallocHost(&b->h_out, sizeof(double) * 5 * ncand) != cudaSuccess)
+      cudaMallocHost(&b->h_out, sizeof(double) * (5 * ncand + 1)) != cudaSuccess)
     return bail(fail(HGX_ERR_NO_MEMORY, "hgx_cyl_batch_create: pinned host memory"));
   long px = 0, rows = 0;
   for (int i = 0; i < ncand; ++i) {
@@ -940,8 +943,14 @@ int hgx_cyl_batch_eval(hgx_cyl_batch_s* b, const double* models, double* out) {
   }
   HGX_CUDA(cudaGraphLaunch(b->exec, st));
   HGX_CUDA(cudaStreamSynchronize(st));
+  unsigned err = 0;
+  memcpy(&err, b->h_out + 5 * b->ncand, sizeof(unsigned));
+  if (err) {  // as hgx_synchronize reports the context's device error bits
+    cudaMemset(b->ctx->d_err, 0, sizeof(unsigned));
+    return fail(HGX_ERR_DEVICE, "hgx_cyl_batch_eval: device error bits set by a kernel on this context");
+  }
   for (int i = 0; i < 5 * b->ncand; ++i) out[i] = b->h_out[i];
-  return hgx_synchronize(b->ctx);
+  return HGX_OK;
 }
 
 // Model intensity of every candidate (no chi^2): intensity = concatenated ROI images.

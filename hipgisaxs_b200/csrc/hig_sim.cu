@@ -284,7 +284,11 @@ __global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
       double m[3];
 #pragma unroll
       for (int j = 0; j < 3; ++j) m[j] = er[3 * j] * qx + er[3 * j + 1] * qy + er[3 * j + 2] * qz;
-      const cf eff = ff_analytic_f32c<SHAPE>(shapes[e], m, elems[e].loc);
+      // the same grain and element in every lane of the warp: the test is warp-uniform; the
+      // split pays when the in-plane sums have four samples or more
+      const cf eff = (er[2] == 0.0 && er[5] == 0.0 && shapes[e].d[0].n >= 4)
+                         ? ff_analytic_f32c_quad<SHAPE>(shapes[e], m, elems[e].loc, k)
+                         : ff_analytic_f32c<SHAPE>(shapes[e], m, elems[e].loc);
       ff = cadd(ff, cmul(cf{(float)elems[e].dre, (float)elems[e].dim}, eff));
     }
     double mr[3];
