@@ -21,6 +21,7 @@ enum { SH_BOX = 2, SH_CUBE = 3, SH_CYLINDER = 4, SH_SPHERE = 5, SH_PRISM3 = 8, S
 
 struct Dist {
   int n;
+  int prog;  // the values form an arithmetic progression (n >= 3, within 1e-12 relative)
   double v[ANA_MAXV];
   double w[ANA_MAXV];
 };

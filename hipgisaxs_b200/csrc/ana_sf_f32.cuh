@@ -51,6 +51,61 @@ __device__ __forceinline__ cf with_phase_f(cf v, const double* m, const double* 
   return cmul(v, expi_f(m[0] * tv[0] + m[1] * tv[1] + m[2] * tv[2]));
 }
 
+// an integer-valued k (|k| < 2^51) is odd
+__device__ __forceinline__ bool odd_integer(double k) { return 0.5 * k != round_fp64(0.5 * k); }
+
+__device__ __forceinline__ float sinpi_f32(float x) {  // |x| <= 1
+  float s, c;
+  sincospi_f32(x, &s, &c);
+  return s;
+}
+
+// sin(pi n u) / sin(pi u) for an integer n >= 1 at an unreduced u (FP64): the sum of
+// e^{2 pi i u (j - (n-1)/2)} over j = 0 .. n-1.  u = k + t with |t| <= 1/2 exactly (FP64); the
+// value is (-1)^(k(n-1)) times the same at t; near t = 0 (|pi n t| < 1/2) the series
+// n [1 - (n^2-1) x^2/6 + (n^2-1)(3n^2-7) x^4/360 - (n^2-1)(3n^4-18n^2+31) x^6/15120], x = pi t
+// (the next term is below 1e-8 of n), elsewhere the two sines with n t reduced modulo 2 in FP64.
+__device__ __forceinline__ float dirichlet_sum_f32(double u, int n) {
+  const double k = round_fp64(u), t = u - k;
+  const bool flip = ((n - 1) & 1) && odd_integer(k);
+  const float nf = (float)n, x = 3.14159265358979f * (float)t;
+  float r;
+  if (fabsf(nf * x) < 0.5f) {
+    const float n2 = nf * nf, x2 = x * x, a = n2 - 1.0f;
+    r = nf * (1.0f - x2 * (a * (1.0f / 6.0f) -
+                           x2 * (a * (3.0f * n2 - 7.0f) * (1.0f / 360.0f) -
+                                 x2 * a * ((3.0f * n2 - 18.0f) * n2 + 31.0f) * (1.0f / 15120.0f))));
+  } else {
+    const double v = (double)n * t;
+    r = sinpi_f32((float)(v - 2.0 * round_fp64(0.5 * v))) / sinpi_f32((float)t);
+  }
+  return flip ? -r : r;
+}
+
+// The height sum of the cylinder, sum_j h_j sinc(qz h_j/2) e^{i qz h_j/2} over its samples
+// (unweighted, as the reference sums them).  Each term is (e^{i qz h_j} - 1)/(i qz); when the
+// samples are evenly stepped, h_j = h_0 + j d (the reference's distributions), the
+// exponentials sum to e^{i qz h_mid} sin(n qz d/2)/sin(qz d/2), so the sum costs one complex
+// exponential, two sines and a division instead of n of each.  Where |qz| h_max < 1/2 the
+// difference from n would cancel: there, and for other samples, the per-sample sum.
+__device__ __forceinline__ cf cyl_height_sum_f32(const Dist& Z, double qz) {
+  const int n = Z.n;
+  if (Z.prog && fabs(qz) * fmax(fabs(Z.v[0]), fabs(Z.v[n - 1])) >= 0.5) {
+    const double d = (Z.v[n - 1] - Z.v[0]) / (n - 1);
+    const float D = dirichlet_sum_f32(qz * d * INV_2PI_A, n);
+    const cf e = expi_f(qz * 0.5 * (Z.v[0] + Z.v[n - 1]));
+    const float re = e.x * D - (float)n, im = e.y * D, iq = (float)(1.0 / qz);
+    return cf{im * iq, -re * iq};
+  }
+  cf gh{0.f, 0.f};
+  for (int i = 0; i < n; ++i) {
+    const double h = Z.v[i], x = qz * 0.5 * h;
+    const cf e = expi_f(x);
+    gh = cadd(gh, cscale(e, sinc_from(x, e.y) * (float)h));
+  }
+  return gh;
+}
+
 // (sin x - x cos x) / x^3 of the sphere, by its series below x = 0.5 (where the difference
 // cancels in FP32)
 __device__ __forceinline__ float sphere_kernel_f(double x) {
@@ -77,12 +132,7 @@ __device__ __forceinline__ cf ff_analytic_f32c(const AnaShape& a, const double* 
       const double r = X.v[i], x = qpar * r;
       if (x * x > CUTINY_REF) fr += (float)(2. * PI_REF * r * r) * (j1f((float)x) / (float)x);
     }
-    cf gh{0.f, 0.f};
-    for (int i = 0; i < Z.n; ++i) {
-      const double h = Z.v[i], x = m[2] * 0.5 * h;
-      const cf e = expi_f(x);
-      gh = cadd(gh, cscale(e, sinc_from(x, e.y) * (float)h));
-    }
+    const cf gh = cyl_height_sum_f32(Z, m[2]);
     out = with_phase_f(cscale(gh, fr), m, tv);
   } else if (SHAPE == SH_SPHERE) {  // ff_ana_sphere.cpp:33-45,95-107 (weighted)
     const double q = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
@@ -115,7 +165,6 @@ __device__ __forceinline__ cf ff_analytic_f32c(const AnaShape& a, const double* 
   return out;
 }
 
-// an integer-valued k (|k| < 2^51) is odd
 // The quad of four lanes (one per DWBA block) of the fused grain kernel: the sum of v over the
 // quad, the same bits in every lane (an xor butterfly of commutative adds).
 __device__ __forceinline__ float quad_sum(float v) {
@@ -142,12 +191,7 @@ __device__ __forceinline__ cf ff_analytic_f32c_quad(const AnaShape& a, const dou
       if (x * x > CUTINY_REF) fr += (float)(2. * PI_REF * r * r) * (j1f((float)x) / (float)x);
     }
     fr = quad_sum(fr);
-    cf gh{0.f, 0.f};
-    for (int i = 0; i < Z.n; ++i) {
-      const double h = Z.v[i], x = m[2] * 0.5 * h;
-      const cf e = expi_f(x);
-      gh = cadd(gh, cscale(e, sinc_from(x, e.y) * (float)h));
-    }
+    const cf gh = cyl_height_sum_f32(Z, m[2]);
     return with_phase_f(cscale(gh, fr), m, tv);
   } else if (SHAPE == SH_BOX) {
     float sx = 0.f, sy = 0.f;
@@ -170,14 +214,6 @@ __device__ __forceinline__ cf ff_analytic_f32c_quad(const AnaShape& a, const dou
     return with_phase_f(cscale(sz, sx * sy), m, tv);
   }
   return ff_analytic_f32c<SHAPE>(a, m, tv);
-}
-
-__device__ __forceinline__ bool odd_integer(double k) { return 0.5 * k != round_fp64(0.5 * k); }
-
-__device__ __forceinline__ float sinpi_f32(float x) {  // |x| <= 1
-  float s, c;
-  sincospi_f32(x, &s, &c);
-  return s;
 }
 
 // sin(N theta_r / 2) / sin(theta_r / 2) on the principal angle theta_r of e^{i theta}
