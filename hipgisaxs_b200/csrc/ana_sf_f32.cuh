@@ -256,4 +256,22 @@ __device__ __forceinline__ cf sf_lattice_f32c(const SfLat& L, const double* m) {
   return cmul(t3, cscale(sb, sa * sc));
 }
 
+// sf_lattice_f32c for a quad whose rotated in-plane q is the same in its four lanes, with an
+// in-plane a vector and an integer b repetition: the a- and b-axis factors do not depend on
+// the block, so the even lanes evaluate the a factor and the odd lanes the b factor (the same
+// code on other arguments) and a shuffle exchanges them; the c factor and the centre phase
+// stay per lane.  Every lane of the warp calls it.
+__device__ __forceinline__ cf sf_lattice_f32c_paired(const SfLat& L, const double* m, int k) {
+  const bool odd = (k & 1) != 0;
+  const double th = odd ? m[0] * L.lb[0] + m[1] * L.lb[1] + L.lb[2] * L.lb[2]
+                        : m[0] * L.la[0] + m[1] * L.la[1] + m[2] * L.la[2];
+  const float own = dirichlet_principal(th, odd ? L.rep[1] : L.rep[0]);
+  const float other = __shfl_xor_sync(0xffffffffu, own, 1);
+  const float sa = odd ? other : own, sb = odd ? own : other;
+  const double tc = m[0] * L.lc[0] + m[1] * L.lc[1] + m[2] * L.lc[2];
+  const float sc = dirichlet_principal(tc, L.rep[2]);
+  const cf t3 = expi_f(m[0] * L.center[0] + m[1] * L.center[1] + m[2] * L.center[2]);
+  return cscale(t3, sb * sa * sc);
+}
+
 }  // namespace hgx

@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
 #pragma unroll
     for (int j = 0; j < 3; ++j) mr[j] = gp[3 * j] * qx + gp[3 * j + 1] * qy + gp[3 * j + 2] * qz;
     const ScaleEntry* sp = scales + (long)g * a.nscale;
+    const bool flat = gp[2] == 0.0 && gp[5] == 0.0;  // the grain rotation keeps qz out of mr[0], mr[1]
     for (int si = 0; si < a.nscale; ++si) {
       cf sfv;
       if (a.sfbuf) {
@@ -310,7 +311,9 @@ __global__ void __launch_bounds__(128) grain_dwba_f32c_kernel(FusedArgs a) {
           L.rep[d] = sp[si].rep[d];
           L.center[d] = gp[9 + d];
         }
-        sfv = sf_lattice_f32c(L, mr);
+        // warp-uniform: the same grain and sample in every lane
+        sfv = (flat && L.la[2] == 0.0 && L.rep[1] == round_fp64(L.rep[1])) ? sf_lattice_f32c_paired(L, mr, k)
+                                                                           : sf_lattice_f32c(L, mr);
       }
       const cf term = cmul(cmul(fc, sfv), ff);
       cf sum{0.f, 0.f};
