@@ -57,24 +57,24 @@ CUB_LAUNCHES_PER_STEP = 6
 #   mesh_backward_kernel     82.5 FP32 per (pixel, triangle)   (the expression: 80)
 #   ff_exact_kernel          611 FP64 per (q-point, triangle)
 #   grain_dwba_kernel        6418 FP64 per (pixel, grain), hcp cylinders (HIG_ENSEMBLE)
-#   grain_dwba_f32c_kernel   1316 FP32 + 472 FP64 per (pixel, grain), the same description
+#   grain_dwba_f32c_kernel   1060 FP32 + 408 FP64 per (pixel, grain), the same description
 #   cyl_pixels_f32c_kernel   221 FP32 + 60 FP64 per ROI pixel (the 256-candidate batch)
 #   cyl_pixels_kernel<double>  1418 FP64 per ROI pixel (the same batch)
-#   grain_dwba_f32c_kernel   2817 FP32 + 668 FP64 and 347 XU-pipe operations per pixel (config 1)
+#   grain_dwba_f32c_kernel   1340 FP32 + 554 FP64 and 159 XU-pipe operations per pixel (config 1)
 #   grain_dwba_kernel        20170 FP64 per pixel (config 1)
 CYL_F32C_FP32_FLOP_PER_PIXEL = 221.0
 CYL_F32C_FP64_FLOP_PER_PIXEL = 60.0
 CYL_F64_FLOP_PER_PIXEL = 1418.0
-CFG1_F32C_FP32_FLOP_PER_PIXEL = 2817.0
-CFG1_F32C_FP64_FLOP_PER_PIXEL = 668.0
-CFG1_F32C_XU_PER_PIXEL = 347.0
+CFG1_F32C_FP32_FLOP_PER_PIXEL = 1340.0
+CFG1_F32C_FP64_FLOP_PER_PIXEL = 554.0
+CFG1_F32C_XU_PER_PIXEL = 159.0
 CFG1_F64_FLOP_PER_PIXEL = 20170.0
 MESH_FWD_FLOP_PER_PIXEL_TRI = FLOP_PER_PIXEL_TRI
 MESH_BWD_FLOP_PER_PIXEL_TRI = 80.0
 EXACT_FP64_FLOP_PER_EVAL = 611.0
 GRAIN_FP64_FLOP_PER_PIXEL_GRAIN = 6418.0
-GRAIN_F32C_FP32_FLOP_PER_PIXEL_GRAIN = 1316.0
-GRAIN_F32C_FP64_FLOP_PER_PIXEL_GRAIN = 472.0
+GRAIN_F32C_FP32_FLOP_PER_PIXEL_GRAIN = 1060.0
+GRAIN_F32C_FP64_FLOP_PER_PIXEL_GRAIN = 408.0
 
 
 def roofline_of(bound, flop_per_unit, units, seconds, peak, unit, source):
@@ -924,7 +924,7 @@ def main():
             hig["f32c"]["roofline"] = roofline_of(
                 "fp32", GRAIN_F32C_FP32_FLOP_PER_PIXEL_GRAIN, pg, hig["f32c"]["ms_per_simulation"] * 1e-3,
                 peak_fp32, "(pixel, grain)", "ncu executed FP32 FLOP of grain_dwba_f32c_kernel (plus 367 "
-                "FP64 per unit); issue-bound (81% in ncu; XU 29%)")
+                "FP64 per unit); issue-bound (80% in ncu; XU 26%)")
 
     cfg1 = None
     if not args.no_config1 and rank == 0 and world == 1:
@@ -933,12 +933,12 @@ def main():
         npx1 = float(cfg1["pixels"])
         t32, t64 = cfg1["f32c"]["ms"] * 1e-3, cfg1["f64"]["ms"] * 1e-3
         r32 = roofline_of("fp32", CFG1_F32C_FP32_FLOP_PER_PIXEL, npx1, t32, peak_fp32, "pixel",
-                          "ncu executed FP32 FLOP of grain_dwba_f32c_kernel (plus 668 FP64 per pixel); "
+                          "ncu executed FP32 FLOP of grain_dwba_f32c_kernel (plus 554 FP64 per pixel); "
                           "the time is the whole simulation (set-up, Fresnel coefficients, grain kernel, sums)")
         xu = CFG1_F32C_XU_PER_PIXEL * npx1 / t32 / 1e9
         r32["sfu"] = {"ops_per_unit": CFG1_F32C_XU_PER_PIXEL, "achieved_gops": xu, "peak_gops": peak_sfu,
                       "frac": xu / peak_sfu, "note": "XU-pipe thread operations (transcendentals and "
-                      "conversions); 42% busy in ncu, the kernel issue-bound (84%)"}
+                      "conversions); 29% busy in ncu, the kernel issue-bound (81%)"}
         cfg1["f32c"]["roofline"] = r32
         cfg1["f64"]["roofline"] = roofline_of("fp64", CFG1_F64_FLOP_PER_PIXEL, npx1, t64, peak_fp64, "pixel",
                                               "ncu executed FP64 FLOP of grain_dwba_kernel; the time is "
