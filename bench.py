@@ -649,8 +649,8 @@ def config1_bench(ctx, steps=3, n=1024, cpu=True):
     res["value"] = res["f32c"]["value"]
     res["fp32c_speedup_vs_fp64"] = res["f64"]["ms"] / res["f32c"]["ms"]
     res["fp32c_vs_fp64_note"] = ("beside FP32 arithmetic the FP32C grain kernel sums the cylinder heights in "
-                                 "closed form and shares the in-plane sums across a pixel's four DWBA lanes; "
-                                 "the FP64 kernel keeps the reference's per-sample sums (1e-11 parity)")
+                                 "closed form; the FP64 kernel keeps the reference's per-sample height sums "
+                                 "(1e-11 parity); both share the in-plane sums across a pixel's four lanes")
     res["timing"] = ("device image, CUDA events on the launching stream (set-up, Fresnel "
                      "coefficients, grain kernel, structure sum); e2e_ms_host_image adds the "
                      "8 MB image copy to pageable host memory")

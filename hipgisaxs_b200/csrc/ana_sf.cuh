@@ -202,6 +202,54 @@ __device__ __forceinline__ zd ff_analytic_eval(const AnaShape& a, const zd* m, c
   return out;
 }
 
+// The quad of four lanes (one per DWBA block) of the fused grain kernel: v summed over the
+// quad, the same bits in every lane (an xor butterfly of commutative adds).
+__device__ __forceinline__ zd quad_sum_zd(zd v) {
+  v.x += __shfl_xor_sync(0xffffffffu, v.x, 1);
+  v.y += __shfl_xor_sync(0xffffffffu, v.y, 1);
+  v.x += __shfl_xor_sync(0xffffffffu, v.x, 2);
+  v.y += __shfl_xor_sync(0xffffffffu, v.y, 2);
+  return v;
+}
+
+// ff_analytic_eval for a quad whose rotated in-plane q (m[0], m[1]) is the same in its four
+// lanes (the element's rotation keeps qz out of them): the cylinder's radial sum and the box's
+// x and y sums, which depend on the in-plane q only, are split among the lanes (lane k takes
+// the samples k, k + 4, ...) and closed by quad_sum_zd; the rest is per lane, as in
+// ff_analytic_eval.  Every lane of the warp calls it (shuffles).
+template <int SHAPE>
+__device__ __forceinline__ zd ff_analytic_eval_quad(const AnaShape& a, const zd* m, const double* tv, int k) {
+  const Dist& X = a.d[0];
+  const Dist& Y = a.d[1];
+  const Dist& Z = a.d[2];
+  if (SHAPE == SH_CYLINDER) {
+    zd qpar = csqrt_(m[0] * m[0] + m[1] * m[1]);
+    zd fr(0, 0), gh(0, 0);
+    for (int i = k; i < X.n; i += 4) {
+      double r = X.v[i];
+      zd t1 = qpar * r;
+      if (norm2(t1) > CUTINY_REF) fr += (zd(j1(t1.x), 0.0) * conj(t1) / norm2(t1)) * (2. * PI_REF * r * r);
+    }
+    fr = quad_sum_zd(fr);
+    for (int i = 0; i < Z.n; ++i) {
+      double h = Z.v[i];
+      gh += (sinc_free((m[2] * 0.5) * h) * h) * cexp_(((zd(0, 0.5)) * m[2]) * h);
+    }
+    return with_phase(fr * gh, m, tv);
+  }
+  if (SHAPE == SH_BOX) {
+    zd sx(0, 0), sy(0, 0), sz(0, 0);
+    for (int i = k; i < X.n; i += 4) sx += sinc_free((m[0] * 0.5) * X.v[i]) * (X.v[i] * X.w[i]);
+    for (int i = k; i < Y.n; i += 4) sy += sinc_free((m[1] * 0.5) * Y.v[i]) * (Y.v[i] * Y.w[i]);
+    sx = quad_sum_zd(sx);
+    sy = quad_sum_zd(sy);
+    for (int i = 0; i < Z.n; ++i)
+      sz += (cexp_((zd(0, 0.5) * m[2]) * Z.v[i]) * sinc_free((m[2] * 0.5) * Z.v[i])) * (Z.v[i] * Z.w[i]);
+    return with_phase(sx * sy * sz, m, tv);
+  }
+  return ff_analytic_eval<SHAPE>(a, m, tv);
+}
+
 // The lattice structure factor at the rotated q (m): the per-q-point body of the lattice
 // structure-factor kernel (sf.cu), shared with the fused grain kernel.  la/lb/lc are the
 // scaled lattice vectors.

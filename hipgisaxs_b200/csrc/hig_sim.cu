@@ -210,7 +210,10 @@ __global__ void __launch_bounds__(128, (SHAPE == SH_PYRAMID || SHAPE == 0) ? 3 :
       for (int r = 0; r < 9; ++r) Re.r[r] = er[r];
       zd m[3];
       rotate_q(Re, qx, qy, qz, m);
-      const zd eff = ff_analytic_eval<SHAPE>(shapes[e], m, elems[e].loc);
+      // the same grain and element in every lane of the warp: the test is warp-uniform
+      const zd eff = (er[2] == 0.0 && er[5] == 0.0 && shapes[e].d[0].n >= 4)
+                         ? ff_analytic_eval_quad<SHAPE>(shapes[e], m, elems[e].loc, k)
+                         : ff_analytic_eval<SHAPE>(shapes[e], m, elems[e].loc);
       const double dre = elems[e].dre, dim = elems[e].dim;
       ff.x = __dadd_rn(ff.x, __dsub_rn(__dmul_rn(dre, eff.x), __dmul_rn(dim, eff.y)));
       ff.y = __dadd_rn(ff.y, __dadd_rn(__dmul_rn(dre, eff.y), __dmul_rn(dim, eff.x)));
