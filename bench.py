@@ -61,14 +61,14 @@ CUB_LAUNCHES_PER_STEP = 6
 #   cyl_pixels_f32c_kernel   221 FP32 + 60 FP64 per ROI pixel (the 256-candidate batch)
 #   cyl_pixels_kernel<double>  1418 FP64 per ROI pixel (the same batch)
 #   grain_dwba_f32c_kernel   1340 FP32 + 554 FP64 and 159 XU-pipe operations per pixel (config 1)
-#   grain_dwba_kernel        20170 FP64 per pixel (config 1)
+#   grain_dwba_kernel        16999 FP64 per pixel (config 1)
 CYL_F32C_FP32_FLOP_PER_PIXEL = 221.0
 CYL_F32C_FP64_FLOP_PER_PIXEL = 60.0
 CYL_F64_FLOP_PER_PIXEL = 1418.0
 CFG1_F32C_FP32_FLOP_PER_PIXEL = 1340.0
 CFG1_F32C_FP64_FLOP_PER_PIXEL = 554.0
 CFG1_F32C_XU_PER_PIXEL = 159.0
-CFG1_F64_FLOP_PER_PIXEL = 20170.0
+CFG1_F64_FLOP_PER_PIXEL = 16999.0
 MESH_FWD_FLOP_PER_PIXEL_TRI = FLOP_PER_PIXEL_TRI
 MESH_BWD_FLOP_PER_PIXEL_TRI = 80.0
 EXACT_FP64_FLOP_PER_EVAL = 611.0
