@@ -491,8 +491,10 @@ __global__ void cyl_weights_kernel(const double* __restrict__ counts, const unsi
 }
 
 // per-candidate sums of the items' partials, fixed order
+// (block 0 also copies the context's device error word behind the results, so that one copy
+// brings both back)
 __global__ void cyl_final_kernel(const CylCand* __restrict__ cands, const double* __restrict__ partial,
-                                 double* __restrict__ out) {
+                                 double* __restrict__ out, const unsigned* __restrict__ err, int ncand) {
   __shared__ double sh[(CYL_THREADS / 32) * 5];
   const CylCand& c = cands[blockIdx.x];
   double acc[5] = {0, 0, 0, 0, 0};
@@ -500,9 +502,15 @@ __global__ void cyl_final_kernel(const CylCand* __restrict__ cands, const double
 #pragma unroll
     for (int q = 0; q < 5; ++q) acc[q] += partial[5 * (c.item0 + i) + q];
   block_sum5<CYL_THREADS>(acc, sh);
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) out[5 * blockIdx.x + q] = acc[q];
+    if (blockIdx.x == 0) {
+      double e = 0.0;
+      *reinterpret_cast<unsigned*>(&e) = *err;
+      out[5 * ncand] = e;
+    }
+  }
 }
 
 // Launches tile shape `shape` of the pixel pass (a recursion over the shape table, so each
@@ -746,11 +754,10 @@ static int cyl_enqueue(hgx_cyl_batch_s* b, bool with_counts, bool with_intensity
   if (with_counts) {
     cyl_final_kernel<<<b->ncand, CYL_THREADS, 0, st>>>((const CylCand*)b->d_cands.p,
                                                       (const double*)b->d_partial.p,
-                                                      (double*)b->d_out.p);
-    HGX_CUDA(cudaMemcpyAsync(b->h_out, b->d_out.p, sizeof(double) * 5 * b->ncand,
-                             cudaMemcpyDeviceToHost, st));
-    // the context's device error word beside the results (read after the one synchronisation)
-    HGX_CUDA(cudaMemcpyAsync(b->h_out + 5 * b->ncand, b->ctx->d_err, sizeof(unsigned),
+                                                      (double*)b->d_out.p, b->ctx->d_err, b->ncand);
+    // the results and, behind them, the context's device error word (read after the one
+    // synchronisation)
+    HGX_CUDA(cudaMemcpyAsync(b->h_out, b->d_out.p, sizeof(double) * (5 * b->ncand + 1),
                              cudaMemcpyDeviceToHost, st));
   }
   HGX_CUDA(cudaGetLastError());
@@ -867,7 +874,7 @@ int hgx_cyl_batch_create(hgx_ctx c, hgx_qgrid g, const double* rowfc, const doub
   b->nrowtab = rows;
   int s = HGX_OK;
   if ((s = b->d_cands.reserve(sizeof(CylCand) * ncand)) || (s = b->d_tab.reserve(sizeof(RowTab) * rows)) ||
-      (s = b->d_out.reserve(sizeof(double) * 5 * ncand)) || (s = b->d_rowfc.reserve(sizeof(double2) * 4 * g->nrow)) ||
+      (s = b->d_out.reserve(sizeof(double) * (5 * ncand + 1))) || (s = b->d_rowfc.reserve(sizeof(double2) * 4 * g->nrow)) ||
       (s = b->d_inten.reserve(sizeof(double) * px)))
     return bail(s);
   cudaStream_t st = c->stream;
