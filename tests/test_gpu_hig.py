@@ -378,3 +378,30 @@ def test_objective_gradient_refuses_what_it_cannot_differentiate(ctx, po):
     with pytest.raises(hg.HgxError):
         d2.objective_grad(ctx, [float(v) for v in range(len(d2.fit_keys()))],
                           np.ones(d2.image_size()), None, "sqrt_unit_l2")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["paracrystal.hig", "percus_yevick.hig"])
+def test_population_with_liquid_structure_factors(ctx, po, tmp_path, name):
+    """A population over a sphere radius where the structure factor is grain-independent
+    (paracrystal, Percus-Yevick: made once at creation and shared by every candidate): each
+    distance equals hgx_hig_objective's (1e-12), FP32C within 1e-5."""
+    text = open(os.path.join(HIG, name)).read().rstrip().rstrip("}").rstrip()
+    text += (',\n\tfitting = {\n\t\tfitparam = { key = "r", variable = "shape[\'sph\']:param[\'radius\']:min", '
+             'range = { min = 3, max = 7 }, init = 5 },\n\t\talgorithm = { algoname = "pso", '
+             'distancemetric = "sqrt_unit_l2" }\n\t}\n}\n')
+    path = tmp_path / name
+    path.write_text(text)
+    d = read_hig(str(path))
+    d.fit_update([5.3])
+    ref_img = po.compute_gisaxs(d.data, HIG).ravel()
+    X = np.array([[4.1], [4.9], [5.3], [6.2], [6.8]])
+    pop = d.population(ctx, len(X), ref_img, None, "sqrt_unit_l2", 0.1)
+    pop32 = d.population(ctx, len(X), ref_img, None, "sqrt_unit_l2", 0.1, "f32c")
+    got, got32 = pop.eval(X), pop32.eval(X)
+    for i, x in enumerate(X):
+        want = d.objective(ctx, x, ref_img, None, "sqrt_unit_l2", 0.1)[0]
+        assert abs(got[i] - want) <= 1e-12 * abs(want), (i, got[i], want)
+        assert abs(got32[i] - want) <= 1e-5 * abs(want), (i, got32[i], want)
+    pop.close()
+    pop32.close()
