@@ -42,7 +42,7 @@ PI_REF = 3.141592653589793
 FLOP_PER_PIXEL_TRI = 40.0
 SFU_PER_PIXEL_TRI = 2.0
 # DRAM bytes per launch of the row kernel: ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one 2048 x 2048 launch with 50,000 triangles (75.2 MB + 84.7 MB; profiles/ff_tri_rows_mesh50k.md)
+# of one 2048 x 2048 launch with 50,000 triangles (75.2 MB read + 84.7 MB written)
 TRAFFIC_BYTES_PER_LAUNCH = 159.9e6
 TRAFFIC_SOURCE = "ncu capture of a 2048x2048 launch (75.2 MB read + 84.7 MB write)"
 # the library's kernels per form-factor step (bounding box 2, Morton keys, tiles, row kernel);
@@ -53,7 +53,7 @@ CUB_LAUNCHES_PER_STEP = 6
 
 # Executed FLOP per unit of the other timed kernels, from ncu thread-instruction counts
 # (2 x FMA + MUL + ADD of each precision) of one launch on the bench's own descriptions,
-# recorded in profiles/roofline_other_kernels.md:
+# each from an ncu capture of its kernel on the workload below:
 #   mesh_backward_kernel     82.5 FP32 per (pixel, triangle)   (the expression: 80)
 #   ff_exact_kernel          611 FP64 per (q-point, triangle)
 #   grain_dwba_kernel        6418 FP64 per (pixel, grain), hcp cylinders (HIG_ENSEMBLE)

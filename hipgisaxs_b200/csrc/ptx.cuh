@@ -1,4 +1,4 @@
-// Small inline-PTX helpers for sm_100a: mbarriers and TMA bulk copies (no cluster multicast).
+// Small inline-PTX helpers for sm_100a: mbarriers and TMA bulk copies into this CTA's own shared memory.
 #pragma once
 #include <stdint.h>
 
