@@ -1129,6 +1129,37 @@ int ff_triangles_device(hgx_ctx c, hgx_qgrid g, const double* sd, int ntri, cons
   }
 }
 
+static size_t esz_of(int ff_type) { return ff_type == HGX_C64 ? sizeof(float2) : sizeof(double2); }
+
+// The triangle tuples on the device: the caller's array, or a copy in the context's staging.
+static int stage_shape_def(hgx_ctx c, const double* shape_def, int ntri, const double** sd) {
+  *sd = shape_def;
+  if (is_device_ptr(shape_def)) return HGX_OK;
+  HGX_TRY(c->staging.reserve(sizeof(double) * 8 * (size_t)ntri));
+  HGX_CUDA(cudaMemcpyAsync(c->staging.p, shape_def, sizeof(double) * 8 * (size_t)ntri,
+                           cudaMemcpyHostToDevice, c->stream));
+  *sd = reinterpret_cast<const double*>(c->staging.p);
+  return HGX_OK;
+}
+
+// Where the kernels write a form factor of `bytes` for the caller's ff: device memory itself;
+// page-locked host memory mapped into the device's address space directly (the kernels' stores
+// cross the bus while they run, so no copy follows them); other host memory through the
+// context's output staging (*staged: the caller copies it back after the kernels).
+static int output_view(hgx_ctx c, void* ff, size_t bytes, void** dout, bool* staged) {
+  *staged = false;
+  *dout = ff;
+  if (is_device_ptr(ff)) return HGX_OK;
+  if (void* m = mapped_host_ptr(ff)) {
+    *dout = m;
+    return HGX_OK;
+  }
+  HGX_TRY(c->shaped_out.reserve(bytes));
+  *dout = c->shaped_out.p;
+  *staged = true;
+  return HGX_OK;
+}
+
 }  // namespace hgx
 
 using namespace hgx;
@@ -1147,26 +1178,15 @@ int hgx_ff_triangles_q_ex(hgx_ctx c, hgx_qgrid g, const double* shape_def, int n
   if (g->ctx != c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles_q: grid of another context");
   HGX_CUDA(cudaSetDevice(c->device));
   cudaStream_t st = c->stream;
-  const double* sd = shape_def;
-  if (!is_device_ptr(shape_def)) {
-    HGX_TRY(c->staging.reserve(sizeof(double) * 8 * (size_t)ntri));
-    HGX_CUDA(cudaMemcpyAsync(c->staging.p, shape_def, sizeof(double) * 8 * (size_t)ntri,
-                             cudaMemcpyHostToDevice, st));
-    sd = reinterpret_cast<const double*>(c->staging.p);
-  }
-  const size_t esz = ff_type == HGX_C64 ? sizeof(float2) : sizeof(double2);
+  const double* sd = nullptr;
+  HGX_TRY(stage_shape_def(c, shape_def, ntri, &sd));
   const bool host_out = !is_device_ptr(ff);
-  void* dout = ff;
-  if (host_out) {  // the context's output staging (the call synchronises before returning)
-    HGX_TRY(c->shaped_out.reserve(esz * (size_t)g->nqz));
-    dout = c->shaped_out.p;
-  }
+  bool staged = false;
+  void* dout = nullptr;
+  HGX_TRY(output_view(c, ff, esz_of(ff_type) * (size_t)g->nqz, &dout, &staged));
   HGX_TRY(ff_triangles_device(c, g, sd, ntri, rot9, precision, dout, ff_type, pixels));
-  if (host_out) {
-    HGX_CUDA(cudaMemcpyAsync(ff, dout, esz * (size_t)g->nqz, cudaMemcpyDeviceToHost, st));
-    return hgx_synchronize(c);
-  }
-  return HGX_OK;
+  if (staged) HGX_CUDA(cudaMemcpyAsync(ff, dout, esz_of(ff_type) * (size_t)g->nqz, cudaMemcpyDeviceToHost, st));
+  return host_out ? hgx_synchronize(c) : HGX_OK;
 }
 
 int hgx_ff_triangles_q(hgx_ctx c, hgx_qgrid g, const double* shape_def, int ntri,
@@ -1253,10 +1273,39 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
   if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_ff_triangles: null context");
   HGX_CUDA(cudaSetDevice(c->device));
   hgx_qgrid g = nullptr;
-  HGX_TRY(shaped_grid(c, nqy, qx, qy, nqz, qz, &g));
-  int s = hgx_ff_triangles_q(c, g, shape_def, ntri, rot9, precision, ff, HGX_C128);
-  if (s == HGX_OK && is_device_ptr(ff)) s = hgx_synchronize(c);
-  return s;
+  bool rows_first = false;
+  if (precision == HGX_F32C && shape_def && ff && qx && qy && qz)
+    HGX_TRY(shaped_rows_begin(c, nqy, qx, qy, nqz, qz, &g, &rows_first));
+  else
+    HGX_TRY(shaped_grid(c, nqy, qx, qy, nqz, qz, &g));
+  if (!rows_first) {
+    int s = hgx_ff_triangles_q(c, g, shape_def, ntri, rot9, precision, ff, HGX_C128);
+    if (s == HGX_OK && is_device_ptr(ff)) s = hgx_synchronize(c);
+    return s;
+  }
+  // The row kernel runs from qx, qy and the row table while the side stream copies the 4N qz
+  // values and checks them; a grid that fails the check (qz not constant along its rows, or
+  // blocks that do not pair as the first q-points of the rows suggested) is finalized from the
+  // full qz and the form factor computed again.
+  const double* sd = nullptr;
+  HGX_TRY(stage_shape_def(c, shape_def, ntri, &sd));
+  bool staged = false;
+  void* dout = nullptr;
+  HGX_TRY(output_view(c, ff, sizeof(double2) * (size_t)nqz, &dout, &staged));
+  int s = ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, dout, HGX_C128, 0);
+  const int s_check = shaped_rows_check(c, g, qz);
+  bool ok = true;
+  const int s_settle = shaped_rows_settle(c, g, &ok);
+  if (s == HGX_OK) s = s_check;
+  if (s == HGX_OK) s = s_settle;
+  if (s == HGX_OK && !ok) s = ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, dout, HGX_C128, 0);
+  if (s == HGX_OK && staged)
+    HGX_CUDA(cudaMemcpyAsync(ff, dout, sizeof(double2) * (size_t)nqz, cudaMemcpyDeviceToHost, c->stream));
+  if (s != HGX_OK) {
+    cudaStreamSynchronize(c->stream);  // leave nothing of this call queued behind the error
+    return s;
+  }
+  return hgx_synchronize(c);
 }
 
 }  // extern "C"

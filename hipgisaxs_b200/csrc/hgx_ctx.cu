@@ -35,6 +35,16 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+void* mapped_host_ptr(const void* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 int DevBuf::reserve(size_t n) {
   if (n <= bytes) return HGX_OK;
   release();
@@ -70,7 +80,7 @@ __global__ void row_table_kernel(const double2* __restrict__ qz, int nqy, int nk
     double2 v = qz[(long)k * nqy + p];
     double2 f = qz[(long)k * nqy + first];
     if (v.x != f.x || v.y != f.y) row_ok = false;
-    if (p == first) rowqz[(long)row * nk + k] = v;
+    if (rowqz && p == first) rowqz[(long)row * nk + k] = v;
     if (v.y != 0.0) paired = false;
   }
   if (nk == 4) {
@@ -168,6 +178,81 @@ int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz,
   return HGX_OK;
 }
 
+int shaped_rows_begin(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
+                      hgx_qgrid* out, bool* rows_first) {
+  *rows_first = false;
+  hgx_qgrid g = c->shaped;
+  if (!g || g->nqy != nqy || g->nqz != nqz || (g->nk != 1 && g->nk != 4) || is_device_ptr(qz))
+    return shaped_grid(c, nqy, qx, qy, nqz, qz, out);
+  int ncol = 0;
+  HGX_TRY(detect_ncol(g, qz, &ncol));  // host array: scans the first row only
+  if (ncol <= 0 || nqy % ncol != 0) return shaped_grid(c, nqy, qx, qy, nqz, qz, out);
+  const int nk = g->nk, nrow = nqy / ncol;
+  // each row's first q-point of every block, and whether the blocks pair (real, qz4 = -qz1,
+  // qz2 = -qz3) there; the check on the side stream holds every q-point to the same values
+  std::vector<double2> rt((size_t)nrow * nk);
+  bool paired = nk == 4;
+  for (int r = 0; r < nrow; ++r) {
+    for (int k = 0; k < nk; ++k) {
+      const double* v = qz + 2 * ((size_t)k * nqy + (size_t)r * ncol);
+      rt[(size_t)r * nk + k] = make_double2(v[0], v[1]);
+      if (v[1] != 0.0) paired = false;
+    }
+    if (nk == 4) {
+      const double2* t = &rt[(size_t)r * 4];
+      if (t[3].x != -t[0].x || t[1].x != -t[2].x) paired = false;
+    }
+  }
+  if (!c->side) {
+    HGX_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    HGX_CUDA(cudaEventCreateWithFlags(&c->side_ev, cudaEventDisableTiming));
+    HGX_CUDA(cudaMalloc(&c->side_flags, 256));
+  }
+  const size_t need = (size_t)nrow * nk;
+  if (need > g->rowqz_cap) {
+    HGX_CUDA(cudaStreamSynchronize(c->stream));  // earlier kernels may still read the old table
+    if (g->rowqz) cudaFree(g->rowqz);
+    g->rowqz = nullptr;
+    g->rowqz_cap = 0;
+    HGX_CUDA(cudaMalloc(&g->rowqz, sizeof(double2) * need));
+    g->rowqz_cap = need;
+  }
+  cudaStream_t st = c->stream;
+  auto kind = [](const void* p) { return is_device_ptr(p) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice; };
+  HGX_CUDA(cudaMemcpyAsync(g->qx, qx, sizeof(double) * nqy, kind(qx), st));
+  HGX_CUDA(cudaMemcpyAsync(g->qy, qy, sizeof(double) * nqy, kind(qy), st));
+  HGX_CUDA(cudaMemcpyAsync(g->rowqz, rt.data(), sizeof(double2) * need, cudaMemcpyHostToDevice, st));
+  // the side stream's copy of qz may start once everything queued so far has run (earlier
+  // kernels that read the grid's qz)
+  HGX_CUDA(cudaEventRecord(c->side_ev, st));
+  g->ncol = ncol;
+  g->nrow = nrow;
+  g->mode = paired ? 1 : 2;
+  *out = g;
+  *rows_first = true;
+  return HGX_OK;
+}
+
+int shaped_rows_check(hgx_ctx c, hgx_qgrid g, const double* qz) {
+  HGX_CUDA(cudaStreamWaitEvent(c->side, c->side_ev, 0));
+  HGX_CUDA(cudaMemsetAsync(c->side_flags, 0, sizeof(unsigned), c->side));
+  HGX_CUDA(cudaMemcpyAsync(g->qz, qz, sizeof(double2) * g->nqz, cudaMemcpyHostToDevice, c->side));
+  const int blocks = (g->nqy + 255) / 256;
+  row_table_kernel<<<blocks, 256, 0, c->side>>>(g->qz, g->nqy, g->nk, g->ncol, nullptr, c->side_flags);
+  HGX_CUDA(cudaGetLastError());
+  return HGX_OK;
+}
+
+int shaped_rows_settle(hgx_ctx c, hgx_qgrid g, bool* ok) {
+  unsigned flags = 0;
+  HGX_CUDA(cudaMemcpyAsync(&flags, c->side_flags, sizeof(unsigned), cudaMemcpyDeviceToHost, c->side));
+  HGX_CUDA(cudaStreamSynchronize(c->side));
+  const int mode = (flags & 1u) ? 0 : ((g->nk == 4 && !(flags & 2u)) ? 1 : 2);
+  *ok = mode == g->mode;
+  if (!*ok) HGX_TRY(qgrid_finalize(g));  // the full qz is on the device: table and mode from it
+  return HGX_OK;
+}
+
 int qgrid_finalize(hgx_qgrid g) {
   g->mode = 0;
   if (g->nk != 1 && g->nk != 4) return HGX_OK;
@@ -255,7 +340,11 @@ int hgx_destroy(hgx_ctx c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   if (c->d_err) cudaFree(c->d_err);
+  if (c->side) cudaStreamSynchronize(c->side);
   if (c->shaped) hgx_qgrid_destroy(c->shaped);
+  if (c->side) cudaStreamDestroy(c->side);
+  if (c->side_ev) cudaEventDestroy(c->side_ev);
+  if (c->side_flags) cudaFree(c->side_flags);
   delete c->mesh;
   if (c->hig && c->hig->grid) hgx_qgrid_destroy(c->hig->grid);
   delete c->hig;
@@ -268,7 +357,14 @@ int hgx_destroy(hgx_ctx c) {
 
 int hgx_set_stream(hgx_ctx c, void* stream) {
   if (!c) return fail(HGX_ERR_INVALID_ARG, "hgx_set_stream: ctx is NULL");
-  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  cudaStream_t next = reinterpret_cast<cudaStream_t>(stream);
+  if (next != c->stream) {
+    // the context's buffers are reused in stream order: work still queued on the old stream
+    // finishes before work on the new one can touch them
+    HGX_CUDA(cudaSetDevice(c->device));
+    HGX_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  c->stream = next;
   return HGX_OK;
 }
 

@@ -38,6 +38,9 @@ enum DeviceError : unsigned {
 // ------------------------------------------------------------- memory kind ----
 // True when p is device (or managed) memory usable by the current device.
 bool is_device_ptr(const void* p);
+// The device address of page-locked host memory mapped into the device's address space
+// (cudaMallocHost / cudaHostAlloc / cudaHostRegister under unified addressing), else nullptr.
+void* mapped_host_ptr(const void* p);
 
 // A device buffer owned by an object.
 struct DevBuf {
@@ -85,15 +88,26 @@ struct HigWork {
   double ext_alpha = 0.0;  // the incidence angle the grid's qz blocks were extended for
   long grid_gen = 0;       // counts the grids made, so that cached results can name theirs
   std::vector<double> fc_key;  // what the Fresnel coefficients in fc were made for
-  // pinned staging of the host tables of one simulation: bump-allocated, reset at its start
-  unsigned char* h_arena = nullptr;
-  size_t arena_cap = 0, arena_off = 0;
+  // pinned staging of the host tables of one simulation: two arenas used in turn, each
+  // bump-allocated from its start, so that the host can fill one while the stream still copies
+  // from the other (a simulation with a device image returns before its copies run); an arena
+  // is refilled only after the event recorded at the end of its last simulation has completed
+  unsigned char* h_arena[2] = {nullptr, nullptr};
+  size_t arena_cap[2] = {0, 0};
+  cudaEvent_t arena_ev[2] = {nullptr, nullptr};
+  int arena_cur = 0;
+  size_t arena_off = 0;  // nonzero between a simulation's first copy and its end
   DevBuf fc, ff, eff, sf, I, img, shapes, elems, gt, er, sc, obj, saxs_qz, ratios;
+  DevBuf ftab;  // the fused grain kernel's tables of one structure, as one block
   // the objective's gradient: the tables' changes, d(distance)/d(image), d(image)/dx
   DevBuf tshapes, telems, tgt, ter, tsc, lam, dimg;
   std::map<std::string, MeshTuples> meshes;  // by resolved path
   ~HigWork() {
-    if (h_arena) cudaFreeHost(h_arena);
+    for (int k = 0; k < 2; ++k) {
+      if (arena_ev[k]) cudaEventSynchronize(arena_ev[k]);
+      if (h_arena[k]) cudaFreeHost(h_arena[k]);
+      if (arena_ev[k]) cudaEventDestroy(arena_ev[k]);
+    }
   }
 };
 // d(image)/dx of hgx_hig_compute_gisaxs for one fit variable, added into dI (hig_sim.cu).
@@ -127,6 +141,11 @@ struct hgx_ctx_s {
   // so that those calls allocate and free no device memory
   hgx_qgrid_s* shaped = nullptr;
   hgx::DevBuf shaped_out;
+  // the reference-shaped FP32C call's side stream: it copies the 4N qz values to the kept grid
+  // and checks them while the row kernel already runs from a row table read on the host
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_ev = nullptr;    // recorded on the context's stream, waited for by the side
+  unsigned* side_flags = nullptr;   // device word: the check's flags (row_table_kernel bits)
   hgx::MeshWork* mesh = nullptr;  // work buffers of the mesh chi^2 and gradient
   hgx::HigWork* hig = nullptr;    // work of the HiG-driven simulation
 };
@@ -156,6 +175,21 @@ int qgrid_reextend(hgx_qgrid g, double alpha_i, double k0, double dn2_re, double
 // place when nqy and nqz match, else a new one (the old one destroyed).
 int shaped_grid(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
                 hgx_qgrid* out);
+// The same grid for the reference-shaped FP32C form factor with qz in host memory, the 4N qz
+// values left for later: when the kept grid has these sizes and the host qz array has a
+// detector-row layout, qx and qy are copied on the context's stream and the row table is read
+// from each row's first q-point of the host array (as row_table_kernel takes it), with the mode
+// guessed from those values; *rows_first is then true and the caller enqueues its row kernels,
+// calls shaped_rows_check(qz) and then shaped_rows_settle.  Otherwise *rows_first is false and
+// the grid is the one shaped_grid makes.
+int shaped_rows_begin(hgx_ctx c, int nqy, const double* qx, const double* qy, int nqz, const double* qz,
+                      hgx_qgrid* out, bool* rows_first);
+// Copies the host qz into the grid on the side stream, after the work already queued on the
+// context's stream, and checks there that it is constant along rows with the guessed pairing.
+int shaped_rows_check(hgx_ctx c, hgx_qgrid g, const double* qz);
+// Waits for that check.  *ok = false when the guess did not hold: the grid has then been
+// finalized from its full qz (row table, mode) and the caller runs its kernels again.
+int shaped_rows_settle(hgx_ctx c, hgx_qgrid g, bool* ok);
 // Lattice vectors a, b, c (abc9) and basis offset t3 of a lattice type (LatticeType code) and
 // hkl string; false when the type has no vectors for that hkl (sf.cu).
 bool lattice_table(int type, const std::string& hkl, double* abc9, double* t3);

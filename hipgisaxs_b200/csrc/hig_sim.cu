@@ -107,25 +107,35 @@ __global__ void image_structure_sum_kernel(const double* __restrict__ I, const d
   out[(long)blockIdx.y * n + z] = sum;
 }
 
-// Copies host data to dev through the context's pinned arena: one asynchronous copy from
-// pinned memory (a copy from pageable memory waits for the host).  The arena is reset at the
-// start of each simulation and grows only after the stream has finished reading it.
-int arena_copy(HigWork& w, cudaStream_t st, void* dev, const void* src, size_t bytes) {
-  if (!bytes) return HGX_OK;
+// Room for `bytes` in the simulation's pinned arena (*host), and copies of host data to dev
+// through it: one asynchronous copy from pinned memory (a copy from pageable memory waits for
+// the host).  The arena in use is reset at the start of each simulation and grows only after
+// the stream has finished reading it (a grown arena starts empty: earlier rooms are given up).
+int arena_block(HigWork& w, cudaStream_t st, size_t bytes, unsigned char** host) {
   const size_t step = (bytes + 255) & ~(size_t)255;
-  if (w.arena_off + step > w.arena_cap) {
-    HGX_CUDA(cudaStreamSynchronize(st));  // copies in flight still read the old arena
-    if (w.h_arena) cudaFreeHost(w.h_arena);
-    w.h_arena = nullptr;
-    w.arena_cap = 0;
+  const int k = w.arena_cur;
+  if (w.arena_off + step > w.arena_cap[k]) {
+    // copies in flight still read the old arena; the copies made so far in this simulation
+    // are complete after the synchronisation, so the new arena starts empty
+    HGX_CUDA(cudaStreamSynchronize(st));
+    if (w.h_arena[k]) cudaFreeHost(w.h_arena[k]);
+    w.h_arena[k] = nullptr;
+    w.arena_cap[k] = 0;
     w.arena_off = 0;
     const size_t cap = std::max<size_t>(2 * step, (size_t)1 << 20);
-    HGX_CUDA(cudaMallocHost(&w.h_arena, cap));
-    w.arena_cap = cap;
+    HGX_CUDA(cudaMallocHost(&w.h_arena[k], cap));
+    w.arena_cap[k] = cap;
   }
-  unsigned char* dst = w.h_arena + w.arena_off;
-  memcpy(dst, src, bytes);
+  *host = w.h_arena[k] + w.arena_off;
   w.arena_off += step;
+  return HGX_OK;
+}
+
+int arena_copy(HigWork& w, cudaStream_t st, void* dev, const void* src, size_t bytes) {
+  if (!bytes) return HGX_OK;
+  unsigned char* dst = nullptr;
+  HGX_TRY(arena_block(w, st, bytes, &dst));
+  memcpy(dst, src, bytes);
   HGX_CUDA(cudaMemcpyAsync(dev, dst, bytes, cudaMemcpyHostToDevice, st));
   return HGX_OK;
 }
@@ -870,26 +880,33 @@ static int fused_structure(hgx_ctx c, hgx_qgrid g, HigWork& w, const hig::Struct
   const std::vector<double>& gt = T.gt;
   const std::vector<double>& er = T.er;
   const int nelem = (int)elems.size();
-  DevBuf &bshapes = w.shapes, &belems = w.elems, &bgt = w.gt, &ber = w.er, &bsf = w.sf, &bsc = w.sc;
+  DevBuf& bsf = w.sf;
+  // the five tables as one block of the arena, sent in one copy
+  auto up = [](size_t o) { return (o + 255) & ~(size_t)255; };
+  const size_t o_el = up(sizeof(AnaShape) * nelem);
+  const size_t o_gt = o_el + up(sizeof(FusedElem) * nelem);
+  const size_t o_er = o_gt + up(sizeof(double) * gt.size());
+  const size_t o_sc = o_er + up(sizeof(double) * er.size());
+  const size_t total = o_sc + sizeof(ScaleEntry) * plan.size();
+  HGX_TRY(w.ftab.reserve(total));
+  unsigned char* h = nullptr;
+  HGX_TRY(arena_block(w, st, total, &h));
   if (nelem > 0) {
-    HGX_TRY(bshapes.reserve(sizeof(AnaShape) * nelem));
-    HGX_TRY(belems.reserve(sizeof(FusedElem) * nelem));
-    HGX_TRY(arena_copy(w, st, bshapes.p, shapes.data(), sizeof(AnaShape) * nelem));
-    HGX_TRY(arena_copy(w, st, belems.p, elems.data(), sizeof(FusedElem) * nelem));
+    memcpy(h, shapes.data(), sizeof(AnaShape) * nelem);
+    memcpy(h + o_el, elems.data(), sizeof(FusedElem) * nelem);
   }
-  HGX_TRY(bgt.reserve(sizeof(double) * gt.size()));
-  HGX_TRY(ber.reserve(sizeof(double) * er.size()));
-  HGX_TRY(arena_copy(w, st, bgt.p, gt.data(), sizeof(double) * gt.size()));
-  HGX_TRY(arena_copy(w, st, ber.p, er.data(), sizeof(double) * er.size()));
-  HGX_TRY(bsc.reserve(sizeof(ScaleEntry) * plan.size()));
-  HGX_TRY(arena_copy(w, st, bsc.p, plan.data(), sizeof(ScaleEntry) * plan.size()));
+  if (!gt.empty()) memcpy(h + o_gt, gt.data(), sizeof(double) * gt.size());
+  if (!er.empty()) memcpy(h + o_er, er.data(), sizeof(double) * er.size());
+  if (!plan.empty()) memcpy(h + o_sc, plan.data(), sizeof(ScaleEntry) * plan.size());
+  HGX_CUDA(cudaMemcpyAsync(w.ftab.p, h, total, cudaMemcpyHostToDevice, st));
+  const unsigned char* d = (const unsigned char*)w.ftab.p;
   FusedArgs a;
-  a.shapes = (const AnaShape*)bshapes.p;
-  a.elems = (const FusedElem*)belems.p;
+  a.shapes = (const AnaShape*)d;
+  a.elems = (const FusedElem*)(d + o_el);
   a.nelem = nelem;
-  a.grains = (const double*)bgt.p;
-  a.elem_rot = (const double*)ber.p;
-  a.scales = (const ScaleEntry*)bsc.p;
+  a.grains = (const double*)(d + o_gt);
+  a.elem_rot = (const double*)(d + o_er);
+  a.scales = (const ScaleEntry*)(d + o_sc);
   a.nscale = nscale;
   a.sfbuf = nullptr;
   if (s.type == "paracrystal") {
@@ -990,6 +1007,10 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
     HGX_CUDA(cudaStreamSynchronize(st));
     w.arena_off = 0;
   }
+  // the other arena: its last simulation's copies must have run before it is refilled (the
+  // previous simulation may still be on the stream when its image is device memory)
+  w.arena_cur ^= 1;
+  if (w.arena_ev[w.arena_cur]) HGX_CUDA(cudaEventSynchronize(w.arena_ev[w.arena_cur]));
   const double key[8] = {(double)cp.resolution[0], (double)cp.resolution[1], cp.minpoint[0], cp.minpoint[1],
                          cp.maxpoint[0], cp.maxpoint[1], alpha_i, k0};
   bool same = w.grid != nullptr;
@@ -1212,9 +1233,14 @@ int compute_at(hgx_ctx c, hgx_hig h, int precision, double alpha_deg, double phi
                                                                         nstruct, n, dimg);
   HGX_CUDA(cudaGetLastError());
   if (!dev_out) HGX_CUDA(cudaMemcpyAsync(image, dimg, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-  const int s_end = hgx_synchronize(c);
+  // the end of this simulation's work on the stream, after which its arena may be refilled
+  if (!w.arena_ev[w.arena_cur])
+    HGX_CUDA(cudaEventCreateWithFlags(&w.arena_ev[w.arena_cur], cudaEventDisableTiming));
+  HGX_CUDA(cudaEventRecord(w.arena_ev[w.arena_cur], st));
   w.arena_off = 0;
-  return s_end;
+  // a host image: synchronous, device errors reported here; a device image: asynchronous on the
+  // context's stream, device errors reported by the next synchronising call
+  return dev_out ? HGX_OK : hgx_synchronize(c);
 }
 
 }  // namespace

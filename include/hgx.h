@@ -51,7 +51,9 @@ int hgx_version(void);
  * destroyed before its q-grid. */
 int hgx_create(int device, hgx_ctx* out);
 int hgx_destroy(hgx_ctx ctx);
-/* Stream for asynchronous work (a cudaStream_t; NULL = the legacy default stream). */
+/* Stream for asynchronous work (a cudaStream_t; NULL = the legacy default stream).  A change
+ * of stream first waits for the work queued on the old one (the context's buffers are reused
+ * in stream order). */
 int hgx_set_stream(hgx_ctx ctx, void* stream);
 void* hgx_get_stream(hgx_ctx ctx);
 /* Waits for the context's stream and reports any error a kernel recorded. */
@@ -458,7 +460,10 @@ int hgx_hig_image_size(hgx_hig h, int* nrow, int* ncol);
  * reference's order), "gaussian", "normal" and "cauchy" orientations; gaussian/cauchy grain
  * scalings and ranged repetitions (the reference's seeded Mersenne Twister).  Other
  * descriptions return HGX_ERR_INVALID_ARG naming the feature.  nslices > 1 gives the
- * reference's zero image (its slicing branch only prints that it is not implemented). */
+ * reference's zero image (its slicing branch only prints that it is not implemented).
+ * With a host image the call is synchronous; with a device image it is asynchronous on the
+ * context's stream (errors of its kernels surface at the next synchronising call, e.g.
+ * hgx_synchronize), so that the host prepares the next simulation while this one runs. */
 int hgx_hig_compute_gisaxs(hgx_ctx ctx, hgx_hig h, int precision, double* image);
 /* Angle scans, as HipGISAXS::run_all_gisaxs walks them (src/sim/hipgisaxs_main.cpp:283-613):
  * the numbers of incidence angles, in-plane rotations and tilts (alphai, inplanerot, tilt

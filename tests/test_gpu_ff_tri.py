@@ -87,6 +87,41 @@ def test_reference_shaped_call(ctx, po, golden_grid):
     assert po.rel_err(out, ref) < TOL32
 
 
+@pytest.mark.parametrize("grid", ["g16", "g16abs"])
+def test_reference_shaped_call_rows_first(po, golden_grid, grid):
+    """From the second reference-shaped FP32C call with host arrays of the same sizes on, the
+    row kernel starts from a row table read on the host while a side stream copies the 4N qz
+    values and checks them.  Results equal the device-grid path bit for bit, with a pageable
+    and with a pinned (mapped, written directly by the kernel) output; a qz that is not
+    constant along a row fails the check and is computed again from the full qz, equal to a
+    fresh context's full path; the next regular grid is back on the fast path."""
+    torch = pytest.importorskip("torch")
+    G, _ = golden_grid(grid)
+    sd = tri_cloud(np.random.default_rng(9), 300)
+    ctx = hg.Context(0)
+    g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    want = hg.ff_triangles(ctx, g, sd, None, "f32c")
+    first = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
+    second = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
+    pinned = torch.zeros(4 * G.n, dtype=torch.complex128).pin_memory()
+    hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c", out=pinned)
+    for got in (first, second, pinned.numpy()):
+        assert np.array_equal(got, want)
+    assert po.rel_err(second, po.ff_approx_triangle(sd, G.qx, G.qy, G.qz_ext)) < TOL32
+    # one q-point of block 0 off its row's value, in the middle of row 3
+    qz2 = G.qz_ext.copy()
+    qz2[3 * G.ncol + G.ncol // 2] += 0.01
+    fresh = hg.Context(0)
+    full = hg.ff_triangles_arrays(fresh, sd, G.qx, G.qy, qz2, None, "f32c")
+    again = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, qz2, None, "f32c")
+    assert np.array_equal(again, full)
+    assert po.rel_err(again, po.ff_approx_triangle(sd, G.qx, G.qy, qz2)) < TOL32
+    back = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
+    assert np.array_equal(back, want)
+    fresh.close()
+    ctx.close()
+
+
 def test_device_qgrid_matches_oracle(ctx, po):
     for dn2 in ((0.0, 0.0), (6e-6, 4e-8)):
         G = po.Grid(40, 30, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0, dn2)

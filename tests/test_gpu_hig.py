@@ -115,6 +115,29 @@ def test_compute_gisaxs_device_output(ctx, po):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32c"])
+def test_device_images_back_to_back(ctx, precision):
+    """With a device image a simulation returns once its work is queued, so the host stages the
+    next one's tables (alternating pinned arenas) while earlier ones still run.  Five
+    simulations in a row with different fit parameters into five device images, synchronised
+    once at the end, equal the same simulations with host images (each synchronous)."""
+    torch = pytest.importorskip("torch")
+    d = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    nrow, ncol = d.image_size()
+    xs = [[4.0, 22.0, 5.0], [5.5, 25.0, 12.0], [3.5, 19.0, 0.0], [6.0, 28.0, 20.0], [4.2, 21.0, 0.3]]
+    outs = [torch.full((nrow * ncol,), -1.0, dtype=torch.float64, device="cuda:0") for _ in xs]
+    for x, out in zip(xs, outs):
+        d.fit_update(x)
+        d.compute_gisaxs(ctx, precision=precision, out=out)
+    ctx.synchronize()
+    for x, out in zip(xs, outs):
+        d.fit_update(x)
+        host = d.compute_gisaxs(ctx, precision=precision)
+        assert np.array_equal(out.cpu().numpy().reshape(nrow, ncol), host)
+    d.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("edit,words", [
     (("scattering = {", 'scattering = { expt = "waxs",'), "experiment"),
     (('stat = "range"', 'stat = "bragg"'), "bragg orientations"),
