@@ -1536,7 +1536,9 @@ namespace {
 struct PopStruct {
   int ngr = 0, nscale = 0, nelem = 0, shape = 0;
   bool liquid = false, f32c = false;
-  size_t o_shapes = 0, o_elems = 0, o_gt = 0, o_er = 0, o_sc = 0;  // byte offsets in the staging block
+  // byte offsets in the staging block of each table's region; a region holds the table of every
+  // candidate in turn (candidate i at i x the table's size)
+  size_t o_shapes = 0, o_elems = 0, o_gt = 0, o_er = 0, o_sc = 0;
   size_t n_gt = 0, n_er = 0, n_sc = 0;                               // per candidate (doubles, doubles, entries)
   long sf_off = 0;                                                    // liquid: offset in sf (complex values)
 };
@@ -1554,8 +1556,8 @@ struct hgx_hig_pop_s {
   int nstruct = 0;
   hgx_qgrid grid = nullptr;
   std::vector<hgx::PopStruct> st;
-  size_t stage_bytes = 0;         // tables of one candidate, all structures
-  unsigned char* h_stage = nullptr;  // pinned: npop x stage_bytes
+  size_t stage_bytes = 0;         // the tables of all candidates and structures
+  unsigned char* h_stage = nullptr;  // pinned: stage_bytes
   double* h_dist = nullptr;       // pinned: npop
   hgx::DevBuf d_stage, fc, sf, I, img, ref, mask, ratios, scratch, dist;
   std::vector<int> variants;      // the paired / per-block choice of every FP64 launch, as recorded
@@ -1613,9 +1615,10 @@ bool pop_paired(const std::vector<std::vector<StructTables>>& all, int k, int g0
 // grains per launch: about FUSED_GRAINS_PER_LAUNCH grain evaluations over all candidates
 int pop_chunk(int npop) { return std::max(1, FUSED_GRAINS_PER_LAUNCH / npop); }
 
+
 int pop_enqueue(hgx_hig_pop_s& P, cudaStream_t st) {
   const long n = P.n;
-  HGX_CUDA(cudaMemcpyAsync(P.d_stage.p, P.h_stage, P.stage_bytes * P.npop, cudaMemcpyHostToDevice, st));
+  HGX_CUDA(cudaMemcpyAsync(P.d_stage.p, P.h_stage, P.stage_bytes, cudaMemcpyHostToDevice, st));
   HGX_CUDA(cudaMemsetAsync(P.I.p, 0, sizeof(double) * n * P.nstruct * P.npop, st));
   const unsigned char* base = (const unsigned char*)P.d_stage.p;
   const int chunk = pop_chunk(P.npop);
@@ -1637,13 +1640,12 @@ int pop_enqueue(hgx_hig_pop_s& P, cudaStream_t st) {
     a.fc = (const double2*)P.fc.p;
     a.n = n;
     a.out = (double*)P.I.p + (size_t)k * n;
-    // candidate strides: the staging block repeats every stage_bytes, a multiple of each record
-    const long sb = (long)P.stage_bytes;
-    a.ps_shape = sb / (long)sizeof(AnaShape);
-    a.ps_elem = sb / (long)sizeof(FusedElem);
-    a.ps_grain = sb / 8;
-    a.ps_er = sb / 8;
-    a.ps_scale = sb / (long)sizeof(ScaleEntry);
+    // candidate strides in records: each region holds one table per candidate
+    a.ps_shape = ps.nelem;
+    a.ps_elem = ps.nelem;
+    a.ps_grain = (long)ps.n_gt;
+    a.ps_er = (long)ps.n_er;
+    a.ps_scale = (long)ps.n_sc;
     a.ps_out = n * P.nstruct;
     const dim3 grid((unsigned)((4 * n + 127) / 128), (unsigned)P.npop);
     for (int g0 = 0; g0 < ps.ngr; g0 += chunk) {
@@ -1794,31 +1796,19 @@ int hgx_hig_population_create(hgx_ctx c, hgx_hig h, int npop, const double* ref,
     ps.n_gt = t.f.gt.size();
     ps.n_er = t.f.er.size();
     ps.n_sc = t.plan.size();
-    ps.o_shapes = take(sizeof(AnaShape) * ps.nelem);
-    ps.o_elems = take(sizeof(FusedElem) * ps.nelem);
-    ps.o_gt = take(sizeof(double) * ps.n_gt);
-    ps.o_er = take(sizeof(double) * ps.n_er);
-    ps.o_sc = take(sizeof(ScaleEntry) * ps.n_sc);
+    ps.o_shapes = take(sizeof(AnaShape) * ps.nelem * npop);
+    ps.o_elems = take(sizeof(FusedElem) * ps.nelem * npop);
+    ps.o_gt = take(sizeof(double) * ps.n_gt * npop);
+    ps.o_er = take(sizeof(double) * ps.n_er * npop);
+    ps.o_sc = take(sizeof(ScaleEntry) * ps.n_sc * npop);
     if (ps.liquid) ps.sf_off = (long)nliquid++ * nq;
     p->st.push_back(ps);
   }
-  // one candidate's block, a multiple of 256 bytes and of every record size (the kernels step
-  // from candidate to candidate by whole records)
-  size_t unit = 256;
-  for (size_t r : {sizeof(AnaShape), sizeof(FusedElem), sizeof(ScaleEntry), sizeof(double)}) {
-    size_t a = unit, b = r;
-    while (b) {
-      const size_t t = a % b;
-      a = b;
-      b = t;
-    }
-    unit = unit / a * r;  // lcm
-  }
-  p->stage_bytes = (off + unit - 1) / unit * unit;
-  if (cudaMallocHost(&p->h_stage, p->stage_bytes * npop) != cudaSuccess ||
+  p->stage_bytes = std::max<size_t>(off, 256);
+  if (cudaMallocHost(&p->h_stage, p->stage_bytes) != cudaSuccess ||
       cudaMallocHost(&p->h_dist, sizeof(double) * npop) != cudaSuccess)
     return bail(fail(HGX_ERR_NO_MEMORY, "hgx_hig_population_create: pinned host memory"));
-  if ((s = p->d_stage.reserve(p->stage_bytes * npop)) || (s = p->I.reserve(sizeof(double) * n * p->nstruct * npop)) ||
+  if ((s = p->d_stage.reserve(p->stage_bytes)) || (s = p->I.reserve(sizeof(double) * n * p->nstruct * npop)) ||
       (s = p->img.reserve(sizeof(double) * n * npop)) || (s = p->ref.reserve(sizeof(double) * n)) ||
       (s = p->ratios.reserve(sizeof(double) * p->nstruct)) ||
       (s = p->scratch.reserve(sizeof(double) * fit_population_scratch(npop))) ||
@@ -1866,18 +1856,21 @@ int hgx_hig_population_eval(hgx_hig_pop p, const double* X, int nx, double* dist
   HGX_CUDA(cudaSetDevice(p->ctx->device));
   cudaStream_t st = p->ctx->stream;
   HGX_CUDA(cudaStreamSynchronize(st));  // the pinned staging block is about to change
+  // every candidate's tables from its own copy of the description, into its place in each
+  // table's region of the staging block
   std::vector<std::vector<StructTables>> all((size_t)p->npop);
   for (int i = 0; i < p->npop; ++i) {
     HGX_TRY(pop_tables(*p, X + (size_t)i * nx, all[i]));
-    unsigned char* blk = p->h_stage + (size_t)i * p->stage_bytes;
+    unsigned char* h = p->h_stage;
     for (int k = 0; k < p->nstruct; ++k) {
       const PopStruct& ps = p->st[k];
       const StructTables& t = all[i][k];
-      memcpy(blk + ps.o_shapes, t.f.shapes.data(), sizeof(AnaShape) * ps.nelem);
-      memcpy(blk + ps.o_elems, t.f.elems.data(), sizeof(FusedElem) * ps.nelem);
-      memcpy(blk + ps.o_gt, t.f.gt.data(), sizeof(double) * ps.n_gt);
-      memcpy(blk + ps.o_er, t.f.er.data(), sizeof(double) * ps.n_er);
-      memcpy(blk + ps.o_sc, t.plan.data(), sizeof(ScaleEntry) * ps.n_sc);
+      const size_t ne = (size_t)ps.nelem;
+      memcpy(h + ps.o_shapes + sizeof(AnaShape) * ne * i, t.f.shapes.data(), sizeof(AnaShape) * ne);
+      memcpy(h + ps.o_elems + sizeof(FusedElem) * ne * i, t.f.elems.data(), sizeof(FusedElem) * ne);
+      memcpy(h + ps.o_gt + sizeof(double) * ps.n_gt * i, t.f.gt.data(), sizeof(double) * ps.n_gt);
+      memcpy(h + ps.o_er + sizeof(double) * ps.n_er * i, t.f.er.data(), sizeof(double) * ps.n_er);
+      memcpy(h + ps.o_sc + sizeof(ScaleEntry) * ps.n_sc * i, t.plan.data(), sizeof(ScaleEntry) * ps.n_sc);
     }
   }
   // the paired / per-block choice of every FP64 launch for this generation
