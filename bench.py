@@ -887,10 +887,22 @@ def main():
         # accuracy of the timed FP32 output against the FP64 kernel (norm-wise)
         d = (out.to(torch.complex128) - out64)
         relerr = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(out64))
+        # pointwise: |F32C - F64| / |F64| on the q-points whose |F|^2 is at least a fraction of
+        # the largest (the weak q-points of a DWBA image carry the smallest amplitudes)
+        a64 = out64.abs()
+        rel = d.abs() / a64.clamp_min(1e-300)
+        pw = {}
+        for frac in (1e-6, 1e-3):
+            r = rel[a64 * a64 >= frac * float((a64 * a64).max())]
+            q = torch.quantile(r[torch.randperm(r.numel(), device=r.device)[:1 << 20]].float(),
+                               torch.tensor([0.5, 0.99], device=r.device))
+            pw[f"intensity_ge_{frac:g}_of_max"] = {"q_points": int(r.numel()), "median": float(q[0]),
+                                                   "p99": float(q[1]), "max": float(r.max())}
         v64 = evals / (ms64 * 1e-3)
         f64 = {"value": v64, "unit": "evals/s", "ms_per_step": ms64, "launches_timed": reps64,
-               "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr}
-        del out64
+               "fp32c_speedup": (value / world) / v64, "fp32c_rel_err_vs_fp64": relerr,
+               "fp32c_pointwise_rel_err": pw}
+        del out64, a64, rel
 
     fit = None
     if not args.no_fitting and world == 1:  # the single-GPU legs stay out of scaling runs

@@ -1295,10 +1295,10 @@ int hgx_ff_triangles(hgx_ctx c, const double* shape_def, int ntri, int nqy, cons
   int s = ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, dout, HGX_C128, 0);
   const int s_check = shaped_rows_check(c, g, qz);
   bool ok = true;
-  const int s_settle = shaped_rows_settle(c, g, &ok);
-  if (s == HGX_OK) s = s_check;
-  if (s == HGX_OK) s = s_settle;
-  if (s == HGX_OK && !ok) s = ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, dout, HGX_C128, 0);
+  const int s_settle = s_check == HGX_OK ? shaped_rows_settle(c, g, &ok) : s_check;
+  if (s_settle != HGX_OK) s = s_settle;
+  // a failed check: the first result (or its refusal of the guessed layout) is replaced
+  else if (!ok) s = ff_triangles_device(c, g, sd, ntri, rot9, HGX_F32C, dout, HGX_C128, 0);
   if (s == HGX_OK && staged)
     HGX_CUDA(cudaMemcpyAsync(ff, dout, sizeof(double2) * (size_t)nqz, cudaMemcpyDeviceToHost, c->stream));
   if (s != HGX_OK) {

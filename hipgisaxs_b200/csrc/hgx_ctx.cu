@@ -186,7 +186,9 @@ int shaped_rows_begin(hgx_ctx c, int nqy, const double* qx, const double* qy, in
     return shaped_grid(c, nqy, qx, qy, nqz, qz, out);
   int ncol = 0;
   HGX_TRY(detect_ncol(g, qz, &ncol));  // host array: scans the first row only
-  if (ncol <= 0 || nqy % ncol != 0) return shaped_grid(c, nqy, qx, qy, nqz, qz, out);
+  // detector rows of at least 64 q-points (shorter runs of equal qz, as on scattered q-points,
+  // take the full path: a row kernel there would be mostly idle lanes)
+  if (ncol < 64 || nqy % ncol != 0) return shaped_grid(c, nqy, qx, qy, nqz, qz, out);
   const int nk = g->nk, nrow = nqy / ncol;
   // each row's first q-point of every block, and whether the blocks pair (real, qz4 = -qz1,
   // qz2 = -qz3) there; the check on the side stream holds every q-point to the same values

@@ -87,19 +87,21 @@ def test_reference_shaped_call(ctx, po, golden_grid):
     assert po.rel_err(out, ref) < TOL32
 
 
-@pytest.mark.parametrize("grid", ["g16", "g16abs"])
-def test_reference_shaped_call_rows_first(po, golden_grid, grid):
-    """From the second reference-shaped FP32C call with host arrays of the same sizes on, the
-    row kernel starts from a row table read on the host while a side stream copies the 4N qz
-    values and checks them.  Results equal the device-grid path bit for bit, with a pageable
-    and with a pinned (mapped, written directly by the kernel) output; a qz that is not
-    constant along a row fails the check and is computed again from the full qz, equal to a
-    fresh context's full path; the next regular grid is back on the fast path."""
+@pytest.mark.parametrize("dn2", [(0.0, 0.0), (6e-6, 4e-8)])
+def test_reference_shaped_call_rows_first(po, dn2):
+    """From the second reference-shaped FP32C call with host arrays of the same sizes on, on a
+    grid with detector rows of at least 64 q-points, the row kernel starts from a row table
+    read on the host while a side stream copies the 4N qz values and checks them.  Results
+    equal the device-grid path bit for bit, with a pageable and with a pinned (mapped, written
+    directly by the kernel) output; a qz that is not constant along a row fails the check and is
+    computed again from the full qz, equal to a fresh context's full path; the next regular grid
+    is back on the fast path.  Real (paired) and absorbing (complex) qz blocks."""
     torch = pytest.importorskip("torch")
-    G, _ = golden_grid(grid)
+    G = po.Grid(128, 24, -2.0, 0.0, 2.0, 3.0, 0.2, 10.0, dn2)
     sd = tri_cloud(np.random.default_rng(9), 300)
     ctx = hg.Context(0)
     g = hg.QGrid.from_arrays(ctx, G.qx, G.qy, G.qz_ext)
+    assert g.mode == (1 if dn2 == (0.0, 0.0) else 2) and g.ncol == 128
     want = hg.ff_triangles(ctx, g, sd, None, "f32c")
     first = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
     second = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
@@ -118,6 +120,13 @@ def test_reference_shaped_call_rows_first(po, golden_grid, grid):
     assert po.rel_err(again, po.ff_approx_triangle(sd, G.qx, G.qy, qz2)) < TOL32
     back = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
     assert np.array_equal(back, want)
+    # scattered q-points (runs of equal qz shorter than 64): the full path, every call
+    perm = np.random.default_rng(3).permutation(G.n)
+    qx3, qy3 = G.qx[perm], G.qy[perm]
+    qz3 = G.qz_ext.reshape(4, G.n)[:, perm].ravel()
+    ref3 = po.ff_approx_triangle(sd, qx3, qy3, qz3)
+    for _ in range(2):
+        assert po.rel_err(hg.ff_triangles_arrays(ctx, sd, qx3, qy3, qz3, None, "f32c"), ref3) < TOL32
     fresh.close()
     ctx.close()
 
