@@ -138,6 +138,37 @@ def test_device_images_back_to_back(ctx, precision):
 
 
 @pytest.mark.gpu
+def test_device_images_across_a_stream_change(ctx):
+    """An asynchronous simulation queued on one stream, then the context moved to another
+    stream and a second simulation queued there: the change of stream waits for the first, so
+    both images equal their synchronous host-image versions."""
+    torch = pytest.importorskip("torch")
+    d = read_hig(os.path.join(HIG, "fit_objective.hig"))
+    nrow, ncol = d.image_size()
+    c2 = hg.Context(0)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    a = torch.full((nrow * ncol,), -1.0, dtype=torch.float64, device="cuda:0")
+    b = torch.full((nrow * ncol,), -1.0, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    c2.set_stream(s1)
+    d.fit_update([5.5, 25.0, 12.0])
+    d.compute_gisaxs(c2, out=a)
+    c2.set_stream(s2)
+    d.fit_update([3.5, 19.0, 0.0])
+    d.compute_gisaxs(c2, out=b)
+    c2.synchronize()
+    got_a, got_b = a.cpu().numpy().reshape(nrow, ncol), b.cpu().numpy().reshape(nrow, ncol)
+    c2.set_stream(None)
+    d.fit_update([5.5, 25.0, 12.0])
+    want_a = d.compute_gisaxs(c2)
+    d.fit_update([3.5, 19.0, 0.0])
+    want_b = d.compute_gisaxs(c2)
+    assert np.array_equal(got_a, want_a) and np.array_equal(got_b, want_b)
+    c2.close()
+    d.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("edit,words", [
     (("scattering = {", 'scattering = { expt = "waxs",'), "experiment"),
     (('stat = "range"', 'stat = "bragg"'), "bragg orientations"),
