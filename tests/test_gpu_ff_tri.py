@@ -120,6 +120,13 @@ def test_reference_shaped_call_rows_first(po, dn2):
     assert po.rel_err(again, po.ff_approx_triangle(sd, G.qx, G.qy, qz2)) < TOL32
     back = hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, G.qz_ext, None, "f32c")
     assert np.array_equal(back, want)
+    # one block (Born): a grid of other sizes, then the same sizes again on the fast path
+    qzb = G.qz + 0j
+    gb = hg.QGrid.from_arrays(ctx, G.qx, G.qy, qzb)
+    assert gb.mode == 2 and gb.ncol == 128
+    want_b = hg.ff_triangles(ctx, gb, sd, None, "f32c")
+    for _ in range(2):
+        assert np.array_equal(hg.ff_triangles_arrays(ctx, sd, G.qx, G.qy, qzb, None, "f32c"), want_b)
     # scattered q-points (runs of equal qz shorter than 64): the full path, every call
     perm = np.random.default_rng(3).permutation(G.n)
     qx3, qy3 = G.qx[perm], G.qy[perm]
