@@ -114,7 +114,12 @@ int hgx_ff_tune(hgx_ctx ctx, hgx_qgrid g, const double* shape_def, int ntri,
                 const double* rot9, int ff_type, int reps, int* best_ppt, double* best_ms,
                 double* times_ms);
 /* The reference-shaped call: explicit q arrays, complex128 output, synchronous.
- * Returns HGX_ERR_INVALID_ARG for ntri < 1 (the reference returns 0 triangles). */
+ * Returns HGX_ERR_INVALID_ARG for ntri < 1 (the reference returns 0 triangles).  The context
+ * keeps the q-grid between calls of the same sizes; from the second FP32C call on, with qz in
+ * host memory laid out by detector rows (at least 64 q-points per row), the kernel starts from
+ * qx, qy and each row's first qz while the 4N qz values are copied and checked beside it (a grid
+ * that fails the check is computed again on the full path: the result is the same either way).
+ * ff in page-locked host memory is written by the kernel directly. */
 int hgx_ff_triangles(hgx_ctx ctx, const double* shape_def, int ntri, int nqy, const double* qx,
                      const double* qy, int nqz, const double* qz, const double* rot9,
                      int precision, double* ff);
