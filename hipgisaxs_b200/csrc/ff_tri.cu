@@ -11,7 +11,7 @@
 // and applied as one complex rotation of the tile's partial sums, and the FP32 phase per
 // (q-point, triangle) only spans the tile's extent.  A mesh far from the origin therefore
 // loses no phase accuracy, and when the tile's in-plane phases stay within a few turns (the
-// CTA's largest |q_par| times the tile's largest offset) the row kernel feeds them to the SFU
+// warp's largest |q_par| times the tile's largest offset) the row kernel feeds them to the SFU
 // without a per-term reduction.
 //
 // Kernels:
@@ -397,7 +397,6 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
   constexpr int NACC = PAIRED ? 8 : 2 * NK;  // float accumulators per pixel
   __shared__ __align__(128) float s_tile[2][TILE_FLOATS];
   __shared__ __align__(8) uint64_t s_bar[2];
-  __shared__ unsigned s_q2max;
   // dynamic: row factors (rows_per_cta x TILE x NF float4), then the compensation terms of
   // the running sums (P x NACC x BLOCK floats, thread-minor so accesses are conflict-free)
   extern __shared__ __align__(16) float4 s_dyn[];
@@ -409,14 +408,17 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
   const int lr = threadIdx.x / tpr;
   const int lane = threadIdx.x - lr * tpr;
   const int row = blockIdx.y * R + lr;
-  const int colbase = blockIdx.x * (tpr * P) + lane;
+  // each warp takes 32 x P neighbouring columns of its row (a thread's pixel i at lane + 32 i of
+  // the warp's block), so that the largest |q_par| of the warp's own pixels decides the explicit
+  // phase reduction: warps near the detector's qy = 0 column skip it on wide tiles
+  const int colbase = blockIdx.x * (tpr * P) + (lane >> 5) * (32 * P) + (lane & 31);
 
   float qxf[P], qyf[P];
   float acc[P][NACC], sum[P][NACC];
   float q2l = 0.f;
 #pragma unroll
   for (int i = 0; i < P; ++i) {
-    int col = colbase + i * tpr;
+    int col = colbase + i * 32;
     bool v = row < a.nrow && col < a.ncol;
     long p = (long)row * a.ncol + col;
     qxf[i] = v ? (float)a.qx[p] : 0.f;
@@ -430,7 +432,6 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
   }
 
   if (threadIdx.x == 0) {
-    s_q2max = 0u;
     mbar_init(&s_bar[0], 1);
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
@@ -442,9 +443,8 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
       bulk_g2s(s_tile[s], a.tiles + (size_t)s * TILE_FLOATS, TILE_BYTES, &s_bar[s]);
     }
   }
-  atomicMax(&s_q2max, __float_as_uint(q2l));  // non-negative floats order as their bits
-  __syncthreads();
-  const float q2max = __uint_as_float(s_q2max);  // the CTA's largest |q_par|^2
+  // the warp's largest |q_par|^2 (non-negative floats order as their bits)
+  const float q2max = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(q2l)));
 
   for (int s = 0; s < a.ntiles; ++s) {
     const int b = s & 1;
@@ -486,7 +486,7 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
     }
 
     const float4* RF = s_rf + (size_t)lr * TILE * NF;
-    if ((float)(anc.w * anc.w) * q2max > WIDE_PHASE2)  // uniform over the CTA
+    if ((float)(anc.w * anc.w) * q2max > WIDE_PHASE2)  // uniform over the warp
       row_tile_sums<P, NK, PAIRED, true>(A, RF, qxf, qyf, acc);
     else
       row_tile_sums<P, NK, PAIRED, false>(A, RF, qxf, qyf, acc);
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
     // phase), then fold them into the running sums (TwoSum; error terms in smem)
 #pragma unroll
     for (int i = 0; i < P; ++i) {
-      const int col = colbase + i * tpr;
+      const int col = colbase + i * 32;
       const bool v = row < a.nrow && col < a.ncol;
       const long p = (long)row * a.ncol + col;
       const float2 e = anchor_phasor(v ? fma(a.qx[p], anc.x, a.qy[p] * anc.y) : 0.0);
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(BLOCK, 2) ff_tri_rows_kernel(RowArgs a) {
   OUT* out = reinterpret_cast<OUT*>(a.out);
 #pragma unroll
   for (int i = 0; i < P; ++i) {
-    int col = colbase + i * tpr;
+    int col = colbase + i * 32;
     if (row >= a.nrow || col >= a.ncol) continue;
     long p = (long)row * a.ncol + col;
     double qx = a.qx[p], qy = a.qy[p];
