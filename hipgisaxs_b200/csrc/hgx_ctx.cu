@@ -205,10 +205,22 @@ int shaped_rows_begin(hgx_ctx c, int nqy, const double* qx, const double* qy, in
       if (t[3].x != -t[0].x || t[1].x != -t[2].x) paired = false;
     }
   }
-  if (!c->side) {
-    HGX_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-    HGX_CUDA(cudaEventCreateWithFlags(&c->side_ev, cudaEventDisableTiming));
-    HGX_CUDA(cudaMalloc(&c->side_flags, 256));
+  if (!c->side) {  // made once per context, kept only when all three exist
+    cudaStream_t sst = nullptr;
+    cudaEvent_t sev = nullptr;
+    void* sfl = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&sst, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&sfl, 256);
+    if (e != cudaSuccess) {
+      if (sfl) cudaFree(sfl);
+      if (sev) cudaEventDestroy(sev);
+      if (sst) cudaStreamDestroy(sst);
+      return cuda_fail(e, "side stream of the reference-shaped call");
+    }
+    c->side = sst;
+    c->side_ev = sev;
+    c->side_flags = static_cast<unsigned*>(sfl);
   }
   const size_t need = (size_t)nrow * nk;
   if (need > g->rowqz_cap) {
