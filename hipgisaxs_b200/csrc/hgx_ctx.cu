@@ -374,9 +374,14 @@ int hgx_set_stream(hgx_ctx c, void* stream) {
   cudaStream_t next = reinterpret_cast<cudaStream_t>(stream);
   if (next != c->stream) {
     // the context's buffers are reused in stream order: work still queued on the old stream
-    // finishes before work on the new one can touch them
+    // finishes before work on the new one can touch them (a stream being captured into a graph
+    // has run nothing yet and is left alone: a synchronisation would end its capture)
     HGX_CUDA(cudaSetDevice(c->device));
-    HGX_CUDA(cudaStreamSynchronize(c->stream));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess)
+      cudaGetLastError();  // the legacy stream while another stream is captured: left alone too
+    else if (cs == cudaStreamCaptureStatusNone)
+      HGX_CUDA(cudaStreamSynchronize(c->stream));
   }
   c->stream = next;
   return HGX_OK;

@@ -53,7 +53,7 @@ int hgx_create(int device, hgx_ctx* out);
 int hgx_destroy(hgx_ctx ctx);
 /* Stream for asynchronous work (a cudaStream_t; NULL = the legacy default stream).  A change
  * of stream first waits for the work queued on the old one (the context's buffers are reused
- * in stream order). */
+ * in stream order), unless the old stream is being captured into a graph. */
 int hgx_set_stream(hgx_ctx ctx, void* stream);
 void* hgx_get_stream(hgx_ctx ctx);
 /* Waits for the context's stream and reports any error a kernel recorded. */
